@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark of the filtered full-recall path: QPS of batched filtered top-K search on the 10M x 128
+FP32 corpus (256 tags, densities log-uniform in [1e-4, 0.6], filters of 1-6 tags whose selectivity
+spreads over 1e-4..1, K = 100, batches of 256 queries), one resident index per GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one batch of queries through the whole path (filter -> candidate scoring -> exact
+rescoring + top-K). `value` is whole-job QPS with queries and index resident in HBM (device-timed,
+max over ranks); `e2e` is the same through the public C-ABI with the batch's queries copied from pinned
+host memory and its results copied back inside the timed region. Under torchrun every rank holds a
+full replica and serves its own batches (weak scaling, no data-path collective).
+
+--impl reference times the reference's own CPU ground-truth scan (CpuTopKBatch, compiled from the
+reference sources into oracle/_ref) on this host's cores for the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "QPS & p99 at 10M x128 filtered top-100, recall 1.0: chosen form vs plain FP32"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--docs", type=int, default=10_000_000)
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--topk", type=int, default=100)
+    ap.add_argument("--queries", type=int, default=2048, help="query pool the steps cycle through")
+    ap.add_argument("--cpu-queries", type=int, default=0, help="CPU baseline sample size (0: 2 per thread)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def workload(args, device):
+    from hybridsearchsystem_b200 import data
+    mix = data.Mixture(128, 256, (1e-4, 0.6), n_clusters=1024, sigma=0.3, n_corr=16, seed=1)
+    if device is not None:
+        vec, bits = mix.corpus_torch(args.docs, device=device, seed=11)
+    else:
+        vec, bits, _ = mix.corpus(args.docs, seed=11)
+    queries = mix.queries(args.queries, seed=2)
+    exprs = data.make_filters(mix, args.queries, n_tags=(1, 6), seed=3, selectivity_range=(1e-4, 1.0))
+    return mix, vec, bits, queries, exprs
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", self.gpu_id], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        self.out.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.out.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(vec, bits, queries, exprs, topk, nq_sample):
+    """The reference's CpuTopKBatch (oracle/_ref, compiled from its sources) on all host threads, or the
+    oracle's restatement of it when the reference build is absent. Returns (record, ids, counts)."""
+    import ctypes
+
+    import oracle
+    threads = os.cpu_count() or 1
+    nq = nq_sample or 2 * threads
+    nq = min(nq, len(queries))
+    q = np.ascontiguousarray(queries[:nq], np.float32)
+    ex = exprs[:nq]
+    topks = np.full(nq, topk, np.int32)
+    t0 = time.perf_counter()
+    if oracle.ref_available():
+        r = oracle.ref()
+        arr = (ctypes.c_char_p * nq)(*[e.encode() for e in ex])
+        ids = np.full((nq, topk), -1, np.int64)
+        counts = np.zeros(nq, np.int32)
+        rc = r.ref_cpu_topk_batch(q.ctypes.data, nq, q.shape[1], arr, topks.ctypes.data, vec.ctypes.data,
+                                  bits.ctypes.data, bits.shape[1] * 64, vec.shape[0], 0, 1, threads, topk,
+                                  ids.ctypes.data, counts.ctypes.data)
+        assert rc == 0
+        kind = "reference"
+    else:
+        _, ids, counts = oracle.topk(q, ex, topks, vec, bits, threads=threads, out_stride=topk)
+        kind = "port"
+    dt = time.perf_counter() - t0
+    rec = {"value": nq / dt, "unit": "QPS", "cores": threads, "kind": kind,
+           "sample": f"{nq} queries (filtered top-{topk}) over the full {vec.shape[0]}-doc corpus, "
+                     f"CpuTopKBatch in {threads} query slices, fp32 mode"}
+    return rec, ids, counts
+
+
+def run_reference(args):
+    rank, local, world = dist_env()
+    if rank != 0:
+        return
+    import torch
+    device = "cuda" if torch.cuda.is_available() else None
+    _, vec, bits, queries, exprs = workload(args, device)
+    threads = os.cpu_count() or 1
+    nq = args.cpu_queries or 2 * threads
+    for _ in range(args.warmup):
+        cpu_baseline(vec, bits, queries, exprs, args.topk, max(1, nq // 4))
+    total_q, total_t = 0, 0.0
+    rec = None
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        rec, _, _ = cpu_baseline(vec, bits, queries, exprs, args.topk, nq)
+        total_t += time.perf_counter() - t0
+        total_q += min(nq, len(queries))
+    v = total_q / total_t
+    rec = dict(rec, value=v)
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "QPS", "n_gpus": world,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                      "data": "synthetic (seeded cluster mixture, HYDSET2 shapes)",
+                      "config": config_of(args, world), "cpu_baseline": rec,
+                      "e2e": {"value": v, "unit": "QPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def config_of(args, world):
+    return {"workload": f"filtered top-{args.topk}, {args.docs} docs x 128 FP32, 256 tags, batch {args.batch}",
+            "docs": args.docs, "dim": 128, "tags": 256, "batch": args.batch, "topk": args.topk,
+            "doc_num_per_segment": 131072, "filters": "1-6 tags AND/OR/NOT, est. selectivity 1e-4..1",
+            "parallelism": f"replica x{world}",
+            "l2": "inputs larger than L2: every step reads the 5.1 GB corpus"}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import hybridsearchsystem_b200 as hss
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    dev = f"cuda:{local}"
+    _, vec, bits, queries, exprs = workload(args, dev)
+    table = hss.DataTable.build(vec, bits, 256, device=local, doc_num_per_segment=131072)
+    B, K = args.batch, args.topk
+    searcher = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=1 << 18)
+    searcher.set_timing(True)
+    nb = max(1, len(queries) // B)
+    filters = [searcher.compile_filters(exprs[i * B:(i + 1) * B]) for i in range(nb)]
+    topks = np.full(B, K, np.uint32)
+    d_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1), device=dev)
+    o_sc = torch.zeros((B, K), dtype=torch.float32, device=dev)
+    o_id = torch.zeros((B, K), dtype=torch.int64, device=dev)
+    o_n = torch.zeros(B, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    def step(i):
+        j = (rank * 7919 + i) % nb
+        rc = searcher.search_device(d_q[j].data_ptr(), B, filters[j], topks, o_sc.data_ptr(), o_id.data_ptr(),
+                                    o_n.data_ptr(), K, sh)
+        assert rc == 0, searcher.last_status(B)
+        return searcher.last_times()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    # device-resident leg
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    cand_ms, launches = [], 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_id) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for i in range(args.steps):
+            t = step(args.warmup + i)
+            cand_ms.append(t["candidates_ms"])
+            launches += t["launches"]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    t_ms = ev0.elapsed_time(ev1)
+    clocks = clk.summary()
+    t_max = torch.tensor([t_ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    t_max = float(t_max.item())
+    value = world * args.steps * B / (t_max / 1e3)
+
+    # end-to-end leg through the C-ABI: pinned host queries in, results out, every step
+    h_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1)).pin_memory()
+    h_sc = torch.zeros((B, K), dtype=torch.float32).pin_memory()
+    h_id = torch.zeros((B, K), dtype=torch.int64).pin_memory()
+    h_n = torch.zeros(B, dtype=torch.int32).pin_memory()
+    d_stage = torch.zeros((B, 128), dtype=torch.float32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(args.steps):
+        j = (rank * 7919 + args.warmup + i) % nb
+        d_stage.copy_(h_q[j], non_blocking=True)
+        f = searcher.compile_filters(exprs[j * B:(j + 1) * B])
+        rc = searcher.search_device(d_stage.data_ptr(), B, f, topks, o_sc.data_ptr(), o_id.data_ptr(),
+                                    o_n.data_ptr(), K, sh)
+        assert rc == 0
+        h_sc.copy_(o_sc, non_blocking=True)
+        h_id.copy_(o_id, non_blocking=True)
+        h_n.copy_(o_n, non_blocking=True)
+        stream.synchronize()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = torch.tensor([e0.elapsed_time(e1)], device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e = world * args.steps * B / (float(e2e_ms.item()) / 1e3)
+
+    # roofline of the dominant kernel (the candidate pass): algorithmic bytes per launch = the corpus
+    # (docs x 128 x 4 B) + the batch's filter bitmaps (B x docs/8 B)
+    info = table.info
+    words = info["segment_num"] * info["doc_num_per_segment"] // 64
+    alg_bytes = args.docs * 128 * 4 + B * words * 8
+    cand_avg = float(np.mean(cand_ms)) if cand_ms else float("nan")
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg_bytes / (cand_avg / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "cand_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("bytes_per_launch_full_workload")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": traffic, "kernel": "cand_simt_kernel", "avg_ms": cand_avg,
+            "peak_source": "measured" if peaks else "fallback"}
+
+    rec = {"metric": METRIC, "value": value, "unit": "QPS", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded cluster mixture, HYDSET2 shapes)",
+           "config": dict(config_of(args, world), form="plain FP32 (SIMT candidate pass + exact FP32 rescoring)"),
+           "e2e": {"value": e2e, "unit": "QPS", "h2d_bytes_per_step": B * 128 * 4,
+                   "d2h_bytes_per_step": B * K * (4 + 8) + B * 4},
+           "roofline": roof, "clocks": clocks, "gpu_launches": launches}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb, ref_ids, ref_counts = cpu_baseline(vec, bits, queries, exprs, K, args.cpu_queries)
+        rec["cpu_baseline"] = cb
+        # parity at full scale: the GPU's ids for the CPU sample's queries (first batches)
+        nq = len(ref_counts)
+        ok = True
+        for j in range((nq + B - 1) // B):
+            rc = searcher.search_device(d_q[j].data_ptr(), B, filters[j], topks, o_sc.data_ptr(), o_id.data_ptr(),
+                                        o_n.data_ptr(), K, sh)
+            torch.cuda.synchronize()
+            g_id, g_n = o_id.cpu().numpy(), o_n.cpu().numpy()
+            for i in range(B):
+                qi = j * B + i
+                if qi >= nq:
+                    break
+                c = int(ref_counts[qi])
+                if int(g_n[i]) != c or set(g_id[i][:c].tolist()) != set(ref_ids[qi][:c].tolist()):
+                    ok = False
+        rec["parity_full_scale"] = {"queries": nq, "ids_match_cpu_ground_truth": ok, "against": cb["kind"]}
+    if rank == 0:
+        print(json.dumps(rec))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

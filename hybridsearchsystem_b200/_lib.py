@@ -1,0 +1,129 @@
+"""ctypes binding of libhss.so (the C-ABI declared in include/hss.h).
+
+The library is built in-tree by ``__graft_entry__.build()`` (``make -C hybridsearchsystem_b200/csrc``).
+Loading fails loudly when it is missing: there is no CPU fallback for any operation.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhss.so")
+
+c_f32p = ctypes.POINTER(ctypes.c_float)
+c_u32p = ctypes.POINTER(ctypes.c_uint32)
+c_i32p = ctypes.POINTER(ctypes.c_int32)
+c_i64p = ctypes.POINTER(ctypes.c_int64)
+c_u64p = ctypes.POINTER(ctypes.c_uint64)
+c_u8p = ctypes.POINTER(ctypes.c_uint8)
+vp = ctypes.c_void_p
+
+HSS_OK = 0
+HSS_ERR_INVALID = -1
+HSS_ERR_CUDA = -2
+HSS_ERR_PARSE = -3
+HSS_ERR_PROGRAM = -4
+HSS_ERR_LIMIT = -5
+HSS_ERR_INDEX = -6
+HSS_ERR_QUERY = -7
+
+HSS_MAX_TOPK = 4096
+HSS_MAX_OPERANDS = 64
+HSS_MAX_PROGRAM = 512
+HSS_FILTER_HEAD_ADDRESSES = 0x80000000
+
+QSTATUS_BAD_PROGRAM = 1
+QSTATUS_BAD_POSTING = 2
+QSTATUS_OVERFLOW = 4
+QSTATUS_TOPK_TOO_LARGE = 8
+
+
+class HssError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libhss error {code}: {msg}")
+        self.code = code
+
+
+class FilterContext(ctypes.Structure):
+    """TextFilterContextData (device_common_external.h:17-25)."""
+
+    _fields_ = [(n, ctypes.c_uint32) for n in
+                ("postingNum", "segmentNum", "segmentLength", "tileNum", "exprLen", "opNum", "flags")]
+
+
+class IndexConfig(ctypes.Structure):
+    _fields_ = [("docNumPerSegment", ctypes.c_uint32), ("densityThreshold", ctypes.c_float),
+                ("matrixPosting", ctypes.c_int32), ("sparsePacked", ctypes.c_int32),
+                ("docOffset", ctypes.c_uint64)]
+
+
+class SearcherConfig(ctypes.Structure):
+    _fields_ = [("maxBatch", ctypes.c_uint32), ("candidateCap", ctypes.c_uint32),
+                ("sampleDocs", ctypes.c_uint32), ("maxRetries", ctypes.c_uint32), ("method", ctypes.c_int32)]
+
+
+# (name, restype, argtypes) for every symbol include/hss.h declares.
+SIGNATURES = [
+    ("hss_vector_score_launch", ctypes.c_int,
+     [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, vp]),
+    ("hss_bitmap_text_filter_launch", ctypes.c_int, [vp, vp, vp, FilterContext, vp, vp, vp]),
+    ("hss_posting_bitlist_to_set_launch", ctypes.c_int, [vp, ctypes.c_uint32, vp, ctypes.c_uint32, vp, vp]),
+    ("hss_aggregator_workspace_size", ctypes.c_size_t, [ctypes.c_uint32]),
+    ("hss_aggregator_launch", ctypes.c_int,
+     [vp, vp, vp, vp, vp, vp, ctypes.c_uint32, vp, ctypes.c_size_t, vp]),
+    ("hss_topk_launch", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32, vp, vp, vp, vp]),
+    ("hss_table_build", ctypes.c_int,
+     [ctypes.c_int32, vp, vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+      ctypes.POINTER(IndexConfig), ctypes.POINTER(vp)]),
+    ("hss_table_load", ctypes.c_int, [ctypes.c_int32, ctypes.c_char_p, ctypes.POINTER(vp)]),
+    ("hss_table_save", ctypes.c_int, [vp, ctypes.c_char_p]),
+    ("hss_table_free", None, [vp]),
+    ("hss_table_info", ctypes.c_int, [vp, c_u64p, c_u32p, c_u32p, c_u32p, c_u32p, c_f32p]),
+    ("hss_table_posting", ctypes.c_int,
+     [vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(c_u8p), c_u32p]),
+    ("hss_table_device_ptrs", ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)]),
+    ("hss_searcher_create", ctypes.c_int, [vp, ctypes.POINTER(SearcherConfig), ctypes.POINTER(vp)]),
+    ("hss_searcher_free", None, [vp]),
+    ("hss_searcher_add_query", ctypes.c_int, [vp, ctypes.c_char_p, vp, ctypes.c_uint32, ctypes.c_uint32]),
+    ("hss_searcher_batch_search", ctypes.c_int, [vp, vp, vp, vp, ctypes.c_uint32]),
+    ("hss_filters_compile", ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_char_p), ctypes.c_uint32, ctypes.POINTER(vp)]),
+    ("hss_filters_free", None, [vp]),
+    ("hss_searcher_search_device", ctypes.c_int,
+     [vp, vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.c_uint32, vp]),
+    ("hss_searcher_filter_device", ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, ctypes.c_uint64, vp, vp]),
+    ("hss_searcher_last_status", ctypes.c_int, [vp, vp, ctypes.c_uint32]),
+    ("hss_searcher_set_timing", ctypes.c_int, [vp, ctypes.c_int32]),
+    ("hss_searcher_last_times", ctypes.c_int, [vp, vp, c_u32p, c_u32p]),
+    ("hss_hash64", ctypes.c_uint64, [ctypes.c_char_p, ctypes.c_uint32]),
+    ("hss_posting_serialize", ctypes.c_int64,
+     [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, vp, ctypes.c_uint64]),
+    ("hss_filter_compile", ctypes.c_int,
+     [vp, ctypes.c_char_p, vp, ctypes.c_uint32, c_u32p, vp, ctypes.c_uint32, c_u32p, c_u32p, c_i32p]),
+    ("hss_last_error", ctypes.c_char_p, []),
+    ("hss_device_count", ctypes.c_int, []),
+]
+
+_lib = None
+
+
+def load():
+    """Loads libhss.so (once) and binds every C-ABI symbol. Raises if the library is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise HssError(HSS_ERR_INVALID, f"{LIB_PATH} not built; run __graft_entry__.build()")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    """Raises HssError for a negative status code."""
+    if rc < 0:
+        msg = load().hss_last_error()
+        raise HssError(rc, msg.decode() if msg else "")
+    return rc

@@ -1,0 +1,243 @@
+"""Python mirror of the reference's host API for the filtered full-recall path.
+
+    DataTable            DataTable::LoadData / the offline builder (src/engine/index/data_table.h)
+    FullRecallSearcher   AddQuery + BatchSearch (src/engine/retrieval/searcher/full_recall_searcher.h)
+    operators            the device operators' launch entry points (include/hss.h)
+
+Device pointers are passed as integers (``tensor.data_ptr()``); streams as integers
+(``torch.cuda.current_stream().cuda_stream``) or 0 for the default stream. Everything runs through
+libhss.so; nothing here computes results on the CPU.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+
+def _np_ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class DataTable:
+    """Index resident on one GPU (device < 0: host only, for building / compiling / saving)."""
+
+    def __init__(self, handle, device):
+        self._h = ctypes.c_void_p(handle)
+        self.device = device
+
+    @classmethod
+    def build(cls, vectors, tag_bits, tag_num, device=0, doc_num_per_segment=131072, density_threshold=1.0 / 64,
+              matrix_posting=False, sparse_packed=False, doc_offset=0):
+        lib = _lib.load()
+        vectors = np.ascontiguousarray(vectors, dtype=np.float32)
+        tag_bits = np.ascontiguousarray(tag_bits, dtype=np.uint64)
+        n, dim = vectors.shape
+        assert tag_bits.shape[0] == n and tag_bits.shape[1] == (tag_num + 63) // 64
+        cfg = _lib.IndexConfig(doc_num_per_segment, density_threshold, int(matrix_posting), int(sparse_packed),
+                               doc_offset)
+        h = ctypes.c_void_p()
+        check(lib.hss_table_build(device, _np_ptr(vectors), _np_ptr(tag_bits), n, dim, tag_num, ctypes.byref(cfg),
+                                  ctypes.byref(h)))
+        return cls(h.value, device)
+
+    @classmethod
+    def load(cls, directory, device=0):
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        check(lib.hss_table_load(device, str(directory).encode(), ctypes.byref(h)))
+        return cls(h.value, device)
+
+    def save(self, directory):
+        check(_lib.load().hss_table_save(self._h, str(directory).encode()))
+
+    def close(self):
+        if self._h:
+            _lib.load().hss_table_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def info(self):
+        n = ctypes.c_uint64()
+        dim, segs, p, rows = (ctypes.c_uint32() for _ in range(4))
+        mx = ctypes.c_float()
+        check(_lib.load().hss_table_info(self._h, ctypes.byref(n), ctypes.byref(dim), ctypes.byref(segs),
+                                         ctypes.byref(p), ctypes.byref(rows), ctypes.byref(mx)))
+        return {"doc_num": n.value, "dim": dim.value, "segment_num": segs.value, "doc_num_per_segment": p.value,
+                "posting_rows": rows.value, "max_norm": mx.value}
+
+    def posting(self, token, segment):
+        """Host bytes of a token's posting in one segment, or None when the token is absent there."""
+        data = _lib.c_u8p()
+        n = ctypes.c_uint32()
+        check(_lib.load().hss_table_posting(self._h, token, segment, ctypes.byref(data), ctypes.byref(n)))
+        if not data or n.value == 0:
+            return None
+        return bytes(ctypes.string_at(data, n.value))
+
+    def device_ptrs(self):
+        v, t, g = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        check(_lib.load().hss_table_device_ptrs(self._h, ctypes.byref(v), ctypes.byref(t), ctypes.byref(g)))
+        return v.value, t.value, g.value
+
+    def compile_filter(self, expr):
+        """(postfix program, operand rows, opNum, empty_tree) of one filter text."""
+        prog = np.zeros(_lib.HSS_MAX_PROGRAM * 4, np.uint32)
+        rows = np.zeros(_lib.HSS_MAX_OPERANDS * 4, np.uint32)
+        pl, rl, opn = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        empty = ctypes.c_int32()
+        check(_lib.load().hss_filter_compile(self._h, expr.encode(), _np_ptr(prog), prog.size, ctypes.byref(pl),
+                                             _np_ptr(rows), rows.size, ctypes.byref(rl), ctypes.byref(opn),
+                                             ctypes.byref(empty)))
+        return prog[:pl.value].copy(), rows[:rl.value].copy(), opn.value, bool(empty.value)
+
+
+class Filters:
+    """A batch's filter texts compiled once (TextFilter::PrepareExpr)."""
+
+    def __init__(self, searcher, exprs):
+        lib = _lib.load()
+        arr = (ctypes.c_char_p * max(1, len(exprs)))(*[e.encode() for e in exprs])
+        h = ctypes.c_void_p()
+        check(lib.hss_filters_compile(searcher._h, arr, len(exprs), ctypes.byref(h)))
+        self._h = h
+        self.n = len(exprs)
+
+    def close(self):
+        if self._h:
+            _lib.load().hss_filters_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FullRecallSearcher:
+    def __init__(self, table, max_batch=256, candidate_cap=1 << 18, sample_docs=32768, max_retries=4, method=0):
+        lib = _lib.load()
+        self.table = table
+        self.dim = table.info["dim"]
+        cfg = _lib.SearcherConfig(max_batch, candidate_cap, sample_docs, max_retries, method)
+        h = ctypes.c_void_p()
+        check(lib.hss_searcher_create(table._h, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.max_batch = max_batch
+        self._pending = 0
+
+    def close(self):
+        if self._h:
+            _lib.load().hss_searcher_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_query(self, filter_expr, vector, topk):
+        v = np.ascontiguousarray(vector, dtype=np.float32)
+        check(_lib.load().hss_searcher_add_query(self._h, (filter_expr or "").encode(), _np_ptr(v), v.size, topk))
+        self._pending += 1
+
+    def batch_search(self, out_stride=None):
+        """Runs the added queries. Returns (scores [n][stride], ids [n][stride], counts [n])."""
+        n = self._pending
+        stride = out_stride or _lib.HSS_MAX_TOPK
+        scores = np.zeros((max(n, 1), stride), np.float32)
+        ids = np.full((max(n, 1), stride), -1, np.int64)
+        counts = np.zeros(max(n, 1), np.uint32)
+        self._pending = 0
+        rc = _lib.load().hss_searcher_batch_search(self._h, _np_ptr(scores), _np_ptr(ids), _np_ptr(counts), stride)
+        if rc != _lib.HSS_ERR_QUERY:
+            check(rc)
+        return scores[:n], ids[:n], counts[:n]
+
+    def compile_filters(self, exprs):
+        return Filters(self, exprs)
+
+    def search_device(self, d_queries, nq, filters, topks, d_scores, d_ids, d_counts, out_stride, stream=0):
+        """Device-resident batch. Returns the status code (HSS_OK or HSS_ERR_QUERY)."""
+        t = np.ascontiguousarray(topks, dtype=np.uint32)
+        rc = _lib.load().hss_searcher_search_device(self._h, d_queries, nq, filters._h, _np_ptr(t), d_scores, d_ids,
+                                                    d_counts, out_stride, stream)
+        if rc != _lib.HSS_ERR_QUERY:
+            check(rc)
+        return rc
+
+    def filter_device(self, filters, nq, d_bits, stride_words, d_pass=None, stream=0):
+        """Filter stage alone: per-query doc bitmaps into d_bits. Returns the status code."""
+        rc = _lib.load().hss_searcher_filter_device(self._h, filters._h, nq, d_bits, stride_words, d_pass, stream)
+        if rc != _lib.HSS_ERR_QUERY:
+            check(rc)
+        return rc
+
+    def last_status(self, n):
+        st = np.zeros(max(n, 1), np.int32)
+        check(_lib.load().hss_searcher_last_status(self._h, _np_ptr(st), n))
+        return st[:n]
+
+    def set_timing(self, on=True):
+        check(_lib.load().hss_searcher_set_timing(self._h, int(on)))
+
+    def last_times(self):
+        ms = np.zeros(5, np.float32)
+        r, l = ctypes.c_uint32(), ctypes.c_uint32()
+        check(_lib.load().hss_searcher_last_times(self._h, _np_ptr(ms), ctypes.byref(r), ctypes.byref(l)))
+        return {"filter_ms": float(ms[0]), "sample_ms": float(ms[1]), "candidates_ms": float(ms[2]),
+                "select_ms": float(ms[3]), "total_ms": float(ms[4]), "retries": r.value, "launches": l.value}
+
+
+# ---- operator entry points (device pointers as ints) ----
+
+def vector_score(d_queries, d_docs, d_out, m, n, k, ld, stream=0):
+    check(_lib.load().hss_vector_score_launch(d_queries, d_docs, d_out, m, n, k, ld, stream))
+
+
+def bitmap_text_filter(d_postings, d_expr, context, d_result, d_status=None, stream=0):
+    check(_lib.load().hss_bitmap_text_filter_launch(d_postings, d_expr, None, context, d_result, d_status, stream))
+
+
+def posting_bitlist_to_set(d_postings, byte_size, d_results, count, d_status=None, stream=0):
+    check(_lib.load().hss_posting_bitlist_to_set_launch(d_postings, byte_size, d_results, count, d_status, stream))
+
+
+def aggregator_workspace_size(doc_number):
+    return _lib.load().hss_aggregator_workspace_size(doc_number)
+
+
+def aggregator(d_filter, d_scores, d_loc, d_out_scores, d_out_loc, d_count, doc_number, d_ws, ws_bytes, stream=0):
+    check(_lib.load().hss_aggregator_launch(d_filter, d_scores, d_loc, d_out_scores, d_out_loc, d_count, doc_number,
+                                            d_ws, ws_bytes, stream))
+
+
+def topk(d_scores, d_locs, d_count, k, d_out_scores, d_out_locs, d_out_count, stream=0):
+    check(_lib.load().hss_topk_launch(d_scores, d_locs, d_count, k, d_out_scores, d_out_locs, d_out_count, stream))
+
+
+def hash64(token):
+    b = token.encode() if isinstance(token, str) else bytes(token)
+    return _lib.load().hss_hash64(b, len(b))
+
+
+def posting_serialize(ids, doc_num, is_matrix=False, density_threshold=1.0 / 64, sparse_packed=False):
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    cap = 8 + max(doc_num, 6 * ((doc_num + 15) // 16), 4 * ids.size) + 64
+    out = np.zeros(cap, np.uint8)
+    n = check(_lib.load().hss_posting_serialize(_np_ptr(ids), ids.size, doc_num, int(is_matrix), density_threshold,
+                                                int(sparse_packed), _np_ptr(out), cap))
+    return out[:n].tobytes()
+
+
+def device_count():
+    return _lib.load().hss_device_count()

@@ -1,0 +1,377 @@
+// capi.cpp -- extern "C" entry points of libhss.so (declared in include/hss.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hss.h"
+#include "hss_device.cuh"
+#include "hss_kernels.h"
+#include "host/hss_host.h"
+
+namespace {
+thread_local std::string g_lastError;
+
+int SetError(int code, const std::string& msg) {
+    g_lastError = msg;
+    return code;
+}
+
+int FromCuda(cudaError_t e) {
+    if (e == cudaSuccess) return HSS_OK;
+    return SetError(HSS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+cudaStream_t S(hss_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+}  // namespace
+
+struct hss_table {
+    std::shared_ptr<hss::DataTable> t;
+};
+
+struct hss_searcher {
+    std::unique_ptr<hss::FullRecallSearcher> s;
+    std::shared_ptr<hss::DataTable> t;
+    std::vector<std::unique_ptr<hss::QueryNode>> owned;  // trees of the added queries
+};
+
+struct hss_filters {
+    std::vector<hss::FilterExpr> exprs;
+};
+
+extern "C" {
+
+const char* hss_last_error(void) { return g_lastError.c_str(); }
+
+int hss_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+// ---------------------------------------------------------------------------------------------
+// operators
+
+int hss_vector_score_launch(const float* queryMatrix, const float* docMatrix, float* resultMatrix, uint32_t m,
+                            uint32_t n, uint32_t k, uint64_t ldResult, hss_stream_t stream) {
+    if (!queryMatrix || !docMatrix || !resultMatrix || k == 0 || k % 4 || k > 4096 || ldResult < n)
+        return SetError(HSS_ERR_INVALID, "hss_vector_score_launch: bad arguments");
+    return FromCuda(hss::launch_exact_score(queryMatrix, docMatrix, resultMatrix, m, n, k, ldResult, S(stream)));
+}
+
+int hss_bitmap_text_filter_launch(const uint64_t* postings, const uint32_t* postOrderExpr, void* resultStack,
+                                  hss_filter_context ctx, uint8_t* result, int32_t* status, hss_stream_t stream) {
+    (void)resultStack;
+    if (!postings || !postOrderExpr || !result || ctx.segmentNum == 0 || ctx.segmentLength == 0 ||
+        ctx.segmentLength % 8 != 0 || (reinterpret_cast<uintptr_t>(result) & 7u))
+        return SetError(HSS_ERR_INVALID, "hss_bitmap_text_filter_launch: bad arguments");
+    if (ctx.postingNum > static_cast<uint32_t>(hss::kMaxOperands) || ctx.exprLen > static_cast<uint32_t>(hss::kMaxProgram))
+        return SetError(HSS_ERR_LIMIT, "filter program beyond HSS_MAX_OPERANDS / HSS_MAX_PROGRAM");
+    if (ctx.exprLen == 0) return SetError(HSS_ERR_PROGRAM, "empty filter program");
+    hss::FilterLaunch F{};
+    F.prog = postOrderExpr;
+    F.prog_off = nullptr;
+    F.opnd_off = nullptr;
+    F.opnd_row = nullptr;
+    F.single_prog_len = ctx.exprLen;
+    F.single_nop = ctx.postingNum;
+    F.table = postings;
+    F.row_stride = 1;
+    F.seg_stride = ctx.postingNum;
+    F.out = reinterpret_cast<uint64_t*>(result);
+    F.out_stride = 0;
+    F.pass_count = nullptr;
+    F.status = status;
+    F.nq = 1;
+    F.seg_num = ctx.segmentNum;
+    F.docs_per_seg = ctx.segmentLength * 16u;
+    F.doc_num = static_cast<uint64_t>(ctx.segmentNum) * F.docs_per_seg;
+    F.max_opnd = ctx.postingNum;
+    F.ref_table = (ctx.flags & HSS_FILTER_HEAD_ADDRESSES) ? 0 : 1;
+    return FromCuda(hss::launch_filter_batch(F, S(stream)));
+}
+
+int hss_posting_bitlist_to_set_launch(const uint64_t* postings, uint32_t byteSizePerSegment,
+                                      const uint64_t* resultPostings, uint32_t count, int32_t* status,
+                                      hss_stream_t stream) {
+    if ((count && (!postings || !resultPostings)) || byteSizePerSegment == 0 || byteSizePerSegment % 8)
+        return SetError(HSS_ERR_INVALID, "hss_posting_bitlist_to_set_launch: bad arguments");
+    return FromCuda(hss::launch_posting_expand(postings, resultPostings, count, byteSizePerSegment,
+                                               byteSizePerSegment * 8u, status, S(stream)));
+}
+
+size_t hss_aggregator_workspace_size(uint32_t docNumber) { return hss::aggregate_workspace_bytes(docNumber); }
+
+int hss_aggregator_launch(const uint8_t* filterResult, const float* docScores, const uint32_t* docLocationConst,
+                          float* outScores, uint32_t* outLocations, uint32_t* effectiveCount, uint32_t docNumber,
+                          void* workspace, size_t workspaceBytes, hss_stream_t stream) {
+    if (!filterResult || !docScores || !outScores || !outLocations || !effectiveCount || !workspace ||
+        (reinterpret_cast<uintptr_t>(filterResult) & 7u))
+        return SetError(HSS_ERR_INVALID, "hss_aggregator_launch: bad arguments");
+    if (workspaceBytes < hss::aggregate_workspace_bytes(docNumber))
+        return SetError(HSS_ERR_INVALID, "hss_aggregator_launch: workspace too small");
+    return FromCuda(hss::launch_aggregate(reinterpret_cast<const uint64_t*>(filterResult), docScores,
+                                          docLocationConst, docNumber, outScores, outLocations, effectiveCount,
+                                          static_cast<uint32_t*>(workspace), S(stream)));
+}
+
+int hss_topk_launch(const float* scores, const uint32_t* locations, const uint32_t* count, uint32_t topK,
+                    float* outScores, uint32_t* outLocations, uint32_t* outCount, hss_stream_t stream) {
+    if (!scores || !locations || !count || !outScores || !outLocations || !outCount)
+        return SetError(HSS_ERR_INVALID, "hss_topk_launch: bad arguments");
+    if (topK > static_cast<uint32_t>(hss::kMaxTopK)) return SetError(HSS_ERR_LIMIT, "topK beyond HSS_MAX_TOPK");
+    return FromCuda(hss::launch_topk_op(scores, locations, count, topK, outScores, outLocations, outCount, S(stream)));
+}
+
+// ---------------------------------------------------------------------------------------------
+// index
+
+int hss_table_build(int32_t deviceId, const float* vectors, const uint64_t* tagBits, uint64_t docNum, uint32_t dim,
+                    uint32_t tagNum, const hss_index_config* cfg, hss_table** out) {
+    if (!vectors || !tagBits || !out) return SetError(HSS_ERR_INVALID, "hss_table_build: null argument");
+    hss::IndexConfig c;
+    if (cfg) {
+        c.docNumPerSegment = cfg->docNumPerSegment;
+        c.densityThreshold = cfg->densityThreshold;
+        c.matrixPosting = cfg->matrixPosting != 0;
+        c.sparsePacked = cfg->sparsePacked != 0;
+        c.docOffset = cfg->docOffset;
+    }
+    auto t = std::make_shared<hss::DataTable>();
+    std::string err;
+    if (!t->Build(deviceId, vectors, tagBits, docNum, dim, tagNum, c, &err)) return SetError(HSS_ERR_INDEX, err);
+    *out = new hss_table{t};
+    return HSS_OK;
+}
+
+int hss_table_load(int32_t deviceId, const char* dir, hss_table** out) {
+    if (!dir || !out) return SetError(HSS_ERR_INVALID, "hss_table_load: null argument");
+    auto t = std::make_shared<hss::DataTable>();
+    std::string err;
+    if (!t->LoadData(deviceId, dir, &err)) return SetError(HSS_ERR_INDEX, err);
+    *out = new hss_table{t};
+    return HSS_OK;
+}
+
+int hss_table_save(const hss_table* table, const char* dir) {
+    if (!table || !dir) return SetError(HSS_ERR_INVALID, "hss_table_save: null argument");
+    std::string err;
+    if (!table->t->Save(dir, &err)) return SetError(HSS_ERR_INDEX, err);
+    return HSS_OK;
+}
+
+void hss_table_free(hss_table* table) { delete table; }
+
+int hss_table_info(const hss_table* table, uint64_t* docNum, uint32_t* dim, uint32_t* segmentNum,
+                   uint32_t* docNumPerSegment, uint32_t* postingRows, float* maxNorm) {
+    if (!table) return SetError(HSS_ERR_INVALID, "null table");
+    const hss::DataTable& t = *table->t;
+    if (docNum) *docNum = t.GetDocNum();
+    if (dim) *dim = t.GetDimension();
+    if (segmentNum) *segmentNum = t.GetSegmentNum();
+    if (docNumPerSegment) *docNumPerSegment = t.GetDocNumPerSegment();
+    if (postingRows) *postingRows = t.PostingRows();
+    if (maxNorm) *maxNorm = t.GetMaxNorm();
+    return HSS_OK;
+}
+
+int hss_table_posting(const hss_table* table, uint64_t token, uint32_t segment, const uint8_t** data, uint32_t* len) {
+    if (!table || !data || !len) return SetError(HSS_ERR_INVALID, "null argument");
+    bool exist = false;
+    const uint32_t row = table->t->TokenRow(token, exist);
+    *data = exist ? table->t->HostPosting(row, segment, len) : nullptr;
+    if (!*data) *len = 0;
+    return HSS_OK;
+}
+
+int hss_table_device_ptrs(const hss_table* table, const float** vectors, const uint64_t** postingTable,
+                          const int64_t** gdocids) {
+    if (!table) return SetError(HSS_ERR_INVALID, "null table");
+    if (vectors) *vectors = table->t->DeviceVectors();
+    if (postingTable) *postingTable = table->t->DevicePostingTable();
+    if (gdocids) *gdocids = table->t->DeviceGDocIds();
+    return HSS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// searcher
+
+int hss_searcher_create(hss_table* table, const hss_searcher_config* cfg, hss_searcher** out) {
+    if (!table || !out) return SetError(HSS_ERR_INVALID, "hss_searcher_create: null argument");
+    hss::SearcherConfig c;
+    if (cfg) {
+        if (cfg->maxBatch) c.maxBatch = cfg->maxBatch;
+        if (cfg->candidateCap) c.candidateCap = cfg->candidateCap;
+        if (cfg->sampleDocs) c.sampleDocs = cfg->sampleDocs;
+        c.maxRetries = cfg->maxRetries;
+        if (cfg->method != 0) return SetError(HSS_ERR_INVALID, "unknown scoring method");
+        c.method = static_cast<hss::ScoreMethod>(cfg->method);
+    }
+    auto* s = new hss_searcher;
+    s->t = table->t;
+    s->s = std::make_unique<hss::FullRecallSearcher>(table->t->GetDeviceId(), table->t, c);
+    if (!s->s->Ok()) {
+        const std::string e = s->s->Error();
+        delete s;
+        return SetError(HSS_ERR_CUDA, e);
+    }
+    *out = s;
+    return HSS_OK;
+}
+
+void hss_searcher_free(hss_searcher* s) { delete s; }
+
+int hss_searcher_add_query(hss_searcher* s, const char* filterExpr, const float* vector, uint32_t dim, uint32_t topK) {
+    if (!s || !vector) return SetError(HSS_ERR_INVALID, "hss_searcher_add_query: null argument");
+    if (dim != s->t->GetDimension()) return SetError(HSS_ERR_INVALID, "query dimension mismatch");
+    bool ok = true;
+    auto ast = hss::ParseFilter(filterExpr ? filterExpr : "", ok);
+    if (!ok) return SetError(HSS_ERR_PARSE, std::string("filter does not parse: ") + (filterExpr ? filterExpr : ""));
+    s->owned.push_back(hss::BuildQueryNode(ast.get(), s->t->GetConfig().postingField));
+    s->s->AddQuery(s->owned.back().get(), std::vector<float>(vector, vector + dim), topK);
+    return HSS_OK;
+}
+
+int hss_searcher_batch_search(hss_searcher* s, float* outScores, int64_t* outIds, uint32_t* outCounts,
+                              uint32_t outStride) {
+    if (!s || !outScores || !outIds || !outCounts) return SetError(HSS_ERR_INVALID, "null argument");
+    std::vector<std::shared_ptr<hss::FullRecallResult>> res;
+    const bool ok = s->s->BatchSearch(res, s->t->GetConfig().vectorField, false);
+    s->owned.clear();
+    if (!ok) return SetError(HSS_ERR_CUDA, s->s->Error());
+    bool failed = false;
+    for (size_t q = 0; q < res.size(); ++q) {
+        const auto& r = *res[q];
+        const uint32_t c = static_cast<uint32_t>(std::min<size_t>(r.docIds.size(), outStride));
+        outCounts[q] = c;
+        for (uint32_t i = 0; i < c; ++i) {
+            outScores[q * static_cast<size_t>(outStride) + i] = r.scores[i];
+            outIds[q * static_cast<size_t>(outStride) + i] = r.docIds[i];
+        }
+    }
+    for (int32_t st : s->s->LastStatus()) failed |= st != 0;
+    if (failed) return SetError(HSS_ERR_QUERY, "some queries failed (see hss_searcher_last_status)");
+    return HSS_OK;
+}
+
+int hss_filters_compile(hss_searcher* s, const char* const* filterExprs, uint32_t n, hss_filters** out) {
+    if (!s || !out || (n && !filterExprs)) return SetError(HSS_ERR_INVALID, "hss_filters_compile: null argument");
+    auto f = std::make_unique<hss_filters>();
+    f->exprs.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        bool ok = true;
+        const char* e = filterExprs[i] ? filterExprs[i] : "";
+        auto ast = hss::ParseFilter(e, ok);
+        if (!ok) return SetError(HSS_ERR_PARSE, std::string("filter does not parse: ") + e);
+        auto tree = hss::BuildQueryNode(ast.get(), s->t->GetConfig().postingField);
+        std::string err;
+        if (!hss::PrepareExpr(tree.get(), *s->t, f->exprs[i], &err)) return SetError(HSS_ERR_PROGRAM, err);
+    }
+    *out = f.release();
+    return HSS_OK;
+}
+
+void hss_filters_free(hss_filters* f) { delete f; }
+
+int hss_searcher_search_device(hss_searcher* s, const float* dQueries, uint32_t nq, const hss_filters* filters,
+                               const uint32_t* topks, float* dOutScores, int64_t* dOutIds, uint32_t* dOutCounts,
+                               uint32_t outStride, hss_stream_t stream) {
+    if (!s || !filters || !topks || (nq && (!dQueries || !dOutScores || !dOutIds || !dOutCounts)))
+        return SetError(HSS_ERR_INVALID, "hss_searcher_search_device: null argument");
+    if (filters->exprs.size() < nq) return SetError(HSS_ERR_INVALID, "fewer filters than queries");
+    std::vector<const hss::FilterExpr*> ptrs(nq);
+    for (uint32_t i = 0; i < nq; ++i) ptrs[i] = &filters->exprs[i];
+    const int rc = s->s->SearchDevice(dQueries, nq, ptrs.data(), topks, dOutScores, dOutIds, dOutCounts, outStride,
+                                      S(stream));
+    if (rc < 0) return SetError(rc == -1 ? HSS_ERR_INVALID : HSS_ERR_CUDA, s->s->Error());
+    if (rc > 0) return SetError(HSS_ERR_QUERY, "some queries failed (see hss_searcher_last_status)");
+    return HSS_OK;
+}
+
+int hss_searcher_filter_device(hss_searcher* s, const hss_filters* filters, uint32_t nq, uint64_t* dOutBits,
+                               uint64_t outStrideWords, uint32_t* dPassCounts, hss_stream_t stream) {
+    if (!s || !filters || (nq && !dOutBits)) return SetError(HSS_ERR_INVALID, "hss_searcher_filter_device: null argument");
+    if (filters->exprs.size() < nq) return SetError(HSS_ERR_INVALID, "fewer filters than queries");
+    std::vector<const hss::FilterExpr*> ptrs(nq);
+    for (uint32_t i = 0; i < nq; ++i) ptrs[i] = &filters->exprs[i];
+    const int rc = s->s->FilterDevice(nq, ptrs.data(), dOutBits, outStrideWords, dPassCounts, S(stream));
+    if (rc < 0) return SetError(rc == -1 ? HSS_ERR_INVALID : HSS_ERR_CUDA, s->s->Error());
+    if (rc > 0) return SetError(HSS_ERR_QUERY, "some filters failed (see hss_searcher_last_status)");
+    return HSS_OK;
+}
+
+int hss_searcher_last_status(const hss_searcher* s, int32_t* status, uint32_t n) {
+    if (!s || (n && !status)) return SetError(HSS_ERR_INVALID, "null argument");
+    const auto& st = s->s->LastStatus();
+    for (uint32_t i = 0; i < n; ++i) status[i] = i < st.size() ? st[i] : 0;
+    return HSS_OK;
+}
+
+int hss_searcher_set_timing(hss_searcher* s, int32_t on) {
+    if (!s) return SetError(HSS_ERR_INVALID, "null searcher");
+    s->s->SetTiming(on != 0);
+    return HSS_OK;
+}
+
+int hss_searcher_last_times(const hss_searcher* s, float* ms5, uint32_t* retries, uint32_t* launches) {
+    if (!s) return SetError(HSS_ERR_INVALID, "null searcher");
+    const hss::StageTimes& t = s->s->LastTimes();
+    if (ms5) {
+        ms5[0] = t.filter;
+        ms5[1] = t.sample;
+        ms5[2] = t.candidates;
+        ms5[3] = t.select;
+        ms5[4] = t.total;
+    }
+    if (retries) *retries = t.retries;
+    if (launches) *launches = t.launches;
+    return HSS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// codec
+
+uint64_t hss_hash64(const char* data, uint32_t len) { return hss::Hash64(data, len); }
+
+int64_t hss_posting_serialize(const uint32_t* ids, uint32_t n, uint32_t docNum, int32_t isMatrix,
+                              float densityThreshold, int32_t sparsePacked, uint8_t* out, uint64_t cap) {
+    if ((n && !ids) || !out) return SetError(HSS_ERR_INVALID, "null argument");
+    std::vector<uint32_t> v(ids, ids + n);
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    std::string buf;
+    if (!hss::PostingSerializer::Serialize(v, docNum, isMatrix != 0, densityThreshold, sparsePacked != 0, buf))
+        return SetError(HSS_ERR_INVALID, "posting cannot be serialised");
+    if (buf.size() > cap) return SetError(HSS_ERR_LIMIT, "output buffer too small");
+    std::memcpy(out, buf.data(), buf.size());
+    return static_cast<int64_t>(buf.size());
+}
+
+int hss_filter_compile(const hss_table* table, const char* filterExpr, uint32_t* prog, uint32_t progCap,
+                       uint32_t* progLen, uint32_t* rows, uint32_t rowCap, uint32_t* rowLen, uint32_t* opNum,
+                       int32_t* emptyTree) {
+    if (!table || !progLen || !rowLen) return SetError(HSS_ERR_INVALID, "null argument");
+    bool ok = true;
+    auto ast = hss::ParseFilter(filterExpr ? filterExpr : "", ok);
+    if (!ok) return SetError(HSS_ERR_PARSE, "filter does not parse");
+    auto tree = hss::BuildQueryNode(ast.get(), table->t->GetConfig().postingField);
+    hss::FilterExpr e;
+    std::string err;
+    if (!hss::PrepareExpr(tree.get(), *table->t, e, &err)) return SetError(HSS_ERR_PROGRAM, err);
+    *progLen = static_cast<uint32_t>(e.postExpr.size());
+    *rowLen = static_cast<uint32_t>(e.postingRows.size());
+    if (opNum) *opNum = e.opNum;
+    if (emptyTree) *emptyTree = e.emptyTree ? 1 : 0;
+    if (*progLen > progCap || *rowLen > rowCap) return SetError(HSS_ERR_LIMIT, "output buffers too small");
+    if (prog) std::copy(e.postExpr.begin(), e.postExpr.end(), prog);
+    if (rows) std::copy(e.postingRows.begin(), e.postingRows.end(), rows);
+    return HSS_OK;
+}
+
+}  // extern "C"

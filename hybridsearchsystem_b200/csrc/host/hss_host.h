@@ -1,0 +1,365 @@
+// hss_host.h -- host-side C++ mirror of the reference's filtered full-recall interface:
+//   Hash64                        (src/engine/core/hash/hash.h:15-20)
+//   FilterNode / ParseFilter      (src/harness/query/filter_expr.h:19-177)
+//   PostingLayout / serializer    (src/engine/format/posting_layout.h:8, posting_serializer.h)
+//   QueryNode family              (src/engine/retrieval/query/query_node.h, query_node_imp.h)
+//   DataTable                     (src/engine/index/data_table.h:10-92)
+//   FullRecallSearcher / Result   (src/engine/retrieval/searcher/full_recall_searcher.h:12-47,
+//                                  src/engine/core/full_recall_result.h:30-50)
+// Names and argument meanings follow the reference; the device work goes to the CUDA kernels of
+// libhss.so instead of the AscendC operators.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+
+namespace hss {
+
+// ---------------------------------------------------------------------------------------------
+// Token hash: MurmurHash3_x64_128(seed 0x20160713), h1 ^ h2 (hash.cpp:10-16).
+uint64_t Hash64(const char* data, uint32_t len);
+inline uint64_t Hash64(const std::string& s) { return Hash64(s.data(), static_cast<uint32_t>(s.size())); }
+
+// ---------------------------------------------------------------------------------------------
+// Filter expression AST and parser. Grammar, precedence NOT > AND > OR, n-ary AND/OR flattening
+// and the empty-expression = match-all rule are the reference's (filter_expr.h:1-8,164-177).
+enum class FilterOp { Term, And, Or, Not };
+
+struct FilterNode {
+    FilterOp op = FilterOp::Term;
+    uint64_t tag = 0;  // valid when op == Term
+    std::vector<std::unique_ptr<FilterNode>> children;
+};
+
+// nullptr with ok = true: empty expression (match all). nullptr with ok = false: parse error.
+std::unique_ptr<FilterNode> ParseFilter(const std::string& expr, bool& ok);
+
+// ---------------------------------------------------------------------------------------------
+// Posting codec (on-disk format contract, posting_serializer.cpp:15-208).
+enum class PostingLayout { DENSE_BITMAP = 0, SPARSE_BITMAP, DENSE_BYTEMAP, SPARSE_IDLIST, SPARSE_PACKED, UNKNOWN };
+
+class PostingSerializer {
+   public:
+    // docIds: the segment-local ids of the hits, sorted ascending without duplicates. Appends the
+    // posting (8-byte head + payload) to `buffer`. SPARSE_IDLIST ids are written ascending.
+    static bool Serialize(const std::vector<uint32_t>& docIds, uint32_t docNum, bool isMatrixType,
+                          float densityThreshold, bool sparsePacked, std::string& buffer);
+    static PostingLayout SelectLayout(bool isMatrixType, uint32_t targetDocNum, uint32_t docNum,
+                                      float densityThreshold, bool sparsePacked);
+};
+
+// Structural check of one posting for a segment of segDocs docs: known layout, payload inside the
+// buffer and legal for the layout, sparse units sorted, strictly increasing and in range.
+bool ValidatePosting(const uint8_t* p, size_t len, uint32_t segDocs, std::string* err);
+
+// ---------------------------------------------------------------------------------------------
+class DataTable;
+
+enum class QueryNodeType { AndNode = 1, OrNode, NotNode, TermNode, TermsNode, OrTermsNode, ConjunctionNode };
+enum FilterOpType : uint32_t { CONJUNCTION = 0, AND = 1, OR = 2, NOT = 3 };
+
+// A compiled filter: the reference's postfix program (query_node_imp.cpp:8-47,65-96,295-342) plus,
+// per operand, the posting row of the DataTable it reads.
+struct FilterExpr {
+    std::vector<uint32_t> postExpr;
+    std::vector<uint32_t> postingRows;
+    uint32_t opNum = 0;
+    bool emptyTree = false;  // match all
+};
+
+class QueryNode {
+   public:
+    virtual ~QueryNode() = default;
+    void AddChild(std::unique_ptr<QueryNode>& child);
+    uint32_t GetChildrenNum() const { return static_cast<uint32_t>(m_children.size()); }
+    virtual QueryNodeType GetNodeType() const = 0;
+    virtual std::string GetName() const = 0;
+    // Appends this subtree's postfix code; false when the subtree contributes nothing.
+    virtual bool GetPostOrderExpression(const DataTable& table, FilterExpr& out) const = 0;
+
+   protected:
+    std::vector<std::unique_ptr<QueryNode>> m_children;
+};
+
+class QueryLeafNode : public QueryNode {
+   public:
+    virtual bool AppendPostings(const DataTable& table, FilterExpr& out) const = 0;
+};
+
+class AndNode : public QueryNode {
+   public:
+    QueryNodeType GetNodeType() const override { return QueryNodeType::AndNode; }
+    std::string GetName() const override { return "and"; }
+    bool GetPostOrderExpression(const DataTable& table, FilterExpr& out) const override;
+};
+
+class OrNode : public QueryNode {
+   public:
+    QueryNodeType GetNodeType() const override { return QueryNodeType::OrNode; }
+    std::string GetName() const override { return "or"; }
+    bool GetPostOrderExpression(const DataTable& table, FilterExpr& out) const override;
+};
+
+class NotNode : public QueryNode {
+   public:
+    QueryNodeType GetNodeType() const override { return QueryNodeType::NotNode; }
+    std::string GetName() const override { return "not"; }
+    bool GetPostOrderExpression(const DataTable& table, FilterExpr& out) const override;
+};
+
+class TermNode : public QueryLeafNode {
+   public:
+    TermNode(const std::string& fieldName, uint64_t token) : m_fieldName(fieldName), m_token(token) {}
+    QueryNodeType GetNodeType() const override { return QueryNodeType::TermNode; }
+    std::string GetName() const override { return "term:" + m_fieldName + ":" + std::to_string(m_token); }
+    bool GetPostOrderExpression(const DataTable& table, FilterExpr& out) const override;
+    bool AppendPostings(const DataTable& table, FilterExpr& out) const override;
+
+   private:
+    std::string m_fieldName;
+    uint64_t m_token;
+};
+
+class TermsNode : public QueryLeafNode {
+   public:
+    TermsNode(const std::string& fieldName, std::vector<uint64_t> tokens)
+        : m_fieldName(fieldName), m_tokens(std::move(tokens)) {}
+    QueryNodeType GetNodeType() const override { return QueryNodeType::TermsNode; }
+    std::string GetName() const override { return "terms:" + m_fieldName; }
+    bool GetPostOrderExpression(const DataTable& table, FilterExpr& out) const override;
+    bool AppendPostings(const DataTable& table, FilterExpr& out) const override;
+
+   private:
+    std::string m_fieldName;
+    std::vector<uint64_t> m_tokens;
+};
+
+class OrTermsNode : public QueryLeafNode {
+   public:
+    QueryNodeType GetNodeType() const override { return QueryNodeType::OrTermsNode; }
+    std::string GetName() const override { return "or_terms"; }
+    bool GetPostOrderExpression(const DataTable& table, FilterExpr& out) const override;
+    bool AppendPostings(const DataTable& table, FilterExpr& out) const override;
+};
+
+class ConjunctionNode : public QueryNode {
+   public:
+    QueryNodeType GetNodeType() const override { return QueryNodeType::ConjunctionNode; }
+    std::string GetName() const override { return "conjunction"; }
+    bool GetPostOrderExpression(const DataTable& table, FilterExpr& out) const override;
+};
+
+// Harness translation of a parsed filter (filter_setup.cpp:96-137): a Term becomes a TermNode on
+// Hash64(decimal tag); a null AST becomes an empty AndNode (match all).
+std::unique_ptr<QueryNode> BuildQueryNode(const FilterNode* n, const std::string& field);
+
+// Builds the postfix program (TextFilter::PrepareExpr, text_filter.cpp:432-467) and validates it
+// (CheckPostExpr, :1314-1352). Returns false on an invalid program.
+bool PrepareExpr(const QueryNode* tree, const DataTable& table, FilterExpr& out, std::string* err);
+bool CheckPostExpr(const std::vector<uint32_t>& postExpr, uint32_t postingNums);
+
+// ---------------------------------------------------------------------------------------------
+struct IndexConfig {
+    uint32_t docNumPerSegment = 131072;  // multiple of 128
+    float densityThreshold = 1.0f / 64.0f;
+    bool matrixPosting = false;  // DENSE_BYTEMAP / SPARSE_IDLIST instead of the bitmap layouts
+    bool sparsePacked = false;   // SPARSE_PACKED instead of SPARSE_BITMAP
+    uint64_t docOffset = 0;      // global doc id of location 0
+    std::string postingField = "content";
+    std::string vectorField = "content";
+};
+
+// Index residency on one GPU. Device layout:
+//   vectors    FP32 [tiles*128][dim] row-major, rows past docNum zero
+//   postings   one arena; every posting copied to a 16-byte aligned slot, zero-padded
+//   postingTable u64 [rows][segments]: device address of token row r's posting in segment s (the
+//              all-zero posting where the token is absent); the last row is the all-zero token
+//   gdocids    int64 [docNum], location -> global doc id
+class DataTable {
+   public:
+    DataTable() = default;
+    ~DataTable();
+    DataTable(const DataTable&) = delete;
+    DataTable& operator=(const DataTable&) = delete;
+
+    // Offline build (fr_converter + fr_builder) from HYDSET2-style arrays: vectors [docNum][dim] and
+    // per-doc tag bitmaps [docNum][ceil(tagNum/64)]; tag t is the token Hash64(to_string(t)).
+    // deviceId < 0 keeps the table on the host only (index build, filter compilation, Save).
+    bool Build(int32_t deviceId, const float* vectors, const uint64_t* tagBits, uint64_t docNum, uint32_t dim,
+               uint32_t tagNum, const IndexConfig& cfg, std::string* err);
+    // DataTable::LoadData (data_table.cpp:35-124) over the index directory Save() writes.
+    bool LoadData(int32_t deviceId, const std::string& dataDir, std::string* err);
+    bool Save(const std::string& dataDir, std::string* err) const;
+
+    int32_t GetDeviceId() const { return m_deviceId; }
+    uint64_t GetDocNum() const { return m_docNum; }
+    uint32_t GetDimension() const { return m_dim; }
+    uint32_t GetSegmentNum() const { return m_segmentNum; }
+    uint32_t GetDocNumPerSegment() const { return m_cfg.docNumPerSegment; }
+    uint32_t GetSegmentLength() const { return m_cfg.docNumPerSegment / 16; }
+    uint32_t GetSegmentByteSize() const { return m_cfg.docNumPerSegment / 8; }
+    uint64_t GetTileNum() const { return (m_docNum + 127) / 128; }
+    uint64_t GetBitmapWords() const { return static_cast<uint64_t>(m_segmentNum) * (m_cfg.docNumPerSegment / 64); }
+    const IndexConfig& GetConfig() const { return m_cfg; }
+    float GetMaxNorm() const { return m_maxNorm; }
+    const std::unordered_set<std::string>& GetPostingFields() const { return m_postingFields; }
+
+    const float* DeviceVectors() const { return m_dVectors; }
+    const uint64_t* DevicePostingTable() const { return m_dPostingTable; }
+    const int64_t* DeviceGDocIds() const { return m_dGDocIds; }
+    uint32_t PostingRows() const { return m_rows; }
+
+    // Row of the posting table for a token; the all-zero row when the token is absent
+    // (PostingFieldData::GetData, posting_field_data.cpp:487-495). tokenExist reports which.
+    uint32_t TokenRow(uint64_t token, bool& tokenExist) const;
+    // Host copy of segment s's posting of a token row (for tests / save); null if absent.
+    const uint8_t* HostPosting(uint32_t row, uint32_t seg, uint32_t* len) const;
+    // Layout code of each posting of a row (PostingFieldData::GetPostingTypes).
+    std::vector<uint8_t> PostingTypes(uint32_t row) const;
+
+   private:
+    bool Upload(std::string* err);
+    void Release();
+
+    int32_t m_deviceId = -1;
+    IndexConfig m_cfg;
+    uint64_t m_docNum = 0;
+    uint32_t m_dim = 0;
+    uint32_t m_segmentNum = 0;
+    uint32_t m_rows = 0;  // token rows + 1 (the all-zero row)
+    float m_maxNorm = 0.0f;
+    std::unordered_set<std::string> m_postingFields;
+
+    // host side
+    std::vector<float> m_vectors;            // [docNum][dim]
+    std::vector<int64_t> m_gdocids;          // [docNum]
+    std::vector<uint64_t> m_tokens;          // row -> token hash
+    std::vector<std::string> m_tokenText;    // row -> token literal
+    std::unordered_map<uint64_t, uint32_t> m_tokenRow;
+    std::vector<std::string> m_segPostings;  // per segment: concatenated postings (4-byte padded)
+    std::vector<std::vector<int64_t>> m_rowSegOffset;  // [row][seg] offset into m_segPostings[seg], -1 absent
+    std::vector<std::vector<uint32_t>> m_rowSegLen;
+
+    // device side
+    float* m_dVectors = nullptr;
+    uint8_t* m_dArena = nullptr;
+    uint64_t* m_dPostingTable = nullptr;
+    int64_t* m_dGDocIds = nullptr;
+};
+
+// ---------------------------------------------------------------------------------------------
+struct ScoreWithIndex {
+    float score;
+    uint32_t index;
+    uint64_t id{0};
+    ScoreWithIndex(float s, uint32_t i) : score(s), index(i) {}
+};
+
+struct FullRecallResult {
+    bool isMultiShard = false;
+    std::vector<ScoreWithIndex> scoreWithIndexes;  // multi-shard form (unsorted merge input)
+    std::vector<float> scores;                     // single-shard form, (score desc, doc id asc)
+    std::vector<int64_t> docIds;
+};
+
+// Scoring method of the bulk candidate pass.
+enum class ScoreMethod : int32_t { SIMT_FP32 = 0 };
+
+struct SearcherConfig {
+    uint32_t maxBatch = 256;
+    uint32_t candidateCap = 1u << 18;  // per-query candidate list capacity (>= 4096)
+    uint32_t sampleDocs = 32768;       // minimum doc sample for the candidate threshold
+    uint32_t maxRetries = 4;           // candidate-overflow re-runs before a query fails
+    ScoreMethod method = ScoreMethod::SIMT_FP32;
+};
+
+// Timing of the stages of the last batch (CUDA events, milliseconds).
+struct StageTimes {
+    float filter = 0, sample = 0, candidates = 0, select = 0, total = 0;
+    uint32_t retries = 0;
+    uint32_t launches = 0;
+};
+
+class FullRecallSearcher {
+   public:
+    FullRecallSearcher(int32_t deviceId, std::shared_ptr<DataTable> dataTable, const SearcherConfig& cfg = {});
+    ~FullRecallSearcher();
+    FullRecallSearcher(const FullRecallSearcher&) = delete;
+    FullRecallSearcher& operator=(const FullRecallSearcher&) = delete;
+
+    bool Ok() const { return m_ok; }
+    const std::string& Error() const { return m_err; }
+
+    // FullRecallSearcher::AddQuery (full_recall_searcher.cpp:93-105); queries stay FP32.
+    void AddQuery(QueryNode* queryTree, const std::vector<float>& queryVector, uint32_t topK);
+    void ClearQueries();
+    // FullRecallSearcher::BatchSearch (full_recall_searcher.cpp:107-231): runs every added query,
+    // fills one result per query, clears the added queries.
+    bool BatchSearch(std::vector<std::shared_ptr<FullRecallResult>>& results, const std::string& vectorFieldName,
+                     bool isMultiShard);
+
+    // Device-resident batch: queries [nq][dim] and results live in device memory; the filters were
+    // compiled by PrepareExpr. Synchronises `stream` once (to read the overflow status).
+    int SearchDevice(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks,
+                     float* dOutScores, int64_t* dOutIds, uint32_t* dOutCounts, uint32_t outStride,
+                     cudaStream_t stream);
+
+    // Filter stage alone (FullRecallSearcher::OneFilter, full_recall_searcher.cpp:233-262): the
+    // per-query doc bitmaps [nq][outStrideWords] and pass counts; synchronises `stream` once.
+    int FilterDevice(uint32_t nq, const FilterExpr* const* exprs, uint64_t* dOutBits, uint64_t outStrideWords,
+                     uint32_t* dPassCounts, cudaStream_t stream);
+
+    const StageTimes& LastTimes() const { return m_times; }
+    void SetTiming(bool on) { m_timing = on; }
+    const SearcherConfig& Config() const { return m_cfg; }
+    // Per-query device status bits of the last batch (kStatus* values).
+    const std::vector<int32_t>& LastStatus() const { return m_lastStatus; }
+
+   private:
+    bool Allocate();
+    int StageAndFilter(uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks, uint64_t* dBits,
+                       uint64_t bitsStride, uint32_t* maxKOut, cudaStream_t stream);
+
+    int32_t m_deviceId;
+    std::shared_ptr<DataTable> m_table;
+    SearcherConfig m_cfg;
+    bool m_ok = false;
+    std::string m_err;
+    int m_numSms = 148;
+
+    std::vector<QueryNode*> m_queries;
+    std::vector<float> m_queryVectors;
+    std::vector<uint32_t> m_topKs;
+
+    // device workspace (allocated once)
+    uint64_t* m_dBits = nullptr;
+    float* m_dCandScore = nullptr;
+    uint32_t* m_dCandLoc = nullptr;
+    unsigned long long* m_dWork = nullptr;
+    float* m_dSampScore = nullptr;
+    uint32_t* m_dSampLoc = nullptr;
+    uint32_t m_sampCap = 0;
+    uint8_t* m_dStage = nullptr;  // packed per-batch inputs (programs, topk, eps) + counters
+    size_t m_stageBytes = 0;
+    uint8_t* m_hStage = nullptr;  // pinned host copy
+    float* m_dQueries = nullptr;  // for BatchSearch
+    float* m_dOutScore = nullptr;
+    int64_t* m_dOutId = nullptr;
+    uint32_t* m_dOutCount = nullptr;
+    float* m_hOutScore = nullptr;
+    int64_t* m_hOutId = nullptr;
+    uint32_t* m_hOutCount = nullptr;
+    cudaEvent_t m_ev[6] = {};
+    bool m_timing = false;
+    StageTimes m_times;
+    std::vector<int32_t> m_lastStatus;
+};
+
+}  // namespace hss

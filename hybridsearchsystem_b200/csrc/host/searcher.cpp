@@ -1,0 +1,494 @@
+// searcher.cpp -- FullRecallSearcher: one batch of filtered full-recall queries on the GPU.
+//
+// Per batch (replacing FullRecallSearcher::BatchSearch, full_recall_searcher.cpp:107-231, with its
+// per-query filter launches, host count round trips and host sort):
+//   1. filter      all queries' postfix programs over all segments -> per-query doc bitmaps
+//   2. eps         per-query error bounds of the approximate scoring passes
+//   3. sample      approximate scores of an evenly spaced doc sample; K-th best -> threshold
+//   4. candidates  approximate scores of every doc; filter bit && score >= threshold -> candidates
+//   5. select      exact FP32 rescoring of the candidates that can still reach the top K, then the
+//                  deterministic top K (score desc, doc id asc) with global doc ids
+// A query whose candidate list overflowed gets a higher (still safe) threshold from step 5 and is
+// re-run through steps 4-5 alone.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "../hss_device.cuh"
+#include "../hss_kernels.h"
+#include "hss_host.h"
+
+namespace hss {
+
+namespace {
+// Error bound of an FP32 FFMA dot product of length d (any summation order) plus the one of the
+// ground truth's own sequential sum, relative to sum |q_i v_i|: 2 * gamma_d, gamma_d = d u/(1 - d u),
+// u = 2^-24, doubled for slack.
+double SimtRelBound(uint32_t d) {
+    const double u = std::ldexp(1.0, -24);
+    const double g = d * u / (1.0 - d * u);
+    return 4.0 * g;
+}
+
+size_t AlignUp(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Offsets of the packed per-batch staging buffer.
+struct StageLayout {
+    size_t progOff, opndOff, topk, epsMain, epsSamp, negInf, theta, qlist, counters, passCount, candCount, sampCount,
+        status, prog, opnd, total;
+};
+
+StageLayout MakeLayout(uint32_t B) {
+    StageLayout L{};
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        const size_t r = at;
+        at = AlignUp(at + bytes, 256);
+        return r;
+    };
+    L.progOff = take((B + 1) * 4ull);
+    L.opndOff = take((B + 1) * 4ull);
+    L.topk = take(B * 4ull);
+    L.epsMain = take(B * 4ull);
+    L.epsSamp = take(B * 4ull);
+    L.negInf = take(B * 4ull);
+    L.theta = take(B * 4ull);
+    L.qlist = take(B * 4ull);
+    L.counters = at;
+    L.passCount = take(B * 4ull);
+    L.candCount = take(B * 4ull);
+    L.sampCount = take(B * 4ull);
+    L.status = take(B * 4ull);
+    L.prog = take(static_cast<size_t>(B) * kMaxProgram * 4ull);
+    L.opnd = take(static_cast<size_t>(B) * kMaxOperands * 4ull);
+    L.total = at;
+    return L;
+}
+}  // namespace
+
+FullRecallSearcher::FullRecallSearcher(int32_t deviceId, std::shared_ptr<DataTable> dataTable,
+                                       const SearcherConfig& cfg)
+    : m_deviceId(deviceId), m_table(std::move(dataTable)), m_cfg(cfg) {
+    if (!m_table) {
+        m_err = "null DataTable";
+        return;
+    }
+    if (m_cfg.candidateCap < static_cast<uint32_t>(kMaxTopK)) m_cfg.candidateCap = kMaxTopK;
+    if (m_cfg.maxBatch == 0) m_cfg.maxBatch = 1;
+    m_ok = Allocate();
+}
+
+FullRecallSearcher::~FullRecallSearcher() {
+    cudaSetDevice(m_deviceId);
+    void* dptrs[] = {m_dBits, m_dCandScore, m_dCandLoc, m_dWork, m_dSampScore, m_dSampLoc,
+                     m_dStage, m_dQueries, m_dOutScore, m_dOutId, m_dOutCount};
+    for (void* p : dptrs)
+        if (p) cudaFree(p);
+    void* hptrs[] = {m_hStage, m_hOutScore, m_hOutId, m_hOutCount};
+    for (void* p : hptrs)
+        if (p) cudaFreeHost(p);
+    for (auto& e : m_ev)
+        if (e) cudaEventDestroy(e);
+}
+
+bool FullRecallSearcher::Allocate() {
+    auto ck = [&](cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return true;
+        m_err = std::string(what) + ": " + cudaGetErrorString(e);
+        return false;
+    };
+    if (!ck(cudaSetDevice(m_deviceId), "cudaSetDevice")) return false;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m_deviceId) == cudaSuccess && sms > 0)
+        m_numSms = sms;
+    const uint64_t B = m_cfg.maxBatch, C = m_cfg.candidateCap;
+    const uint64_t words = m_table->GetBitmapWords();
+    // Sample buffer: room for the sample a K of up to 1024 asks for (see SearchDevice); a larger K's
+    // sample overflows it, which only weakens its threshold (the stored part is still a subset).
+    const uint64_t forK = (4ull * 1024 * m_table->GetDocNum() + C - 1) / C;
+    m_sampCap = static_cast<uint32_t>(std::min<uint64_t>(
+        std::max<uint64_t>({forK, m_cfg.sampleDocs, static_cast<uint64_t>(kMaxTopK)}), 1u << 19));
+    const uint32_t dim = m_table->GetDimension();
+    const StageLayout L = MakeLayout(static_cast<uint32_t>(B));
+    m_stageBytes = L.total;
+    if (!ck(cudaMalloc(&m_dBits, B * words * 8), "cudaMalloc bitmaps")) return false;
+    if (!ck(cudaMalloc(&m_dCandScore, B * C * 4), "cudaMalloc candidates")) return false;
+    if (!ck(cudaMalloc(&m_dCandLoc, B * C * 4), "cudaMalloc candidates")) return false;
+    if (!ck(cudaMalloc(&m_dWork, B * C * 8), "cudaMalloc select workspace")) return false;
+    if (!ck(cudaMalloc(&m_dSampScore, B * m_sampCap * 4ull), "cudaMalloc sample")) return false;
+    if (!ck(cudaMalloc(&m_dSampLoc, B * m_sampCap * 4ull), "cudaMalloc sample")) return false;
+    if (!ck(cudaMalloc(&m_dStage, m_stageBytes), "cudaMalloc staging")) return false;
+    if (!ck(cudaMallocHost(&m_hStage, m_stageBytes), "cudaMallocHost staging")) return false;
+    std::memset(m_hStage, 0, m_stageBytes);
+    float* negInf = reinterpret_cast<float*>(m_hStage + L.negInf);
+    for (uint64_t i = 0; i < B; ++i) negInf[i] = -INFINITY;
+    if (!ck(cudaMalloc(&m_dQueries, B * dim * 4ull), "cudaMalloc queries")) return false;
+    if (!ck(cudaMalloc(&m_dOutScore, B * kMaxTopK * 4ull), "cudaMalloc results")) return false;
+    if (!ck(cudaMalloc(&m_dOutId, B * kMaxTopK * 8ull), "cudaMalloc results")) return false;
+    if (!ck(cudaMalloc(&m_dOutCount, B * 4ull), "cudaMalloc results")) return false;
+    if (!ck(cudaMallocHost(&m_hOutScore, B * kMaxTopK * 4ull), "cudaMallocHost results")) return false;
+    if (!ck(cudaMallocHost(&m_hOutId, B * kMaxTopK * 8ull), "cudaMallocHost results")) return false;
+    if (!ck(cudaMallocHost(&m_hOutCount, B * 4ull), "cudaMallocHost results")) return false;
+    for (auto& e : m_ev)
+        if (!ck(cudaEventCreate(&e), "cudaEventCreate")) return false;
+    return true;
+}
+
+void FullRecallSearcher::AddQuery(QueryNode* queryTree, const std::vector<float>& queryVector, uint32_t topK) {
+    m_queries.push_back(queryTree);
+    m_queryVectors.insert(m_queryVectors.end(), queryVector.begin(), queryVector.end());
+    m_topKs.push_back(topK);
+}
+
+void FullRecallSearcher::ClearQueries() {
+    m_queries.clear();
+    m_queryVectors.clear();
+    m_topKs.clear();
+}
+
+int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks,
+                                       uint64_t* dBits, uint64_t bitsStride, uint32_t* maxKOut, cudaStream_t stream) {
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    uint8_t* H = m_hStage;
+    uint8_t* D = m_dStage;
+    auto* progOff = reinterpret_cast<uint32_t*>(H + SL.progOff);
+    auto* opndOff = reinterpret_cast<uint32_t*>(H + SL.opndOff);
+    auto* topk = reinterpret_cast<uint32_t*>(H + SL.topk);
+    auto* prog = reinterpret_cast<uint32_t*>(H + SL.prog);
+    auto* opnd = reinterpret_cast<uint32_t*>(H + SL.opnd);
+    uint32_t np = 0, no = 0, maxOpnd = 0, maxK = 0;
+    for (uint32_t q = 0; q < nq; ++q) {
+        progOff[q] = np;
+        opndOff[q] = no;
+        topk[q] = topks ? topks[q] : 0u;
+        maxK = std::max(maxK, topk[q]);
+        const FilterExpr* e = exprs[q];
+        if (e == nullptr || e->emptyTree) continue;  // empty program: match all
+        const uint32_t pl = static_cast<uint32_t>(e->postExpr.size());
+        const uint32_t ol = static_cast<uint32_t>(e->postingRows.size());
+        if (pl > static_cast<uint32_t>(kMaxProgram) || ol > static_cast<uint32_t>(kMaxOperands) || pl == 0) {
+            // Over the kernel's limits: reported in the status and run as match-nothing
+            // ([AND, 1, 0] over the all-zero posting row).
+            m_lastStatus[q] |= kStatusBadProgram;
+            prog[np++] = AND;
+            prog[np++] = 1;
+            prog[np++] = 0;
+            opnd[no++] = m_table->PostingRows() - 1;
+            maxOpnd = std::max(maxOpnd, 1u);
+            continue;
+        }
+        std::memcpy(prog + np, e->postExpr.data(), pl * 4ull);
+        std::memcpy(opnd + no, e->postingRows.data(), ol * 4ull);
+        np += pl;
+        no += ol;
+        maxOpnd = std::max(maxOpnd, ol);
+    }
+    progOff[nq] = np;
+    opndOff[nq] = no;
+    for (uint32_t q = 0; q < nq; ++q)
+        if (topk[q] > static_cast<uint32_t>(kMaxTopK)) m_lastStatus[q] |= kStatusTopKTooLarge;
+    *maxKOut = maxK;
+
+    cudaError_t ce = cudaSuccess;
+    auto ck = [&](cudaError_t e) {
+        if (ce == cudaSuccess && e != cudaSuccess) ce = e;
+    };
+    // one H2D for the small per-batch inputs (offsets, topk, programs, operands)
+    ck(cudaMemcpyAsync(D, H, SL.counters, cudaMemcpyHostToDevice, stream));
+    ck(cudaMemcpyAsync(D + SL.prog, H + SL.prog, np * 4ull, cudaMemcpyHostToDevice, stream));
+    ck(cudaMemcpyAsync(D + SL.opnd, H + SL.opnd, no * 4ull, cudaMemcpyHostToDevice, stream));
+    ck(cudaMemsetAsync(D + SL.counters, 0, SL.prog - SL.counters, stream));
+
+    const DataTable& T = *m_table;
+    FilterLaunch F{};
+    F.prog = reinterpret_cast<const uint32_t*>(D + SL.prog);
+    F.prog_off = reinterpret_cast<const uint32_t*>(D + SL.progOff);
+    F.opnd_row = reinterpret_cast<const uint32_t*>(D + SL.opnd);
+    F.opnd_off = reinterpret_cast<const uint32_t*>(D + SL.opndOff);
+    F.table = T.DevicePostingTable();
+    F.row_stride = T.GetSegmentNum();
+    F.seg_stride = 1;
+    F.out = dBits;
+    F.out_stride = bitsStride;
+    F.pass_count = reinterpret_cast<uint32_t*>(D + SL.passCount);
+    F.status = reinterpret_cast<int32_t*>(D + SL.status);
+    F.nq = nq;
+    F.seg_num = T.GetSegmentNum();
+    F.docs_per_seg = T.GetDocNumPerSegment();
+    F.doc_num = T.GetDocNum();
+    F.max_opnd = maxOpnd;
+    ck(launch_filter_batch(F, stream));
+    return ce == cudaSuccess ? 0 : static_cast<int>(ce);
+}
+
+int FullRecallSearcher::FilterDevice(uint32_t nq, const FilterExpr* const* exprs, uint64_t* dOutBits,
+                                     uint64_t outStrideWords, uint32_t* dPassCounts, cudaStream_t stream) {
+    if (!m_ok) return -1;
+    m_lastStatus.assign(nq, 0);
+    if (nq == 0) return 0;
+    if (nq > m_cfg.maxBatch || outStrideWords < m_table->GetBitmapWords()) {
+        m_err = "batch larger than maxBatch or bitmap row too short";
+        return -1;
+    }
+    if (cudaSetDevice(m_deviceId) != cudaSuccess) return -2;
+    uint32_t maxK = 0;
+    if (StageAndFilter(nq, exprs, nullptr, dOutBits, outStrideWords, &maxK, stream) != 0) return -2;
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    auto* hStatus = reinterpret_cast<int32_t*>(m_hStage + SL.status);
+    cudaError_t e = cudaSuccess;
+    if (dPassCounts)
+        e = cudaMemcpyAsync(dPassCounts, m_dStage + SL.passCount, nq * 4ull, cudaMemcpyDeviceToDevice, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hStatus, m_dStage + SL.status, nq * 4ull, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        m_err = cudaGetErrorString(e);
+        return -2;
+    }
+    int bad = 0;
+    for (uint32_t q = 0; q < nq; ++q) {
+        m_lastStatus[q] |= hStatus[q];
+        bad += m_lastStatus[q] != 0;
+    }
+    return bad;
+}
+
+int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs,
+                                     const uint32_t* topks, float* dOutScores, int64_t* dOutIds,
+                                     uint32_t* dOutCounts, uint32_t outStride, cudaStream_t stream) {
+    if (!m_ok) return -1;
+    m_times = StageTimes{};
+    m_lastStatus.assign(nq, 0);
+    if (nq == 0) return 0;
+    if (nq > m_cfg.maxBatch) {
+        m_err = "batch larger than the searcher's maxBatch";
+        return -1;
+    }
+    for (uint32_t q = 0; q < nq; ++q) {
+        // the result rows hold outStride entries; a K the kernel accepts must fit in them
+        if (std::min(topks[q], static_cast<uint32_t>(kMaxTopK)) > outStride) {
+            m_err = "topK larger than the output row stride";
+            return -1;
+        }
+    }
+    if (cudaSetDevice(m_deviceId) != cudaSuccess) return -2;
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    uint8_t* H = m_hStage;
+    uint8_t* D = m_dStage;
+    cudaError_t ce = cudaSuccess;
+    auto ck = [&](cudaError_t e) {
+        if (ce == cudaSuccess && e != cudaSuccess) ce = e;
+    };
+    auto* dTopk = reinterpret_cast<uint32_t*>(D + SL.topk);
+    auto* dEpsMain = reinterpret_cast<float*>(D + SL.epsMain);
+    auto* dEpsSamp = reinterpret_cast<float*>(D + SL.epsSamp);
+    auto* dNegInf = reinterpret_cast<float*>(D + SL.negInf);
+    auto* dTheta = reinterpret_cast<float*>(D + SL.theta);
+    auto* dQlist = reinterpret_cast<uint32_t*>(D + SL.qlist);
+    auto* dCandCount = reinterpret_cast<uint32_t*>(D + SL.candCount);
+    auto* dSampCount = reinterpret_cast<uint32_t*>(D + SL.sampCount);
+    auto* dStatus = reinterpret_cast<int32_t*>(D + SL.status);
+
+    const DataTable& T = *m_table;
+    const uint64_t words = T.GetBitmapWords();
+    const uint64_t tiles = T.GetTileNum();
+    const uint32_t dim = T.GetDimension();
+    uint32_t launches = 0;
+    if (m_timing) ck(cudaEventRecord(m_ev[0], stream));
+    uint32_t maxK = 0;
+    if (StageAndFilter(nq, exprs, topks, m_dBits, words, &maxK, stream) != 0) ck(cudaErrorUnknown);
+    ++launches;
+
+    const double rel = SimtRelBound(dim);
+    ck(launch_query_eps(dQueries, nq, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
+    ++launches;
+    if (m_timing) ck(cudaEventRecord(m_ev[1], stream));
+
+    // doc sample: evenly spaced tiles, sized so the K-th best sample score sits near rank cap/4
+    const uint64_t want = std::max<uint64_t>(m_cfg.sampleDocs,
+                                             (4ull * std::max<uint32_t>(maxK, 1u) * T.GetDocNum() +
+                                              m_cfg.candidateCap - 1) / m_cfg.candidateCap);
+    const uint64_t sampTiles = std::min<uint64_t>(tiles, std::max<uint64_t>(1, (want + 127) / 128));
+    const uint64_t step = std::max<uint64_t>(1, tiles / sampTiles);
+    const uint32_t sampCapUsed = static_cast<uint32_t>(std::min<uint64_t>(m_sampCap, sampTiles * 128));
+    CandLaunch S{};
+    S.vec = T.DeviceVectors();
+    S.qry = dQueries;
+    S.bits = m_dBits;
+    S.bits_stride = words;
+    S.theta = dNegInf;
+    S.qlist = nullptr;
+    S.nq_list = nq;
+    S.cand_score = m_dSampScore;
+    S.cand_loc = m_dSampLoc;
+    S.cand_count = dSampCount;
+    S.cap = sampCapUsed;
+    S.dim = dim;
+    S.tile_begin = 0;
+    S.tile_step = step;
+    S.tile_count = std::min<uint64_t>(sampTiles, (tiles + step - 1) / step);
+    ck(launch_cand_simt(S, m_numSms, stream));
+    ++launches;
+    SampleThresholdLaunch ST{};
+    ST.score = m_dSampScore;
+    ST.count = dSampCount;
+    ST.cap = sampCapUsed;
+    ST.topk = dTopk;
+    ST.eps_sample = dEpsSamp;
+    ST.eps_main = dEpsMain;
+    ST.theta = dTheta;
+    ST.qlist = nullptr;
+    ST.nq_list = nq;
+    ck(launch_sample_threshold(ST, stream));
+    ++launches;
+    if (m_timing) ck(cudaEventRecord(m_ev[2], stream));
+
+    CandLaunch M = S;
+    M.theta = dTheta;
+    M.cand_score = m_dCandScore;
+    M.cand_loc = m_dCandLoc;
+    M.cand_count = dCandCount;
+    M.cap = m_cfg.candidateCap;
+    M.tile_begin = 0;
+    M.tile_step = 1;
+    M.tile_count = tiles;
+    ck(launch_cand_simt(M, m_numSms, stream));
+    ++launches;
+    if (m_timing) ck(cudaEventRecord(m_ev[3], stream));
+
+    SelectLaunch SE{};
+    SE.vec = T.DeviceVectors();
+    SE.qry = dQueries;
+    SE.dim = dim;
+    SE.cand_score = m_dCandScore;
+    SE.cand_loc = m_dCandLoc;
+    SE.cand_count = dCandCount;
+    SE.cap = m_cfg.candidateCap;
+    SE.work = m_dWork;
+    SE.topk = dTopk;
+    SE.eps_main = dEpsMain;
+    SE.theta = dTheta;
+    SE.gdocid = T.DeviceGDocIds();
+    SE.out_score = dOutScores;
+    SE.out_id = dOutIds;
+    SE.out_count = dOutCounts;
+    SE.out_stride = outStride;
+    SE.status = dStatus;
+    SE.qlist = nullptr;
+    SE.nq_list = nq;
+    ck(launch_select_topk(SE, stream));
+    ++launches;
+    if (m_timing) ck(cudaEventRecord(m_ev[4], stream));
+
+    auto* hStatus = reinterpret_cast<int32_t*>(H + SL.status);
+    auto* hQlist = reinterpret_cast<uint32_t*>(H + SL.qlist);
+    uint32_t retries = 0;
+    for (;;) {
+        ck(cudaMemcpyAsync(hStatus, dStatus, nq * 4ull, cudaMemcpyDeviceToHost, stream));
+        ck(cudaStreamSynchronize(stream));
+        if (ce != cudaSuccess) break;
+        uint32_t nre = 0;
+        for (uint32_t q = 0; q < nq; ++q) {
+            m_lastStatus[q] |= hStatus[q] & ~kStatusOverflow;
+            if (hStatus[q] & kStatusOverflow) hQlist[nre++] = q;
+        }
+        if (nre == 0) break;
+        if (retries >= m_cfg.maxRetries) {
+            for (uint32_t i = 0; i < nre; ++i) m_lastStatus[hQlist[i]] |= kStatusOverflow;
+            break;
+        }
+        ++retries;
+        ck(cudaMemcpyAsync(dQlist, hQlist, nre * 4ull, cudaMemcpyHostToDevice, stream));
+        ck(cudaMemsetAsync(dCandCount, 0, nq * 4ull, stream));
+        ck(cudaMemsetAsync(dStatus, 0, nq * 4ull, stream));
+        M.qlist = dQlist;
+        M.nq_list = nre;
+        ck(launch_cand_simt(M, m_numSms, stream));
+        SE.qlist = dQlist;
+        SE.nq_list = nre;
+        ck(launch_select_topk(SE, stream));
+        launches += 2;
+    }
+    if (m_timing && ce == cudaSuccess) {
+        cudaEventSynchronize(m_ev[4]);
+        cudaEventElapsedTime(&m_times.filter, m_ev[0], m_ev[1]);
+        cudaEventElapsedTime(&m_times.sample, m_ev[1], m_ev[2]);
+        cudaEventElapsedTime(&m_times.candidates, m_ev[2], m_ev[3]);
+        cudaEventElapsedTime(&m_times.select, m_ev[3], m_ev[4]);
+        cudaEventElapsedTime(&m_times.total, m_ev[0], m_ev[4]);
+    }
+    m_times.retries = retries;
+    m_times.launches = launches;
+    if (ce != cudaSuccess) {
+        m_err = cudaGetErrorString(ce);
+        return -2;
+    }
+    int bad = 0;
+    for (uint32_t q = 0; q < nq; ++q) bad += m_lastStatus[q] != 0;
+    return bad;
+}
+
+bool FullRecallSearcher::BatchSearch(std::vector<std::shared_ptr<FullRecallResult>>& results,
+                                     const std::string& vectorFieldName, bool isMultiShard) {
+    const uint32_t nq = static_cast<uint32_t>(m_queries.size());
+    const uint32_t dim = m_table ? m_table->GetDimension() : 0;
+    auto finish = [&](bool ok) {
+        ClearQueries();
+        return ok;
+    };
+    if (!m_ok) return finish(false);
+    if (vectorFieldName != m_table->GetConfig().vectorField) {
+        m_err = "unknown vector field " + vectorFieldName;
+        return finish(false);
+    }
+    if (m_queryVectors.size() != static_cast<size_t>(nq) * dim) {
+        m_err = "query vector dimension mismatch";
+        return finish(false);
+    }
+    results.clear();
+    for (uint32_t b0 = 0; b0 < nq; b0 += m_cfg.maxBatch) {
+        const uint32_t nb = std::min(m_cfg.maxBatch, nq - b0);
+        std::vector<FilterExpr> exprs(nb);
+        std::vector<const FilterExpr*> ptrs(nb);
+        for (uint32_t i = 0; i < nb; ++i) {
+            if (!PrepareExpr(m_queries[b0 + i], *m_table, exprs[i], &m_err)) return finish(false);
+            ptrs[i] = &exprs[i];
+        }
+        cudaStream_t stream = nullptr;
+        if (cudaSetDevice(m_deviceId) != cudaSuccess) return finish(false);
+        if (cudaMemcpyAsync(m_dQueries, m_queryVectors.data() + static_cast<size_t>(b0) * dim, nb * dim * 4ull,
+                            cudaMemcpyHostToDevice, stream) != cudaSuccess)
+            return finish(false);
+        const int rc = SearchDevice(m_dQueries, nb, ptrs.data(), m_topKs.data() + b0, m_dOutScore, m_dOutId,
+                                    m_dOutCount, kMaxTopK, stream);
+        if (rc < 0) return finish(false);
+        cudaMemcpyAsync(m_hOutCount, m_dOutCount, nb * 4ull, cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(m_hOutScore, m_dOutScore, nb * kMaxTopK * 4ull, cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(m_hOutId, m_dOutId, nb * kMaxTopK * 8ull, cudaMemcpyDeviceToHost, stream);
+        if (cudaStreamSynchronize(stream) != cudaSuccess) return finish(false);
+        for (uint32_t i = 0; i < nb; ++i) {
+            auto r = std::make_shared<FullRecallResult>();
+            r->isMultiShard = isMultiShard;
+            const uint32_t c = m_lastStatus[i] ? 0u : m_hOutCount[i];
+            const float* sc = m_hOutScore + static_cast<size_t>(i) * kMaxTopK;
+            const int64_t* id = m_hOutId + static_cast<size_t>(i) * kMaxTopK;
+            for (uint32_t j = 0; j < c; ++j) {
+                if (isMultiShard) {
+                    ScoreWithIndex s(sc[j], static_cast<uint32_t>(id[j] - static_cast<int64_t>(m_table->GetConfig().docOffset)));
+                    s.id = static_cast<uint64_t>(id[j]);
+                    r->scoreWithIndexes.push_back(s);
+                } else {
+                    r->scores.push_back(sc[j]);
+                    r->docIds.push_back(id[j]);
+                }
+            }
+            results.push_back(r);
+        }
+        if (rc > 0) {
+            m_err = "some queries failed (see per-query status)";
+        }
+    }
+    return finish(true);
+}
+
+}  // namespace hss

@@ -1,0 +1,109 @@
+// hss_kernels.h -- launch descriptors and host-side launchers of the CUDA kernels (internal to
+// libhss.so; the public C-ABI is include/hss.h).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hss {
+
+// Batched postfix filter (filter.cu). Operand i of query q at segment s is the posting at device
+// address table[row * row_stride + s * seg_stride], row = opnd_row[opnd_off[q] + i] (or i when
+// opnd_row is null). An address of 0 is an all-zero posting.
+struct FilterLaunch {
+    const uint32_t* prog;      // concatenated postfix programs
+    const uint32_t* prog_off;  // [nq + 1]
+    const uint32_t* opnd_row;  // concatenated operand rows, or null
+    const uint32_t* opnd_off;  // [nq + 1]
+    const uint64_t* table;     // posting address table
+    uint64_t row_stride;
+    uint64_t seg_stride;
+    uint64_t* out;             // [nq][out_stride] bitmap words
+    uint64_t out_stride;
+    uint32_t* pass_count;      // [nq] docs passing, accumulated (zeroed by the caller), or null
+    int32_t* status;           // [nq] error bits, or null
+    uint32_t nq;
+    uint32_t seg_num;
+    uint32_t docs_per_seg;     // multiple of 128
+    uint64_t doc_num;
+    uint32_t max_opnd;         // largest operand count of any query in the batch (<= 64)
+    // Single-query form: when prog_off is null, query 0's program is prog[0..single_prog_len) over
+    // single_nop operands.
+    uint32_t single_prog_len;
+    uint32_t single_nop;
+    // Table entries follow the reference's convention (untagged = dense bitset address, bit 0 =
+    // sparse posting head, 2 = empty) instead of being posting head addresses.
+    int ref_table;
+};
+
+// Bulk candidate pass (score.cu). Processes tiles tile_begin + i * tile_step, i < tile_count, of
+// 128 docs each, for the queries qlist[0..nq_list) (or 0..nq_list-1 when qlist is null).
+struct CandLaunch {
+    const float* vec;          // [tiles * 128][dim] FP32 corpus, rows 16-byte aligned
+    const float* qry;          // [nq][dim]
+    const uint64_t* bits;      // [nq][bits_stride] filter bitmaps
+    uint64_t bits_stride;
+    const float* theta;        // [nq] candidate thresholds
+    const uint32_t* qlist;
+    uint32_t nq_list;
+    float* cand_score;         // [nq][cap]
+    uint32_t* cand_loc;        // [nq][cap]
+    uint32_t* cand_count;      // [nq] (may exceed cap: overflow)
+    uint32_t cap;
+    uint32_t dim;              // multiple of 4
+    uint64_t tile_begin, tile_step, tile_count;
+};
+
+struct SampleThresholdLaunch {
+    const float* score;        // [nq][cap] sample scores
+    const uint32_t* count;     // [nq]
+    uint32_t cap;
+    const uint32_t* topk;      // [nq]
+    const float* eps_sample;   // [nq] error bound of the sample pass
+    const float* eps_main;     // [nq] error bound of the main pass
+    float* theta;              // [nq] out
+    const uint32_t* qlist;
+    uint32_t nq_list;
+};
+
+struct SelectLaunch {
+    const float* vec;
+    const float* qry;
+    uint32_t dim;
+    const float* cand_score;
+    const uint32_t* cand_loc;
+    const uint32_t* cand_count;
+    uint32_t cap;
+    unsigned long long* work;  // [nq][cap]
+    const uint32_t* topk;
+    const float* eps_main;
+    float* theta;              // raised on overflow
+    const int64_t* gdocid;     // location -> global doc id, or null (identity)
+    float* out_score;          // [nq][out_stride]
+    int64_t* out_id;
+    uint32_t* out_count;       // [nq]
+    uint32_t out_stride;
+    int32_t* status;
+    const uint32_t* qlist;
+    uint32_t nq_list;
+};
+
+cudaError_t launch_filter_batch(const FilterLaunch& L, cudaStream_t stream);
+cudaError_t launch_posting_expand(const uint64_t* src, const uint64_t* dst, uint32_t count, uint32_t byte_size,
+                                  uint32_t seg_docs, int32_t* status, cudaStream_t stream);
+cudaError_t launch_exact_score(const float* qry, const float* docs, float* out, uint32_t m, uint32_t n, uint32_t dim,
+                               uint64_t ldc, cudaStream_t stream);
+cudaError_t launch_cand_simt(const CandLaunch& L, int num_sms, cudaStream_t stream);
+cudaError_t launch_sample_threshold(const SampleThresholdLaunch& L, cudaStream_t stream);
+cudaError_t launch_select_topk(const SelectLaunch& L, cudaStream_t stream);
+cudaError_t launch_query_eps(const float* qry, uint32_t nq, uint32_t dim, float max_norm, double c_main,
+                             double c_sample, float* eps_main, float* eps_sample, cudaStream_t stream);
+size_t aggregate_workspace_bytes(uint32_t n);
+cudaError_t launch_aggregate(const uint64_t* bits, const float* scores, const uint32_t* loc_in, uint32_t n,
+                             float* out_scores, uint32_t* out_loc, uint32_t* total, uint32_t* workspace,
+                             cudaStream_t stream);
+cudaError_t launch_topk_op(const float* scores, const uint32_t* locs, const uint32_t* count, uint32_t k,
+                           float* out_scores, uint32_t* out_locs, uint32_t* out_count, cudaStream_t stream);
+
+}  // namespace hss

@@ -1,0 +1,451 @@
+// select.cu -- selection kernels.
+//
+//  * sample_threshold_kernel: per query, the K-th best approximate score of a doc sample, lowered by
+//    the error bounds into a threshold that every true top-K doc is guaranteed to clear.
+//  * select_topk_kernel: per query, from the candidate list: the K-th best approximate score, the
+//    set of candidates that can still reach the top K, their exact FP32 rescoring in the ground
+//    truth's order, and the final deterministic top K (score desc, doc id asc).
+//  * aggregate_* kernels: stable compaction of (score, location) by the filter bitmap -- the
+//    reference's Aggregator operator (kernel_aggregator.h:18-206) without the host count round trip.
+//  * topk_op_kernel: exact top K of a compacted (score, location) list -- the reference's TOPK
+//    operator (kernel_topk.h:27-419), which there is only a pivot pre-select followed by a host sort.
+#include "hss_device.cuh"
+#include "hss_kernels.h"
+
+namespace hss {
+namespace {
+
+constexpr int kST = 1024;             // threads of the selection CTAs
+constexpr int kWarps = kST / 32;
+
+struct SelectSmem {
+    uint32_t hist[kWarps][256];                 // per-warp radix histograms
+    unsigned long long sortbuf[kMaxTopK];       // bitonic sort buffer
+    uint32_t bcast[4];
+    uint32_t counter;
+};
+
+// Merges the per-warp histograms into hist[0] and picks, from the top, the digit holding the k-th
+// largest key. Returns the digit and updates *krem to the rank inside that digit.
+__device__ inline uint32_t pick_digit(SelectSmem& S, uint32_t* krem) {
+    const uint32_t tid = threadIdx.x;
+    if (tid < 256) {
+        uint32_t s = 0;
+        for (int w = 0; w < kWarps; ++w) s += S.hist[w][tid];
+        S.hist[0][tid] = s;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t cum = 0, chosen = 0, kr = *krem;
+        for (int d = 255; d >= 0; --d) {
+            const uint32_t h = S.hist[0][d];
+            if (cum + h >= kr) {
+                chosen = static_cast<uint32_t>(d);
+                kr -= cum;
+                break;
+            }
+            cum += h;
+        }
+        S.bcast[0] = chosen;
+        S.bcast[1] = kr;
+    }
+    __syncthreads();
+    const uint32_t chosen = S.bcast[0];
+    *krem = S.bcast[1];
+    __syncthreads();
+    return chosen;
+}
+
+__device__ inline void clear_hist(SelectSmem& S) {
+    for (uint32_t i = threadIdx.x; i < kWarps * 256; i += blockDim.x) (&S.hist[0][0])[i] = 0;
+    __syncthreads();
+}
+
+// k-th largest (1-based, k <= n) of n u32 keys produced by key(i).
+template <class KeyFn>
+__device__ uint32_t kth_largest_u32(KeyFn key, uint32_t n, uint32_t k, SelectSmem& S) {
+    uint32_t prefix = 0, mask = 0, krem = k;
+    const uint32_t warp = threadIdx.x >> 5;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        clear_hist(S);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t v = key(i);
+            if ((v & mask) == prefix) atomicAdd(&S.hist[warp][(v >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        const uint32_t d = pick_digit(S, &krem);
+        prefix |= d << shift;
+        mask |= 255u << shift;
+    }
+    return prefix;
+}
+
+template <class KeyFn>
+__device__ uint64_t kth_largest_u64(KeyFn key, uint32_t n, uint32_t k, SelectSmem& S) {
+    uint64_t prefix = 0, mask = 0;
+    uint32_t krem = k;
+    const uint32_t warp = threadIdx.x >> 5;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        clear_hist(S);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint64_t v = key(i);
+            if ((v & mask) == prefix) atomicAdd(&S.hist[warp][(v >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        const uint64_t d = pick_digit(S, &krem);
+        prefix |= d << shift;
+        mask |= 255ull << shift;
+    }
+    return prefix;
+}
+
+// Sorts S.sortbuf[0..m) descending; m is a power of two <= kMaxTopK.
+__device__ void bitonic_desc(SelectSmem& S, uint32_t m) {
+    for (uint32_t k = 2; k <= m; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long a = S.sortbuf[i], b = S.sortbuf[ixj];
+                    const bool desc = (i & k) == 0;
+                    if (desc ? (a < b) : (a > b)) {
+                        S.sortbuf[i] = b;
+                        S.sortbuf[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__device__ inline uint32_t pow2_at_least(uint32_t x) {
+    uint32_t m = 1;
+    while (m < x) m <<= 1;
+    return m;
+}
+
+// Top `kq` (<= kMaxTopK) of n distinct u64 keys key(i), sorted descending into S.sortbuf[0..kq).
+template <class KeyFn>
+__device__ void top_keys(KeyFn key, uint32_t n, uint32_t kq, SelectSmem& S) {
+    if (n <= static_cast<uint32_t>(kMaxTopK)) {
+        const uint32_t m = pow2_at_least(n);
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) S.sortbuf[i] = i < n ? key(i) : 0ull;
+        __syncthreads();
+        bitonic_desc(S, m);
+        return;
+    }
+    const uint64_t kth = kth_largest_u64(key, n, kq, S);
+    if (threadIdx.x == 0) S.counter = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint64_t v = key(i);
+        if (v >= kth) {
+            const uint32_t pos = atomicAdd(&S.counter, 1u);
+            if (pos < static_cast<uint32_t>(kMaxTopK)) S.sortbuf[pos] = v;
+        }
+    }
+    __syncthreads();
+    const uint32_t got = min(S.counter, static_cast<uint32_t>(kMaxTopK));
+    const uint32_t m = pow2_at_least(got);
+    for (uint32_t i = got + threadIdx.x; i < m; i += blockDim.x) S.sortbuf[i] = 0ull;
+    __syncthreads();
+    bitonic_desc(S, m);
+}
+
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kST) sample_threshold_kernel(SampleThresholdLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SelectSmem& S = *reinterpret_cast<SelectSmem*>(smem_raw);
+    const uint32_t qi = L.qlist ? L.qlist[blockIdx.x] : blockIdx.x;
+    const uint32_t k = L.topk[qi];
+    const uint32_t n = min(L.count[qi], L.cap);
+    float theta = -INFINITY;
+    if (k > 0 && n >= k) {
+        const float* sc = L.score + static_cast<uint64_t>(qi) * L.cap;
+        const uint32_t kk = kth_largest_u32([&](uint32_t i) { return float_key(sc[i]); }, n, k, S);
+        // k sample docs score >= t approximately, so the true K-th best exact score is >= t - eps_s;
+        // a true top-K doc therefore scores >= t - eps_s - eps_m under the main pass's arithmetic.
+        theta = __fsub_rd(__fsub_rd(key_float(kk), L.eps_sample[qi]), L.eps_main[qi]);
+    }
+    if (threadIdx.x == 0) L.theta[qi] = theta;
+}
+
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SelectSmem& S = *reinterpret_cast<SelectSmem*>(smem_raw);
+    float* sq = reinterpret_cast<float*>(smem_raw + sizeof(SelectSmem));
+    const uint32_t qi = L.qlist ? L.qlist[blockIdx.x] : blockIdx.x;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t k = L.topk[qi];
+    const uint64_t row = static_cast<uint64_t>(qi) * L.cap;
+    if (k > static_cast<uint32_t>(kMaxTopK)) {
+        if (tid == 0) {
+            L.out_count[qi] = 0;
+            atomicOr(L.status + qi, kStatusTopKTooLarge);
+        }
+        return;
+    }
+    const uint32_t cnt = L.cand_count[qi];
+    const uint32_t n = min(cnt, L.cap);
+    const float* sc = L.cand_score + row;
+    const uint32_t* lc = L.cand_loc + row;
+    const float eps = L.eps_main[qi];
+    if (cnt > L.cap) {
+        // The stored candidates are a subset of the qualifying docs, so their K-th best still bounds
+        // the true K-th best from below: raise the threshold and let the host re-run this query.
+        float theta = L.theta[qi];
+        if (n >= k && k > 0) {
+            const uint32_t kk = kth_largest_u32([&](uint32_t i) { return float_key(sc[i]); }, n, k, S);
+            theta = fmaxf(theta, __fsub_rd(key_float(kk), 2.0f * eps));
+        }
+        if (tid == 0) {
+            L.theta[qi] = theta;
+            L.out_count[qi] = 0;
+            atomicOr(L.status + qi, kStatusOverflow);
+        }
+        return;
+    }
+    if (n == 0 || k == 0) {
+        if (tid == 0) L.out_count[qi] = 0;
+        return;
+    }
+    const uint32_t kq = min(k, n);
+    for (uint32_t i = tid; i < L.dim; i += blockDim.x) sq[i] = L.qry[static_cast<uint64_t>(qi) * L.dim + i];
+    float thr = -INFINITY;
+    if (n > kq) {
+        const uint32_t kk = kth_largest_u32([&](uint32_t i) { return float_key(sc[i]); }, n, kq, S);
+        thr = __fsub_rd(key_float(kk), 2.0f * eps);
+    }
+    if (tid == 0) S.counter = 0;
+    __syncthreads();
+    unsigned long long* ws = L.work + row;
+    for (uint32_t i0 = 0; i0 < n; i0 += blockDim.x) {
+        const uint32_t i = i0 + tid;
+        bool take = false;
+        unsigned long long key = 0;
+        if (i < n && sc[i] >= thr) {
+            const uint32_t loc = lc[i];
+            const float e = exact_dot(sq, L.vec + static_cast<uint64_t>(loc) * L.dim, L.dim);
+            key = result_key(e, loc);
+            take = true;
+        }
+        const uint32_t mask = __ballot_sync(0xffffffffu, take);
+        if (mask) {
+            const uint32_t lane = tid & 31;
+            const uint32_t leader = __ffs(mask) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&S.counter, __popc(mask));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (take) ws[base + __popc(mask & ((1u << lane) - 1u))] = key;
+        }
+    }
+    __syncthreads();
+    const uint32_t nf = S.counter;
+    __syncthreads();
+    top_keys([&](uint32_t i) { return static_cast<uint64_t>(ws[i]); }, nf, kq, S);
+    const uint64_t orow = static_cast<uint64_t>(qi) * L.out_stride;
+    for (uint32_t i = tid; i < kq; i += blockDim.x) {
+        const uint64_t key = S.sortbuf[i];
+        const uint32_t loc = result_key_loc(key);
+        L.out_score[orow + i] = result_key_score(key);
+        L.out_id[orow + i] = L.gdocid ? L.gdocid[loc] : static_cast<int64_t>(loc);
+    }
+    if (tid == 0) L.out_count[qi] = kq;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Aggregator: stable compaction in three launches (count per block, scan, scatter).
+constexpr int kAggT = 1024;  // docs per aggregation block (one per thread)
+
+__global__ void __launch_bounds__(kAggT) aggregate_count_kernel(const uint64_t* __restrict__ bits, uint32_t n,
+                                                                 uint32_t* __restrict__ block_count) {
+    __shared__ uint32_t part[kAggT / 32];
+    const uint32_t doc = blockIdx.x * kAggT + threadIdx.x;
+    const bool hit = doc < n && ((bits[doc >> 6] >> (doc & 63)) & 1ull);
+    const uint32_t c = __popc(__ballot_sync(0xffffffffu, hit));
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint32_t v = part[threadIdx.x];
+        v = warp_sum(v);
+        if (threadIdx.x == 0) block_count[blockIdx.x] = v;
+    }
+}
+
+// Exclusive scan of nb block counts in place (one CTA); writes the total to *total.
+__global__ void __launch_bounds__(1024) aggregate_scan_kernel(uint32_t* __restrict__ block_count, uint32_t nb,
+                                                              uint32_t* __restrict__ total) {
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t b0 = 0; b0 < nb; b0 += blockDim.x) {
+        const uint32_t i = b0 + threadIdx.x;
+        const uint32_t v = i < nb ? block_count[i] : 0;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= static_cast<uint32_t>(o)) x += y;
+        }
+        if (lane == 31) warp_tot[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t t = warp_tot[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= static_cast<uint32_t>(o)) t += y;
+            }
+            warp_tot[lane] = t;  // inclusive over warps
+        }
+        __syncthreads();
+        const uint32_t warp_excl = warp ? warp_tot[warp - 1] : 0;
+        const uint32_t excl = carry + warp_excl + x - v;
+        if (i < nb) block_count[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(kAggT) aggregate_scatter_kernel(const uint64_t* __restrict__ bits,
+                                                                  const float* __restrict__ scores,
+                                                                  const uint32_t* __restrict__ loc_in, uint32_t n,
+                                                                  const uint32_t* __restrict__ block_off,
+                                                                  float* __restrict__ out_scores,
+                                                                  uint32_t* __restrict__ out_loc) {
+    __shared__ uint32_t woff[kAggT / 32];
+    const uint32_t doc = blockIdx.x * kAggT + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool hit = doc < n && ((bits[doc >> 6] >> (doc & 63)) & 1ull);
+    const uint32_t m = __ballot_sync(0xffffffffu, hit);
+    if (lane == 0) woff[warp] = __popc(m);
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t v = woff[lane], x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= static_cast<uint32_t>(o)) x += y;
+        }
+        woff[lane] = x - v;
+    }
+    __syncthreads();
+    if (hit) {
+        const uint32_t pos = block_off[blockIdx.x] + woff[warp] + __popc(m & ((1u << lane) - 1u));
+        out_scores[pos] = scores[doc];
+        out_loc[pos] = loc_in ? loc_in[doc] : doc;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// TOPK operator: exact top K of one compacted list, one CTA.
+__global__ void __launch_bounds__(kST) topk_op_kernel(const float* __restrict__ scores,
+                                                      const uint32_t* __restrict__ locs,
+                                                      const uint32_t* __restrict__ count, uint32_t k,
+                                                      float* __restrict__ out_scores, uint32_t* __restrict__ out_locs,
+                                                      uint32_t* __restrict__ out_count) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SelectSmem& S = *reinterpret_cast<SelectSmem*>(smem_raw);
+    const uint32_t n = *count;
+    const uint32_t kq = min(k, n);
+    if (kq == 0) {
+        if (threadIdx.x == 0) *out_count = 0;
+        return;
+    }
+    top_keys([&](uint32_t i) { return result_key(scores[i], locs[i]); }, n, kq, S);
+    for (uint32_t i = threadIdx.x; i < kq; i += blockDim.x) {
+        const uint64_t key = S.sortbuf[i];
+        out_scores[i] = result_key_score(key);
+        out_locs[i] = result_key_loc(key);
+    }
+    if (threadIdx.x == 0) *out_count = kq;
+}
+
+// Per-query error bounds: eps = c * ||q||_2 * max_doc ||v||_2 (Cauchy-Schwarz on sum |q_i v_i|),
+// computed in double and rounded up to float.
+__global__ void query_eps_kernel(const float* __restrict__ qry, uint32_t nq, uint32_t dim, float max_norm,
+                                 double c_main, double c_sample, float* __restrict__ eps_main,
+                                 float* __restrict__ eps_sample) {
+    const uint32_t q = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31;
+    if (q >= nq) return;
+    double s = 0.0;
+    for (uint32_t d = lane; d < dim; d += 32) {
+        const double x = qry[static_cast<uint64_t>(q) * dim + d];
+        s += x * x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        const double base = sqrt(s) * (1.0 + 1e-12) * static_cast<double>(max_norm);
+        eps_main[q] = __double2float_ru(c_main * base + 1e-30);
+        eps_sample[q] = __double2float_ru(c_sample * base + 1e-30);
+    }
+}
+
+template <class K>
+cudaError_t set_smem(K kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
+}  // namespace
+
+cudaError_t launch_sample_threshold(const SampleThresholdLaunch& L, cudaStream_t stream) {
+    if (L.nq_list == 0) return cudaSuccess;
+    const size_t smem = sizeof(SelectSmem);
+    cudaError_t e = set_smem(sample_threshold_kernel, smem);
+    if (e != cudaSuccess) return e;
+    sample_threshold_kernel<<<L.nq_list, kST, smem, stream>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_select_topk(const SelectLaunch& L, cudaStream_t stream) {
+    if (L.nq_list == 0) return cudaSuccess;
+    const size_t smem = sizeof(SelectSmem) + static_cast<size_t>(L.dim) * sizeof(float);
+    cudaError_t e = set_smem(select_topk_kernel, smem);
+    if (e != cudaSuccess) return e;
+    select_topk_kernel<<<L.nq_list, kST, smem, stream>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_query_eps(const float* qry, uint32_t nq, uint32_t dim, float max_norm, double c_main,
+                             double c_sample, float* eps_main, float* eps_sample, cudaStream_t stream) {
+    if (nq == 0) return cudaSuccess;
+    query_eps_kernel<<<(nq + 7) / 8, 256, 0, stream>>>(qry, nq, dim, max_norm, c_main, c_sample, eps_main, eps_sample);
+    return cudaGetLastError();
+}
+
+size_t aggregate_workspace_bytes(uint32_t n) {
+    const size_t nb = (static_cast<size_t>(n) + kAggT - 1) / kAggT;
+    return (nb > 0 ? nb : 1) * sizeof(uint32_t);
+}
+
+cudaError_t launch_aggregate(const uint64_t* bits, const float* scores, const uint32_t* loc_in, uint32_t n,
+                             float* out_scores, uint32_t* out_loc, uint32_t* total, uint32_t* workspace,
+                             cudaStream_t stream) {
+    const uint32_t nb = (n + kAggT - 1) / kAggT;
+    if (nb == 0) return cudaMemsetAsync(total, 0, sizeof(uint32_t), stream);
+    aggregate_count_kernel<<<nb, kAggT, 0, stream>>>(bits, n, workspace);
+    aggregate_scan_kernel<<<1, 1024, 0, stream>>>(workspace, nb, total);
+    aggregate_scatter_kernel<<<nb, kAggT, 0, stream>>>(bits, scores, loc_in, n, workspace, out_scores, out_loc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_topk_op(const float* scores, const uint32_t* locs, const uint32_t* count, uint32_t k,
+                           float* out_scores, uint32_t* out_locs, uint32_t* out_count, cudaStream_t stream) {
+    if (k > static_cast<uint32_t>(kMaxTopK)) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(SelectSmem);
+    cudaError_t e = set_smem(topk_op_kernel, smem);
+    if (e != cudaSuccess) return e;
+    topk_op_kernel<<<1, kST, smem, stream>>>(scores, locs, count, k, out_scores, out_locs, out_count);
+    return cudaGetLastError();
+}
+
+}  // namespace hss

@@ -1,0 +1,215 @@
+/*
+ * hss.h -- C-ABI of libhss.so, the B200 implementation of the filtered full-recall path.
+ *
+ * Two layers:
+ *   1. Operator entry points: drop-ins for the reference's device operators, which its host code
+ *      launches through the generated aclrtlaunch_* headers (ACLRT_LAUNCH_KERNEL(name)(blockDim, stream,
+ *      args...)). Each takes device pointers plus a cudaStream_t in place of the ACL stream and
+ *      returns a status code instead of having none.
+ *   2. Index and searcher handles: DataTable load / build and the FullRecallSearcher batch call.
+ *
+ * Paths in citations are relative to the reference project root. All sizes are in elements unless
+ * named *Bytes. No function allocates device memory on the calling thread's behalf except the
+ * table/searcher constructors, which allocate their whole arena once.
+ */
+#ifndef HSS_H
+#define HSS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t without pulling in the CUDA headers */
+typedef struct CUstream_st* hss_stream_t;
+
+/* ---- status codes ---- */
+#define HSS_OK 0
+#define HSS_ERR_INVALID (-1) /* bad argument */
+#define HSS_ERR_CUDA (-2)    /* CUDA runtime error (message in hss_last_error) */
+#define HSS_ERR_PARSE (-3)   /* filter expression does not parse */
+#define HSS_ERR_PROGRAM (-4) /* malformed postfix filter program */
+#define HSS_ERR_LIMIT (-5)   /* a size beyond one of the limits below */
+#define HSS_ERR_INDEX (-6)   /* index build / load failure */
+#define HSS_ERR_QUERY (-7)   /* some queries of the batch failed: see hss_searcher_last_status */
+
+/* ---- limits ---- */
+#define HSS_MAX_TOPK 4096       /* largest K per query */
+#define HSS_MAX_OPERANDS 64     /* postings one filter program reads */
+#define HSS_MAX_PROGRAM 512     /* u32 words of one postfix program */
+#define HSS_MAX_STACK 16        /* evaluation stack depth of one program */
+
+/* per-query status bits (hss_searcher_last_status) */
+#define HSS_QSTATUS_BAD_PROGRAM 1
+#define HSS_QSTATUS_BAD_POSTING 2
+#define HSS_QSTATUS_OVERFLOW 4   /* candidate list still over capacity after all re-runs */
+#define HSS_QSTATUS_TOPK_TOO_LARGE 8
+
+/* TextFilterContextData (src/engine/retrieval/device/device_common_external.h:17-25). */
+typedef struct hss_filter_context {
+    uint32_t postingNum;    /* operands (postings) of the program */
+    uint32_t segmentNum;
+    uint32_t segmentLength; /* u16 bitset units per segment = docNumPerSegment / 16; a multiple of 8 */
+    uint32_t tileNum;       /* ignored: one pass per segment tile */
+    uint32_t exprLen;       /* u32 words of postOrderExpr */
+    uint32_t opNum;         /* operators in postOrderExpr */
+    uint32_t flags;         /* HSS_FILTER_HEAD_ADDRESSES, other bits ignored */
+} hss_filter_context;
+
+/* postings[] holds posting head addresses (the 8-byte [layout:4|hits:28][payloadLen] head), any of
+ * the five layouts, 0 = all-zero posting. Without this flag the reference's convention applies
+ * (text_filter.cpp:720-745): an untagged entry is a dense bitset address (head + 8), an entry with
+ * bit 0 set (SPARSE_OPERAND_TAG) is a sparse posting's head, and EMPTY_OPERAND_TAG (2) an all-zero
+ * operand. */
+#define HSS_FILTER_HEAD_ADDRESSES 0x80000000u
+
+/* Replaces kernel_vector_mmad (scorer/kernel_vector_mmad_op.cpp:3-11, launched by
+ * VectorScorerMmad::BatchComputeLaunch, vector_scorer_mmad.cpp:32-168):
+ *   resultMatrix[i * ldResult + j] = sum_d queryMatrix[i][d] * docMatrix[j][d]
+ * for i < m, j < n. FP32 in and out, row-major contiguous docMatrix (not the zN tiling), computed in
+ * the ground truth's order (sequential over d, multiply then add, no FMA), so every entry equals the
+ * CPU oracle's score bit for bit. k % 4 == 0, k <= 4096. */
+int hss_vector_score_launch(const float* queryMatrix, const float* docMatrix, float* resultMatrix, uint32_t m,
+                            uint32_t n, uint32_t k, uint64_t ldResult, hss_stream_t stream);
+
+/* Replaces BitmapTextFilter (filter/kernel_bitmap_text_filter.cpp:52-119, launched by
+ * TextFilter::BitmapTextFilter, text_filter.cpp:1071-1129): evaluates one postfix program
+ * (query_node_imp.cpp form: [AND|OR|NOT, postingNum, stackNum] / [CONJUNCTION, parts, n_1..n_parts])
+ * over postings[segment * postingNum + i] for every segment, writing segmentNum * segmentLength u16
+ * units of result bits (bit i of unit u = doc 16u+i). All five posting layouts are decoded in place,
+ * so the PostingBitListToSet pre-pass is not needed. resultStack is unused (the stack lives on chip)
+ * and may be NULL. status (device int32, may be NULL) gets HSS_QSTATUS_* bits. result must be
+ * 8-byte aligned. */
+int hss_bitmap_text_filter_launch(const uint64_t* postings, const uint32_t* postOrderExpr, void* resultStack,
+                                  hss_filter_context context, uint8_t* result, int32_t* status,
+                                  hss_stream_t stream);
+
+/* Replaces PostingBitListToSet (filter/kernel_bitmap_text_filter.cpp:18-43, bitlist_to_set.h): expands
+ * the posting at postings[i] (head address, any layout) into the dense bitset resultPostings[i] of
+ * byteSizePerSegment bytes, for i < count. The reference's core-split arguments (former/tail) and
+ * ablation switches have no counterpart. byteSizePerSegment % 8 == 0. */
+int hss_posting_bitlist_to_set_launch(const uint64_t* postings, uint32_t byteSizePerSegment,
+                                      const uint64_t* resultPostings, uint32_t count, int32_t* status,
+                                      hss_stream_t stream);
+
+/* Replaces Aggregator (aggregator/kernel_aggregator.cpp:4-13, kernel_aggregator.h:18-206, launched by
+ * ResultAggregator::Aggregator, result_aggregator.cpp:1054-1147): keeps (docScores[i],
+ * docLocationConst[i]) for every i < docNumber whose filter bit is set, in order, and writes the
+ * total to effectiveCount[0] on the device (no per-core count slots, no host round trip).
+ * docLocationConst may be NULL (identity). The outputs must not alias the inputs. `workspace` is
+ * device scratch of hss_aggregator_workspace_size(docNumber) bytes. */
+size_t hss_aggregator_workspace_size(uint32_t docNumber);
+int hss_aggregator_launch(const uint8_t* filterResult, const float* docScores, const uint32_t* docLocationConst,
+                          float* outScores, uint32_t* outLocations, uint32_t* effectiveCount, uint32_t docNumber,
+                          void* workspace, size_t workspaceBytes, hss_stream_t stream);
+
+/* Replaces TOPK (topk/kernel_topk.cpp:4-13, launched by ResultAggregator::TopK,
+ * result_aggregator.cpp:1180-1252) and the host nth_element + sort after it
+ * (AggregatorResultFillExtract, :846-1032): the exact top min(topK, *count) of the compacted list,
+ * ordered by score descending then location ascending. count / outCount are device pointers.
+ * topK <= HSS_MAX_TOPK. */
+int hss_topk_launch(const float* scores, const uint32_t* locations, const uint32_t* count, uint32_t topK,
+                    float* outScores, uint32_t* outLocations, uint32_t* outCount, hss_stream_t stream);
+
+/* ---- index (DataTable, src/engine/index/data_table.h:10-92) ---- */
+typedef struct hss_table hss_table;
+
+typedef struct hss_index_config {
+    uint32_t docNumPerSegment; /* multiple of 128 (the reference needs a multiple of 8) */
+    float densityThreshold;    /* posting is sparse below this density (1/64 in the configs) */
+    int32_t matrixPosting;     /* 1: DENSE_BYTEMAP / SPARSE_IDLIST layouts */
+    int32_t sparsePacked;      /* 1: SPARSE_PACKED instead of SPARSE_BITMAP (NPUR_SPARSE_PACKED) */
+    uint64_t docOffset;        /* global doc id of the first doc */
+} hss_index_config;
+
+/* Offline build (fr_converter + fr_builder) from HYDSET2-shaped host arrays: vectors [docNum][dim]
+ * float32 and tag bitmaps [docNum][ceil(tagNum/64)] uint64; tag t is indexed as the token
+ * Hash64(decimal string of t). The result is resident on deviceId. */
+int hss_table_build(int32_t deviceId, const float* vectors, const uint64_t* tagBits, uint64_t docNum, uint32_t dim,
+                    uint32_t tagNum, const hss_index_config* cfg, hss_table** out);
+/* DataTable::LoadData(deviceId, dir) (data_table.cpp:35-124) over a directory hss_table_save wrote. */
+int hss_table_load(int32_t deviceId, const char* dir, hss_table** out);
+int hss_table_save(const hss_table* table, const char* dir);
+void hss_table_free(hss_table* table);
+int hss_table_info(const hss_table* table, uint64_t* docNum, uint32_t* dim, uint32_t* segmentNum,
+                   uint32_t* docNumPerSegment, uint32_t* postingRows, float* maxNorm);
+/* Host copy of a token's posting in one segment (len 0 and *data NULL when absent). */
+int hss_table_posting(const hss_table* table, uint64_t token, uint32_t segment, const uint8_t** data, uint32_t* len);
+/* Device arrays: vectors [ceil(docNum/128)*128][dim], posting table [postingRows][segmentNum] of
+ * posting head addresses (last row: the all-zero posting), global doc ids [docNum]. */
+int hss_table_device_ptrs(const hss_table* table, const float** vectors, const uint64_t** postingTable,
+                          const int64_t** gdocids);
+
+/* ---- searcher (FullRecallSearcher, full_recall_searcher.h:12-47) ---- */
+typedef struct hss_searcher hss_searcher;
+typedef struct hss_filters hss_filters; /* compiled filter programs of one batch */
+
+typedef struct hss_searcher_config {
+    uint32_t maxBatch;     /* queries per batch (default 256) */
+    uint32_t candidateCap; /* per-query candidate capacity (default 262144, >= HSS_MAX_TOPK) */
+    uint32_t sampleDocs;   /* minimum doc sample for the candidate threshold (default 32768) */
+    uint32_t maxRetries;   /* re-runs of a query whose candidates overflowed (default 4) */
+    int32_t method;        /* scoring method of the candidate pass: 0 = FP32 SIMT */
+} hss_searcher_config;
+
+/* cfg may be NULL for the defaults. The searcher allocates its whole device arena here. */
+int hss_searcher_create(hss_table* table, const hss_searcher_config* cfg, hss_searcher** out);
+void hss_searcher_free(hss_searcher* s);
+
+/* FullRecallSearcher::AddQuery (full_recall_searcher.cpp:93-105): the filter is given as text in the
+ * reference grammar (filter_expr.h: tag ids, AND / OR / NOT, parentheses; empty = match all). */
+int hss_searcher_add_query(hss_searcher* s, const char* filterExpr, const float* vector, uint32_t dim,
+                           uint32_t topK);
+/* FullRecallSearcher::BatchSearch (full_recall_searcher.cpp:107-231) over the added queries, results
+ * copied to host arrays of outStride entries per query: scores (descending) and global doc ids, ties
+ * broken by ascending doc id. Clears the added queries. HSS_ERR_QUERY when some queries failed. */
+int hss_searcher_batch_search(hss_searcher* s, float* outScores, int64_t* outIds, uint32_t* outCounts,
+                              uint32_t outStride);
+
+/* Compile a batch's filter texts once (TextFilter::PrepareExpr, text_filter.cpp:432-467). */
+int hss_filters_compile(hss_searcher* s, const char* const* filterExprs, uint32_t n, hss_filters** out);
+void hss_filters_free(hss_filters* f);
+/* Device-resident batch: dQueries [nq][dim] and the outputs are device arrays; filters[i] is the
+ * filter of query i. Synchronises `stream` once per batch (candidate-overflow check). */
+int hss_searcher_search_device(hss_searcher* s, const float* dQueries, uint32_t nq, const hss_filters* filters,
+                               const uint32_t* topks, float* dOutScores, int64_t* dOutIds, uint32_t* dOutCounts,
+                               uint32_t outStride, hss_stream_t stream);
+
+/* The filter stage alone (FullRecallSearcher::OneFilter, full_recall_searcher.cpp:233-262): row q of
+ * dOutBits (outStrideWords u64 per row, >= segmentNum * docNumPerSegment / 64) gets query q's doc
+ * bitmap (bit b of word w = doc 64w+b, docs past docNum cleared) and dPassCounts[q] (may be NULL) its
+ * popcount. Synchronises `stream` once. */
+int hss_searcher_filter_device(hss_searcher* s, const hss_filters* filters, uint32_t nq, uint64_t* dOutBits,
+                               uint64_t outStrideWords, uint32_t* dPassCounts, hss_stream_t stream);
+
+/* Per-query HSS_QSTATUS_* bits of the last batch. */
+int hss_searcher_last_status(const hss_searcher* s, int32_t* status, uint32_t n);
+/* Stage times of the last batch in ms (filter, sample, candidates, select, total; needs
+ * hss_searcher_set_timing(s, 1)), candidate re-runs and kernel launches. */
+int hss_searcher_set_timing(hss_searcher* s, int32_t on);
+int hss_searcher_last_times(const hss_searcher* s, float* ms5, uint32_t* retries, uint32_t* launches);
+
+/* ---- host-side codec (the index format contract) ---- */
+/* Hash64 (src/engine/core/hash/hash.cpp:10-16). */
+uint64_t hss_hash64(const char* data, uint32_t len);
+/* PostingSerializer::Serialize (src/engine/format/posting_serializer.cpp:81-101) of sorted local ids;
+ * returns the byte length or a negative status. */
+int64_t hss_posting_serialize(const uint32_t* ids, uint32_t n, uint32_t docNum, int32_t isMatrix,
+                              float densityThreshold, int32_t sparsePacked, uint8_t* out, uint64_t cap);
+/* The postfix program and operand rows of one filter text over a table (QueryNode lowering,
+ * query_node_imp.cpp). *emptyTree = 1 for match-all. */
+int hss_filter_compile(const hss_table* table, const char* filterExpr, uint32_t* prog, uint32_t progCap,
+                       uint32_t* progLen, uint32_t* rows, uint32_t rowCap, uint32_t* rowLen, uint32_t* opNum,
+                       int32_t* emptyTree);
+
+/* Last error message of this thread ("" when none). */
+const char* hss_last_error(void);
+/* Number of visible CUDA devices (0 without a GPU). */
+int hss_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
