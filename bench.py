@@ -28,6 +28,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "QPS & p99 at 10M x128 filtered top-100, recall 1.0: chosen form vs plain FP32"
+METHODS = {"simt": 0, "tf32": 1, "bf16": 2, "e4m3": 3}
+FORMS = {"simt": "plain FP32 (SIMT FFMA candidate pass + exact FP32 rescoring)",
+         "tf32": "plain FP32 (TF32 tensor-core candidate pass over the FP32 rows + exact FP32 rescoring)",
+         "bf16": "BF16 copy (tensor-core candidate pass + exact FP32 rescoring)",
+         "e4m3": "FP8 E4M3 copy with per-vector scales (tensor-core candidate pass + exact FP32 rescoring)"}
 
 
 def parse_args():
@@ -42,6 +47,9 @@ def parse_args():
     ap.add_argument("--queries", type=int, default=2048, help="query pool the steps cycle through")
     ap.add_argument("--cpu-queries", type=int, default=0, help="CPU baseline sample size (0: 2 per thread)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cand-cap", type=int, default=1 << 18, help="per-query candidate capacity")
+    ap.add_argument("--method", default="tf32", choices=list(METHODS),
+                    help="candidate pass: simt (FP32 FFMA), tf32 (tensor cores over the FP32 rows), bf16, e4m3")
     return ap.parse_args()
 
 
@@ -195,7 +203,7 @@ def run_ours(args):
     _, vec, bits, queries, exprs = workload(args, dev)
     table = hss.DataTable.build(vec, bits, 256, device=local, doc_num_per_segment=131072)
     B, K = args.batch, args.topk
-    searcher = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=1 << 18)
+    searcher = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[args.method])
     searcher.set_timing(True)
     nb = max(1, len(queries) // B)
     filters = [searcher.compile_filters(exprs[i * B:(i + 1) * B]) for i in range(nb)]
@@ -223,7 +231,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     # device-resident leg
     gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
-    cand_ms, launches = [], 0
+    cand_ms, launches, stage_ms = [], 0, []
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(gpu_id) as clk:
         barrier()
@@ -232,6 +240,7 @@ def run_ours(args):
         for i in range(args.steps):
             t = step(args.warmup + i)
             cand_ms.append(t["candidates_ms"])
+            stage_ms.append([t["filter_ms"], t["sample_ms"], t["candidates_ms"], t["select_ms"], t["total_ms"]])
             launches += t["launches"]
         ev1.record(stream)
         torch.cuda.synchronize()
@@ -277,7 +286,8 @@ def run_ours(args):
     # (docs x 128 x 4 B) + the batch's filter bitmaps (B x docs/8 B)
     info = table.info
     words = info["segment_num"] * info["doc_num_per_segment"] // 64
-    alg_bytes = args.docs * 128 * 4 + B * words * 8
+    elem = {"simt": 4, "tf32": 4, "bf16": 2, "e4m3": 1}[args.method]
+    alg_bytes = args.docs * 128 * elem + B * words * 8 + (args.docs * 4 if args.method == "e4m3" else 0)
     cand_avg = float(np.mean(cand_ms)) if cand_ms else float("nan")
     peaks = {}
     try:
@@ -293,16 +303,19 @@ def run_ours(args):
         with open(tpath) as f:
             traffic = json.load(f).get("bytes_per_launch_full_workload")
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": traffic, "kernel": "cand_simt_kernel", "avg_ms": cand_avg,
+            "traffic": traffic, "kernel": "cand_simt_kernel" if args.method == "simt" else "tc_cand_kernel",
+            "avg_ms": cand_avg,
             "peak_source": "measured" if peaks else "fallback"}
 
     rec = {"metric": METRIC, "value": value, "unit": "QPS", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded cluster mixture, HYDSET2 shapes)",
-           "config": dict(config_of(args, world), form="plain FP32 (SIMT candidate pass + exact FP32 rescoring)"),
+           "config": dict(config_of(args, world), form=FORMS[args.method], method=args.method),
            "e2e": {"value": e2e, "unit": "QPS", "h2d_bytes_per_step": B * 128 * 4,
                    "d2h_bytes_per_step": B * K * (4 + 8) + B * 4},
-           "roofline": roof, "clocks": clocks, "gpu_launches": launches}
+           "roofline": roof, "clocks": clocks, "gpu_launches": launches,
+           "stages_ms": dict(zip(["filter", "sample", "candidates", "select", "total"],
+                                 [round(float(x), 4) for x in np.mean(np.array(stage_ms), axis=0)]))}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, ref_ids, ref_counts = cpu_baseline(vec, bits, queries, exprs, K, args.cpu_queries)

@@ -91,6 +91,8 @@ SIGNATURES = [
      [vp, vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.c_uint32, vp]),
     ("hss_searcher_filter_device", ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, ctypes.c_uint64, vp, vp]),
     ("hss_searcher_last_status", ctypes.c_int, [vp, vp, ctypes.c_uint32]),
+    ("hss_searcher_last_candidates", ctypes.c_int,
+     [vp, ctypes.c_uint32, vp, vp, ctypes.c_uint32, c_u32p, c_f32p, c_f32p]),
     ("hss_searcher_set_timing", ctypes.c_int, [vp, ctypes.c_int32]),
     ("hss_searcher_last_times", ctypes.c_int, [vp, vp, c_u32p, c_u32p]),
     ("hss_hash64", ctypes.c_uint64, [ctypes.c_char_p, ctypes.c_uint32]),

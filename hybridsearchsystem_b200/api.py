@@ -187,6 +187,16 @@ class FullRecallSearcher:
         check(_lib.load().hss_searcher_last_status(self._h, _np_ptr(st), n))
         return st[:n]
 
+    def last_candidates(self, query, cap=1 << 20):
+        """(approximate scores, locations, count, theta, eps) of one query of the last batch."""
+        sc = np.zeros(cap, np.float32)
+        loc = np.zeros(cap, np.uint32)
+        n, th, ep = ctypes.c_uint32(), ctypes.c_float(), ctypes.c_float()
+        check(_lib.load().hss_searcher_last_candidates(self._h, query, _np_ptr(sc), _np_ptr(loc), cap,
+                                                       ctypes.byref(n), ctypes.byref(th), ctypes.byref(ep)))
+        k = min(n.value, cap)
+        return sc[:k], loc[:k], n.value, th.value, ep.value
+
     def set_timing(self, on=True):
         check(_lib.load().hss_searcher_set_timing(self._h, int(on)))
 

@@ -210,7 +210,7 @@ int hss_searcher_create(hss_table* table, const hss_searcher_config* cfg, hss_se
         if (cfg->candidateCap) c.candidateCap = cfg->candidateCap;
         if (cfg->sampleDocs) c.sampleDocs = cfg->sampleDocs;
         c.maxRetries = cfg->maxRetries;
-        if (cfg->method != 0) return SetError(HSS_ERR_INVALID, "unknown scoring method");
+        if (cfg->method < 0 || cfg->method > 3) return SetError(HSS_ERR_INVALID, "unknown scoring method");
         c.method = static_cast<hss::ScoreMethod>(cfg->method);
     }
     auto* s = new hss_searcher;
@@ -310,6 +310,15 @@ int hss_searcher_last_status(const hss_searcher* s, int32_t* status, uint32_t n)
     if (!s || (n && !status)) return SetError(HSS_ERR_INVALID, "null argument");
     const auto& st = s->s->LastStatus();
     for (uint32_t i = 0; i < n; ++i) status[i] = i < st.size() ? st[i] : 0;
+    return HSS_OK;
+}
+
+int hss_searcher_last_candidates(hss_searcher* s, uint32_t query, float* scores, uint32_t* locations, uint32_t cap,
+                                 uint32_t* count, float* theta, float* eps) {
+    if (!s || !count || !theta || !eps || (cap && (!scores || !locations)))
+        return SetError(HSS_ERR_INVALID, "hss_searcher_last_candidates: null argument");
+    const int rc = s->s->LastCandidates(query, scores, locations, cap, count, theta, eps);
+    if (rc < 0) return SetError(rc == -1 ? HSS_ERR_INVALID : HSS_ERR_CUDA, "hss_searcher_last_candidates");
     return HSS_OK;
 }
 

@@ -116,8 +116,11 @@ __device__ inline void resolve_operand(OperandInfo& o, const uint8_t* addr, uint
     if (layout == kSparsePacked) o.k = o.plen / 4;
     if (layout == kSparseIdList) o.k = o.plen / 4;
     if (layout == kSparseBitmap || layout == kSparsePacked) {
-        o.lo = sparse_lower_bound(o, unit_lo);
-        o.hi = sparse_lower_bound(o, unit_hi);
+        // a tile spanning the whole segment needs every entry: no search (each step of it is a
+        // dependent global load)
+        const uint32_t units = (seg_docs + 15) / 16;
+        o.lo = unit_lo == 0 ? 0 : sparse_lower_bound(o, unit_lo);
+        o.hi = unit_hi >= units ? static_cast<int32_t>(o.k) : sparse_lower_bound(o, unit_hi);
     }
 }
 
@@ -128,8 +131,71 @@ __device__ inline uint64_t tail_mask(uint64_t gw, uint64_t doc_num) {
     return valid >= 64 ? ~0ull : ((1ull << valid) - 1);
 }
 
+// Postfix evaluation of one word: the reference's interpretation of the program
+// (kernel_bitmap_text_filter.cpp:52-119). Returns false for a malformed program.
+__device__ inline bool eval_word(const uint32_t* prog, uint32_t plen, const uint64_t* slots, uint32_t slot_stride,
+                                 uint32_t w, uint32_t nop, uint64_t* result) {
+    uint64_t st[kMaxStack];
+    int sp = 0;
+    uint32_t next = 0, pc = 0;
+    while (pc < plen) {
+        const uint32_t op = prog[pc];
+        if (op == kOpAnd || op == kOpOr || op == kOpNot) {
+            if (pc + 2 >= plen) return false;
+            const uint32_t pn = prog[pc + 1], sn = prog[pc + 2];
+            pc += 3;
+            const bool ok = op == kOpNot ? (pn + sn == 1) : (pn + sn > 0);
+            if (!ok || next + pn > nop || sn > static_cast<uint32_t>(sp)) return false;
+            uint64_t acc;
+            if (op == kOpNot) {
+                acc = pn ? ~slots[next * slot_stride + w] : ~st[--sp];
+            } else {
+                acc = op == kOpAnd ? ~0ull : 0ull;
+                for (uint32_t k = 0; k < pn; ++k) {
+                    const uint64_t v = slots[(next + k) * slot_stride + w];
+                    acc = op == kOpAnd ? (acc & v) : (acc | v);
+                }
+                for (uint32_t k = 0; k < sn; ++k) {
+                    const uint64_t v = st[--sp];
+                    acc = op == kOpAnd ? (acc & v) : (acc | v);
+                }
+            }
+            next += pn;
+            if (sp >= kMaxStack) return false;
+            st[sp++] = acc;
+        } else if (op == kOpConjunction) {
+            if (pc + 1 >= plen) return false;
+            const uint32_t parts = prog[pc + 1];
+            if (parts == 0 || pc + 2 + parts > plen) return false;
+            uint64_t acc = ~0ull;
+            for (uint32_t p = 0; p < parts; ++p) {
+                const uint32_t pn = prog[pc + 2 + p];
+                if (pn == 0 || next + pn > nop) return false;
+                uint64_t o = 0;
+                for (uint32_t k = 0; k < pn; ++k) o |= slots[(next + k) * slot_stride + w];
+                acc &= o;
+                next += pn;
+            }
+            pc += 2 + parts;
+            if (sp >= kMaxStack) return false;
+            st[sp++] = acc;
+        } else {
+            return false;
+        }
+    }
+    if (sp != 1 || next != nop) return false;
+    *result = st[0];
+    return true;
+}
+
+// One CTA per (query, segment tile of WPT * 256 words). Operands are decoded into shared-memory
+// slots of the tile (dense: each thread its own words; sparse: zeroed, then scattered), then every
+// word is run through the program. Grid: x = query (fastest, so all queries of a tile share the
+// tile's postings in L2), y = segment tile.
+template <int WPT>
 __global__ void __launch_bounds__(kTile) filter_batch_kernel(FilterLaunch L) {
-    extern __shared__ uint64_t slots[];  // [nop][kTile]
+    constexpr uint32_t TW = kTile * WPT;  // words per CTA
+    extern __shared__ uint64_t slots[];   // [nop][TW]
     __shared__ OperandInfo s_op[kMaxOperands];
     __shared__ uint32_t s_prog[kMaxProgram];
     __shared__ int s_bad;
@@ -137,13 +203,13 @@ __global__ void __launch_bounds__(kTile) filter_batch_kernel(FilterLaunch L) {
     const uint32_t q = blockIdx.x;
     const uint32_t t = threadIdx.x;
     const uint32_t seg_words = L.docs_per_seg / 64;
-    const uint32_t tiles = (seg_words + kTile - 1) / kTile;
+    const uint32_t tiles = (seg_words + TW - 1) / TW;
     const uint32_t seg = blockIdx.y / tiles;
-    const uint32_t w0 = (blockIdx.y % tiles) * kTile;
-    const uint32_t nw = min(static_cast<uint32_t>(kTile), seg_words - w0);
+    const uint32_t w0 = (blockIdx.y % tiles) * TW;
+    const uint32_t nw = min(TW, seg_words - w0);
     const uint64_t seg_doc0 = static_cast<uint64_t>(seg) * L.docs_per_seg;
     const uint32_t seg_docs = static_cast<uint32_t>(min(static_cast<uint64_t>(L.docs_per_seg), L.doc_num - seg_doc0));
-    const uint64_t gw = static_cast<uint64_t>(seg) * seg_words + w0 + t;
+    const uint64_t gw0 = static_cast<uint64_t>(seg) * seg_words + w0;
     uint64_t* out_row = L.out + static_cast<uint64_t>(q) * L.out_stride;
 
     const uint32_t p0 = L.prog_off ? L.prog_off[q] : 0u;
@@ -154,16 +220,24 @@ __global__ void __launch_bounds__(kTile) filter_batch_kernel(FilterLaunch L) {
     const uint32_t plen = p1 - p0;
 
     if (plen == 0) {  // empty program: match all (the reference memsets 0xff, text_filter.cpp:553-559)
-        const uint64_t v = t < nw ? tail_mask(gw, L.doc_num) : 0ull;
-        if (t < nw) out_row[gw] = v;
+        uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k < WPT; ++k) {
+            const uint32_t w = k * kTile + t;
+            if (w < nw) {
+                const uint64_t v = tail_mask(gw0 + w, L.doc_num);
+                out_row[gw0 + w] = v;
+                c += __popcll(v);
+            }
+        }
         if (L.pass_count) {
-            const uint32_t c = warp_sum(__popcll(v));
+            c = warp_sum(c);
             if ((t & 31) == 0 && c) atomicAdd(L.pass_count + q, c);
         }
         return;
     }
     if (nop > L.max_opnd || nop > static_cast<uint32_t>(kMaxOperands) || plen > static_cast<uint32_t>(kMaxProgram)) {
-        if (t < nw) out_row[gw] = 0;
+        for (uint32_t w = t; w < nw; w += kTile) out_row[gw0 + w] = 0;
         if (t == 0 && L.status) atomicOr(L.status + q, kStatusBadProgram);
         return;
     }
@@ -192,21 +266,25 @@ __global__ void __launch_bounds__(kTile) filter_batch_kernel(FilterLaunch L) {
     }
     __syncthreads();
 
-    // Dense operands: each thread its own word. Sparse ones: zero, then scatter below.
+    // Dense operands: each thread its own words (coalesced). Sparse ones: zero, then scatter below.
     for (uint32_t i = 0; i < nop; ++i) {
         const OperandInfo& o = s_op[i];
-        uint64_t v = 0;
-        if (t < nw) {
-            if (o.layout == kDenseBitmap) v = dense_word(o, w0 + t);
-            else if (o.layout == kDenseBytemap) v = bytemap_word(o, w0 + t);
+#pragma unroll
+        for (int k = 0; k < WPT; ++k) {
+            const uint32_t w = k * kTile + t;
+            uint64_t v = 0;
+            if (w < nw) {
+                if (o.layout == kDenseBitmap) v = dense_word(o, w0 + w);
+                else if (o.layout == kDenseBytemap) v = bytemap_word(o, w0 + w);
+            }
+            slots[i * TW + w] = v;
         }
-        slots[i * kTile + t] = v;
     }
     __syncthreads();
     for (uint32_t i = 0; i < nop; ++i) {
         const OperandInfo& o = s_op[i];
         if (o.layout == kSparseBitmap || o.layout == kSparsePacked) {
-            uint16_t* units = reinterpret_cast<uint16_t*>(slots + i * kTile);
+            uint16_t* units = reinterpret_cast<uint16_t*>(slots + i * TW);
             for (int32_t e = o.lo + static_cast<int32_t>(t); e < o.hi; e += kTile) {
                 uint32_t unit, mask;
                 if (o.layout == kSparseBitmap) {
@@ -221,7 +299,7 @@ __global__ void __launch_bounds__(kTile) filter_batch_kernel(FilterLaunch L) {
                 if (rel < nw * 4u) units[rel] = static_cast<uint16_t>(mask);
             }
         } else if (o.layout == kSparseIdList) {
-            uint32_t* bits = reinterpret_cast<uint32_t*>(slots + i * kTile);
+            uint32_t* bits = reinterpret_cast<uint32_t*>(slots + i * TW);
             for (uint32_t e = t; e < o.k; e += kTile) {
                 const uint32_t id = ld32(o.addr + 8 + 4u * e);
                 const uint32_t rel = id - w0 * 64u;
@@ -231,71 +309,25 @@ __global__ void __launch_bounds__(kTile) filter_batch_kernel(FilterLaunch L) {
     }
     __syncthreads();
 
-    bool bad = s_bad != 0;
-    uint64_t result = 0;
-    if (t < nw && !bad) {
-        uint64_t st[kMaxStack];
-        int sp = 0;
-        uint32_t next = 0;
-        uint32_t pc = 0;
-        while (pc < plen && !bad) {
-            const uint32_t op = s_prog[pc];
-            if (op == kOpAnd || op == kOpOr || op == kOpNot) {
-                if (pc + 2 >= plen) { bad = true; break; }
-                const uint32_t pn = s_prog[pc + 1], sn = s_prog[pc + 2];
-                pc += 3;
-                const bool ok = op == kOpNot ? (pn + sn == 1) : (pn + sn > 0);
-                if (!ok || next + pn > nop || sn > static_cast<uint32_t>(sp)) { bad = true; break; }
-                uint64_t acc = op == kOpAnd ? ~0ull : 0ull;
-                if (op == kOpNot) {
-                    acc = pn ? ~slots[next * kTile + t] : ~st[--sp];
-                } else {
-                    for (uint32_t k = 0; k < pn; ++k) {
-                        const uint64_t v = slots[(next + k) * kTile + t];
-                        acc = op == kOpAnd ? (acc & v) : (acc | v);
-                    }
-                    for (uint32_t k = 0; k < sn; ++k) {
-                        const uint64_t v = st[--sp];
-                        acc = op == kOpAnd ? (acc & v) : (acc | v);
-                    }
-                }
-                next += pn;
-                if (sp >= kMaxStack) { bad = true; break; }
-                st[sp++] = acc;
-            } else if (op == kOpConjunction) {
-                if (pc + 1 >= plen) { bad = true; break; }
-                const uint32_t parts = s_prog[pc + 1];
-                if (parts == 0 || pc + 2 + parts > plen) { bad = true; break; }
-                uint64_t acc = ~0ull;
-                for (uint32_t p = 0; p < parts && !bad; ++p) {
-                    const uint32_t pn = s_prog[pc + 2 + p];
-                    if (pn == 0 || next + pn > nop) { bad = true; break; }
-                    uint64_t o = 0;
-                    for (uint32_t k = 0; k < pn; ++k) o |= slots[(next + k) * kTile + t];
-                    acc &= o;
-                    next += pn;
-                }
-                pc += 2 + parts;
-                if (bad || sp >= kMaxStack) { bad = true; break; }
-                st[sp++] = acc;
-            } else {
-                bad = true;
-            }
-        }
-        if (!bad && (sp != 1 || next != nop)) bad = true;
-        if (!bad) result = st[0];
-    }
-    if (t < nw) {
-        result &= tail_mask(gw, L.doc_num);
-        out_row[gw] = result;
+    const bool bad_posting = s_bad != 0;
+    bool bad = bad_posting;
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < WPT; ++k) {
+        const uint32_t w = k * kTile + t;
+        if (w >= nw) continue;
+        uint64_t r = 0;
+        if (!bad && !eval_word(s_prog, plen, slots, TW, w, nop, &r)) bad = true;
+        if (bad) r = 0;
+        r &= tail_mask(gw0 + w, L.doc_num);
+        out_row[gw0 + w] = r;
+        c += __popcll(r);
     }
     if (L.pass_count) {
-        const uint32_t c = warp_sum(t < nw ? __popcll(result) : 0u);
+        c = warp_sum(c);
         if ((t & 31) == 0 && c) atomicAdd(L.pass_count + q, c);
     }
-    if (L.status && t < nw && bad) {
-        atomicOr(L.status + q, s_bad ? kStatusBadPosting : kStatusBadProgram);
-    }
+    if (L.status && bad && t < nw) atomicOr(L.status + q, bad_posting ? kStatusBadPosting : kStatusBadProgram);
 }
 
 // One CTA per posting: expand `src[i]` (any layout) into the dense bitset `dst[i]` of
@@ -351,23 +383,43 @@ __global__ void __launch_bounds__(256) posting_expand_kernel(const uint64_t* src
     }
 }
 
-}  // namespace
 
-cudaError_t launch_filter_batch(const FilterLaunch& L, cudaStream_t stream) {
-    if (L.nq == 0 || L.seg_num == 0) return cudaSuccess;
+template <int WPT>
+cudaError_t launch_filter_wpt(const FilterLaunch& L, cudaStream_t stream) {
+    constexpr uint32_t TW = kTile * WPT;
     const uint32_t seg_words = L.docs_per_seg / 64;
-    const uint32_t tiles = (seg_words + kTile - 1) / kTile;
+    const uint32_t tiles = (seg_words + TW - 1) / TW;
     const uint64_t gy = static_cast<uint64_t>(L.seg_num) * tiles;
-    if (gy > 65535u || L.max_opnd > static_cast<uint32_t>(kMaxOperands)) return cudaErrorInvalidValue;
-    const size_t smem = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * kTile * sizeof(uint64_t);
+    if (gy > 65535u) return cudaErrorInvalidValue;
+    const size_t smem = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * TW * sizeof(uint64_t);
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(filter_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(filter_batch_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(smem));
         if (e != cudaSuccess) return e;
     }
     dim3 grid(L.nq, static_cast<uint32_t>(gy));
-    filter_batch_kernel<<<grid, kTile, smem, stream>>>(L);
+    filter_batch_kernel<WPT><<<grid, kTile, smem, stream>>>(L);
     return cudaGetLastError();
+}
+
+}  // namespace
+
+// The tile is as wide as the segment allows (up to 2048 words = 131072 docs) while the operand slots
+// stay within 96 KB of shared memory.
+cudaError_t launch_filter_batch(const FilterLaunch& L, cudaStream_t stream) {
+    if (L.nq == 0 || L.seg_num == 0) return cudaSuccess;
+    if (L.max_opnd > static_cast<uint32_t>(kMaxOperands)) return cudaErrorInvalidValue;
+    const uint32_t seg_words = L.docs_per_seg / 64;
+    const size_t per_word = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * sizeof(uint64_t);
+    int wpt = 8;
+    while (wpt > 1 && (static_cast<size_t>(wpt) * kTile * per_word > 96 * 1024 || static_cast<uint32_t>(wpt / 2) * kTile >= seg_words))
+        wpt /= 2;
+    switch (wpt) {
+        case 8: return launch_filter_wpt<8>(L, stream);
+        case 4: return launch_filter_wpt<4>(L, stream);
+        case 2: return launch_filter_wpt<2>(L, stream);
+        default: return launch_filter_wpt<1>(L, stream);
+    }
 }
 
 cudaError_t launch_posting_expand(const uint64_t* src, const uint64_t* dst, uint32_t count, uint32_t byte_size,

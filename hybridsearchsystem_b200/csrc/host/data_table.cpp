@@ -19,6 +19,7 @@
 #include <sys/stat.h>
 #include <thread>
 
+#include "../hss_kernels.h"
 #include "hss_host.h"
 
 namespace hss {
@@ -86,9 +87,65 @@ std::string JsonGet(const std::string& s, const std::string& key) {
 
 DataTable::~DataTable() { Release(); }
 
+bool DataTable::EnableFormat(int format, std::string* err) {
+    if (format < 0 || format > 2) return Fail(err, "unknown tensor-core format");
+    if (m_fmtReady[format]) return true;
+    if (m_dVectors == nullptr) return Fail(err, "table has no device residency");
+    if (!CudaOk(cudaSetDevice(m_deviceId), err, "cudaSetDevice")) return false;
+    const uint64_t rows = GetTileNum() * 128;
+    const uint32_t elem = format == kTcBF16 ? 2 : (format == kTcE4M3 ? 1 : 4);
+    if ((static_cast<uint64_t>(m_dim) * elem) % 128 != 0)
+        return Fail(err, "dim * element size must be a multiple of 128 bytes for the tensor-core formats");
+    void* out = nullptr;
+    if (format != kTcTF32 && !CudaOk(cudaMalloc(&out, rows * m_dim * elem), err, "cudaMalloc quantised rows"))
+        return false;
+    float *scale = nullptr, *norm = nullptr, *errn = nullptr;
+    bool ok = CudaOk(cudaMalloc(&norm, rows * sizeof(float)), err, "cudaMalloc norms") &&
+              CudaOk(cudaMalloc(&errn, rows * sizeof(float)), err, "cudaMalloc norms");
+    if (ok && format == kTcE4M3) ok = CudaOk(cudaMalloc(&scale, rows * sizeof(float)), err, "cudaMalloc scales");
+    if (ok)
+        ok = CudaOk(launch_quantize_docs(m_dVectors, rows, m_docNum, m_dim, format, out, scale, norm, errn, nullptr), err,
+                    "quantise");
+    std::vector<float> hn(rows), he(rows);
+    if (ok) ok = CudaOk(cudaMemcpy(hn.data(), norm, rows * 4, cudaMemcpyDeviceToHost), err, "download norms");
+    if (ok) ok = CudaOk(cudaMemcpy(he.data(), errn, rows * 4, cudaMemcpyDeviceToHost), err, "download norms");
+    if (ok && format == kTcE4M3) {
+        ok = CudaOk(cudaMalloc(&m_dTileScale, GetTileNum() * sizeof(float2)), err, "cudaMalloc tile scales") &&
+             CudaOk(launch_tile_scale_minmax(scale, GetTileNum(), m_dTileScale, nullptr), err, "tile scales");
+        m_dDocScale = scale;
+        scale = nullptr;
+    }
+    cudaFree(norm);
+    cudaFree(errn);
+    if (scale) cudaFree(scale);
+    if (!ok || !CudaOk(cudaDeviceSynchronize(), err, "quantise")) {
+        if (out) cudaFree(out);
+        return false;
+    }
+    double nm = 0, em = 0;
+    for (uint64_t i = 0; i < rows; ++i) {
+        nm = std::max(nm, static_cast<double>(hn[i]));
+        em = std::max(em, static_cast<double>(he[i]));
+    }
+    m_dQuant[format] = out;
+    m_fmtNormMax[format] = nm;
+    m_fmtErrMax[format] = em;
+    m_fmtReady[format] = true;
+    return true;
+}
+
 void DataTable::Release() {
+    for (int f = 0; f < 3; ++f) m_fmtReady[f] = false;
     if (m_dVectors == nullptr && m_dArena == nullptr && m_dPostingTable == nullptr && m_dGDocIds == nullptr) return;
     if (m_deviceId >= 0) cudaSetDevice(m_deviceId);
+    for (int f = 1; f < 3; ++f) {
+        if (m_dQuant[f]) cudaFree(m_dQuant[f]);
+        m_dQuant[f] = nullptr;
+    }
+    if (m_dDocScale) cudaFree(m_dDocScale);
+    if (m_dTileScale) cudaFree(m_dTileScale);
+    m_dDocScale = nullptr;
+    m_dTileScale = nullptr;
     if (m_dVectors) cudaFree(m_dVectors);
     if (m_dArena) cudaFree(m_dArena);
     if (m_dPostingTable) cudaFree(m_dPostingTable);

@@ -10,6 +10,7 @@
 // libhss.so instead of the AscendC operators.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -219,6 +220,16 @@ class DataTable {
     // Row of the posting table for a token; the all-zero row when the token is absent
     // (PostingFieldData::GetData, posting_field_data.cpp:487-495). tokenExist reports which.
     uint32_t TokenRow(uint64_t token, bool& tokenExist) const;
+    // Tensor-core scoring formats (TcFormat: 0 TF32 over the FP32 rows, 1 BF16 copy, 2 E4M3 copy with
+    // per-vector scales). Builds the copy on the device and measures max ||v|| and max ||v~ - v||.
+    bool EnableFormat(int format, std::string* err);
+    bool HasFormat(int format) const { return format >= 0 && format < 3 && m_fmtReady[format]; }
+    const void* DeviceRows(int format) const { return format == 0 ? static_cast<const void*>(m_dVectors) : m_dQuant[format]; }
+    const float* DeviceDocScale() const { return m_dDocScale; }
+    const float2* DeviceTileScale() const { return m_dTileScale; }
+    double NormMax(int format) const { return m_fmtNormMax[format]; }
+    double ErrMax(int format) const { return m_fmtErrMax[format]; }
+
     // Host copy of segment s's posting of a token row (for tests / save); null if absent.
     const uint8_t* HostPosting(uint32_t row, uint32_t seg, uint32_t* len) const;
     // Layout code of each posting of a row (PostingFieldData::GetPostingTypes).
@@ -249,6 +260,12 @@ class DataTable {
 
     // device side
     float* m_dVectors = nullptr;
+    void* m_dQuant[3] = {nullptr, nullptr, nullptr};
+    float* m_dDocScale = nullptr;
+    float2* m_dTileScale = nullptr;
+    bool m_fmtReady[3] = {false, false, false};
+    double m_fmtNormMax[3] = {0, 0, 0};
+    double m_fmtErrMax[3] = {0, 0, 0};
     uint8_t* m_dArena = nullptr;
     uint64_t* m_dPostingTable = nullptr;
     int64_t* m_dGDocIds = nullptr;
@@ -269,8 +286,10 @@ struct FullRecallResult {
     std::vector<int64_t> docIds;
 };
 
-// Scoring method of the bulk candidate pass.
-enum class ScoreMethod : int32_t { SIMT_FP32 = 0 };
+// Scoring method of the bulk candidate pass: FP32 FFMA on the SIMT cores, or the tensor cores over
+// the FP32 rows (TF32), a BF16 copy or an FP8 E4M3 copy of the corpus. Every method is followed by
+// the same exact FP32 rescoring, so all return the ground truth's results.
+enum class ScoreMethod : int32_t { SIMT_FP32 = 0, TC_TF32 = 1, TC_BF16 = 2, TC_E4M3 = 3 };
 
 struct SearcherConfig {
     uint32_t maxBatch = 256;
@@ -316,6 +335,11 @@ class FullRecallSearcher {
     int FilterDevice(uint32_t nq, const FilterExpr* const* exprs, uint64_t* dOutBits, uint64_t outStrideWords,
                      uint32_t* dPassCounts, cudaStream_t stream);
 
+    // The last batch's candidate list of query q (approximate scores, locations), its threshold and
+    // error bound; for checking the approximate pass against the exact scores.
+    int LastCandidates(uint32_t q, float* scores, uint32_t* locs, uint32_t cap, uint32_t* count, float* theta,
+                       float* eps);
+
     const StageTimes& LastTimes() const { return m_times; }
     void SetTiming(bool on) { m_timing = on; }
     const SearcherConfig& Config() const { return m_cfg; }
@@ -356,6 +380,14 @@ class FullRecallSearcher {
     float* m_hOutScore = nullptr;
     int64_t* m_hOutId = nullptr;
     uint32_t* m_hOutCount = nullptr;
+    // tensor-core pass
+    int m_tcFormat = -1;  // TcFormat, or -1 for the SIMT pass
+    uint32_t m_tcKblocks = 0, m_tcStages = 0;
+    CUtensorMap m_docMap{};
+    CUtensorMap m_qryMap{};
+    void* m_dStaged = nullptr;  // [256][dim] staged queries in the pass's format
+    float* m_dQScale = nullptr;
+    int32_t* m_dError = nullptr;
     cudaEvent_t m_ev[6] = {};
     bool m_timing = false;
     StageTimes m_times;

@@ -75,13 +75,15 @@ FullRecallSearcher::FullRecallSearcher(int32_t deviceId, std::shared_ptr<DataTab
     }
     if (m_cfg.candidateCap < static_cast<uint32_t>(kMaxTopK)) m_cfg.candidateCap = kMaxTopK;
     if (m_cfg.maxBatch == 0) m_cfg.maxBatch = 1;
+    // the tensor-core pass stages at most 2 x 128 query rows per launch
+    if (m_cfg.method != ScoreMethod::SIMT_FP32 && m_cfg.maxBatch > 256) m_cfg.maxBatch = 256;
     m_ok = Allocate();
 }
 
 FullRecallSearcher::~FullRecallSearcher() {
     cudaSetDevice(m_deviceId);
-    void* dptrs[] = {m_dBits, m_dCandScore, m_dCandLoc, m_dWork, m_dSampScore, m_dSampLoc,
-                     m_dStage, m_dQueries, m_dOutScore, m_dOutId, m_dOutCount};
+    void* dptrs[] = {m_dBits,    m_dCandScore, m_dCandLoc, m_dWork,     m_dSampScore, m_dSampLoc, m_dStage,
+                     m_dQueries, m_dOutScore,  m_dOutId,   m_dOutCount, m_dStaged,    m_dQScale,  m_dError};
     for (void* p : dptrs)
         if (p) cudaFree(p);
     void* hptrs[] = {m_hStage, m_hOutScore, m_hOutId, m_hOutCount};
@@ -131,6 +133,29 @@ bool FullRecallSearcher::Allocate() {
     if (!ck(cudaMallocHost(&m_hOutCount, B * 4ull), "cudaMallocHost results")) return false;
     for (auto& e : m_ev)
         if (!ck(cudaEventCreate(&e), "cudaEventCreate")) return false;
+    if (m_cfg.method != ScoreMethod::SIMT_FP32) {
+        m_tcFormat = static_cast<int>(m_cfg.method) - 1;
+        if (!m_table->EnableFormat(m_tcFormat, &m_err)) return false;
+        const uint32_t elem = m_tcFormat == kTcTF32 ? 4 : (m_tcFormat == kTcBF16 ? 2 : 1);
+        m_tcKblocks = dim * elem / 128;
+        if (!ck(cudaMalloc(&m_dStaged, 256ull * dim * 4), "cudaMalloc staged queries")) return false;
+        if (!ck(cudaMalloc(&m_dQScale, 256 * sizeof(float)), "cudaMalloc query scales")) return false;
+        if (!ck(cudaMalloc(&m_dError, sizeof(int32_t)), "cudaMalloc error word")) return false;
+        if (!ck(cudaMemset(m_dError, 0, sizeof(int32_t)), "cudaMemset error word")) return false;
+        if (!make_tc_map(&m_docMap, m_tcFormat, m_table->DeviceRows(m_tcFormat), m_table->GetTileNum() * 128, dim) ||
+            !make_tc_map(&m_qryMap, m_tcFormat, m_dStaged, 256, dim)) {
+            m_err = "cuTensorMapEncodeTiled failed";
+            return false;
+        }
+        // as many k-block stages as shared memory holds next to the resident queries (2 halves)
+        const size_t budget = 232448;
+        const size_t fixed = tc_smem_bytes(2, m_tcKblocks, 0);
+        m_tcStages = static_cast<uint32_t>(std::min<size_t>(kMaxTcStages, (budget - fixed) / 16384));
+        if (m_tcStages < 2) {
+            m_err = "vector dimension too large for the tensor-core pass";
+            return false;
+        }
+    }
     return true;
 }
 
@@ -299,10 +324,80 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     if (StageAndFilter(nq, exprs, topks, m_dBits, words, &maxK, stream) != 0) ck(cudaErrorUnknown);
     ++launches;
 
-    const double rel = SimtRelBound(dim);
-    ck(launch_query_eps(dQueries, nq, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
+    const bool tc = m_tcFormat >= 0;
+    // Error bounds (and, for the tensor-core pass, the staged queries in its format).
+    auto stage = [&](const uint32_t* dList, uint32_t rows) {
+        if (!tc) {
+            const double rel = SimtRelBound(dim);
+            ck(launch_query_eps(dQueries, nq, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
+            return;
+        }
+        StageQueriesLaunch Q{};
+        Q.qry = dQueries;
+        Q.qlist = dList;
+        Q.nq_rows = rows;
+        Q.rows_alloc = 256;
+        Q.dim = dim;
+        Q.format = m_tcFormat;
+        Q.staged = m_dStaged;
+        Q.q_scale = m_dQScale;
+        Q.eps_main = dEpsMain;
+        Q.eps_sample = dEpsSamp;
+        Q.doc_norm_max = T.NormMax(m_tcFormat);
+        Q.doc_err_max = T.ErrMax(m_tcFormat);
+        Q.acc_rel = dim * std::ldexp(1.0, -22) + std::ldexp(1.0, -21);
+        ck(launch_stage_queries(Q, stream));
+    };
+    stage(nullptr, nq);
     ++launches;
     if (m_timing) ck(cudaEventRecord(m_ev[1], stream));
+
+    // Candidate pass over tiles [begin + i * step, i < count) for `rows` queries (dList or 0..rows-1).
+    auto cand = [&](const float* theta, float* score, uint32_t* loc, uint32_t* count, uint32_t cap,
+                    uint64_t begin, uint64_t step, uint64_t countTiles, const uint32_t* dList, uint32_t rows,
+                    bool simt = false) {
+        if (!tc || simt) {
+            CandLaunch C{};
+            C.vec = T.DeviceVectors();
+            C.qry = dQueries;
+            C.bits = m_dBits;
+            C.bits_stride = words;
+            C.theta = theta;
+            C.qlist = dList;
+            C.nq_list = rows;
+            C.cand_score = score;
+            C.cand_loc = loc;
+            C.cand_count = count;
+            C.cap = cap;
+            C.dim = dim;
+            C.tile_begin = begin;
+            C.tile_step = step;
+            C.tile_count = countTiles;
+            ck(launch_cand_simt(C, m_numSms, stream));
+            return;
+        }
+        TcCandLaunch C{};
+        C.format = m_tcFormat;
+        C.kblocks = m_tcKblocks;
+        C.stages = m_tcStages;
+        C.doc_scale = T.DeviceDocScale();
+        C.tile_scale = T.DeviceTileScale();
+        C.q_scale = m_dQScale;
+        C.bits = m_dBits;
+        C.bits_stride = words;
+        C.theta = theta;
+        C.qlist = dList;
+        C.nq_rows = rows;
+        C.cand_score = score;
+        C.cand_loc = loc;
+        C.cand_count = count;
+        C.cap = cap;
+        C.tile_begin = begin;
+        C.tile_step = step;
+        C.tile_count = countTiles;
+        C.error = m_dError;
+        ck(launch_tc_cand(C, m_docMap, m_qryMap, m_numSms, stream));
+    };
 
     // doc sample: evenly spaced tiles, sized so the K-th best sample score sits near rank cap/4
     const uint64_t want = std::max<uint64_t>(m_cfg.sampleDocs,
@@ -311,23 +406,8 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     const uint64_t sampTiles = std::min<uint64_t>(tiles, std::max<uint64_t>(1, (want + 127) / 128));
     const uint64_t step = std::max<uint64_t>(1, tiles / sampTiles);
     const uint32_t sampCapUsed = static_cast<uint32_t>(std::min<uint64_t>(m_sampCap, sampTiles * 128));
-    CandLaunch S{};
-    S.vec = T.DeviceVectors();
-    S.qry = dQueries;
-    S.bits = m_dBits;
-    S.bits_stride = words;
-    S.theta = dNegInf;
-    S.qlist = nullptr;
-    S.nq_list = nq;
-    S.cand_score = m_dSampScore;
-    S.cand_loc = m_dSampLoc;
-    S.cand_count = dSampCount;
-    S.cap = sampCapUsed;
-    S.dim = dim;
-    S.tile_begin = 0;
-    S.tile_step = step;
-    S.tile_count = std::min<uint64_t>(sampTiles, (tiles + step - 1) / step);
-    ck(launch_cand_simt(S, m_numSms, stream));
+    cand(dNegInf, m_dSampScore, m_dSampLoc, dSampCount, sampCapUsed, 0, step,
+         std::min<uint64_t>(sampTiles, (tiles + step - 1) / step), nullptr, nq);
     ++launches;
     SampleThresholdLaunch ST{};
     ST.score = m_dSampScore;
@@ -343,16 +423,7 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     ++launches;
     if (m_timing) ck(cudaEventRecord(m_ev[2], stream));
 
-    CandLaunch M = S;
-    M.theta = dTheta;
-    M.cand_score = m_dCandScore;
-    M.cand_loc = m_dCandLoc;
-    M.cand_count = dCandCount;
-    M.cap = m_cfg.candidateCap;
-    M.tile_begin = 0;
-    M.tile_step = 1;
-    M.tile_count = tiles;
-    ck(launch_cand_simt(M, m_numSms, stream));
+    cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, m_cfg.candidateCap, 0, 1, tiles, nullptr, nq);
     ++launches;
     if (m_timing) ck(cudaEventRecord(m_ev[3], stream));
 
@@ -401,13 +472,42 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         ck(cudaMemcpyAsync(dQlist, hQlist, nre * 4ull, cudaMemcpyHostToDevice, stream));
         ck(cudaMemsetAsync(dCandCount, 0, nq * 4ull, stream));
         ck(cudaMemsetAsync(dStatus, 0, nq * 4ull, stream));
-        M.qlist = dQlist;
-        M.nq_list = nre;
-        ck(launch_cand_simt(M, m_numSms, stream));
+        // A tensor-core re-run helps when the first threshold was loose. When the docs inside the
+        // 2 eps band around the K-th score alone overflow the list, only a tighter bound helps: from the
+        // second re-run on, the queries go through the FP32 SIMT pass (bound ~2 gamma_d |q||v|). Their
+        // thresholds stay valid (every bound derived so far was at least the SIMT one).
+        const bool simt = tc && retries >= 2;
+        if (simt) {
+            // the plain path for these queries: SIMT bounds, a SIMT doc sample for a fresh threshold
+            const double rel = SimtRelBound(dim);
+            ck(launch_query_eps(dQueries, nq, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
+            ck(cudaMemsetAsync(dSampCount, 0, nq * 4ull, stream));
+            cand(dNegInf, m_dSampScore, m_dSampLoc, dSampCount, sampCapUsed, 0, step,
+                 std::min<uint64_t>(sampTiles, (tiles + step - 1) / step), dQlist, nre, true);
+            SampleThresholdLaunch RT = ST;
+            RT.qlist = dQlist;
+            RT.nq_list = nre;
+            ck(launch_sample_threshold(RT, stream));
+            launches += 3;
+        } else if (tc) {
+            stage(dQlist, nre);  // the staged rows become the re-run queries (their bounds unchanged)
+            ++launches;
+        }
+        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, m_cfg.candidateCap, 0, 1, tiles, dQlist, nre, simt);
         SE.qlist = dQlist;
         SE.nq_list = nre;
         ck(launch_select_topk(SE, stream));
         launches += 2;
+    }
+    if (tc && ce == cudaSuccess) {
+        int32_t herr = 0;
+        ck(cudaMemcpy(&herr, m_dError, sizeof(herr), cudaMemcpyDeviceToHost));
+        if (herr != 0) {
+            m_err = "tensor-core candidate pass timed out waiting on its pipeline (error bits " +
+                    std::to_string(herr) + ")";
+            cudaMemset(m_dError, 0, sizeof(int32_t));
+            return -2;
+        }
     }
     if (m_timing && ce == cudaSuccess) {
         cudaEventSynchronize(m_ev[4]);
@@ -426,6 +526,26 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     int bad = 0;
     for (uint32_t q = 0; q < nq; ++q) bad += m_lastStatus[q] != 0;
     return bad;
+}
+
+int FullRecallSearcher::LastCandidates(uint32_t q, float* scores, uint32_t* locs, uint32_t cap, uint32_t* count,
+                                       float* theta, float* eps) {
+    if (!m_ok || q >= m_cfg.maxBatch) return -1;
+    if (cudaSetDevice(m_deviceId) != cudaSuccess) return -2;
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    uint32_t n = 0;
+    cudaError_t e = cudaMemcpy(&n, m_dStage + SL.candCount + 4ull * q, 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(theta, m_dStage + SL.theta + 4ull * q, 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(eps, m_dStage + SL.epsMain + 4ull * q, 4, cudaMemcpyDeviceToHost);
+    *count = n;
+    const uint32_t k = std::min({n, cap, m_cfg.candidateCap});
+    if (e == cudaSuccess && k)
+        e = cudaMemcpy(scores, m_dCandScore + static_cast<uint64_t>(q) * m_cfg.candidateCap, 4ull * k,
+                       cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && k)
+        e = cudaMemcpy(locs, m_dCandLoc + static_cast<uint64_t>(q) * m_cfg.candidateCap, 4ull * k,
+                       cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? 0 : -2;
 }
 
 bool FullRecallSearcher::BatchSearch(std::vector<std::shared_ptr<FullRecallResult>>& results,

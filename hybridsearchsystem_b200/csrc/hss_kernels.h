@@ -2,9 +2,11 @@
 // libhss.so; the public C-ABI is include/hss.h).
 #pragma once
 
+#include <cuda.h>
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <cstdint>
-#include <cuda_runtime.h>
 
 namespace hss {
 
@@ -88,6 +90,57 @@ struct SelectLaunch {
     const uint32_t* qlist;
     uint32_t nq_list;
 };
+
+// Tensor-core candidate pass (score_tc.cu).
+enum TcFormat : int { kTcTF32 = 0, kTcBF16 = 1, kTcE4M3 = 2 };
+constexpr int kMaxTcStages = 12;
+
+struct TcCandLaunch {
+    int format;                // TcFormat of both the corpus copy and the staged queries
+    uint32_t kblocks;          // dim * element bytes / 128
+    uint32_t stages;           // k-block stages in the TMA ring
+    const float* doc_scale;    // E4M3: per-doc dequantisation scale
+    const float2* tile_scale;  // E4M3: per 128-doc tile (min, max) of doc_scale
+    const float* q_scale;      // E4M3: per staged query row
+    const uint64_t* bits;      // [nq][bits_stride] filter bitmaps
+    uint64_t bits_stride;
+    const float* theta;        // [nq]
+    const uint32_t* qlist;     // staged row r is query qlist[r] (or r)
+    uint32_t nq_rows;          // staged rows in use (<= 256)
+    float* cand_score;
+    uint32_t* cand_loc;
+    uint32_t* cand_count;
+    uint32_t cap;
+    uint64_t tile_begin, tile_step, tile_count;
+    int32_t* error;            // device error bits (bounded waits that expired)
+};
+
+size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages);
+cudaError_t launch_tc_cand(const TcCandLaunch& L, const CUtensorMap& doc_map, const CUtensorMap& qry_map, int sms,
+                           cudaStream_t stream);
+// 2D tensor map over [rows][dim] elements of `format`, 128-byte swizzle, box {128 bytes, 128 rows}.
+bool make_tc_map(CUtensorMap* map, int format, const void* base, uint64_t rows, uint32_t dim);
+
+// Quantised copies of the corpus for the tensor-core formats (quant.cu): bf16 / e4m3 rows with
+// per-doc scale (e4m3), per-doc norm and quantisation-error norm (FP64, rounded up to float).
+cudaError_t launch_quantize_docs(const float* vec, uint64_t rows, uint64_t valid_rows, uint32_t dim, int format,
+                                 void* out, float* scale, float* norm, float* err_norm, cudaStream_t stream);
+cudaError_t launch_tile_scale_minmax(const float* scale, uint64_t tiles, float2* out, cudaStream_t stream);
+// Stage a batch of queries in a tensor-core format (rows past nq zero) and compute the per-query error
+// bounds of the candidate pass (see score_tc.cu / searcher.cpp).
+struct StageQueriesLaunch {
+    const float* qry;      // [nq][dim]
+    const uint32_t* qlist; // staged row r = query qlist[r], or r
+    uint32_t nq_rows, rows_alloc, dim;
+    int format;
+    void* staged;          // [rows_alloc][dim] in `format`
+    float* q_scale;        // E4M3
+    float* eps_main;       // [nq] (indexed by query)
+    float* eps_sample;
+    double doc_norm_max, doc_err_max;  // corpus-wide max ||v|| and max ||quantised v - v||
+    double acc_rel;        // relative accumulation bound of the tensor-core dot products
+};
+cudaError_t launch_stage_queries(const StageQueriesLaunch& L, cudaStream_t stream);
 
 cudaError_t launch_filter_batch(const FilterLaunch& L, cudaStream_t stream);
 cudaError_t launch_posting_expand(const uint64_t* src, const uint64_t* dst, uint32_t count, uint32_t byte_size,

@@ -1,0 +1,436 @@
+// score_tc.cu -- the candidate pass on the 5th-generation tensor cores (tcgen05 + TMA + TMEM).
+//
+// D[query, doc] = Q . D^T for a 128-doc tile and up to 256 staged queries per CTA iteration:
+//   A = staged queries   (M = 128 per half, 1 or 2 halves), resident in shared memory
+//   B = the corpus tile  (N = 128 docs), streamed by TMA through a ring of 16 KB k-block stages
+//   D = FP32 accumulators in TMEM, double buffered (2 x halves x 128 columns)
+// Operands are K-major with the 128-byte swizzle that TMA writes and UMMA reads. Formats: FP32 corpus
+// read as TF32 (kind::tf32), BF16 (kind::f16) and FP8 E4M3 with per-vector scales (kind::f8f6f4).
+//
+// Warp roles (persistent CTA, one per SM): warp 0 issues TMA, warp 1 owns TMEM and issues MMAs
+// (one elected lane), warps 2 .. 2+4*halves-1 drain the accumulators. Each epilogue thread owns one
+// query (its TMEM lane), so the threshold test is a single compare per score; only the few scores at
+// or above the threshold look at the filter bitmap and are appended to the query's candidate list.
+//
+// Every mbarrier wait is bounded (a clock budget); on expiry the CTA records an error, stops issuing
+// and drains, releases TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "hss_device.cuh"
+#include "hss_kernels.h"
+
+namespace hss {
+namespace {
+
+constexpr int kStageBytes = 16384;        // one k-block of a 128-row tile: 128 rows x 128 bytes
+constexpr int kRows = 128;
+constexpr long long kWaitBudget = 4000000000ll;  // clock cycles (~2 s) before a wait gives up
+
+struct TcShared {
+    unsigned long long full[kMaxTcStages];
+    unsigned long long empty[kMaxTcStages];
+    unsigned long long acc_full[2];
+    unsigned long long acc_empty[2];
+    unsigned long long qbar;
+    unsigned long long drain;
+    uint32_t tmem_base;
+    uint32_t n_issued, n_consumed;  // stage loads issued by TMA / waited for by the MMA issuer
+    volatile int abort;
+};
+
+__device__ inline uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ inline void mbar_init(unsigned long long* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ inline void mbar_expect_tx(unsigned long long* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ inline void mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ inline bool mbar_try(unsigned long long* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait that ignores the abort flag (draining copies and MMAs still in flight).
+__device__ inline bool mbar_wait_drain(unsigned long long* bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity))
+        if (clock64() - t0 > kWaitBudget) return false;
+    return true;
+}
+
+// Bounded wait for the phase of `parity`; false (and the CTA marked aborted) when the budget runs out
+// or another role already aborted.
+__device__ inline bool mbar_wait(unsigned long long* bar, uint32_t parity, TcShared& S, int32_t* err, int code) {
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity)) {
+        if (S.abort) return false;
+        if (clock64() - t0 > kWaitBudget) {
+            S.abort = 1;
+            if (err) atomicOr(err, code);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ inline void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major operand with the 128-byte swizzle, 8-row groups 1024 bytes
+// apart (stride byte offset), sm_100 descriptor version 1.
+__device__ inline uint64_t smem_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((addr >> 4) & 0x3fffu);
+    d |= static_cast<uint64_t>(1u) << 16;            // leading byte offset (unused for this layout)
+    d |= static_cast<uint64_t>(1024u >> 4) << 32;    // stride byte offset
+    d |= static_cast<uint64_t>(1u) << 46;            // version
+    d |= static_cast<uint64_t>(2u) << 61;            // SWIZZLE_128B
+    return d;
+}
+
+template <int F>
+struct Fmt;
+template <>
+struct Fmt<kTcTF32> {
+    static constexpr int elem = 4;
+    static constexpr uint32_t ab = 2;  // TF32
+};
+template <>
+struct Fmt<kTcBF16> {
+    static constexpr int elem = 2;
+    static constexpr uint32_t ab = 1;  // BF16
+};
+template <>
+struct Fmt<kTcE4M3> {
+    static constexpr int elem = 1;
+    static constexpr uint32_t ab = 0;  // E4M3
+};
+
+// Instruction descriptor: FP32 accumulate, A/B format, both K-major, N = 128, M = 128.
+template <int F>
+__device__ constexpr uint32_t instr_desc() {
+    return (1u << 4) | (Fmt<F>::ab << 7) | (Fmt<F>::ab << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+template <int F>
+__device__ inline void mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    const uint32_t idesc = instr_desc<F>();
+    if constexpr (F == kTcTF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    } else if constexpr (F == kTcBF16) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    }
+}
+
+__device__ inline void mma_commit(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ inline void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ inline void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+// 32 lanes x 32 consecutive FP32 columns; thread i gets lane (base lane + i).
+__device__ inline void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <int F, int H>
+__global__ void __launch_bounds__(64 + 128 * H, 1) tc_cand_kernel(const __grid_constant__ CUtensorMap doc_map,
+                                                                  const __grid_constant__ CUtensorMap qry_map,
+                                                                  TcCandLaunch L) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte aligned operand region: queries [H][kb][16 KB], then the stage ring
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t kb_n = L.kblocks;
+    unsigned char* qsm = base;
+    unsigned char* ring = base + static_cast<size_t>(H) * kb_n * kStageBytes;
+    TcShared& S = *reinterpret_cast<TcShared*>(ring + static_cast<size_t>(L.stages) * kStageBytes);
+
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t stages = L.stages;
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < stages; ++s) {
+            mbar_init(&S.full[s], 1);
+            mbar_init(&S.empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&S.acc_full[b], 1);
+            mbar_init(&S.acc_empty[b], 128 * H);
+        }
+        mbar_init(&S.qbar, 1);
+        mbar_init(&S.drain, 1);
+        S.abort = 0;
+        S.n_issued = 0;
+        S.n_consumed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
+                     "r"(static_cast<uint32_t>(256 * H)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = S.tmem_base;
+    const uint64_t ntiles = L.tile_count;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // queries once
+            mbar_expect_tx(&S.qbar, static_cast<uint32_t>(H) * kb_n * kStageBytes);
+            for (int h = 0; h < H; ++h)
+                for (uint32_t kb = 0; kb < kb_n; ++kb)
+                    tma_load_2d(qsm + (static_cast<size_t>(h) * kb_n + kb) * kStageBytes, &qry_map,
+                                static_cast<int>(kb * (128 / Fmt<F>::elem)), h * kRows, &S.qbar);
+            uint32_t n = 0;
+            for (uint64_t it = blockIdx.x; it < ntiles && !S.abort; it += gridDim.x) {
+                const int y = static_cast<int>((L.tile_begin + it * L.tile_step) * kRows);
+                for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                    const uint32_t s = n % stages, ph = (n / stages) & 1u;
+                    if (!mbar_wait(&S.empty[s], ph ^ 1u, S, L.error, 1)) break;
+                    mbar_expect_tx(&S.full[s], kStageBytes);
+                    tma_load_2d(ring + static_cast<size_t>(s) * kStageBytes, &doc_map,
+                                static_cast<int>(kb * (128 / Fmt<F>::elem)), y, &S.full[s]);
+                }
+            }
+            S.n_issued = n;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            uint32_t n = 0, iter = 0;
+            if (!mbar_wait(&S.qbar, 0, S, L.error, 2)) iter = 0xffffffffu;  // nothing to issue
+            for (uint64_t it = blockIdx.x; iter != 0xffffffffu && it < ntiles && !S.abort; it += gridDim.x, ++iter) {
+                const uint32_t buf = iter & 1u;
+                if (!mbar_wait(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4)) break;
+                fence_after();
+                bool ok = true;
+                for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                    const uint32_t s = n % stages, ph = (n / stages) & 1u;
+                    if (!mbar_wait(&S.full[s], ph, S, L.error, 8)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint64_t bdesc = smem_desc(smem_u32(ring + static_cast<size_t>(s) * kStageBytes));
+#pragma unroll
+                    for (uint32_t ks = 0; ks < 4; ++ks) {  // 32 bytes of K per instruction
+#pragma unroll
+                        for (int h = 0; h < H; ++h) {
+                            const uint64_t adesc =
+                                smem_desc(smem_u32(qsm + (static_cast<size_t>(h) * kb_n + kb) * kStageBytes));
+                            mma<F>(tmem + (buf * H + h) * 128u, adesc + ks * 2u, bdesc + ks * 2u, (kb | ks) != 0);
+                        }
+                    }
+                    mma_commit(&S.empty[s]);  // frees the stage once these MMAs have read it
+                }
+                if (!ok) break;
+                mma_commit(&S.acc_full[buf]);
+            }
+            S.n_consumed = n;
+            // every MMA this thread issued has completed before TMEM and the stages are released
+            mma_commit(&S.drain);
+            if (!mbar_wait_drain(&S.drain, 0) && L.error) atomicOr(L.error, 32);
+        }
+    } else {
+        // epilogue: warp w drains TMEM lanes [32 * (w % 4), +32) of half (w - 2) / 4
+        const uint32_t ew = warp - 2;
+        const uint32_t half = ew / 4;
+        const uint32_t sub = warp & 3u;
+        const uint32_t row = half * 128u + sub * 32u + lane;
+        const bool valid = row < L.nq_rows;
+        const uint32_t qi = valid ? (L.qlist ? L.qlist[row] : row) : 0u;
+        const float theta = valid ? L.theta[qi] : INFINITY;
+        const float qs = (F == kTcE4M3 && valid) ? L.q_scale[row] : 1.0f;
+        const uint64_t* brow = L.bits + static_cast<uint64_t>(qi) * L.bits_stride;
+        uint32_t iter = 0;
+        for (uint64_t it = blockIdx.x; it < ntiles; it += gridDim.x, ++iter) {
+            const uint32_t buf = iter & 1u;
+            const uint64_t tile = L.tile_begin + it * L.tile_step;
+            // the query's filter bits of the tile's 128 docs, fetched before the accumulator wait so
+            // the load overlaps the tile's MMAs
+            uint64_t fw0 = 0, fw1 = 0;
+            if (valid) {
+                fw0 = brow[tile * 2];
+                fw1 = brow[tile * 2 + 1];
+            }
+            // threshold on the raw accumulator: acc * qs * ds >= theta
+            float t = theta;
+            if (F == kTcE4M3) {
+                const float2 mm = L.tile_scale[tile];  // (min, max) doc scale of the tile
+                const float tq = theta / qs;
+                t = tq > 0.0f ? tq / mm.y : tq / mm.x;
+                t = t == t ? t : -INFINITY;
+                t = __fmul_rd(t, 1.0f - 1e-6f) - 1e-30f;  // stay on the safe side of the rounding
+            }
+            if (!mbar_wait(&S.acc_full[buf], (iter >> 1) & 1u, S, L.error, 16)) break;
+            fence_after();
+            const uint32_t tbase = tmem + ((sub * 32u) << 16) + (buf * H + half) * 128u;
+#pragma unroll 1
+            for (uint32_t c = 0; c < 4; ++c) {
+                const uint32_t m32 = static_cast<uint32_t>((c < 2 ? fw0 : fw1) >> ((c & 1u) * 32u));
+                // docs of this chunk that no query of the warp lets through need no scores at all
+                if (!__any_sync(0xffffffffu, m32 != 0u)) continue;
+                float v[32];
+                tmem_ld32(tbase + c * 32u, v);
+                if (m32 == 0u) continue;
+                bool any = false;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) any |= v[j] >= t;
+                if (!any) continue;
+                uint32_t pass = 0;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) pass |= (v[j] >= t ? 1u : 0u) << j;
+                pass &= m32;
+                const uint64_t doc0 = tile * kRows + c * 32u;
+                if (F == kTcE4M3) {  // the tile threshold is conservative: apply the doc's own scale
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (((pass >> j) & 1u) && !(v[j] * qs * L.doc_scale[doc0 + j] >= theta)) pass &= ~(1u << j);
+                }
+                if (pass == 0u) continue;
+                const uint32_t base = atomicAdd(L.cand_count + qi, static_cast<uint32_t>(__popc(pass)));
+                uint32_t k = 0;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    if (!((pass >> j) & 1u)) continue;
+                    float s = v[j];
+                    if (F == kTcE4M3) s = s * qs * L.doc_scale[doc0 + j];
+                    const uint32_t idx = base + k++;
+                    if (idx < L.cap) {
+                        L.cand_score[static_cast<uint64_t>(qi) * L.cap + idx] = s;
+                        L.cand_loc[static_cast<uint64_t>(qi) * L.cap + idx] = static_cast<uint32_t>(doc0 + j);
+                    }
+                }
+            }
+            fence_before();
+            mbar_arrive(&S.acc_empty[buf]);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && S.n_consumed < S.n_issued) {
+        // aborted: wait (bounded) for the copies still landing in the stage ring
+        for (uint32_t k = S.n_consumed; k < S.n_issued; ++k)
+            if (!mbar_wait_drain(&S.full[k % stages], (k / stages) & 1u)) break;
+    }
+    if (threadIdx.x == 0 && !mbar_try(&S.qbar, 0)) mbar_wait_drain(&S.qbar, 0);
+    __syncthreads();
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(static_cast<uint32_t>(256 * H)));
+    }
+}
+
+template <int F, int H>
+cudaError_t launch_tc_typed(const TcCandLaunch& L, const CUtensorMap& dmap, const CUtensorMap& qmap, int sms,
+                            cudaStream_t stream) {
+    const size_t smem = tc_smem_bytes(H, L.kblocks, L.stages);
+    cudaError_t e = cudaFuncSetAttribute(tc_cand_kernel<F, H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const uint32_t grid = static_cast<uint32_t>(L.tile_count < static_cast<uint64_t>(sms) ? L.tile_count : sms);
+    tc_cand_kernel<F, H><<<grid, 64 + 128 * H, smem, stream>>>(dmap, qmap, L);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages) {
+    return 1024 + static_cast<size_t>(halves) * kblocks * kStageBytes + static_cast<size_t>(stages) * kStageBytes +
+           sizeof(TcShared);
+}
+
+cudaError_t launch_tc_cand(const TcCandLaunch& L, const CUtensorMap& doc_map, const CUtensorMap& qry_map, int sms,
+                           cudaStream_t stream) {
+    if (L.tile_count == 0 || L.nq_rows == 0) return cudaSuccess;
+    if (L.stages < 2 || L.stages > static_cast<uint32_t>(kMaxTcStages) || L.kblocks == 0) return cudaErrorInvalidValue;
+    const int H = L.nq_rows > 128 ? 2 : 1;
+    switch (L.format) {
+        case kTcTF32: return H == 2 ? launch_tc_typed<kTcTF32, 2>(L, doc_map, qry_map, sms, stream)
+                                    : launch_tc_typed<kTcTF32, 1>(L, doc_map, qry_map, sms, stream);
+        case kTcBF16: return H == 2 ? launch_tc_typed<kTcBF16, 2>(L, doc_map, qry_map, sms, stream)
+                                    : launch_tc_typed<kTcBF16, 1>(L, doc_map, qry_map, sms, stream);
+        case kTcE4M3: return H == 2 ? launch_tc_typed<kTcE4M3, 2>(L, doc_map, qry_map, sms, stream)
+                                    : launch_tc_typed<kTcE4M3, 1>(L, doc_map, qry_map, sms, stream);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Tensor maps (cuTensorMapEncodeTiled through the runtime's driver entry point; no libcuda link).
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+}  // namespace
+
+bool make_tc_map(CUtensorMap* map, int format, const void* base, uint64_t rows, uint32_t dim) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const uint32_t elem = format == kTcTF32 ? 4 : (format == kTcBF16 ? 2 : 1);
+    const CUtensorMapDataType dt = format == kTcTF32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : format == kTcBF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                       : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    if ((reinterpret_cast<uintptr_t>(base) & 15u) || (static_cast<uint64_t>(dim) * elem) % 128 != 0) return false;
+    cuuint64_t gdim[2] = {dim, rows};
+    cuuint64_t gstride[1] = {static_cast<cuuint64_t>(dim) * elem};
+    cuuint32_t box[2] = {128u / elem, 128u};
+    cuuint32_t estride[2] = {1, 1};
+    const CUresult r = fn(map, dt, 2, const_cast<void*>(base), gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+}  // namespace hss

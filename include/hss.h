@@ -151,7 +151,9 @@ typedef struct hss_searcher_config {
     uint32_t candidateCap; /* per-query candidate capacity (default 262144, >= HSS_MAX_TOPK) */
     uint32_t sampleDocs;   /* minimum doc sample for the candidate threshold (default 32768) */
     uint32_t maxRetries;   /* re-runs of a query whose candidates overflowed (default 4) */
-    int32_t method;        /* scoring method of the candidate pass: 0 = FP32 SIMT */
+    int32_t method;        /* candidate pass: 0 FP32 SIMT, 1 tensor cores TF32 over the FP32 rows,
+                              2 tensor cores over a BF16 copy, 3 tensor cores over an FP8 E4M3 copy
+                              with per-vector scales (every method returns the exact FP32 results) */
 } hss_searcher_config;
 
 /* cfg may be NULL for the defaults. The searcher allocates its whole device arena here. */
@@ -186,6 +188,11 @@ int hss_searcher_filter_device(hss_searcher* s, const hss_filters* filters, uint
 
 /* Per-query HSS_QSTATUS_* bits of the last batch. */
 int hss_searcher_last_status(const hss_searcher* s, int32_t* status, uint32_t n);
+/* Inspection of the last batch's approximate pass for one query (its batch row): up to `cap` of its
+ * candidates (approximate scores, locations), the candidate count, the threshold theta the pass used
+ * and the query's error bound eps (|approximate - exact FP32 score| <= eps for every doc). */
+int hss_searcher_last_candidates(hss_searcher* s, uint32_t query, float* scores, uint32_t* locations, uint32_t cap,
+                                 uint32_t* count, float* theta, float* eps);
 /* Stage times of the last batch in ms (filter, sample, candidates, select, total; needs
  * hss_searcher_set_timing(s, 1)), candidate re-runs and kernel launches. */
 int hss_searcher_set_timing(hss_searcher* s, int32_t on);

@@ -1,0 +1,102 @@
+"""The tensor-core candidate pass (tcgen05 + TMA + TMEM) in its three formats -- TF32 over the FP32
+rows, a BF16 copy, an FP8 E4M3 copy with per-vector scales -- through the C-ABI.
+
+1. The approximate pass itself: every emitted candidate passes the filter and its approximate score is
+   within the query's proven bound eps of the exact FP32 score, and every filtered doc whose exact
+   score reaches theta + eps was emitted (nothing the top K could need is missing).
+2. End to end: ids bit-exact and in order, scores bit-exact, against the oracle (tolerance 0)."""
+import numpy as np
+import pytest
+
+import hybridsearchsystem_b200 as hss
+import oracle
+from hybridsearchsystem_b200 import data
+
+pytestmark = pytest.mark.gpu
+
+METHODS = {"tf32": 1, "bf16": 2, "e4m3": 3}
+
+
+def _seq_scores(q, v):
+    s = np.zeros(v.shape[0], np.float32)
+    for d in range(v.shape[1]):
+        s = (s + (v[:, d] * q[d]).astype(np.float32)).astype(np.float32)
+    return s
+
+
+def _corpus(n=24000, tags=64, seed=31, p=8192):
+    mix = data.Mixture(128, tags, (1e-3, 0.5), n_clusters=64, seed=seed)
+    vec, bits, _ = mix.corpus(n, seed=seed + 1)
+    return mix, vec, bits
+
+
+@pytest.mark.parametrize("method", list(METHODS))
+@pytest.mark.parametrize("nq", [40, 200])
+def test_approximate_pass_respects_its_bound(torch_cuda, method, nq):
+    mix, vec, bits = _corpus()
+    table = hss.DataTable.build(vec, bits, 64, device=0, doc_num_per_segment=8192)
+    q = mix.queries(nq, seed=32)
+    exprs = data.make_filters(mix, nq, n_tags=(1, 3), seed=33)
+    exprs[0] = ""
+    s = hss.FullRecallSearcher(table, max_batch=256, method=METHODS[method])
+    for a, e in zip(q, exprs):
+        s.add_query(e, a, 50)
+    scores, ids, counts = s.batch_search()
+    want = oracle.topk(q, exprs, 50, vec, bits, threads=8)
+    for i in range(0, nq, max(1, nq // 12)):
+        sc, loc, n, theta, eps = s.last_candidates(i)
+        assert n == len(sc), "candidate list overflowed in a small test"
+        assert eps > 0 and eps < 0.2
+        passing = np.nonzero(np.unpackbits(oracle.filter_bits(exprs[i], bits).view(np.uint8),
+                                           bitorder="little")[:vec.shape[0]])[0]
+        exact = _seq_scores(q[i], vec[passing])
+        ex_of = dict(zip(passing.tolist(), exact.tolist()))
+        for a, l in zip(sc, loc):
+            assert int(l) in ex_of, "a candidate that fails the filter"
+            assert abs(float(a) - ex_of[int(l)]) <= eps, (method, i, float(a), ex_of[int(l)], eps)
+        need = set(passing[exact >= theta + eps].tolist())
+        assert need <= set(loc.tolist()), (method, i, len(need - set(loc.tolist())))
+        c = int(want[2][i])
+        assert (ids[i][:c] == want[1][i][:c]).all()
+        assert (scores[i][:c].view(np.uint32) == want[0][i][:c].view(np.uint32)).all()
+
+
+@pytest.mark.parametrize("method", list(METHODS))
+def test_tensor_core_search_is_exact_mixed_k(torch_cuda, method):
+    mix = data.Mixture(128, 128, (1e-3, 0.6), n_clusters=128, seed=41)
+    vec, bits, _ = mix.corpus(40000, seed=42)
+    table = hss.DataTable.build(vec, bits, 128, device=0, doc_num_per_segment=16384, sparse_packed=True)
+    nq = 96
+    q = mix.queries(nq, seed=43)
+    exprs = data.make_filters(mix, nq, n_tags=(1, 6), seed=44, selectivity_range=(1e-4, 1.0))
+    topks = np.array([1, 10, 100, 1000] * (nq // 4))
+    s = hss.FullRecallSearcher(table, max_batch=nq, method=METHODS[method])
+    for a, e, k in zip(q, exprs, topks):
+        s.add_query(e, a, int(k))
+    scores, ids, counts = s.batch_search()
+    ws, wi, wc = oracle.topk(q, exprs, topks, vec, bits, threads=8)
+    for i in range(nq):
+        c = int(wc[i])
+        assert int(counts[i]) == c
+        assert (ids[i][:c] == wi[i][:c]).all(), (method, i)
+        assert (scores[i][:c].view(np.uint32) == ws[i][:c].view(np.uint32)).all(), (method, i)
+
+
+@pytest.mark.parametrize("method", list(METHODS))
+def test_tensor_core_overflow_reruns_are_exact(torch_cuda, method):
+    mix = data.Mixture(128, 32, (0.3, 0.9), n_clusters=8, seed=51)
+    vec, bits, _ = mix.corpus(50000, seed=52)
+    table = hss.DataTable.build(vec, bits, 32, device=0, doc_num_per_segment=8192)
+    nq = 24
+    q = mix.queries(nq, seed=53)
+    exprs = [""] * 12 + ["1 OR 2"] * 12
+    s = hss.FullRecallSearcher(table, max_batch=nq, candidate_cap=4096, sample_docs=4096, method=METHODS[method])
+    for a, e in zip(q, exprs):
+        s.add_query(e, a, 3000)
+    scores, ids, counts = s.batch_search()
+    ws, wi, wc = oracle.topk(q, exprs, 3000, vec, bits, threads=8)
+    for i in range(nq):
+        c = int(wc[i])
+        assert int(counts[i]) == c
+        assert (ids[i][:c] == wi[i][:c]).all(), (method, i)
+        assert (scores[i][:c].view(np.uint32) == ws[i][:c].view(np.uint32)).all(), (method, i)
