@@ -27,6 +27,7 @@ HSS_ERR_INDEX = -6
 HSS_ERR_QUERY = -7
 
 HSS_MAX_TOPK = 4096
+HSS_AGGREGATOR_NOALLOC_MAX_DOCS = 16777216
 HSS_MAX_OPERANDS = 64
 HSS_MAX_PROGRAM = 512
 HSS_FILTER_HEAD_ADDRESSES = 0x80000000
@@ -70,6 +71,7 @@ SIGNATURES = [
     ("hss_aggregator_workspace_size", ctypes.c_size_t, [ctypes.c_uint32]),
     ("hss_aggregator_launch", ctypes.c_int,
      [vp, vp, vp, vp, vp, vp, ctypes.c_uint32, vp, ctypes.c_size_t, vp]),
+    ("hss_aggregator_launch_noalloc", ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_uint32, vp]),
     ("hss_topk_launch", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32, vp, vp, vp, vp]),
     ("hss_table_build", ctypes.c_int,
      [ctypes.c_int32, vp, vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,

@@ -231,6 +231,14 @@ def aggregator(d_filter, d_scores, d_loc, d_out_scores, d_out_loc, d_count, doc_
                                             d_ws, ws_bytes, stream))
 
 
+def aggregator_noalloc(d_filter, d_scores, d_loc, d_out_scores, d_out_loc, d_count, doc_number, stream=0):
+    """hss_aggregator_launch_noalloc: the aggregator with its scratch compiled into the library (no
+    workspace, no allocation; doc_number <= HSS_AGGREGATOR_NOALLOC_MAX_DOCS; calls on one device must
+    not overlap on the GPU)."""
+    check(_lib.load().hss_aggregator_launch_noalloc(d_filter, d_scores, d_loc, d_out_scores, d_out_loc, d_count,
+                                                    doc_number, stream))
+
+
 def topk(d_scores, d_locs, d_count, k, d_out_scores, d_out_locs, d_out_count, stream=0):
     check(_lib.load().hss_topk_launch(d_scores, d_locs, d_count, k, d_out_scores, d_out_locs, d_out_count, stream))
 

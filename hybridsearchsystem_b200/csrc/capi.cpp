@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -119,6 +120,49 @@ int hss_aggregator_launch(const uint8_t* filterResult, const float* docScores, c
     return FromCuda(hss::launch_aggregate(reinterpret_cast<const uint64_t*>(filterResult), docScores,
                                           docLocationConst, docNumber, outScores, outLocations, effectiveCount,
                                           static_cast<uint32_t*>(workspace), S(stream)));
+}
+
+namespace {
+// Address of the aggregator's module-scope scratch on each device, looked up once per device (with
+// that device current) on the first allocation-free call made there.
+constexpr int kMaxDevices = 64;
+std::mutex g_staticScratchMu;
+uint32_t* g_staticScratch[kMaxDevices] = {};
+
+int StaticAggregateScratch(uint32_t** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return FromCuda(e);
+    if (dev < 0 || dev >= kMaxDevices) return SetError(HSS_ERR_LIMIT, "hss_aggregator_launch_noalloc: device index");
+    std::lock_guard<std::mutex> lock(g_staticScratchMu);
+    if (!g_staticScratch[dev]) {
+        uint32_t* p = nullptr;
+        e = hss::aggregate_static_scratch(&p);
+        if (e != cudaSuccess) return FromCuda(e);
+        if (!p) return SetError(HSS_ERR_CUDA, "hss_aggregator_launch_noalloc: scratch symbol has no address");
+        g_staticScratch[dev] = p;
+    }
+    *out = g_staticScratch[dev];
+    return HSS_OK;
+}
+}  // namespace
+
+int hss_aggregator_launch_noalloc(const uint8_t* filterResult, const float* docScores,
+                                  const uint32_t* docLocationConst, float* outScores, uint32_t* outLocations,
+                                  uint32_t* effectiveCount, uint32_t docNumber, hss_stream_t stream) {
+    if (!filterResult || !docScores || !outScores || !outLocations || !effectiveCount ||
+        (reinterpret_cast<uintptr_t>(filterResult) & 7u))
+        return SetError(HSS_ERR_INVALID, "hss_aggregator_launch_noalloc: bad arguments");
+    if (docNumber > hss::kAggStaticMaxDocs)
+        return SetError(HSS_ERR_LIMIT, "hss_aggregator_launch_noalloc: docNumber " + std::to_string(docNumber) +
+                                           " exceeds HSS_AGGREGATOR_NOALLOC_MAX_DOCS (" +
+                                           std::to_string(hss::kAggStaticMaxDocs) + ")");
+    uint32_t* scratch = nullptr;
+    const int rc = StaticAggregateScratch(&scratch);
+    if (rc != HSS_OK) return rc;
+    return FromCuda(hss::launch_aggregate(reinterpret_cast<const uint64_t*>(filterResult), docScores,
+                                          docLocationConst, docNumber, outScores, outLocations, effectiveCount,
+                                          scratch, S(stream)));
 }
 
 int hss_topk_launch(const float* scores, const uint32_t* locations, const uint32_t* count, uint32_t topK,

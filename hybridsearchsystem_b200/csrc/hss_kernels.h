@@ -153,6 +153,12 @@ cudaError_t launch_select_topk(const SelectLaunch& L, cudaStream_t stream);
 cudaError_t launch_query_eps(const float* qry, uint32_t nq, uint32_t dim, float max_norm, double c_main,
                              double c_sample, float* eps_main, float* eps_sample, cudaStream_t stream);
 size_t aggregate_workspace_bytes(uint32_t n);
+// Allocation-free aggregator scratch: kAggStaticBlocks block counts in a module-scope device array;
+// aggregate_static_scratch returns its address on the current device (the runtime may load the
+// module on the first call on a device).
+constexpr uint32_t kAggStaticBlocks = 16384;
+constexpr uint32_t kAggStaticMaxDocs = kAggStaticBlocks * 1024u;
+cudaError_t aggregate_static_scratch(uint32_t** scratch);
 cudaError_t launch_aggregate(const uint64_t* bits, const float* scores, const uint32_t* loc_in, uint32_t n,
                              float* out_scores, uint32_t* out_loc, uint32_t* total, uint32_t* workspace,
                              cudaStream_t stream);

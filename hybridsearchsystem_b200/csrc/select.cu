@@ -438,6 +438,18 @@ cudaError_t launch_aggregate(const uint64_t* bits, const float* scores, const ui
     return cudaGetLastError();
 }
 
+// Scratch of the allocation-free aggregator: one block count per kAggT docs, kAggStaticBlocks of
+// them (64 KB, docNumber <= 16,777,216). Module-scope, so it exists once per device for the life of
+// the process and every call on that device shares it. The count kernel writes every entry a call
+// reads before the scan reads it, so a call never sees an earlier call's contents and nothing has to
+// be cleared; two calls that overlap on the GPU (different streams, no ordering) do race on it.
+__device__ __align__(256) uint32_t g_aggregate_scratch[kAggStaticBlocks];
+static_assert(kAggStaticMaxDocs == kAggStaticBlocks * static_cast<uint32_t>(kAggT), "one block count per kAggT docs");
+
+cudaError_t aggregate_static_scratch(uint32_t** scratch) {
+    return cudaGetSymbolAddress(reinterpret_cast<void**>(scratch), g_aggregate_scratch);
+}
+
 cudaError_t launch_topk_op(const float* scores, const uint32_t* locs, const uint32_t* count, uint32_t k,
                            float* out_scores, uint32_t* out_locs, uint32_t* out_count, cudaStream_t stream) {
     if (k > static_cast<uint32_t>(kMaxTopK)) return cudaErrorInvalidValue;

@@ -105,6 +105,22 @@ int hss_aggregator_launch(const uint8_t* filterResult, const float* docScores, c
                           float* outScores, uint32_t* outLocations, uint32_t* effectiveCount, uint32_t docNumber,
                           void* workspace, size_t workspaceBytes, hss_stream_t stream);
 
+/* Allocation-free aggregator. NO COUNTERPART IN THE REFERENCE (whose Aggregator always takes
+ * pool-allocated scratch). Same arguments and results as hss_aggregator_launch minus the workspace:
+ * for callers that must not allocate device memory per call or hold a workspace of their own --
+ * a request handler running under a fixed memory budget, or code between setup and a stream
+ * capture that may not call cudaMalloc. Its scratch is a 64 KB array compiled into the library,
+ * one per device, so docNumber <= HSS_AGGREGATOR_NOALLOC_MAX_DOCS (else HSS_ERR_LIMIT, nothing
+ * launched). It calls no allocator. The first call on each device looks the array's address up
+ * (cudaGetSymbolAddress, with that device current), which may load the module: make that first
+ * call before any stream capture. Every call on a device shares the one array: calls that can
+ * overlap on the GPU (different streams without ordering between them) race and must not be made;
+ * calls ordered on one stream are safe, since each call rewrites all the scratch it reads. */
+#define HSS_AGGREGATOR_NOALLOC_MAX_DOCS 16777216u
+int hss_aggregator_launch_noalloc(const uint8_t* filterResult, const float* docScores,
+                                  const uint32_t* docLocationConst, float* outScores, uint32_t* outLocations,
+                                  uint32_t* effectiveCount, uint32_t docNumber, hss_stream_t stream);
+
 /* Replaces TOPK (topk/kernel_topk.cpp:4-13, launched by ResultAggregator::TopK,
  * result_aggregator.cpp:1180-1252) and the host nth_element + sort after it
  * (AggregatorResultFillExtract, :846-1032): the exact top min(topK, *count) of the compacted list,
