@@ -59,7 +59,8 @@ class IndexConfig(ctypes.Structure):
 
 class SearcherConfig(ctypes.Structure):
     _fields_ = [("maxBatch", ctypes.c_uint32), ("candidateCap", ctypes.c_uint32),
-                ("sampleDocs", ctypes.c_uint32), ("maxRetries", ctypes.c_uint32), ("method", ctypes.c_int32)]
+                ("sampleDocs", ctypes.c_uint32), ("maxRetries", ctypes.c_uint32), ("method", ctypes.c_int32),
+                ("decodeInPlace", ctypes.c_int32)]
 
 
 # (name, restype, argtypes) for every symbol include/hss.h declares.

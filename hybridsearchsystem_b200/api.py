@@ -123,11 +123,12 @@ class Filters:
 
 
 class FullRecallSearcher:
-    def __init__(self, table, max_batch=256, candidate_cap=1 << 18, sample_docs=32768, max_retries=4, method=0):
+    def __init__(self, table, max_batch=256, candidate_cap=1 << 18, sample_docs=32768, max_retries=4, method=0,
+                 decode_in_place=False):
         lib = _lib.load()
         self.table = table
         self.dim = table.info["dim"]
-        cfg = _lib.SearcherConfig(max_batch, candidate_cap, sample_docs, max_retries, method)
+        cfg = _lib.SearcherConfig(max_batch, candidate_cap, sample_docs, max_retries, method, int(decode_in_place))
         h = ctypes.c_void_p()
         check(lib.hss_searcher_create(table._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

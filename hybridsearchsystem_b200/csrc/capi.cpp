@@ -256,6 +256,7 @@ int hss_searcher_create(hss_table* table, const hss_searcher_config* cfg, hss_se
         c.maxRetries = cfg->maxRetries;
         if (cfg->method < 0 || cfg->method > 3) return SetError(HSS_ERR_INVALID, "unknown scoring method");
         c.method = static_cast<hss::ScoreMethod>(cfg->method);
+        c.densePostings = cfg->decodeInPlace == 0;
     }
     auto* s = new hss_searcher;
     s->t = table->t;

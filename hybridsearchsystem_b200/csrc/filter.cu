@@ -330,6 +330,112 @@ __global__ void __launch_bounds__(kTile) filter_batch_kernel(FilterLaunch L) {
     if (L.status && bad && t < nw) atomicOr(L.status + q, bad_posting ? kStatusBadPosting : kStatusBadProgram);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Batch filter over the dense posting matrix (every posting pre-expanded, DataTable::
+// EnableDensePostings): operand words need no decoding and no dependent loads, so a CTA copies its
+// operands' words for a tile straight into shared memory (cp.async, 16 bytes per thread per
+// operand), then runs every word through the program. Small tiles keep many CTAs resident per SM.
+__device__ inline void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+constexpr int kDenseT = 256;  // threads of a dense-filter CTA
+
+template <int WPT>
+__global__ void __launch_bounds__(kDenseT) filter_dense_kernel(DenseFilterLaunch L) {
+    constexpr uint32_t TW = kDenseT * WPT;  // words per CTA
+    extern __shared__ __align__(16) uint64_t dslots[];  // [nop][TW]
+    __shared__ uint32_t s_prog[kMaxProgram];
+    __shared__ uint32_t s_row[kMaxOperands];
+
+    const uint32_t q = blockIdx.x;
+    const uint32_t t = threadIdx.x;
+    const uint32_t seg_words = L.seg_words;
+    const uint32_t tiles = (seg_words + TW - 1) / TW;
+    const uint32_t seg = blockIdx.y / tiles;
+    const uint32_t w0 = (blockIdx.y % tiles) * TW;
+    const uint32_t nw = min(TW, seg_words - w0);
+    const uint64_t gw0 = static_cast<uint64_t>(seg) * seg_words + w0;
+    uint64_t* out_row = L.out + static_cast<uint64_t>(q) * L.out_stride;
+
+    const uint32_t p0 = L.prog_off[q], p1 = L.prog_off[q + 1];
+    const uint32_t o0 = L.opnd_off[q], o1 = L.opnd_off[q + 1];
+    const uint32_t nop = o1 - o0;
+    const uint32_t plen = p1 - p0;
+    if (plen == 0) {  // empty program: match all (text_filter.cpp:553-559)
+        uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k < WPT; ++k) {
+            const uint32_t w = k * kDenseT + t;
+            if (w < nw) {
+                const uint64_t v = tail_mask(gw0 + w, L.doc_num);
+                out_row[gw0 + w] = v;
+                c += __popcll(v);
+            }
+        }
+        if (L.pass_count) {
+            c = warp_sum(c);
+            if ((t & 31) == 0 && c) atomicAdd(L.pass_count + q, c);
+        }
+        return;
+    }
+    if (nop > L.max_opnd || nop > static_cast<uint32_t>(kMaxOperands) || plen > static_cast<uint32_t>(kMaxProgram)) {
+        for (uint32_t w = t; w < nw; w += kDenseT) out_row[gw0 + w] = 0;
+        if (t == 0 && L.status) atomicOr(L.status + q, kStatusBadProgram);
+        return;
+    }
+    for (uint32_t i = t; i < plen; i += kDenseT) s_prog[i] = L.prog[p0 + i];
+    if (t < nop) {
+        const uint32_t r = L.opnd_row[o0 + t];
+        s_row[t] = r < L.rows ? r : L.rows - 1;  // a row past the table reads the all-zero row
+    }
+    __syncthreads();
+    // nw is even (segments hold a multiple of 128 docs): 16-byte pieces, one per thread per operand
+    for (uint32_t i = 0; i < nop; ++i) {
+        const uint64_t* src = L.dense + (static_cast<uint64_t>(s_row[i]) * L.seg_num + seg) * seg_words + w0;
+        for (uint32_t c = t; c < nw / 2; c += kDenseT) cp_async16(dslots + i * TW + 2 * c, src + 2 * c);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    bool bad = false;
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < WPT; ++k) {
+        const uint32_t w = k * kDenseT + t;
+        if (w >= nw) continue;
+        uint64_t r = 0;
+        if (!bad && !eval_word(s_prog, plen, dslots, TW, w, nop, &r)) bad = true;
+        if (bad) r = 0;
+        r &= tail_mask(gw0 + w, L.doc_num);
+        out_row[gw0 + w] = r;
+        c += __popcll(r);
+    }
+    if (L.pass_count) {
+        c = warp_sum(c);
+        if ((t & 31) == 0 && c) atomicAdd(L.pass_count + q, c);
+    }
+    if (L.status && bad) atomicOr(L.status + q, kStatusBadProgram);
+}
+
+template <int WPT>
+cudaError_t launch_filter_dense_wpt(const DenseFilterLaunch& L, cudaStream_t stream) {
+    constexpr uint32_t TW = kDenseT * WPT;
+    const uint32_t tiles = (L.seg_words + TW - 1) / TW;
+    const uint64_t gy = static_cast<uint64_t>(L.seg_num) * tiles;
+    if (gy > 65535u) return cudaErrorInvalidValue;
+    const size_t smem = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * TW * sizeof(uint64_t);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(filter_dense_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    filter_dense_kernel<WPT><<<dim3(L.nq, static_cast<uint32_t>(gy)), kDenseT, smem, stream>>>(L);
+    return cudaGetLastError();
+}
+
 // One CTA per posting: expand `src[i]` (any layout) into the dense bitset `dst[i]` of
 // byte_size bytes (the PostingBitListToSet operator, bitlist_to_set.h:6-155).
 __global__ void __launch_bounds__(256) posting_expand_kernel(const uint64_t* src, const uint64_t* dst, uint32_t count,
@@ -420,6 +526,17 @@ cudaError_t launch_filter_batch(const FilterLaunch& L, cudaStream_t stream) {
         case 2: return launch_filter_wpt<2>(L, stream);
         default: return launch_filter_wpt<1>(L, stream);
     }
+}
+
+// Two words per thread (4 KB of each operand per CTA) while the operand slots fit 48 KB, else one.
+cudaError_t launch_filter_dense(const DenseFilterLaunch& L, cudaStream_t stream) {
+    if (L.nq == 0 || L.seg_num == 0) return cudaSuccess;
+    if (L.max_opnd > static_cast<uint32_t>(kMaxOperands) || L.rows == 0 || L.seg_words == 0 || (L.seg_words & 1u) ||
+        (reinterpret_cast<uintptr_t>(L.dense) & 15u))
+        return cudaErrorInvalidValue;
+    const size_t per_word = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * sizeof(uint64_t);
+    if (2 * kDenseT * per_word <= 48 * 1024) return launch_filter_dense_wpt<2>(L, stream);
+    return launch_filter_dense_wpt<1>(L, stream);
 }
 
 cudaError_t launch_posting_expand(const uint64_t* src, const uint64_t* dst, uint32_t count, uint32_t byte_size,

@@ -134,8 +134,65 @@ bool DataTable::EnableFormat(int format, std::string* err) {
     return true;
 }
 
+bool DataTable::EnableDensePostings(uint64_t budgetBytes, std::string* err) {
+    if (m_dDense) return true;
+    if (m_dPostingTable == nullptr) return Fail(err, "table has no device residency");
+    const uint64_t segBytes = GetSegmentByteSize();
+    const uint64_t n = static_cast<uint64_t>(m_rows) * m_segmentNum;
+    if (n * segBytes > budgetBytes) return true;  // over budget: batches keep decoding postings in place
+    if (!CudaOk(cudaSetDevice(m_deviceId), err, "cudaSetDevice")) return false;
+    uint64_t* dense = nullptr;
+    uint64_t* ptrs = nullptr;  // [2][n]: source posting addresses, destination bitmap addresses
+    int32_t* status = nullptr;
+    bool ok = CudaOk(cudaMalloc(&dense, n * segBytes), err, "cudaMalloc dense postings") &&
+              CudaOk(cudaMalloc(&ptrs, 2 * n * sizeof(uint64_t)), err, "cudaMalloc dense postings") &&
+              CudaOk(cudaMalloc(&status, sizeof(int32_t)), err, "cudaMalloc dense postings") &&
+              CudaOk(cudaMemset(status, 0, sizeof(int32_t)), err, "cudaMemset");
+    // ordered full segments first, then the last (possibly partial) segment, which decodes with its
+    // own doc count
+    std::vector<uint64_t> table(n), hp(2 * n);
+    if (ok) ok = CudaOk(cudaMemcpy(table.data(), m_dPostingTable, n * 8, cudaMemcpyDeviceToHost), err, "download");
+    const uint32_t S = m_segmentNum;
+    uint64_t at = 0;
+    for (int pass = 0; pass < 2 && ok; ++pass)
+        for (uint32_t r = 0; r < m_rows; ++r)
+            for (uint32_t s = 0; s < S; ++s) {
+                if ((s + 1 == S) != (pass == 1)) continue;
+                hp[at] = table[static_cast<uint64_t>(r) * S + s];
+                hp[n + at] = reinterpret_cast<uint64_t>(dense) + (static_cast<uint64_t>(r) * S + s) * segBytes;
+                ++at;
+            }
+    if (ok) ok = CudaOk(cudaMemcpy(ptrs, hp.data(), 2 * n * 8, cudaMemcpyHostToDevice), err, "upload");
+    const uint64_t full = static_cast<uint64_t>(m_rows) * (S - 1);
+    const uint32_t lastDocs = static_cast<uint32_t>(m_docNum - static_cast<uint64_t>(S - 1) * m_cfg.docNumPerSegment);
+    if (ok && full)
+        ok = CudaOk(launch_posting_expand(ptrs, ptrs + n, static_cast<uint32_t>(full), static_cast<uint32_t>(segBytes),
+                                          m_cfg.docNumPerSegment, status, nullptr),
+                    err, "expand postings");
+    if (ok)
+        ok = CudaOk(launch_posting_expand(ptrs + full, ptrs + n + full, m_rows, static_cast<uint32_t>(segBytes),
+                                          lastDocs, status, nullptr),
+                    err, "expand postings");
+    int32_t hs = 0;
+    if (ok) ok = CudaOk(cudaMemcpy(&hs, status, 4, cudaMemcpyDeviceToHost), err, "expand postings");
+    cudaFree(ptrs);
+    cudaFree(status);
+    if (!ok || hs != 0) {
+        // a malformed posting: leave the in-place path, which reports it per query
+        if (dense) cudaFree(dense);
+        return ok;
+    }
+    m_dDense = dense;
+    return true;
+}
+
 void DataTable::Release() {
     for (int f = 0; f < 3; ++f) m_fmtReady[f] = false;
+    if (m_dDense) {
+        if (m_deviceId >= 0) cudaSetDevice(m_deviceId);
+        cudaFree(m_dDense);
+        m_dDense = nullptr;
+    }
     if (m_dVectors == nullptr && m_dArena == nullptr && m_dPostingTable == nullptr && m_dGDocIds == nullptr) return;
     if (m_deviceId >= 0) cudaSetDevice(m_deviceId);
     for (int f = 1; f < 3; ++f) {

@@ -230,6 +230,12 @@ class DataTable {
     double NormMax(int format) const { return m_fmtNormMax[format]; }
     double ErrMax(int format) const { return m_fmtErrMax[format]; }
 
+    // Every posting of the table expanded into a dense bitmap (all five layouts decoded once):
+    // u64 [rows][segments][docNumPerSegment / 64], 16-byte aligned rows, when its size fits
+    // budgetBytes (else nothing is built and batches decode the postings in place). A malformed
+    // posting also leaves it unbuilt, so the in-place path reports it per query.
+    bool EnableDensePostings(uint64_t budgetBytes, std::string* err);
+    const uint64_t* DeviceDensePostings() const { return m_dDense; }
     // Host copy of segment s's posting of a token row (for tests / save); null if absent.
     const uint8_t* HostPosting(uint32_t row, uint32_t seg, uint32_t* len) const;
     // Layout code of each posting of a row (PostingFieldData::GetPostingTypes).
@@ -269,6 +275,7 @@ class DataTable {
     uint8_t* m_dArena = nullptr;
     uint64_t* m_dPostingTable = nullptr;
     int64_t* m_dGDocIds = nullptr;
+    uint64_t* m_dDense = nullptr;  // EnableDensePostings
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -297,6 +304,7 @@ struct SearcherConfig {
     uint32_t sampleDocs = 32768;       // minimum doc sample for the candidate threshold
     uint32_t maxRetries = 4;           // candidate-overflow re-runs before a query fails
     ScoreMethod method = ScoreMethod::SIMT_FP32;
+    bool densePostings = true;         // filter batches over the table's dense posting matrix
 };
 
 // Timing of the stages of the last batch (CUDA events, milliseconds).
@@ -392,6 +400,7 @@ class FullRecallSearcher {
     bool m_timing = false;
     StageTimes m_times;
     std::vector<int32_t> m_lastStatus;
+    std::vector<std::pair<uint32_t, uint32_t>> m_lastSegs;  // per query: (segments, entries per segment)
 };
 
 }  // namespace hss

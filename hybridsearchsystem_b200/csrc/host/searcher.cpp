@@ -54,13 +54,14 @@ StageLayout MakeLayout(uint32_t B) {
     L.negInf = take(B * 4ull);
     L.theta = take(B * 4ull);
     L.qlist = take(B * 4ull);
-    L.counters = at;
+    L.counters = at;  // zeroed per batch: passCount and status
     L.passCount = take(B * 4ull);
-    L.candCount = take(B * 4ull);
-    L.sampCount = take(B * 4ull);
     L.status = take(B * 4ull);
     L.prog = take(static_cast<size_t>(B) * kMaxProgram * 4ull);
     L.opnd = take(static_cast<size_t>(B) * kMaxOperands * 4ull);
+    // per-segment candidate counts: every producing CTA writes its own, no clearing
+    L.candCount = take(static_cast<size_t>(B) * kMaxCandSegs * 4ull);
+    L.sampCount = take(static_cast<size_t>(B) * kMaxCandSegs * 4ull);
     L.total = at;
     return L;
 }
@@ -77,6 +78,7 @@ FullRecallSearcher::FullRecallSearcher(int32_t deviceId, std::shared_ptr<DataTab
     if (m_cfg.maxBatch == 0) m_cfg.maxBatch = 1;
     // the tensor-core pass stages at most 2 x 128 query rows per launch
     if (m_cfg.method != ScoreMethod::SIMT_FP32 && m_cfg.maxBatch > 256) m_cfg.maxBatch = 256;
+    if (m_cfg.maxBatch > kMaxSimtBatch) m_cfg.maxBatch = kMaxSimtBatch;
     m_ok = Allocate();
 }
 
@@ -105,11 +107,13 @@ bool FullRecallSearcher::Allocate() {
         m_numSms = sms;
     const uint64_t B = m_cfg.maxBatch, C = m_cfg.candidateCap;
     const uint64_t words = m_table->GetBitmapWords();
-    // Sample buffer: room for the sample a K of up to 1024 asks for (see SearchDevice); a larger K's
-    // sample overflows it, which only weakens its threshold (the stored part is still a subset).
+    // Sample buffer: room for the sample a K of up to 1024 asks for (see SearchDevice) plus the
+    // rounding of its tiles to segments; a larger K's sample overflows it, which only weakens its
+    // threshold (the stored part is still a subset).
     const uint64_t forK = (4ull * 1024 * m_table->GetDocNum() + C - 1) / C;
-    m_sampCap = static_cast<uint32_t>(std::min<uint64_t>(
-        std::max<uint64_t>({forK, m_cfg.sampleDocs, static_cast<uint64_t>(kMaxTopK)}), 1u << 19));
+    m_sampCap = static_cast<uint32_t>(
+        std::min<uint64_t>(std::max<uint64_t>({forK, m_cfg.sampleDocs, static_cast<uint64_t>(kMaxTopK)}), 1u << 19) +
+        128ull * kMaxCandSegs);
     const uint32_t dim = m_table->GetDimension();
     const StageLayout L = MakeLayout(static_cast<uint32_t>(B));
     m_stageBytes = L.total;
@@ -133,6 +137,12 @@ bool FullRecallSearcher::Allocate() {
     if (!ck(cudaMallocHost(&m_hOutCount, B * 4ull), "cudaMallocHost results")) return false;
     for (auto& e : m_ev)
         if (!ck(cudaEventCreate(&e), "cudaEventCreate")) return false;
+    if (m_cfg.densePostings) {
+        // every posting decoded once into a dense bitmap when that takes at most 40% of free memory
+        size_t freeB = 0, totalB = 0;
+        if (!ck(cudaMemGetInfo(&freeB, &totalB), "cudaMemGetInfo")) return false;
+        if (!m_table->EnableDensePostings(static_cast<uint64_t>(freeB) / 5 * 2, &m_err)) return false;
+    }
     if (m_cfg.method != ScoreMethod::SIMT_FP32) {
         m_tcFormat = static_cast<int>(m_cfg.method) - 1;
         if (!m_table->EnableFormat(m_tcFormat, &m_err)) return false;
@@ -225,6 +235,26 @@ int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exp
     ck(cudaMemsetAsync(D + SL.counters, 0, SL.prog - SL.counters, stream));
 
     const DataTable& T = *m_table;
+    if (m_cfg.densePostings && T.DeviceDensePostings()) {
+        DenseFilterLaunch F{};
+        F.prog = reinterpret_cast<const uint32_t*>(D + SL.prog);
+        F.prog_off = reinterpret_cast<const uint32_t*>(D + SL.progOff);
+        F.opnd_row = reinterpret_cast<const uint32_t*>(D + SL.opnd);
+        F.opnd_off = reinterpret_cast<const uint32_t*>(D + SL.opndOff);
+        F.dense = T.DeviceDensePostings();
+        F.rows = T.PostingRows();
+        F.seg_words = T.GetDocNumPerSegment() / 64;
+        F.out = dBits;
+        F.out_stride = bitsStride;
+        F.pass_count = reinterpret_cast<uint32_t*>(D + SL.passCount);
+        F.status = reinterpret_cast<int32_t*>(D + SL.status);
+        F.nq = nq;
+        F.seg_num = T.GetSegmentNum();
+        F.doc_num = T.GetDocNum();
+        F.max_opnd = maxOpnd;
+        ck(launch_filter_dense(F, stream));
+        return ce == cudaSuccess ? 0 : static_cast<int>(ce);
+    }
     FilterLaunch F{};
     F.prog = reinterpret_cast<const uint32_t*>(D + SL.prog);
     F.prog_off = reinterpret_cast<const uint32_t*>(D + SL.progOff);
@@ -352,10 +382,21 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     ++launches;
     if (m_timing) ck(cudaEventRecord(m_ev[1], stream));
 
-    // Candidate pass over tiles [begin + i * step, i < count) for `rows` queries (dList or 0..rows-1).
-    auto cand = [&](const float* theta, float* score, uint32_t* loc, uint32_t* count, uint32_t cap,
-                    uint64_t begin, uint64_t step, uint64_t countTiles, const uint32_t* dList, uint32_t rows,
-                    bool simt = false) {
+    // Candidate passes. A pass covers tiles begin + i * step (or, with skip >= 2, all tiles that are not
+    // multiples of skip), i < countTiles, for `rows` queries (dList or 0..rows-1), and writes the
+    // list segments [segBase, segBase + its segments) of seg_cap entries each.
+    auto ctasOf = [&](uint64_t countTiles, uint32_t cap, bool simt) {
+        return (!tc || simt) ? cand_simt_segments(countTiles, m_numSms, cap)
+                             : tc_cand_segments(countTiles, m_numSms, cap);
+    };
+    auto segsOf = [&](uint64_t countTiles, uint32_t cap, bool simt) {
+        const uint32_t g = ctasOf(countTiles, cap, simt);
+        return (!tc || simt) ? g : 2 * g;  // a tensor-core CTA fills two segments
+    };
+    auto cand = [&](const float* theta, float* score, uint32_t* loc, uint32_t* count, uint32_t cap, uint32_t segBase,
+                    uint32_t segCap, uint64_t begin, uint64_t step, uint32_t skip, uint64_t countTiles,
+                    const uint32_t* dList, uint32_t rows, bool simt) {
+        const uint32_t g = ctasOf(countTiles, cap, simt);
         if (!tc || simt) {
             CandLaunch C{};
             C.vec = T.DeviceVectors();
@@ -369,10 +410,14 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
             C.cand_loc = loc;
             C.cand_count = count;
             C.cap = cap;
+            C.segs = g;
+            C.seg_cap = segCap;
+            C.seg_base = segBase;
             C.dim = dim;
             C.tile_begin = begin;
             C.tile_step = step;
             C.tile_count = countTiles;
+            C.tile_skip = skip;
             ck(launch_cand_simt(C, m_numSms, stream));
             return;
         }
@@ -392,41 +437,62 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         C.cand_loc = loc;
         C.cand_count = count;
         C.cap = cap;
+        C.segs = g;
+        C.seg_cap = segCap;
+        C.seg_base = segBase;
         C.tile_begin = begin;
         C.tile_step = step;
         C.tile_count = countTiles;
+        C.tile_skip = skip;
         C.error = m_dError;
         ck(launch_tc_cand(C, m_docMap, m_qryMap, m_numSms, stream));
     };
+    // segment capacity of a pass over countTiles tiles into `segs` segments: the docs a segment can
+    // see at most, within the list's share
+    auto segCapOf = [&](uint64_t countTiles, uint32_t cap, uint32_t segs, bool simt) {
+        const uint32_t g = ctasOf(countTiles, cap, simt);
+        const uint64_t perSeg = (countTiles + g - 1) / g * ((!tc || simt) ? 128ull : 64ull);
+        return static_cast<uint32_t>(std::min<uint64_t>(perSeg, cap / segs));
+    };
 
-    // doc sample: evenly spaced tiles, sized so the K-th best sample score sits near rank cap/4
+    // 1. doc sample: evenly spaced tiles, every filtered doc kept; its K-th best bounds the threshold
     const uint64_t want = std::max<uint64_t>(m_cfg.sampleDocs,
                                              (4ull * std::max<uint32_t>(maxK, 1u) * T.GetDocNum() +
                                               m_cfg.candidateCap - 1) / m_cfg.candidateCap);
     const uint64_t sampTiles = std::min<uint64_t>(tiles, std::max<uint64_t>(1, (want + 127) / 128));
     const uint64_t step = std::max<uint64_t>(1, tiles / sampTiles);
-    const uint32_t sampCapUsed = static_cast<uint32_t>(std::min<uint64_t>(m_sampCap, sampTiles * 128));
-    cand(dNegInf, m_dSampScore, m_dSampLoc, dSampCount, sampCapUsed, 0, step,
-         std::min<uint64_t>(sampTiles, (tiles + step - 1) / step), nullptr, nq);
-    ++launches;
-    SampleThresholdLaunch ST{};
-    ST.score = m_dSampScore;
-    ST.count = dSampCount;
-    ST.cap = sampCapUsed;
-    ST.topk = dTopk;
-    ST.eps_sample = dEpsSamp;
-    ST.eps_main = dEpsMain;
-    ST.theta = dTheta;
-    ST.qlist = nullptr;
-    ST.nq_list = nq;
-    ck(launch_sample_threshold(ST, stream));
-    ++launches;
+    const uint64_t sampCount = std::min<uint64_t>(sampTiles, (tiles + step - 1) / step);
+    auto sample = [&](const uint32_t* dList, uint32_t rows, bool simt) {
+        const uint32_t segs = segsOf(sampCount, m_sampCap, simt);
+        const uint32_t segCap = segCapOf(sampCount, m_sampCap, segs, simt);
+        cand(dNegInf, m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, segCap, 0, step, 0, sampCount, dList, rows,
+             simt);
+        SampleThresholdLaunch ST{};
+        ST.score = m_dSampScore;
+        ST.count = dSampCount;
+        ST.cap = m_sampCap;
+        ST.segs = segs;
+        ST.seg_cap = segCap;
+        ST.raise_only = 0;
+        ST.topk = dTopk;
+        ST.eps_sample = dEpsSamp;
+        ST.eps_main = dEpsMain;
+        ST.theta = dTheta;
+        ST.qlist = dList;
+        ST.nq_list = rows;
+        ck(launch_sample_threshold(ST, stream));
+    };
+    sample(nullptr, nq, false);
+    launches += 2;
     if (m_timing) ck(cudaEventRecord(m_ev[2], stream));
 
-    cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, m_cfg.candidateCap, 0, 1, tiles, nullptr, nq);
-    ++launches;
-    if (m_timing) ck(cudaEventRecord(m_ev[3], stream));
-
+    // 2. the full pass, progressively: first every split-th tile (about sqrt(sample / corpus) of it)
+    // with the sample's threshold; the K-th best of that part then raises each query's threshold
+    // (every doc of the top K scores at least K-th best - 2 eps) for the remaining tiles. Both parts'
+    // candidates form one segmented list.
+    const uint32_t C = m_cfg.candidateCap;
+    uint32_t split = static_cast<uint32_t>(std::sqrt(static_cast<double>(tiles) / static_cast<double>(sampCount)));
+    split = std::min<uint32_t>(split, 64);
     SelectLaunch SE{};
     SE.vec = T.DeviceVectors();
     SE.qry = dQueries;
@@ -434,7 +500,7 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     SE.cand_score = m_dCandScore;
     SE.cand_loc = m_dCandLoc;
     SE.cand_count = dCandCount;
-    SE.cap = m_cfg.candidateCap;
+    SE.cap = C;
     SE.work = m_dWork;
     SE.topk = dTopk;
     SE.eps_main = dEpsMain;
@@ -447,6 +513,41 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     SE.status = dStatus;
     SE.qlist = nullptr;
     SE.nq_list = nq;
+    if (split >= 2) {
+        const uint64_t countA = (tiles + split - 1) / split, countB = tiles - countA;
+        const uint32_t segsA = segsOf(countA, C, false), segsB = segsOf(countB, C, false);
+        const uint32_t segCap =
+            std::min(segCapOf(countA, C, segsA + segsB, false), segCapOf(countB, C, segsA + segsB, false));
+        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, split, 0, countA, nullptr, nq, false);
+        SampleThresholdLaunch RT{};
+        RT.score = m_dCandScore;
+        RT.count = dCandCount;
+        RT.cap = C;
+        RT.segs = segsA;
+        RT.seg_cap = segCap;
+        RT.raise_only = 1;
+        RT.topk = dTopk;
+        RT.eps_sample = dEpsMain;  // t - 2 eps_main
+        RT.eps_main = dEpsMain;
+        RT.theta = dTheta;
+        RT.qlist = nullptr;
+        RT.nq_list = nq;
+        ck(launch_sample_threshold(RT, stream));
+        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, segsA, segCap, 0, 1, split, countB, nullptr, nq, false);
+        launches += 3;
+        SE.segs = segsA + segsB;
+        SE.seg_cap = segCap;
+    } else {
+        const uint32_t segs = segsOf(tiles, C, false);
+        SE.segs = segs;
+        SE.seg_cap = segCapOf(tiles, C, segs, false);
+        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tiles, nullptr, nq, false);
+        ++launches;
+    }
+    m_lastSegs.assign(nq, {SE.segs, SE.seg_cap});
+    if (m_timing) ck(cudaEventRecord(m_ev[3], stream));
+
+    // 3. exact rescoring and the top K
     ck(launch_select_topk(SE, stream));
     ++launches;
     if (m_timing) ck(cudaEventRecord(m_ev[4], stream));
@@ -470,7 +571,6 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         }
         ++retries;
         ck(cudaMemcpyAsync(dQlist, hQlist, nre * 4ull, cudaMemcpyHostToDevice, stream));
-        ck(cudaMemsetAsync(dCandCount, 0, nq * 4ull, stream));
         ck(cudaMemsetAsync(dStatus, 0, nq * 4ull, stream));
         // A tensor-core re-run helps when the first threshold was loose. When the docs inside the
         // 2 eps band around the K-th score alone overflow the list, only a tighter bound helps: from the
@@ -481,19 +581,19 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
             // the plain path for these queries: SIMT bounds, a SIMT doc sample for a fresh threshold
             const double rel = SimtRelBound(dim);
             ck(launch_query_eps(dQueries, nq, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
-            ck(cudaMemsetAsync(dSampCount, 0, nq * 4ull, stream));
-            cand(dNegInf, m_dSampScore, m_dSampLoc, dSampCount, sampCapUsed, 0, step,
-                 std::min<uint64_t>(sampTiles, (tiles + step - 1) / step), dQlist, nre, true);
-            SampleThresholdLaunch RT = ST;
-            RT.qlist = dQlist;
-            RT.nq_list = nre;
-            ck(launch_sample_threshold(RT, stream));
+            sample(dQlist, nre, true);
             launches += 3;
         } else if (tc) {
             stage(dQlist, nre);  // the staged rows become the re-run queries (their bounds unchanged)
             ++launches;
         }
-        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, m_cfg.candidateCap, 0, 1, tiles, dQlist, nre, simt);
+        // one pass over every tile with the raised threshold
+        const uint32_t segs = segsOf(tiles, C, simt);
+        const uint32_t segCap = segCapOf(tiles, C, segs, simt);
+        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, 1, 0, tiles, dQlist, nre, simt);
+        for (uint32_t i = 0; i < nre; ++i) m_lastSegs[hQlist[i]] = {segs, segCap};
+        SE.segs = segs;
+        SE.seg_cap = segCap;
         SE.qlist = dQlist;
         SE.nq_list = nre;
         ck(launch_select_topk(SE, stream));
@@ -532,19 +632,27 @@ int FullRecallSearcher::LastCandidates(uint32_t q, float* scores, uint32_t* locs
                                        float* theta, float* eps) {
     if (!m_ok || q >= m_cfg.maxBatch) return -1;
     if (cudaSetDevice(m_deviceId) != cudaSuccess) return -2;
+    if (q >= m_lastSegs.size()) return -1;
     const StageLayout SL = MakeLayout(m_cfg.maxBatch);
-    uint32_t n = 0;
-    cudaError_t e = cudaMemcpy(&n, m_dStage + SL.candCount + 4ull * q, 4, cudaMemcpyDeviceToHost);
+    const auto sg = m_lastSegs[q];
+    std::vector<uint32_t> cnt(kMaxCandSegs);
+    cudaError_t e = cudaMemcpy(cnt.data(), m_dStage + SL.candCount + 4ull * kMaxCandSegs * q, 4ull * kMaxCandSegs,
+                               cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(theta, m_dStage + SL.theta + 4ull * q, 4, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(eps, m_dStage + SL.epsMain + 4ull * q, 4, cudaMemcpyDeviceToHost);
-    *count = n;
-    const uint32_t k = std::min({n, cap, m_cfg.candidateCap});
-    if (e == cudaSuccess && k)
-        e = cudaMemcpy(scores, m_dCandScore + static_cast<uint64_t>(q) * m_cfg.candidateCap, 4ull * k,
-                       cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && k)
-        e = cudaMemcpy(locs, m_dCandLoc + static_cast<uint64_t>(q) * m_cfg.candidateCap, 4ull * k,
-                       cudaMemcpyDeviceToHost);
+    // the stored entries of every segment, in segment order
+    uint32_t total = 0, got = 0;
+    const uint64_t row = static_cast<uint64_t>(q) * m_cfg.candidateCap;
+    for (uint32_t g = 0; g < sg.first && e == cudaSuccess; ++g) {
+        total += cnt[g];
+        const uint32_t k = std::min({cnt[g], sg.second, cap - got});
+        if (k == 0) continue;
+        const uint64_t at = row + static_cast<uint64_t>(g) * sg.second;
+        e = cudaMemcpy(scores + got, m_dCandScore + at, 4ull * k, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(locs + got, m_dCandLoc + at, 4ull * k, cudaMemcpyDeviceToHost);
+        got += k;
+    }
+    *count = total;
     return e == cudaSuccess ? 0 : -2;
 }
 

@@ -87,4 +87,10 @@ __device__ inline float exact_dot(const float* __restrict__ q, const float* __re
     return s;
 }
 
+// Tile of iteration `it` of a candidate pass: begin + it * step, or, with skip >= 2, the it-th tile
+// that is not a multiple of skip.
+__host__ __device__ inline uint64_t pass_tile(uint64_t begin, uint64_t step, uint32_t skip, uint64_t it) {
+    return skip >= 2 ? it + it / (skip - 1) + 1 : begin + it * step;
+}
+
 }  // namespace hss

@@ -39,8 +39,40 @@ struct FilterLaunch {
     int ref_table;
 };
 
+// Batched filter over the dense posting matrix (filter.cu): operand i of query q at segment s is
+// dense[(opnd_row[opnd_off[q] + i] * seg_num + s) * seg_words ...], already decoded.
+struct DenseFilterLaunch {
+    const uint32_t* prog;      // concatenated postfix programs
+    const uint32_t* prog_off;  // [nq + 1]
+    const uint32_t* opnd_row;  // concatenated operand rows
+    const uint32_t* opnd_off;  // [nq + 1]
+    const uint64_t* dense;     // [rows][seg_num][seg_words], 16-byte aligned
+    uint32_t rows;
+    uint32_t seg_words;        // docs per segment / 64 (even)
+    uint64_t* out;             // [nq][out_stride] bitmap words
+    uint64_t out_stride;
+    uint32_t* pass_count;      // [nq] docs passing, accumulated (zeroed by the caller), or null
+    int32_t* status;           // [nq] error bits, or null
+    uint32_t nq;
+    uint32_t seg_num;
+    uint64_t doc_num;
+    uint32_t max_opnd;         // largest operand count of any query in the batch (<= 64)
+};
+cudaError_t launch_filter_dense(const DenseFilterLaunch& L, cudaStream_t stream);
+
+// Candidate lists are segmented so that no producer needs a global atomic: query q's region
+// [q * cap, (q + 1) * cap) is cut into segments of seg_cap entries; segment g (at g * seg_cap) is
+// written by exactly one producer thread group, and counts[q * kMaxCandSegs + g] is how many
+// candidates it found for q (more than seg_cap means the segment overflowed; only seg_cap are
+// stored). A pass writes the segments [seg_base, seg_base + its segments): a SIMT pass one per CTA,
+// a tensor-core pass two per CTA. Each producer writes its count for every query it serves, so the
+// counts need no clearing. Tiles of a pass: tile_begin + i * tile_step, or, when tile_skip >= 2,
+// every tile that is not a multiple of tile_skip (the complement of a step-tile_skip pass).
+constexpr uint32_t kMaxCandSegs = 1024;
+
 // Bulk candidate pass (score.cu). Processes tiles tile_begin + i * tile_step, i < tile_count, of
-// 128 docs each, for the queries qlist[0..nq_list) (or 0..nq_list-1 when qlist is null).
+// 128 docs each, for the queries qlist[0..nq_list) (or 0..nq_list-1 when qlist is null), with
+// `segs` CTAs (one candidate segment each).
 struct CandLaunch {
     const float* vec;          // [tiles * 128][dim] FP32 corpus, rows 16-byte aligned
     const float* qry;          // [nq][dim]
@@ -49,18 +81,34 @@ struct CandLaunch {
     const float* theta;        // [nq] candidate thresholds
     const uint32_t* qlist;
     uint32_t nq_list;
-    float* cand_score;         // [nq][cap]
-    uint32_t* cand_loc;        // [nq][cap]
-    uint32_t* cand_count;      // [nq] (may exceed cap: overflow)
+    float* cand_score;         // [nq][cap], segmented
+    uint32_t* cand_loc;        // [nq][cap], segmented
+    uint32_t* cand_count;      // [nq][kMaxCandSegs] per-segment counts
     uint32_t cap;
+    uint32_t segs, seg_cap;    // CTAs of the launch (cand_simt_segments) and entries per segment
+    uint32_t seg_base;         // first segment this pass writes
     uint32_t dim;              // multiple of 4
     uint64_t tile_begin, tile_step, tile_count;
+    uint32_t tile_skip;
 };
+// Largest query count of one SIMT candidate pass (its per-query counts live in shared memory).
+constexpr uint32_t kMaxSimtBatch = 4096;
+// CTAs of a SIMT / tensor-core candidate pass over tile_count tiles into lists of `cap` entries:
+// the kernel's natural grid, but few enough that two passes' segments fit kMaxCandSegs with at least
+// kMinSegCap entries each (a small list split too finely would overflow on uneven segments).
+constexpr uint32_t kMinSegCap = 256;
+uint32_t cand_simt_segments(uint64_t tile_count, int num_sms, uint32_t cap);
+uint32_t tc_cand_segments(uint64_t tile_count, int num_sms, uint32_t cap);
 
+// Threshold from the K-th best approximate score of a segmented list (segments [0, segs)):
+// theta = kth - eps_sample - eps_main. With raise_only the result is max(old theta, that), and a list
+// with fewer than K entries keeps the old theta.
 struct SampleThresholdLaunch {
-    const float* score;        // [nq][cap] sample scores
-    const uint32_t* count;     // [nq]
+    const float* score;        // [nq][cap] sample scores, segmented
+    const uint32_t* count;     // [nq][kMaxCandSegs]
     uint32_t cap;
+    uint32_t segs, seg_cap;
+    int raise_only;
     const uint32_t* topk;      // [nq]
     const float* eps_sample;   // [nq] error bound of the sample pass
     const float* eps_main;     // [nq] error bound of the main pass
@@ -73,10 +121,11 @@ struct SelectLaunch {
     const float* vec;
     const float* qry;
     uint32_t dim;
-    const float* cand_score;
+    const float* cand_score;   // segmented lists (see kMaxCandSegs)
     const uint32_t* cand_loc;
-    const uint32_t* cand_count;
+    const uint32_t* cand_count;  // [nq][kMaxCandSegs]
     uint32_t cap;
+    uint32_t segs, seg_cap;    // segments [0, segs) hold the candidates
     unsigned long long* work;  // [nq][cap]
     const uint32_t* topk;
     const float* eps_main;
@@ -107,11 +156,14 @@ struct TcCandLaunch {
     const float* theta;        // [nq]
     const uint32_t* qlist;     // staged row r is query qlist[r] (or r)
     uint32_t nq_rows;          // staged rows in use (<= 256)
-    float* cand_score;
+    float* cand_score;         // segmented lists (see kMaxCandSegs)
     uint32_t* cand_loc;
-    uint32_t* cand_count;
+    uint32_t* cand_count;      // [nq][kMaxCandSegs]
     uint32_t cap;
+    uint32_t segs, seg_cap;    // segs = CTAs of the launch (tc_cand_segments)
+    uint32_t seg_base;         // first segment this pass writes
     uint64_t tile_begin, tile_step, tile_count;
+    uint32_t tile_skip;
     int32_t* error;            // device error bits (bounded waits that expired)
 };
 

@@ -47,6 +47,7 @@ constexpr int kDPad = kDocTile + 4;
 constexpr int kQPad = kCQ + 4;
 
 __global__ void __launch_bounds__(kCT) cand_simt_kernel(CandLaunch L) {
+    extern __shared__ uint32_t sCount[];  // [nq_list] candidates this CTA found per query
     __shared__ __align__(16) float sD[kCK][kDPad];
     __shared__ __align__(16) float sQ[kCK][kQPad];
     __shared__ uint64_t sBits[kCQ][2];
@@ -58,9 +59,10 @@ __global__ void __launch_bounds__(kCT) cand_simt_kernel(CandLaunch L) {
     const uint32_t qg = tid >> 5;  // warp
     const uint32_t nchunks = (L.nq_list + kCQ - 1) / kCQ;
     const uint32_t kchunks = (L.dim + kCK - 1) / kCK;
+    for (uint32_t i = tid; i < L.nq_list; i += kCT) sCount[i] = 0;
 
     for (uint64_t it = blockIdx.x; it < L.tile_count; it += gridDim.x) {
-        const uint64_t tile = L.tile_begin + it * L.tile_step;
+        const uint64_t tile = pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it);
         const uint64_t doc0 = tile * kDocTile;
         for (uint32_t chunk = 0; chunk < nchunks; ++chunk) {
             float acc[4][8];
@@ -132,7 +134,8 @@ __global__ void __launch_bounds__(kCT) cand_simt_kernel(CandLaunch L) {
                 }
             }
 
-            // Epilogue: filter bit && score >= theta -> append (score, location).
+            // Epilogue: filter bit && score >= theta -> append (score, location) to this CTA's segment
+            // of the query's list (a shared-memory count per query; no global atomics).
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 const uint32_t qq = qg * 8 + j;
@@ -140,6 +143,8 @@ __global__ void __launch_bounds__(kCT) cand_simt_kernel(CandLaunch L) {
                 if (qi == 0xffffffffu) continue;  // warp-uniform
                 const float th = sTheta[qq];
                 const uint64_t w0 = sBits[qq][0], w1 = sBits[qq][1];
+                const uint64_t seg =
+                    static_cast<uint64_t>(qi) * L.cap + static_cast<uint64_t>(L.seg_base + blockIdx.x) * L.seg_cap;
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
                     const uint32_t dl = dg * 4 + r;
@@ -149,18 +154,23 @@ __global__ void __launch_bounds__(kCT) cand_simt_kernel(CandLaunch L) {
                     if (mask == 0) continue;
                     uint32_t base = 0;
                     const uint32_t leader = __ffs(mask) - 1;
-                    if (dg == leader) base = atomicAdd(L.cand_count + qi, __popc(mask));
+                    if (dg == leader) base = atomicAdd(&sCount[chunk * kCQ + qq], __popc(mask));
                     base = __shfl_sync(0xffffffffu, base, leader);
                     if (pred) {
                         const uint32_t idx = base + __popc(mask & ((1u << dg) - 1u));
-                        if (idx < L.cap) {
-                            L.cand_score[static_cast<uint64_t>(qi) * L.cap + idx] = acc[r][j];
-                            L.cand_loc[static_cast<uint64_t>(qi) * L.cap + idx] = static_cast<uint32_t>(doc0 + dl);
+                        if (idx < L.seg_cap) {
+                            L.cand_score[seg + idx] = acc[r][j];
+                            L.cand_loc[seg + idx] = static_cast<uint32_t>(doc0 + dl);
                         }
                     }
                 }
             }
         }
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < L.nq_list; i += kCT) {
+        const uint32_t qi = L.qlist ? L.qlist[i] : i;
+        L.cand_count[static_cast<uint64_t>(qi) * kMaxCandSegs + L.seg_base + blockIdx.x] = sCount[i];
     }
 }
 
@@ -181,11 +191,22 @@ cudaError_t launch_exact_score(const float* qry, const float* docs, float* out, 
     return cudaGetLastError();
 }
 
+uint32_t cand_simt_segments(uint64_t tile_count, int num_sms, uint32_t cap) {
+    uint64_t g = static_cast<uint64_t>(num_sms) * 3;
+    g = tile_count < g ? tile_count : g;
+    g = g < kMaxCandSegs / 2 ? g : kMaxCandSegs / 2;  // one segment per CTA, room for two passes
+    const uint64_t by_cap = cap / (2 * kMinSegCap) > 0 ? cap / (2 * kMinSegCap) : 1;
+    return static_cast<uint32_t>(g < by_cap ? g : by_cap);
+}
+
 cudaError_t launch_cand_simt(const CandLaunch& L, int num_sms, cudaStream_t stream) {
     if (L.tile_count == 0 || L.nq_list == 0) return cudaSuccess;
-    const uint64_t want = static_cast<uint64_t>(num_sms) * 3;
-    const uint32_t grid = static_cast<uint32_t>(L.tile_count < want ? L.tile_count : want);
-    cand_simt_kernel<<<grid, kCT, 0, stream>>>(L);
+    const uint64_t seg_end = static_cast<uint64_t>(L.seg_base) + L.segs;
+    if (L.segs != cand_simt_segments(L.tile_count, num_sms, L.cap) || L.seg_cap == 0 || seg_end > kMaxCandSegs ||
+        seg_end * L.seg_cap > L.cap || L.nq_list > kMaxSimtBatch)
+        return cudaErrorInvalidValue;
+    const size_t smem = static_cast<size_t>(L.nq_list) * sizeof(uint32_t);
+    cand_simt_kernel<<<L.segs, kCT, smem, stream>>>(L);
     return cudaGetLastError();
 }
 

@@ -8,9 +8,12 @@
 // read as TF32 (kind::tf32), BF16 (kind::f16) and FP8 E4M3 with per-vector scales (kind::f8f6f4).
 //
 // Warp roles (persistent CTA, one per SM): warp 0 issues TMA, warp 1 owns TMEM and issues MMAs
-// (one elected lane), warps 2 .. 2+4*halves-1 drain the accumulators. Each epilogue thread owns one
-// query (its TMEM lane), so the threshold test is a single compare per score; only the few scores at
-// or above the threshold look at the filter bitmap and are appended to the query's candidate list.
+// (one elected lane), warps 2 .. 2+8*halves-1 drain the accumulators. Each epilogue thread owns one
+// query (its TMEM lane) and one half of the tile's doc columns for the whole launch: it pulls its 64
+// scores out of TMEM in one batch, releases the accumulator, tests a 32-doc chunk with one max
+// reduction against the query's threshold, and only for a chunk that clears it applies the filter
+// bits and appends the survivors to its own segment of the query's candidate list (a
+// register-held count, no atomics).
 //
 // Every mbarrier wait is bounded (a clock budget); on expiry the CTA records an error, stops issuing
 // and drains, releases TMEM and returns.
@@ -161,9 +164,9 @@ __device__ inline void mma_commit(unsigned long long* bar) {
 __device__ inline void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ inline void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
-// 32 lanes x 32 consecutive FP32 columns; thread i gets lane (base lane + i).
-__device__ inline void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
+// 32 lanes x 32 consecutive FP32 columns; thread i gets lane (base lane + i). The registers are
+// written asynchronously: they are valid only after tmem_wait_ld() and a reg_fence() over them.
+__device__ inline void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
@@ -172,13 +175,39 @@ __device__ inline void tmem_ld32(uint32_t taddr, float (&v)[32]) {
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ inline void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Ties 32 registers to this point of the program (after tmem_wait_ld), so no use of them -- and no
+// copy the compiler might make -- is placed before the wait.
+__device__ inline void reg_fence(uint32_t (&r)[32]) {
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                   "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                   "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
+}
+
+// Three-input maximum (one instruction on sm_100).
+__device__ inline float max3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+__device__ inline float max32(const uint32_t (&r)[32]) {
+    float m = __uint_as_float(r[0]);
 #pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 1; i < 31; i += 2) m = max3(m, __uint_as_float(r[i]), __uint_as_float(r[i + 1]));
+    return fmaxf(m, __uint_as_float(r[31]));
 }
 
 template <int F, int H>
-__global__ void __launch_bounds__(64 + 128 * H, 1) tc_cand_kernel(const __grid_constant__ CUtensorMap doc_map,
+__global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_constant__ CUtensorMap doc_map,
                                                                   const __grid_constant__ CUtensorMap qry_map,
                                                                   TcCandLaunch L) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -199,7 +228,7 @@ __global__ void __launch_bounds__(64 + 128 * H, 1) tc_cand_kernel(const __grid_c
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&S.acc_full[b], 1);
-            mbar_init(&S.acc_empty[b], 128 * H);
+            mbar_init(&S.acc_empty[b], 256 * H);
         }
         mbar_init(&S.qbar, 1);
         mbar_init(&S.drain, 1);
@@ -228,7 +257,7 @@ __global__ void __launch_bounds__(64 + 128 * H, 1) tc_cand_kernel(const __grid_c
                                 static_cast<int>(kb * (128 / Fmt<F>::elem)), h * kRows, &S.qbar);
             uint32_t n = 0;
             for (uint64_t it = blockIdx.x; it < ntiles && !S.abort; it += gridDim.x) {
-                const int y = static_cast<int>((L.tile_begin + it * L.tile_step) * kRows);
+                const int y = static_cast<int>(pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it) * kRows);
                 for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
                     if (!mbar_wait(&S.empty[s], ph ^ 1u, S, L.error, 1)) break;
@@ -276,9 +305,14 @@ __global__ void __launch_bounds__(64 + 128 * H, 1) tc_cand_kernel(const __grid_c
             if (!mbar_wait_drain(&S.drain, 0) && L.error) atomicOr(L.error, 32);
         }
     } else {
-        // epilogue: warp w drains TMEM lanes [32 * (w % 4), +32) of half (w - 2) / 4
-        const uint32_t ew = warp - 2;
-        const uint32_t half = ew / 4;
+        // Epilogue: 8 warps per accumulator half. Warp w may only touch TMEM lanes 32 * (w % 4) ..
+        // +31, so the warps of group g = (w - 2) / 4 cover the four lane quarters of half g / 2, and
+        // the two groups of a half split its 128 doc columns (64 each). A thread owns one staged query
+        // row and one column half for the whole launch: its candidate count lives in a register and
+        // its candidates go to its own segment (2 per CTA) of the query's list, no atomics.
+        const uint32_t g = (warp - 2) / 4;
+        const uint32_t half = g / 2;
+        const uint32_t colh = g % 2;
         const uint32_t sub = warp & 3u;
         const uint32_t row = half * 128u + sub * 32u + lane;
         const bool valid = row < L.nq_rows;
@@ -286,17 +320,19 @@ __global__ void __launch_bounds__(64 + 128 * H, 1) tc_cand_kernel(const __grid_c
         const float theta = valid ? L.theta[qi] : INFINITY;
         const float qs = (F == kTcE4M3 && valid) ? L.q_scale[row] : 1.0f;
         const uint64_t* brow = L.bits + static_cast<uint64_t>(qi) * L.bits_stride;
+        const uint32_t segment = L.seg_base + 2u * blockIdx.x + colh;
+        const uint64_t seg = static_cast<uint64_t>(qi) * L.cap + static_cast<uint64_t>(segment) * L.seg_cap;
+        float* out_score = L.cand_score + seg;
+        uint32_t* out_loc = L.cand_loc + seg;
+        const uint32_t seg_cap = L.seg_cap;
+        uint32_t ncand = 0;
         uint32_t iter = 0;
         for (uint64_t it = blockIdx.x; it < ntiles; it += gridDim.x, ++iter) {
             const uint32_t buf = iter & 1u;
-            const uint64_t tile = L.tile_begin + it * L.tile_step;
-            // the query's filter bits of the tile's 128 docs, fetched before the accumulator wait so
-            // the load overlaps the tile's MMAs
-            uint64_t fw0 = 0, fw1 = 0;
-            if (valid) {
-                fw0 = brow[tile * 2];
-                fw1 = brow[tile * 2 + 1];
-            }
+            const uint64_t tile = pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it);
+            // the query's filter bits of this thread's 64 docs, fetched before the accumulator wait
+            // so the load overlaps the tile's MMAs
+            const uint64_t fw = valid ? brow[tile * 2 + colh] : 0ull;
             // threshold on the raw accumulator: acc * qs * ds >= theta
             float t = theta;
             if (F == kTcE4M3) {
@@ -306,49 +342,54 @@ __global__ void __launch_bounds__(64 + 128 * H, 1) tc_cand_kernel(const __grid_c
                 t = t == t ? t : -INFINITY;
                 t = __fmul_rd(t, 1.0f - 1e-6f) - 1e-30f;  // stay on the safe side of the rounding
             }
+            const uint32_t m[2] = {static_cast<uint32_t>(fw), static_cast<uint32_t>(fw >> 32)};
+            // 32-doc chunks that no query of the warp lets through are not read from TMEM at all
+            bool live[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) live[c] = __any_sync(0xffffffffu, m[c] != 0u);
             if (!mbar_wait(&S.acc_full[buf], (iter >> 1) & 1u, S, L.error, 16)) break;
             fence_after();
-            const uint32_t tbase = tmem + ((sub * 32u) << 16) + (buf * H + half) * 128u;
-#pragma unroll 1
-            for (uint32_t c = 0; c < 4; ++c) {
-                const uint32_t m32 = static_cast<uint32_t>((c < 2 ? fw0 : fw1) >> ((c & 1u) * 32u));
-                // docs of this chunk that no query of the warp lets through need no scores at all
-                if (!__any_sync(0xffffffffu, m32 != 0u)) continue;
-                float v[32];
-                tmem_ld32(tbase + c * 32u, v);
-                if (m32 == 0u) continue;
-                bool any = false;
+            const uint32_t tbase = tmem + ((sub * 32u) << 16) + (buf * H + half) * 128u + colh * 64u;
+            uint32_t v[2][32];
 #pragma unroll
-                for (int j = 0; j < 32; ++j) any |= v[j] >= t;
-                if (!any) continue;
+            for (int c = 0; c < 2; ++c)
+                if (live[c]) tmem_ld32(tbase + c * 32u, v[c]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 2; ++c) reg_fence(v[c]);
+            // the accumulator is in registers: hand the TMEM buffer back to the MMA issuer now
+            fence_before();
+            mbar_arrive(&S.acc_empty[buf]);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (!live[c] || m[c] == 0u) continue;
+                if (!(max32(v[c]) >= t)) continue;
                 uint32_t pass = 0;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) pass |= (v[j] >= t ? 1u : 0u) << j;
-                pass &= m32;
-                const uint64_t doc0 = tile * kRows + c * 32u;
+                for (int j = 0; j < 32; ++j) pass |= (__uint_as_float(v[c][j]) >= t ? 1u : 0u) << j;
+                pass &= m[c];
+                const uint64_t doc0 = tile * kRows + colh * 64u + c * 32u;
                 if (F == kTcE4M3) {  // the tile threshold is conservative: apply the doc's own scale
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
-                        if (((pass >> j) & 1u) && !(v[j] * qs * L.doc_scale[doc0 + j] >= theta)) pass &= ~(1u << j);
+                        if (((pass >> j) & 1u) && !(__uint_as_float(v[c][j]) * qs * L.doc_scale[doc0 + j] >= theta))
+                            pass &= ~(1u << j);
                 }
                 if (pass == 0u) continue;
-                const uint32_t base = atomicAdd(L.cand_count + qi, static_cast<uint32_t>(__popc(pass)));
-                uint32_t k = 0;
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     if (!((pass >> j) & 1u)) continue;
-                    float s = v[j];
-                    if (F == kTcE4M3) s = s * qs * L.doc_scale[doc0 + j];
-                    const uint32_t idx = base + k++;
-                    if (idx < L.cap) {
-                        L.cand_score[static_cast<uint64_t>(qi) * L.cap + idx] = s;
-                        L.cand_loc[static_cast<uint64_t>(qi) * L.cap + idx] = static_cast<uint32_t>(doc0 + j);
+                    float sc = __uint_as_float(v[c][j]);
+                    if (F == kTcE4M3) sc = sc * qs * L.doc_scale[doc0 + j];
+                    if (ncand < seg_cap) {
+                        out_score[ncand] = sc;
+                        out_loc[ncand] = static_cast<uint32_t>(doc0 + j);
                     }
+                    ++ncand;
                 }
             }
-            fence_before();
-            mbar_arrive(&S.acc_empty[buf]);
         }
+        if (valid) L.cand_count[static_cast<uint64_t>(qi) * kMaxCandSegs + segment] = ncand;
     }
     __syncthreads();
     if (threadIdx.x == 0 && S.n_consumed < S.n_issued) {
@@ -371,12 +412,23 @@ cudaError_t launch_tc_typed(const TcCandLaunch& L, const CUtensorMap& dmap, cons
     cudaError_t e = cudaFuncSetAttribute(tc_cand_kernel<F, H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    const uint32_t grid = static_cast<uint32_t>(L.tile_count < static_cast<uint64_t>(sms) ? L.tile_count : sms);
-    tc_cand_kernel<F, H><<<grid, 64 + 128 * H, smem, stream>>>(dmap, qmap, L);
+    // CTA b writes segments seg_base + 2b and seg_base + 2b + 1
+    const uint64_t seg_end = static_cast<uint64_t>(L.seg_base) + 2ull * L.segs;
+    if (L.segs != tc_cand_segments(L.tile_count, sms, L.cap) || L.seg_cap == 0 || seg_end > kMaxCandSegs ||
+        seg_end * L.seg_cap > L.cap)
+        return cudaErrorInvalidValue;
+    tc_cand_kernel<F, H><<<L.segs, 64 + 256 * H, smem, stream>>>(dmap, qmap, L);
     return cudaGetLastError();
 }
 
 }  // namespace
+
+uint32_t tc_cand_segments(uint64_t tile_count, int num_sms, uint32_t cap) {
+    uint64_t g = tile_count < static_cast<uint64_t>(num_sms) ? tile_count : static_cast<uint64_t>(num_sms);
+    g = g < kMaxCandSegs / 4 ? g : kMaxCandSegs / 4;  // two segments per CTA, room for two passes
+    const uint64_t by_cap = cap / (4 * kMinSegCap) > 0 ? cap / (4 * kMinSegCap) : 1;
+    return static_cast<uint32_t>(g < by_cap ? g : by_cap);
+}
 
 size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages) {
     return 1024 + static_cast<size_t>(halves) * kblocks * kStageBytes + static_cast<size_t>(stages) * kStageBytes +

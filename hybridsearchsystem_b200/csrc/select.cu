@@ -21,6 +21,7 @@ constexpr int kWarps = kST / 32;
 struct SelectSmem {
     uint32_t hist[kWarps][256];                 // per-warp radix histograms
     unsigned long long sortbuf[kMaxTopK];       // bitonic sort buffer
+    uint32_t segn[kMaxCandSegs];                // stored entries of each candidate segment
     uint32_t bcast[4];
     uint32_t counter;
 };
@@ -61,23 +62,67 @@ __device__ inline void clear_hist(SelectSmem& S) {
     __syncthreads();
 }
 
-// k-th largest (1-based, k <= n) of n u32 keys produced by key(i).
-template <class KeyFn>
-__device__ uint32_t kth_largest_u32(KeyFn key, uint32_t n, uint32_t k, SelectSmem& S) {
+// k-th largest (1-based, k <= the number of keys) of the u32 keys that visit(fn) hands to fn.
+template <class Visit>
+__device__ uint32_t kth_largest_u32_visit(Visit visit, uint32_t k, SelectSmem& S) {
     uint32_t prefix = 0, mask = 0, krem = k;
     const uint32_t warp = threadIdx.x >> 5;
     for (int shift = 24; shift >= 0; shift -= 8) {
         clear_hist(S);
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-            const uint32_t v = key(i);
+        visit([&](uint32_t v) {
             if ((v & mask) == prefix) atomicAdd(&S.hist[warp][(v >> shift) & 255u], 1u);
-        }
+        });
         __syncthreads();
         const uint32_t d = pick_digit(S, &krem);
         prefix |= d << shift;
         mask |= 255u << shift;
     }
     return prefix;
+}
+
+// k-th largest (1-based, k <= n) of n u32 keys produced by key(i).
+template <class KeyFn>
+__device__ uint32_t kth_largest_u32(KeyFn key, uint32_t n, uint32_t k, SelectSmem& S) {
+    return kth_largest_u32_visit(
+        [&](auto fn) {
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) fn(key(i));
+        },
+        k, S);
+}
+
+// Loads the per-segment counts of one query's segmented candidate list (kMaxCandSegs layout) into
+// S.segn (clamped to seg_cap). Returns the stored total; *overflow = some segment lost entries.
+__device__ uint32_t load_segments(SelectSmem& S, const uint32_t* counts, uint32_t segs, uint32_t seg_cap,
+                                  bool* overflow) {
+    if (threadIdx.x == 0) {
+        S.bcast[2] = 0;
+        S.bcast[3] = 0;
+    }
+    __syncthreads();
+    for (uint32_t g = threadIdx.x; g < segs; g += blockDim.x) {
+        const uint32_t c = counts[g];
+        const uint32_t st = min(c, seg_cap);
+        S.segn[g] = st;
+        if (st) atomicAdd(&S.bcast[2], st);
+        if (c > seg_cap) atomicOr(&S.bcast[3], 1u);
+    }
+    __syncthreads();
+    const uint32_t n = S.bcast[2];
+    *overflow = S.bcast[3] != 0;
+    __syncthreads();
+    return n;
+}
+
+// Calls fn(index, valid) for every stored entry of a segmented list: warp w walks segments w,
+// w + 32, ..., its lanes 32 consecutive entries at a time, so every call is made by a full warp
+// (valid = false for the lanes past a segment's end) and fn may use warp collectives.
+template <class Fn>
+__device__ inline void for_each_segment_entry(const SelectSmem& S, uint32_t segs, uint32_t seg_cap, Fn fn) {
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (uint32_t g = warp; g < segs; g += blockDim.x >> 5) {
+        const uint32_t n = S.segn[g];
+        for (uint32_t o0 = 0; o0 < n; o0 += 32) fn(g * seg_cap + o0 + lane, o0 + lane < n);
+    }
 }
 
 template <class KeyFn>
@@ -159,15 +204,24 @@ __global__ void __launch_bounds__(kST) sample_threshold_kernel(SampleThresholdLa
     SelectSmem& S = *reinterpret_cast<SelectSmem*>(smem_raw);
     const uint32_t qi = L.qlist ? L.qlist[blockIdx.x] : blockIdx.x;
     const uint32_t k = L.topk[qi];
-    const uint32_t n = min(L.count[qi], L.cap);
-    float theta = -INFINITY;
+    bool lost = false;  // a sample segment that overflowed only lowers the sample's K-th best
+    const uint32_t n = load_segments(S, L.count + static_cast<uint64_t>(qi) * kMaxCandSegs, L.segs, L.seg_cap, &lost);
+    float theta = L.raise_only ? L.theta[qi] : -INFINITY;
     if (k > 0 && n >= k) {
         const float* sc = L.score + static_cast<uint64_t>(qi) * L.cap;
-        const uint32_t kk = kth_largest_u32([&](uint32_t i) { return float_key(sc[i]); }, n, k, S);
+        const uint32_t kk = kth_largest_u32_visit(
+            [&](auto fn) {
+                for_each_segment_entry(S, L.segs, L.seg_cap, [&](uint32_t i, bool ok) {
+                    if (ok) fn(float_key(sc[i]));
+                });
+            },
+            k, S);
         // k sample docs score >= t approximately, so the true K-th best exact score is >= t - eps_s;
         // a true top-K doc therefore scores >= t - eps_s - eps_m under the main pass's arithmetic.
-        theta = __fsub_rd(__fsub_rd(key_float(kk), L.eps_sample[qi]), L.eps_main[qi]);
+        const float t = __fsub_rd(__fsub_rd(key_float(kk), L.eps_sample[qi]), L.eps_main[qi]);
+        theta = L.raise_only ? fmaxf(theta, t) : t;
     }
+    __syncthreads();  // every thread has read the old theta
     if (threadIdx.x == 0) L.theta[qi] = theta;
 }
 
@@ -187,17 +241,23 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
         }
         return;
     }
-    const uint32_t cnt = L.cand_count[qi];
-    const uint32_t n = min(cnt, L.cap);
+    bool overflow = false;
+    const uint32_t n =
+        load_segments(S, L.cand_count + static_cast<uint64_t>(qi) * kMaxCandSegs, L.segs, L.seg_cap, &overflow);
     const float* sc = L.cand_score + row;
     const uint32_t* lc = L.cand_loc + row;
     const float eps = L.eps_main[qi];
-    if (cnt > L.cap) {
+    auto visit_scores = [&](auto fn) {
+        for_each_segment_entry(S, L.segs, L.seg_cap, [&](uint32_t i, bool ok) {
+            if (ok) fn(float_key(sc[i]));
+        });
+    };
+    if (overflow) {
         // The stored candidates are a subset of the qualifying docs, so their K-th best still bounds
         // the true K-th best from below: raise the threshold and let the host re-run this query.
         float theta = L.theta[qi];
         if (n >= k && k > 0) {
-            const uint32_t kk = kth_largest_u32([&](uint32_t i) { return float_key(sc[i]); }, n, k, S);
+            const uint32_t kk = kth_largest_u32_visit(visit_scores, k, S);
             theta = fmaxf(theta, __fsub_rd(key_float(kk), 2.0f * eps));
         }
         if (tid == 0) {
@@ -215,17 +275,16 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
     for (uint32_t i = tid; i < L.dim; i += blockDim.x) sq[i] = L.qry[static_cast<uint64_t>(qi) * L.dim + i];
     float thr = -INFINITY;
     if (n > kq) {
-        const uint32_t kk = kth_largest_u32([&](uint32_t i) { return float_key(sc[i]); }, n, kq, S);
+        const uint32_t kk = kth_largest_u32_visit(visit_scores, kq, S);
         thr = __fsub_rd(key_float(kk), 2.0f * eps);
     }
     if (tid == 0) S.counter = 0;
     __syncthreads();
     unsigned long long* ws = L.work + row;
-    for (uint32_t i0 = 0; i0 < n; i0 += blockDim.x) {
-        const uint32_t i = i0 + tid;
+    for_each_segment_entry(S, L.segs, L.seg_cap, [&](uint32_t i, bool ok) {
         bool take = false;
         unsigned long long key = 0;
-        if (i < n && sc[i] >= thr) {
+        if (ok && sc[i] >= thr) {
             const uint32_t loc = lc[i];
             const float e = exact_dot(sq, L.vec + static_cast<uint64_t>(loc) * L.dim, L.dim);
             key = result_key(e, loc);
@@ -240,7 +299,7 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
             base = __shfl_sync(0xffffffffu, base, leader);
             if (take) ws[base + __popc(mask & ((1u << lane) - 1u))] = key;
         }
-    }
+    });
     __syncthreads();
     const uint32_t nf = S.counter;
     __syncthreads();
@@ -397,8 +456,15 @@ cudaError_t set_smem(K kernel, size_t bytes) {
 
 }  // namespace
 
+namespace {
+bool bad_segments(uint32_t segs, uint32_t seg_cap, uint32_t cap) {
+    return segs == 0 || segs > kMaxCandSegs || seg_cap == 0 || static_cast<uint64_t>(segs) * seg_cap > cap;
+}
+}  // namespace
+
 cudaError_t launch_sample_threshold(const SampleThresholdLaunch& L, cudaStream_t stream) {
     if (L.nq_list == 0) return cudaSuccess;
+    if (bad_segments(L.segs, L.seg_cap, L.cap)) return cudaErrorInvalidValue;
     const size_t smem = sizeof(SelectSmem);
     cudaError_t e = set_smem(sample_threshold_kernel, smem);
     if (e != cudaSuccess) return e;
@@ -408,6 +474,7 @@ cudaError_t launch_sample_threshold(const SampleThresholdLaunch& L, cudaStream_t
 
 cudaError_t launch_select_topk(const SelectLaunch& L, cudaStream_t stream) {
     if (L.nq_list == 0) return cudaSuccess;
+    if (bad_segments(L.segs, L.seg_cap, L.cap)) return cudaErrorInvalidValue;
     const size_t smem = sizeof(SelectSmem) + static_cast<size_t>(L.dim) * sizeof(float);
     cudaError_t e = set_smem(select_topk_kernel, smem);
     if (e != cudaSuccess) return e;

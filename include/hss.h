@@ -163,13 +163,17 @@ typedef struct hss_searcher hss_searcher;
 typedef struct hss_filters hss_filters; /* compiled filter programs of one batch */
 
 typedef struct hss_searcher_config {
-    uint32_t maxBatch;     /* queries per batch (default 256) */
+    uint32_t maxBatch;     /* queries per batch (default 256; at most 256 for the tensor-core methods,
+                              4096 for SIMT: larger values are clamped) */
     uint32_t candidateCap; /* per-query candidate capacity (default 262144, >= HSS_MAX_TOPK) */
     uint32_t sampleDocs;   /* minimum doc sample for the candidate threshold (default 32768) */
     uint32_t maxRetries;   /* re-runs of a query whose candidates overflowed (default 4) */
     int32_t method;        /* candidate pass: 0 FP32 SIMT, 1 tensor cores TF32 over the FP32 rows,
                               2 tensor cores over a BF16 copy, 3 tensor cores over an FP8 E4M3 copy
                               with per-vector scales (every method returns the exact FP32 results) */
+    int32_t decodeInPlace; /* 0: filter over a dense bitmap of every posting, decoded once when the
+                              searcher is created if it takes at most 40% of free device memory;
+                              1: always decode the postings in place (no extra memory) */
 } hss_searcher_config;
 
 /* cfg may be NULL for the defaults. The searcher allocates its whole device arena here. */

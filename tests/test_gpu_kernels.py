@@ -29,13 +29,14 @@ def _bits_of(words, n):
     return np.unpackbits(np.ascontiguousarray(words).view(np.uint8), bitorder="little")[:n]
 
 
+@pytest.mark.parametrize("in_place", [False, True], ids=["dense_matrix", "in_place"])
 @pytest.mark.parametrize("layout", ["bitmap", "packed", "matrix"])
-def test_batched_filter_matches_oracle(torch_cuda, layout):
+def test_batched_filter_matches_oracle(torch_cuda, layout, in_place):
     torch = torch_cuda
     mix, vec, bits, table = _table(torch, layout)
     info = table.info
     exprs = data.make_filters(mix, 60, n_tags=(1, 6), seed=9) + _edge_filters()
-    s = hss.FullRecallSearcher(table, max_batch=len(exprs), candidate_cap=4096)
+    s = hss.FullRecallSearcher(table, max_batch=len(exprs), candidate_cap=4096, decode_in_place=in_place)
     f = s.compile_filters(exprs)
     words = info["segment_num"] * info["doc_num_per_segment"] // 64
     out = torch.zeros((len(exprs), words), dtype=torch.int64, device="cuda")

@@ -46,8 +46,9 @@ def test_cfg1_single_segment_top100(torch_cuda):
     _run(table, vec, bits, q, exprs, [100] * nq, max_batch=32)
 
 
+@pytest.mark.parametrize("in_place", [False, True], ids=["dense_matrix", "in_place"])
 @pytest.mark.parametrize("layout", ["bitmap", "packed", "matrix"])
-def test_many_segments_mixed_k(torch_cuda, layout):
+def test_many_segments_mixed_k(torch_cuda, layout, in_place):
     kw = {"bitmap": {}, "packed": {"sparse_packed": True}, "matrix": {"matrix_posting": True}}[layout]
     mix = data.Mixture(64, 96, (1e-3, 0.6), n_clusters=64, seed=4)
     vec, bits, _ = mix.corpus(20000, seed=14)  # 5 segments of 4096, the last one partial
@@ -57,7 +58,7 @@ def test_many_segments_mixed_k(torch_cuda, layout):
     exprs = data.make_filters(mix, nq, n_tags=(1, 6), seed=6, selectivity_range=(1e-4, 1.0))
     exprs[0], exprs[1], exprs[2], exprs[3] = "", "NOT 3", "3 AND NOT 3", "95"
     topks = np.array([1, 10, 100, 1000] * (nq // 4))
-    _run(table, vec, bits, q, exprs, topks, max_batch=48)
+    _run(table, vec, bits, q, exprs, topks, max_batch=48, decode_in_place=in_place)
 
 
 @pytest.mark.parametrize("levels", [2, 3, 8])
