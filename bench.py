@@ -38,7 +38,7 @@ FORMS = {"simt": "plain FP32 (SIMT FFMA candidate pass + exact FP32 rescoring)",
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--docs", type=int, default=10_000_000)
@@ -70,7 +70,9 @@ def workload(args, device):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms while running. Entering waits until
+    the first sample has been written (nvidia-smi takes a while to start); that sample predates the
+    timed region and is dropped from the summary."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -84,10 +86,13 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", self.gpu_id], stdout=self.out,
+                                          "-lms", "50", "-i", self.gpu_id], stdout=self.out,
                                          stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        t0 = time.time()
+        while self.proc and time.time() - t0 < 10 and os.path.getsize(self.out.name) == 0:
+            time.sleep(0.01)
         return self
 
     def __exit__(self, *a):
@@ -103,7 +108,7 @@ class ClockSampler:
         self.out.seek(0)
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.out.read().splitlines():
+        for line in self.out.read().splitlines()[1:]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue

@@ -390,7 +390,7 @@ class FullRecallSearcher {
     uint32_t* m_hOutCount = nullptr;
     // tensor-core pass
     int m_tcFormat = -1;  // TcFormat, or -1 for the SIMT pass
-    uint32_t m_tcKblocks = 0, m_tcStages = 0;
+    uint32_t m_tcKblocks = 0;
     CUtensorMap m_docMap{};
     CUtensorMap m_qryMap{};
     void* m_dStaged = nullptr;  // [256][dim] staged queries in the pass's format

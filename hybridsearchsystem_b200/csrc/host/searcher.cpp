@@ -157,11 +157,8 @@ bool FullRecallSearcher::Allocate() {
             m_err = "cuTensorMapEncodeTiled failed";
             return false;
         }
-        // as many k-block stages as shared memory holds next to the resident queries (2 halves)
-        const size_t budget = 232448;
-        const size_t fixed = tc_smem_bytes(2, m_tcKblocks, 0);
-        m_tcStages = static_cast<uint32_t>(std::min<size_t>(kMaxTcStages, (budget - fixed) / 16384));
-        if (m_tcStages < 2) {
+        // the resident queries (128 rows per SM) and at least two k-block stages fit shared memory
+        if (tc_pair_smem_bytes(m_tcKblocks, 2) > 232448 || tc_smem_bytes(1, m_tcKblocks, 2) > 232448) {
             m_err = "vector dimension too large for the tensor-core pass";
             return false;
         }
@@ -383,21 +380,34 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     if (m_timing) ck(cudaEventRecord(m_ev[1], stream));
 
     // Candidate passes. A pass covers tiles begin + i * step (or, with skip >= 2, all tiles that are not
-    // multiples of skip), i < countTiles, for `rows` queries (dList or 0..rows-1), and writes the
-    // list segments [segBase, segBase + its segments) of seg_cap entries each.
-    auto ctasOf = [&](uint64_t countTiles, uint32_t cap, bool simt) {
-        return (!tc || simt) ? cand_simt_segments(countTiles, m_numSms, cap)
-                             : tc_cand_segments(countTiles, m_numSms, cap);
+    // multiples of skip), i < countTiles, for `rows` queries (dList or 0..rows-1), and writes the list
+    // segments [segBase, segBase + its segments) of segCap entries each. Tiles hold unitOf() docs:
+    // 128 for the SIMT pass and the single-SM tensor-core pass, 256 for the SM-pair pass.
+    auto useSimt = [&](bool simt) { return !tc || simt; };
+    auto unitOf = [&](uint32_t rows, bool simt) { return useSimt(simt) ? 128u : tc_tile_docs(rows); };
+    auto tilesOf = [&](uint32_t unit) { return (T.GetDocNum() + unit - 1) / unit; };
+    auto ctasOf = [&](uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) {
+        return useSimt(simt) ? cand_simt_segments(countTiles, m_numSms, cap)
+                             : tc_cand_ctas(rows, countTiles, m_numSms, cap);
     };
-    auto segsOf = [&](uint64_t countTiles, uint32_t cap, bool simt) {
-        const uint32_t g = ctasOf(countTiles, cap, simt);
-        return (!tc || simt) ? g : 2 * g;  // a tensor-core CTA fills two segments
+    auto segsOf = [&](uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) {
+        const uint32_t g = ctasOf(rows, countTiles, cap, simt);
+        return useSimt(simt) ? g : 2 * g;  // a tensor-core CTA fills two segments
+    };
+    // entries per segment: the docs one segment can see at most, within the list's share
+    auto segCapOf = [&](uint32_t rows, uint64_t countTiles, uint32_t cap, uint32_t segs, bool simt) {
+        const uint32_t g = ctasOf(rows, countTiles, cap, simt);
+        // SIMT: a CTA's tiles; single SM: half of a CTA's tiles' docs; pair: a quarter of a pair's
+        const uint64_t groups = useSimt(simt) ? g : (unitOf(rows, simt) == 256 ? g / 2 : g);
+        const uint64_t perTile = useSimt(simt) ? 128ull : 64ull;
+        const uint64_t perSeg = (countTiles + groups - 1) / groups * perTile;
+        return static_cast<uint32_t>(std::min<uint64_t>(perSeg, cap / segs));
     };
     auto cand = [&](const float* theta, float* score, uint32_t* loc, uint32_t* count, uint32_t cap, uint32_t segBase,
                     uint32_t segCap, uint64_t begin, uint64_t step, uint32_t skip, uint64_t countTiles,
                     const uint32_t* dList, uint32_t rows, bool simt) {
-        const uint32_t g = ctasOf(countTiles, cap, simt);
-        if (!tc || simt) {
+        const uint32_t g = ctasOf(rows, countTiles, cap, simt);
+        if (useSimt(simt)) {
             CandLaunch C{};
             C.vec = T.DeviceVectors();
             C.qry = dQueries;
@@ -424,7 +434,6 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         TcCandLaunch C{};
         C.format = m_tcFormat;
         C.kblocks = m_tcKblocks;
-        C.stages = m_tcStages;
         C.doc_scale = T.DeviceDocScale();
         C.tile_scale = T.DeviceTileScale();
         C.q_scale = m_dQScale;
@@ -437,35 +446,31 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         C.cand_loc = loc;
         C.cand_count = count;
         C.cap = cap;
-        C.segs = g;
+        C.ctas = g;
         C.seg_cap = segCap;
         C.seg_base = segBase;
         C.tile_begin = begin;
         C.tile_step = step;
         C.tile_count = countTiles;
         C.tile_skip = skip;
+        C.tiles128 = tiles;
         C.error = m_dError;
         ck(launch_tc_cand(C, m_docMap, m_qryMap, m_numSms, stream));
-    };
-    // segment capacity of a pass over countTiles tiles into `segs` segments: the docs a segment can
-    // see at most, within the list's share
-    auto segCapOf = [&](uint64_t countTiles, uint32_t cap, uint32_t segs, bool simt) {
-        const uint32_t g = ctasOf(countTiles, cap, simt);
-        const uint64_t perSeg = (countTiles + g - 1) / g * ((!tc || simt) ? 128ull : 64ull);
-        return static_cast<uint32_t>(std::min<uint64_t>(perSeg, cap / segs));
     };
 
     // 1. doc sample: evenly spaced tiles, every filtered doc kept; its K-th best bounds the threshold
     const uint64_t want = std::max<uint64_t>(m_cfg.sampleDocs,
                                              (4ull * std::max<uint32_t>(maxK, 1u) * T.GetDocNum() +
                                               m_cfg.candidateCap - 1) / m_cfg.candidateCap);
-    const uint64_t sampTiles = std::min<uint64_t>(tiles, std::max<uint64_t>(1, (want + 127) / 128));
-    const uint64_t step = std::max<uint64_t>(1, tiles / sampTiles);
-    const uint64_t sampCount = std::min<uint64_t>(sampTiles, (tiles + step - 1) / step);
     auto sample = [&](const uint32_t* dList, uint32_t rows, bool simt) {
-        const uint32_t segs = segsOf(sampCount, m_sampCap, simt);
-        const uint32_t segCap = segCapOf(sampCount, m_sampCap, segs, simt);
-        cand(dNegInf, m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, segCap, 0, step, 0, sampCount, dList, rows,
+        const uint32_t unit = unitOf(rows, simt);
+        const uint64_t tilesU = tilesOf(unit);
+        const uint64_t sampTiles = std::min<uint64_t>(tilesU, std::max<uint64_t>(1, (want + unit - 1) / unit));
+        const uint64_t step = std::max<uint64_t>(1, tilesU / sampTiles);
+        const uint64_t count = std::min<uint64_t>(sampTiles, (tilesU + step - 1) / step);
+        const uint32_t segs = segsOf(rows, count, m_sampCap, simt);
+        const uint32_t segCap = segCapOf(rows, count, m_sampCap, segs, simt);
+        cand(dNegInf, m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, segCap, 0, step, 0, count, dList, rows,
              simt);
         SampleThresholdLaunch ST{};
         ST.score = m_dSampScore;
@@ -481,8 +486,9 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         ST.qlist = dList;
         ST.nq_list = rows;
         ck(launch_sample_threshold(ST, stream));
+        return count;
     };
-    sample(nullptr, nq, false);
+    const uint64_t sampCount = sample(nullptr, nq, false);
     launches += 2;
     if (m_timing) ck(cudaEventRecord(m_ev[2], stream));
 
@@ -491,7 +497,8 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     // (every doc of the top K scores at least K-th best - 2 eps) for the remaining tiles. Both parts'
     // candidates form one segmented list.
     const uint32_t C = m_cfg.candidateCap;
-    uint32_t split = static_cast<uint32_t>(std::sqrt(static_cast<double>(tiles) / static_cast<double>(sampCount)));
+    const uint64_t tilesM = tilesOf(unitOf(nq, false));
+    uint32_t split = static_cast<uint32_t>(std::sqrt(static_cast<double>(tilesM) / static_cast<double>(sampCount)));
     split = std::min<uint32_t>(split, 64);
     SelectLaunch SE{};
     SE.vec = T.DeviceVectors();
@@ -514,10 +521,10 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     SE.qlist = nullptr;
     SE.nq_list = nq;
     if (split >= 2) {
-        const uint64_t countA = (tiles + split - 1) / split, countB = tiles - countA;
-        const uint32_t segsA = segsOf(countA, C, false), segsB = segsOf(countB, C, false);
-        const uint32_t segCap =
-            std::min(segCapOf(countA, C, segsA + segsB, false), segCapOf(countB, C, segsA + segsB, false));
+        const uint64_t countA = (tilesM + split - 1) / split, countB = tilesM - countA;
+        const uint32_t segsA = segsOf(nq, countA, C, false), segsB = segsOf(nq, countB, C, false);
+        const uint32_t segCap = std::min(segCapOf(nq, countA, C, segsA + segsB, false),
+                                         segCapOf(nq, countB, C, segsA + segsB, false));
         cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, split, 0, countA, nullptr, nq, false);
         SampleThresholdLaunch RT{};
         RT.score = m_dCandScore;
@@ -538,10 +545,10 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         SE.segs = segsA + segsB;
         SE.seg_cap = segCap;
     } else {
-        const uint32_t segs = segsOf(tiles, C, false);
+        const uint32_t segs = segsOf(nq, tilesM, C, false);
         SE.segs = segs;
-        SE.seg_cap = segCapOf(tiles, C, segs, false);
-        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tiles, nullptr, nq, false);
+        SE.seg_cap = segCapOf(nq, tilesM, C, segs, false);
+        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tilesM, nullptr, nq, false);
         ++launches;
     }
     m_lastSegs.assign(nq, {SE.segs, SE.seg_cap});
@@ -581,16 +588,17 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
             // the plain path for these queries: SIMT bounds, a SIMT doc sample for a fresh threshold
             const double rel = SimtRelBound(dim);
             ck(launch_query_eps(dQueries, nq, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
-            sample(dQlist, nre, true);
+            (void)sample(dQlist, nre, true);
             launches += 3;
         } else if (tc) {
             stage(dQlist, nre);  // the staged rows become the re-run queries (their bounds unchanged)
             ++launches;
         }
         // one pass over every tile with the raised threshold
-        const uint32_t segs = segsOf(tiles, C, simt);
-        const uint32_t segCap = segCapOf(tiles, C, segs, simt);
-        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, 1, 0, tiles, dQlist, nre, simt);
+        const uint64_t tilesR = tilesOf(unitOf(nre, simt));
+        const uint32_t segs = segsOf(nre, tilesR, C, simt);
+        const uint32_t segCap = segCapOf(nre, tilesR, C, segs, simt);
+        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, 1, 0, tilesR, dQlist, nre, simt);
         for (uint32_t i = 0; i < nre; ++i) m_lastSegs[hQlist[i]] = {segs, segCap};
         SE.segs = segs;
         SE.seg_cap = segCap;

@@ -93,12 +93,11 @@ struct CandLaunch {
 };
 // Largest query count of one SIMT candidate pass (its per-query counts live in shared memory).
 constexpr uint32_t kMaxSimtBatch = 4096;
-// CTAs of a SIMT / tensor-core candidate pass over tile_count tiles into lists of `cap` entries:
-// the kernel's natural grid, but few enough that two passes' segments fit kMaxCandSegs with at least
-// kMinSegCap entries each (a small list split too finely would overflow on uneven segments).
+// CTAs of a SIMT candidate pass over tile_count tiles into lists of `cap` entries (one list segment
+// each): the kernel's natural grid, but few enough that two passes' segments fit kMaxCandSegs with
+// at least kMinSegCap entries each (a small list split too finely would overflow on uneven segments).
 constexpr uint32_t kMinSegCap = 256;
 uint32_t cand_simt_segments(uint64_t tile_count, int num_sms, uint32_t cap);
-uint32_t tc_cand_segments(uint64_t tile_count, int num_sms, uint32_t cap);
 
 // Threshold from the K-th best approximate score of a segmented list (segments [0, segs)):
 // theta = kth - eps_sample - eps_main. With raise_only the result is max(old theta, that), and a list
@@ -147,7 +146,7 @@ constexpr int kMaxTcStages = 12;
 struct TcCandLaunch {
     int format;                // TcFormat of both the corpus copy and the staged queries
     uint32_t kblocks;          // dim * element bytes / 128
-    uint32_t stages;           // k-block stages in the TMA ring
+    uint32_t stages;           // k-block stages in the TMA ring (set by launch_tc_cand)
     const float* doc_scale;    // E4M3: per-doc dequantisation scale
     const float2* tile_scale;  // E4M3: per 128-doc tile (min, max) of doc_scale
     const float* q_scale;      // E4M3: per staged query row
@@ -160,14 +159,22 @@ struct TcCandLaunch {
     uint32_t* cand_loc;
     uint32_t* cand_count;      // [nq][kMaxCandSegs]
     uint32_t cap;
-    uint32_t segs, seg_cap;    // segs = CTAs of the launch (tc_cand_segments)
-    uint32_t seg_base;         // first segment this pass writes
-    uint64_t tile_begin, tile_step, tile_count;
+    uint32_t ctas, seg_cap;    // CTAs of the launch (tc_cand_ctas); entries per list segment
+    uint32_t seg_base;         // first segment this pass writes (it writes 2 per CTA)
+    uint64_t tile_begin, tile_step, tile_count;  // tiles of tc_tile_docs(nq_rows) docs
     uint32_t tile_skip;
+    uint64_t tiles128;         // 128-doc tiles of the corpus (rows of the tensor map / 128)
     int32_t* error;            // device error bits (bounded waits that expired)
 };
 
+// Docs per tile of a tensor-core pass over `rows` staged queries: 128 (one SM per tile, rows <= 128)
+// or 256 (an SM pair per tile, cta_group::2, rows 129..256).
+uint32_t tc_tile_docs(uint32_t rows);
+// CTAs of a tensor-core pass over tile_count such tiles into lists of `cap` entries; it writes two
+// list segments per CTA.
+uint32_t tc_cand_ctas(uint32_t rows, uint64_t tile_count, int num_sms, uint32_t cap);
 size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages);
+size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages);
 cudaError_t launch_tc_cand(const TcCandLaunch& L, const CUtensorMap& doc_map, const CUtensorMap& qry_map, int sms,
                            cudaStream_t stream);
 // 2D tensor map over [rows][dim] elements of `format`, 128-byte swizzle, box {128 bytes, 128 rows}.

@@ -164,6 +164,81 @@ __device__ inline void mma_commit(unsigned long long* bar) {
 __device__ inline void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ inline void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
+// ---- SM-pair (cta_group::2) primitives ----
+__device__ inline uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// Address of the same shared-memory object in CTA `rank` of the cluster.
+__device__ inline uint32_t peer_addr(const void* p, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+    return r;
+}
+
+// Arrive on a barrier of another CTA of the cluster. Release at CTA scope (the default): what it
+// publishes are async-proxy results (TMA writes, completed TMEM reads) that are complete before the
+// arrive executes; a cluster-scope release would also wait for this thread's unrelated loads.
+__device__ inline void mbar_arrive_cluster(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+__device__ inline void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Wait on a local barrier that other CTAs of the cluster arrive on (acquire at cluster scope).
+__device__ inline bool mbar_try_cluster(unsigned long long* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Pair MMA: D (this CTA's 128 query rows x 256 doc columns, in each CTA's TMEM) += A (128 query rows in
+// each CTA) x B (128 doc rows in each CTA), issued by the even CTA for both.
+template <int F>
+__device__ inline void mma_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    if constexpr (F == kTcTF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    } else if constexpr (F == kTcBF16) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    }
+}
+
+// Arrives on `bar` (same offset) in both CTAs of the pair once the pair MMAs issued so far complete.
+__device__ inline void mma_commit_pair(unsigned long long* bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"(static_cast<unsigned short>(3))
+        : "memory");
+}
+
+// Arrives on this CTA's `bar` once the pair MMAs issued so far complete.
+__device__ inline void mma_commit_pair_local(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
 // 32 lanes x 32 consecutive FP32 columns; thread i gets lane (base lane + i). The registers are
 // written asynchronously: they are valid only after tmem_wait_ld() and a reg_fence() over them.
 __device__ inline void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
@@ -206,6 +281,45 @@ __device__ inline float max32(const uint32_t (&r)[32]) {
     return fmaxf(m, __uint_as_float(r[31]));
 }
 
+// One 32-doc chunk of a thread's E4M3 scores (its query, raw accumulators v): the docs whose filter
+// bit (m) is set and whose dequantised score clears the threshold go to the thread's list segment.
+// Warp-collective: the warp leaves at once when no lane's chunk clears its tile threshold t, and the
+// emission loop visits only doc positions that some lane keeps (E4M3's wide bound lets many chunks
+// through; for TF32 / BF16 the per-lane form in the kernels measured faster).
+template <int F>
+__device__ __forceinline__ void emit_chunk(bool live, uint32_t m, const uint32_t (&v)[32], float t, float theta,
+                                           float qs, const float* doc_scale, uint64_t doc0, float* out_score,
+                                           uint32_t* out_loc, uint32_t seg_cap, uint32_t& ncand) {
+    const bool hot = live && m != 0u && max32(v) >= t;
+    if (!__any_sync(0xffffffffu, hot)) return;
+    uint32_t pass = 0;
+    if (hot) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) pass |= (__uint_as_float(v[j]) >= t ? 1u : 0u) << j;
+        pass &= m;
+        if (F == kTcE4M3) {  // the tile threshold is conservative: apply the doc's own scale
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (((pass >> j) & 1u) && !(__uint_as_float(v[j]) * qs * doc_scale[doc0 + j] >= theta))
+                    pass &= ~(1u << j);
+        }
+    }
+    const uint32_t any = __reduce_or_sync(0xffffffffu, pass);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        if (!((any >> j) & 1u)) continue;  // warp-uniform
+        if ((pass >> j) & 1u) {
+            float sc = __uint_as_float(v[j]);
+            if (F == kTcE4M3) sc = sc * qs * doc_scale[doc0 + j];
+            if (ncand < seg_cap) {
+                out_score[ncand] = sc;
+                out_loc[ncand] = static_cast<uint32_t>(doc0 + j);
+            }
+            ++ncand;
+        }
+    }
+}
+
 template <int F, int H>
 __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_constant__ CUtensorMap doc_map,
                                                                   const __grid_constant__ CUtensorMap qry_map,
@@ -228,7 +342,7 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&S.acc_full[b], 1);
-            mbar_init(&S.acc_empty[b], 256 * H);
+            mbar_init(&S.acc_empty[b], 8 * H);  // one arrival per epilogue warp
         }
         mbar_init(&S.qbar, 1);
         mbar_init(&S.drain, 1);
@@ -327,12 +441,16 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
         const uint32_t seg_cap = L.seg_cap;
         uint32_t ncand = 0;
         uint32_t iter = 0;
+        // the query's filter bits of this thread's 64 docs, loaded one tile ahead so the (uncoalesced)
+        // load is in flight during the previous tile's work
+        uint64_t fw_next = 0;
+        if (valid && blockIdx.x < ntiles) fw_next = brow[pass_tile(L.tile_begin, L.tile_step, L.tile_skip, blockIdx.x) * 2 + colh];
         for (uint64_t it = blockIdx.x; it < ntiles; it += gridDim.x, ++iter) {
             const uint32_t buf = iter & 1u;
             const uint64_t tile = pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it);
-            // the query's filter bits of this thread's 64 docs, fetched before the accumulator wait
-            // so the load overlaps the tile's MMAs
-            const uint64_t fw = valid ? brow[tile * 2 + colh] : 0ull;
+            const uint64_t fw = fw_next;
+            if (valid && it + gridDim.x < ntiles)
+                fw_next = brow[pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it + gridDim.x) * 2 + colh];
             // threshold on the raw accumulator: acc * qs * ds >= theta
             float t = theta;
             if (F == kTcE4M3) {
@@ -347,7 +465,10 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
             bool live[2];
 #pragma unroll
             for (int c = 0; c < 2; ++c) live[c] = __any_sync(0xffffffffu, m[c] != 0u);
-            if (!mbar_wait(&S.acc_full[buf], (iter >> 1) & 1u, S, L.error, 16)) break;
+            // every lane waits; the warp leaves together if any lane gave up (the warp collectives
+            // below need all 32 lanes)
+            const bool ready = mbar_wait(&S.acc_full[buf], (iter >> 1) & 1u, S, L.error, 16);
+            if (!__all_sync(0xffffffffu, ready)) break;
             fence_after();
             const uint32_t tbase = tmem + ((sub * 32u) << 16) + (buf * H + half) * 128u + colh * 64u;
             uint32_t v[2][32];
@@ -359,33 +480,31 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
             for (int c = 0; c < 2; ++c) reg_fence(v[c]);
             // the accumulator is in registers: hand the TMEM buffer back to the MMA issuer now
             fence_before();
-            mbar_arrive(&S.acc_empty[buf]);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&S.acc_empty[buf]);
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
-                if (!live[c] || m[c] == 0u) continue;
-                if (!(max32(v[c]) >= t)) continue;
-                uint32_t pass = 0;
-#pragma unroll
-                for (int j = 0; j < 32; ++j) pass |= (__uint_as_float(v[c][j]) >= t ? 1u : 0u) << j;
-                pass &= m[c];
                 const uint64_t doc0 = tile * kRows + colh * 64u + c * 32u;
-                if (F == kTcE4M3) {  // the tile threshold is conservative: apply the doc's own scale
+                if constexpr (F == kTcE4M3) {
+                    emit_chunk<F>(live[c], m[c], v[c], t, theta, qs, L.doc_scale, doc0, out_score, out_loc, seg_cap,
+                                  ncand);
+                } else {
+                    if (!live[c] || m[c] == 0u) continue;
+                    if (!(max32(v[c]) >= t)) continue;
+                    uint32_t pass = 0;
 #pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                        if (((pass >> j) & 1u) && !(__uint_as_float(v[c][j]) * qs * L.doc_scale[doc0 + j] >= theta))
-                            pass &= ~(1u << j);
-                }
-                if (pass == 0u) continue;
+                    for (int j = 0; j < 32; ++j) pass |= (__uint_as_float(v[c][j]) >= t ? 1u : 0u) << j;
+                    pass &= m[c];
+                    if (pass == 0u) continue;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    if (!((pass >> j) & 1u)) continue;
-                    float sc = __uint_as_float(v[c][j]);
-                    if (F == kTcE4M3) sc = sc * qs * L.doc_scale[doc0 + j];
-                    if (ncand < seg_cap) {
-                        out_score[ncand] = sc;
-                        out_loc[ncand] = static_cast<uint32_t>(doc0 + j);
+                    for (int j = 0; j < 32; ++j) {
+                        if (!((pass >> j) & 1u)) continue;
+                        if (ncand < seg_cap) {
+                            out_score[ncand] = __uint_as_float(v[c][j]);
+                            out_loc[ncand] = static_cast<uint32_t>(doc0 + j);
+                        }
+                        ++ncand;
                     }
-                    ++ncand;
                 }
             }
         }
@@ -405,29 +524,323 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
     }
 }
 
-template <int F, int H>
-cudaError_t launch_tc_typed(const TcCandLaunch& L, const CUtensorMap& dmap, const CUtensorMap& qmap, int sms,
-                            cudaStream_t stream) {
-    const size_t smem = tc_smem_bytes(H, L.kblocks, L.stages);
-    cudaError_t e = cudaFuncSetAttribute(tc_cand_kernel<F, H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// ---------------------------------------------------------------------------------------------
+// SM-pair candidate pass (rows 129..256). A cluster of two CTAs on two SMs computes D[256 queries,
+// 256 docs] per tile with one cta_group::2 MMA per 32 bytes of K: CTA r holds queries
+// [128 r, 128 r + 128) (A) and streams docs [256 t + 128 r, +128) of tile t (B); each CTA's TMEM holds
+// its 128 query rows x 256 doc columns. Per MMA each SM reads 8 KB of shared memory for 128 x 256
+// outputs -- half the operand traffic per output of the single-SM form, which saturates shared
+// memory bandwidth before the tensor pipe.
+//
+// Each CTA's TMA loads complete on its own barriers; warp 1 of the odd CTA forwards each completed
+// stage (and the queries) to the even CTA with a remote arrive, so each CTA can always drain its own
+// copies. The even CTA's warp 1 issues the MMAs and commits them to both CTAs' barriers. Epilogue
+// warps of both CTAs return an accumulator buffer with a remote arrive on the even CTA's acc_empty.
+struct PairShared {
+    unsigned long long full[kMaxTcStages];   // this CTA's stage loaded (TMA)
+    unsigned long long empty[kMaxTcStages];  // stage free (pair MMA commit, both CTAs)
+    unsigned long long pfull[kMaxTcStages];  // even CTA: the odd CTA's stage loaded (forwarded)
+    unsigned long long acc_full[2];          // accumulator buffer ready (pair MMA commit, both CTAs)
+    unsigned long long acc_empty[2];         // even CTA: buffer drained by the epilogue warps of both CTAs
+    unsigned long long qbar;                 // this CTA's queries loaded
+    unsigned long long pqbar;                // even CTA: the odd CTA's queries loaded (forwarded)
+    unsigned long long drain;
+    uint32_t tmem_base;
+    uint32_t n_issued, n_consumed;  // stage loads issued by TMA / waited for by the MMA issuer or forwarder
+    volatile int abort;
+};
+
+constexpr int kPairEpiWarps = 16;  // 4 column groups x 4 TMEM lane quarters
+constexpr int kPairThreads = 64 + 32 * kPairEpiWarps;
+
+template <int F>
+__device__ inline bool pair_wait(unsigned long long* bar, uint32_t parity, PairShared& S, int32_t* err, int code,
+                                 bool cluster_scope) {
+    const long long t0 = clock64();
+    while (!(cluster_scope ? mbar_try_cluster(bar, parity) : mbar_try(bar, parity))) {
+        if (S.abort) return false;
+        if (clock64() - t0 > kWaitBudget) {
+            S.abort = 1;
+            if (err) atomicOr(err, code);
+            return false;
+        }
+    }
+    return true;
+}
+
+template <int F>
+__global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_constant__ CUtensorMap doc_map,
+                                                                  const __grid_constant__ CUtensorMap qry_map,
+                                                                  TcCandLaunch L) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t kb_n = L.kblocks;
+    unsigned char* qsm = base;
+    unsigned char* ring = base + static_cast<size_t>(kb_n) * kStageBytes;
+    PairShared& S = *reinterpret_cast<PairShared*>(ring + static_cast<size_t>(L.stages) * kStageBytes);
+
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t stages = L.stages;
+    const uint32_t rank = cluster_rank();
+    const uint32_t pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < stages; ++s) {
+            mbar_init(&S.full[s], 1);
+            mbar_init(&S.empty[s], 1);
+            mbar_init(&S.pfull[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&S.acc_full[b], 1);
+            mbar_init(&S.acc_empty[b], 2 * kPairEpiWarps);
+        }
+        mbar_init(&S.qbar, 1);
+        mbar_init(&S.pqbar, 1);
+        mbar_init(&S.drain, 1);
+        S.abort = 0;
+        S.n_issued = 0;
+        S.n_consumed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
+                     "r"(512u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    __syncthreads();
+    cluster_sync();  // both CTAs' barriers are initialised before any remote arrive
+    fence_after();
+    const uint32_t tmem = S.tmem_base;
+    const uint64_t ntiles = L.tile_count;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            mbar_expect_tx(&S.qbar, kb_n * kStageBytes);
+            for (uint32_t kb = 0; kb < kb_n; ++kb)
+                tma_load_2d(qsm + static_cast<size_t>(kb) * kStageBytes, &qry_map,
+                            static_cast<int>(kb * (128 / Fmt<F>::elem)), static_cast<int>(rank * kRows), &S.qbar);
+            uint32_t n = 0;
+            for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs) {
+                const int y = static_cast<int>(pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it) * 2 * kRows +
+                                               rank * kRows);
+                for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                    const uint32_t s = n % stages, ph = (n / stages) & 1u;
+                    if (!pair_wait<F>(&S.empty[s], ph ^ 1u, S, L.error, 1, false)) break;
+                    mbar_expect_tx(&S.full[s], kStageBytes);
+                    tma_load_2d(ring + static_cast<size_t>(s) * kStageBytes, &doc_map,
+                                static_cast<int>(kb * (128 / Fmt<F>::elem)), y, &S.full[s]);
+                }
+            }
+            S.n_issued = n;
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && rank == 1) {
+            // forwarder: the even CTA's MMAs read this CTA's queries and stages; tell it when they land
+            uint32_t n = 0;
+            if (pair_wait<F>(&S.qbar, 0, S, L.error, 2, false)) {
+                mbar_arrive_cluster(peer_addr(&S.pqbar, 0));
+                for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs) {
+                    bool ok = true;
+                    for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                        const uint32_t s = n % stages, ph = (n / stages) & 1u;
+                        if (!pair_wait<F>(&S.full[s], ph, S, L.error, 8, false)) {
+                            ok = false;
+                            break;
+                        }
+                        mbar_arrive_cluster(peer_addr(&S.pfull[s], 0));
+                    }
+                    if (!ok) break;
+                }
+            }
+            S.n_consumed = n;
+        } else if (lane == 0) {
+            // MMA issuer of the pair
+            constexpr uint32_t idesc =
+                (1u << 4) | (Fmt<F>::ab << 7) | (Fmt<F>::ab << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
+            uint32_t n = 0, iter = 0;
+            bool ok = pair_wait<F>(&S.qbar, 0, S, L.error, 2, false) && pair_wait<F>(&S.pqbar, 0, S, L.error, 2, true);
+            for (uint64_t it = pair; ok && it < ntiles && !S.abort; it += npairs, ++iter) {
+                const uint32_t buf = iter & 1u;
+                if (!pair_wait<F>(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4, true)) break;
+                fence_after();
+                for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                    const uint32_t s = n % stages, ph = (n / stages) & 1u;
+                    if (!pair_wait<F>(&S.full[s], ph, S, L.error, 8, false) ||
+                        !pair_wait<F>(&S.pfull[s], ph, S, L.error, 8, true)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint64_t adesc = smem_desc(smem_u32(qsm + static_cast<size_t>(kb) * kStageBytes));
+                    const uint64_t bdesc = smem_desc(smem_u32(ring + static_cast<size_t>(s) * kStageBytes));
+#pragma unroll
+                    for (uint32_t ks = 0; ks < 4; ++ks)  // 32 bytes of K per instruction
+                        mma_pair<F>(tmem + buf * 256u, adesc + ks * 2u, bdesc + ks * 2u, idesc, (kb | ks) != 0);
+                    mma_commit_pair(&S.empty[s]);  // frees the stage in both CTAs once read
+                }
+                if (!ok) break;
+                mma_commit_pair(&S.acc_full[buf]);
+            }
+            S.n_consumed = n;
+            mma_commit_pair_local(&S.drain);  // every pair MMA issued has completed
+            if (!mbar_wait_drain(&S.drain, 0) && L.error) atomicOr(L.error, 32);
+        }
+    } else {
+        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (query rows) and doc columns
+        // [64 g, 64 g + 64) of the 256, g = (w - 2) / 4. A thread owns one query row and one 64-doc
+        // column group for the whole launch: candidates go to its own list segment, no atomics.
+        const uint32_t g = (warp - 2) / 4;
+        const uint32_t sub = warp & 3u;
+        const uint32_t row = rank * 128u + sub * 32u + lane;
+        const bool valid = row < L.nq_rows;
+        const uint32_t qi = valid ? (L.qlist ? L.qlist[row] : row) : 0u;
+        const float theta = valid ? L.theta[qi] : INFINITY;
+        const float qs = (F == kTcE4M3 && valid) ? L.q_scale[row] : 1.0f;
+        const uint64_t* brow = L.bits + static_cast<uint64_t>(qi) * L.bits_stride;
+        const uint32_t segment = L.seg_base + 4u * pair + g;
+        const uint64_t seg = static_cast<uint64_t>(qi) * L.cap + static_cast<uint64_t>(segment) * L.seg_cap;
+        float* out_score = L.cand_score + seg;
+        uint32_t* out_loc = L.cand_loc + seg;
+        const uint32_t seg_cap = L.seg_cap;
+        const uint32_t acc_empty_addr0 = peer_addr(&S.acc_empty[0], 0);
+        const uint32_t acc_empty_addr1 = peer_addr(&S.acc_empty[1], 0);
+        uint32_t ncand = 0;
+        uint32_t iter = 0;
+        // filter word of this thread's 64 docs of a tile (past the bitmap: none pass)
+        auto word_of = [&](uint64_t it) -> uint64_t {
+            const uint64_t w = pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it) * 4 + g;
+            return (valid && w < L.bits_stride) ? brow[w] : 0ull;
+        };
+        uint64_t fw_next = pair < ntiles ? word_of(pair) : 0ull;
+        for (uint64_t it = pair; it < ntiles; it += npairs, ++iter) {
+            const uint32_t buf = iter & 1u;
+            const uint64_t tile = pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it);
+            const uint64_t fw = fw_next;
+            if (it + npairs < ntiles) fw_next = word_of(it + npairs);
+            float t = theta;
+            if (F == kTcE4M3) {
+                uint64_t ts = tile * 2 + g / 2;  // 128-doc tile holding this thread's docs
+                ts = ts < L.tiles128 ? ts : L.tiles128 - 1;
+                const float2 mm = L.tile_scale[ts];
+                const float tq = theta / qs;
+                t = tq > 0.0f ? tq / mm.y : tq / mm.x;
+                t = t == t ? t : -INFINITY;
+                t = __fmul_rd(t, 1.0f - 1e-6f) - 1e-30f;
+            }
+            const uint32_t m[2] = {static_cast<uint32_t>(fw), static_cast<uint32_t>(fw >> 32)};
+            bool live[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) live[c] = __any_sync(0xffffffffu, m[c] != 0u);
+            const bool ready = pair_wait<F>(&S.acc_full[buf], (iter >> 1) & 1u, S, L.error, 16, false);
+            if (!__all_sync(0xffffffffu, ready)) break;
+            fence_after();
+            const uint32_t tbase = tmem + ((sub * 32u) << 16) + buf * 256u + g * 64u;
+            uint32_t v[2][32];
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                if (live[c]) tmem_ld32(tbase + c * 32u, v[c]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 2; ++c) reg_fence(v[c]);
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(buf ? acc_empty_addr1 : acc_empty_addr0);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const uint64_t doc0 = tile * 256u + g * 64u + c * 32u;
+                if constexpr (F == kTcE4M3) {
+                    emit_chunk<F>(live[c], m[c], v[c], t, theta, qs, L.doc_scale, doc0, out_score, out_loc, seg_cap,
+                                  ncand);
+                } else {
+                    if (!live[c] || m[c] == 0u) continue;
+                    if (!(max32(v[c]) >= t)) continue;
+                    uint32_t pass = 0;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) pass |= (__uint_as_float(v[c][j]) >= t ? 1u : 0u) << j;
+                    pass &= m[c];
+                    if (pass == 0u) continue;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (!((pass >> j) & 1u)) continue;
+                        if (ncand < seg_cap) {
+                            out_score[ncand] = __uint_as_float(v[c][j]);
+                            out_loc[ncand] = static_cast<uint32_t>(doc0 + j);
+                        }
+                        ++ncand;
+                    }
+                }
+            }
+        }
+        if (valid) L.cand_count[static_cast<uint64_t>(qi) * kMaxCandSegs + segment] = ncand;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && S.n_consumed < S.n_issued) {
+        // aborted: wait (bounded) for this CTA's copies still landing in its stage ring
+        for (uint32_t k = S.n_consumed; k < S.n_issued; ++k)
+            if (!mbar_wait_drain(&S.full[k % stages], (k / stages) & 1u)) break;
+    }
+    if (threadIdx.x == 0 && !mbar_try(&S.qbar, 0)) mbar_wait_drain(&S.qbar, 0);
+    __syncthreads();
+    // neither CTA leaves (or frees TMEM) while the pair's MMAs or the other CTA's remote arrives may
+    // still touch its shared memory
+    cluster_sync();
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u));
+    }
+}
+
+template <int F>
+cudaError_t launch_tc2_typed(const TcCandLaunch& L, const CUtensorMap& dmap, const CUtensorMap& qmap,
+                             cudaStream_t stream) {
+    const size_t smem = tc_pair_smem_bytes(L.kblocks, L.stages);
+    cudaError_t e = cudaFuncSetAttribute(tc2_cand_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    // CTA b writes segments seg_base + 2b and seg_base + 2b + 1
-    const uint64_t seg_end = static_cast<uint64_t>(L.seg_base) + 2ull * L.segs;
-    if (L.segs != tc_cand_segments(L.tile_count, sms, L.cap) || L.seg_cap == 0 || seg_end > kMaxCandSegs ||
-        seg_end * L.seg_cap > L.cap)
-        return cudaErrorInvalidValue;
-    tc_cand_kernel<F, H><<<L.segs, 64 + 256 * H, smem, stream>>>(dmap, qmap, L);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(L.ctas, 1, 1);
+    cfg.blockDim = dim3(kPairThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, tc2_cand_kernel<F>, dmap, qmap, L);
+}
+
+template <int F>
+cudaError_t launch_tc1_typed(const TcCandLaunch& L, const CUtensorMap& dmap, const CUtensorMap& qmap,
+                             cudaStream_t stream) {
+    const size_t smem = tc_smem_bytes(1, L.kblocks, L.stages);
+    cudaError_t e = cudaFuncSetAttribute(tc_cand_kernel<F, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    tc_cand_kernel<F, 1><<<L.ctas, 64 + 256, smem, stream>>>(dmap, qmap, L);
     return cudaGetLastError();
 }
 
+constexpr size_t kSmemBudget = 232448;  // dynamic shared memory of one CTA
+
 }  // namespace
 
-uint32_t tc_cand_segments(uint64_t tile_count, int num_sms, uint32_t cap) {
-    uint64_t g = tile_count < static_cast<uint64_t>(num_sms) ? tile_count : static_cast<uint64_t>(num_sms);
-    g = g < kMaxCandSegs / 4 ? g : kMaxCandSegs / 4;  // two segments per CTA, room for two passes
-    const uint64_t by_cap = cap / (4 * kMinSegCap) > 0 ? cap / (4 * kMinSegCap) : 1;
-    return static_cast<uint32_t>(g < by_cap ? g : by_cap);
+uint32_t tc_tile_docs(uint32_t rows) { return rows > 128 ? 256u : 128u; }
+
+uint32_t tc_cand_ctas(uint32_t rows, uint64_t tile_count, int num_sms, uint32_t cap) {
+    // every CTA fills two list segments; two passes' segments must fit kMaxCandSegs with at least
+    // kMinSegCap entries each
+    const uint64_t unit = rows > 128 ? 2 : 1;  // CTAs per tile group
+    uint64_t g = static_cast<uint64_t>(num_sms) / unit;
+    g = tile_count < g ? tile_count : g;
+    const uint64_t by_segs = kMaxCandSegs / (4 * unit);
+    g = g < by_segs ? g : by_segs;
+    uint64_t by_cap = cap / (4 * unit * kMinSegCap);
+    by_cap = by_cap > 0 ? by_cap : 1;
+    g = g < by_cap ? g : by_cap;
+    return static_cast<uint32_t>(g * unit);
 }
 
 size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages) {
@@ -435,18 +848,34 @@ size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages) {
            sizeof(TcShared);
 }
 
-cudaError_t launch_tc_cand(const TcCandLaunch& L, const CUtensorMap& doc_map, const CUtensorMap& qry_map, int sms,
+size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages) {
+    return 1024 + static_cast<size_t>(kblocks) * kStageBytes + static_cast<size_t>(stages) * kStageBytes +
+           sizeof(PairShared);
+}
+
+cudaError_t launch_tc_cand(const TcCandLaunch& Lin, const CUtensorMap& doc_map, const CUtensorMap& qry_map, int sms,
                            cudaStream_t stream) {
-    if (L.tile_count == 0 || L.nq_rows == 0) return cudaSuccess;
-    if (L.stages < 2 || L.stages > static_cast<uint32_t>(kMaxTcStages) || L.kblocks == 0) return cudaErrorInvalidValue;
-    const int H = L.nq_rows > 128 ? 2 : 1;
+    if (Lin.tile_count == 0 || Lin.nq_rows == 0) return cudaSuccess;
+    if (Lin.kblocks == 0 || Lin.nq_rows > 256 || Lin.tiles128 == 0) return cudaErrorInvalidValue;
+    TcCandLaunch L = Lin;
+    const bool pair = L.nq_rows > 128;
+    // as many stages as shared memory holds next to the resident queries
+    const size_t fixed = pair ? tc_pair_smem_bytes(L.kblocks, 0) : tc_smem_bytes(1, L.kblocks, 0);
+    if (fixed + 2 * kStageBytes > kSmemBudget) return cudaErrorInvalidValue;
+    const size_t st = (kSmemBudget - fixed) / kStageBytes;
+    L.stages = static_cast<uint32_t>(st < static_cast<size_t>(kMaxTcStages) ? st : kMaxTcStages);
+    // every CTA writes segments seg_base + 2 b and seg_base + 2 b + 1 (pair: 4 per pair)
+    const uint64_t seg_end = static_cast<uint64_t>(L.seg_base) + 2ull * L.ctas;
+    if (L.ctas != tc_cand_ctas(L.nq_rows, L.tile_count, sms, L.cap) || L.seg_cap == 0 || seg_end > kMaxCandSegs ||
+        seg_end * L.seg_cap > L.cap)
+        return cudaErrorInvalidValue;
     switch (L.format) {
-        case kTcTF32: return H == 2 ? launch_tc_typed<kTcTF32, 2>(L, doc_map, qry_map, sms, stream)
-                                    : launch_tc_typed<kTcTF32, 1>(L, doc_map, qry_map, sms, stream);
-        case kTcBF16: return H == 2 ? launch_tc_typed<kTcBF16, 2>(L, doc_map, qry_map, sms, stream)
-                                    : launch_tc_typed<kTcBF16, 1>(L, doc_map, qry_map, sms, stream);
-        case kTcE4M3: return H == 2 ? launch_tc_typed<kTcE4M3, 2>(L, doc_map, qry_map, sms, stream)
-                                    : launch_tc_typed<kTcE4M3, 1>(L, doc_map, qry_map, sms, stream);
+        case kTcTF32: return pair ? launch_tc2_typed<kTcTF32>(L, doc_map, qry_map, stream)
+                                  : launch_tc1_typed<kTcTF32>(L, doc_map, qry_map, stream);
+        case kTcBF16: return pair ? launch_tc2_typed<kTcBF16>(L, doc_map, qry_map, stream)
+                                  : launch_tc1_typed<kTcBF16>(L, doc_map, qry_map, stream);
+        case kTcE4M3: return pair ? launch_tc2_typed<kTcE4M3>(L, doc_map, qry_map, stream)
+                                  : launch_tc1_typed<kTcE4M3>(L, doc_map, qry_map, stream);
     }
     return cudaErrorInvalidValue;
 }

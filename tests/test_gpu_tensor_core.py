@@ -61,12 +61,13 @@ def test_approximate_pass_respects_its_bound(torch_cuda, method, nq):
         assert (scores[i][:c].view(np.uint32) == want[0][i][:c].view(np.uint32)).all()
 
 
+@pytest.mark.parametrize("nq", [96, 256], ids=["one_sm", "sm_pair"])
 @pytest.mark.parametrize("method", list(METHODS))
-def test_tensor_core_search_is_exact_mixed_k(torch_cuda, method):
+def test_tensor_core_search_is_exact_mixed_k(torch_cuda, method, nq):
+    # 40000 docs = 313 tiles of 128: the SM-pair pass (more than 128 queries) ends on a half tile
     mix = data.Mixture(128, 128, (1e-3, 0.6), n_clusters=128, seed=41)
     vec, bits, _ = mix.corpus(40000, seed=42)
     table = hss.DataTable.build(vec, bits, 128, device=0, doc_num_per_segment=16384, sparse_packed=True)
-    nq = 96
     q = mix.queries(nq, seed=43)
     exprs = data.make_filters(mix, nq, n_tags=(1, 6), seed=44, selectivity_range=(1e-4, 1.0))
     topks = np.array([1, 10, 100, 1000] * (nq // 4))
@@ -82,14 +83,14 @@ def test_tensor_core_search_is_exact_mixed_k(torch_cuda, method):
         assert (scores[i][:c].view(np.uint32) == ws[i][:c].view(np.uint32)).all(), (method, i)
 
 
+@pytest.mark.parametrize("nq", [24, 160], ids=["one_sm", "sm_pair"])
 @pytest.mark.parametrize("method", list(METHODS))
-def test_tensor_core_overflow_reruns_are_exact(torch_cuda, method):
+def test_tensor_core_overflow_reruns_are_exact(torch_cuda, method, nq):
     mix = data.Mixture(128, 32, (0.3, 0.9), n_clusters=8, seed=51)
     vec, bits, _ = mix.corpus(50000, seed=52)
     table = hss.DataTable.build(vec, bits, 32, device=0, doc_num_per_segment=8192)
-    nq = 24
     q = mix.queries(nq, seed=53)
-    exprs = [""] * 12 + ["1 OR 2"] * 12
+    exprs = [""] * (nq // 2) + ["1 OR 2"] * (nq - nq // 2)
     s = hss.FullRecallSearcher(table, max_batch=nq, candidate_cap=4096, sample_docs=4096, method=METHODS[method])
     for a, e in zip(q, exprs):
         s.add_query(e, a, 3000)
