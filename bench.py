@@ -57,6 +57,23 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+def max_over_ranks(ms, device):
+    """The slowest rank's time: every rank's number, all-reduced with MAX (one collective, taken by
+    every rank in the same order)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_qps(world, steps, batch, t_max_ms):
+    """Weak scaling: every rank serves `steps` batches of `batch` queries; the job takes the slowest
+    rank's time."""
+    return world * steps * batch / (t_max_ms / 1e3)
+
+
 def workload(args, device):
     from hybridsearchsystem_b200 import data
     mix = data.Mixture(128, 256, (1e-4, 0.6), n_clusters=1024, sigma=0.3, n_corr=16, seed=1)
@@ -252,11 +269,8 @@ def run_ours(args):
         barrier()
     t_ms = ev0.elapsed_time(ev1)
     clocks = clk.summary()
-    t_max = torch.tensor([t_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    t_max = float(t_max.item())
-    value = world * args.steps * B / (t_max / 1e3)
+    t_max = max_over_ranks(t_ms, dev)
+    value = whole_job_qps(world, args.steps, B, t_max)
 
     # end-to-end leg through the C-ABI: pinned host queries in, results out, every step
     h_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1)).pin_memory()
@@ -282,10 +296,7 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1)], device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    e2e = world * args.steps * B / (float(e2e_ms.item()) / 1e3)
+    e2e = whole_job_qps(world, args.steps, B, max_over_ranks(e0.elapsed_time(e1), dev))
 
     # roofline of the dominant kernel (the candidate pass): algorithmic bytes per launch = the corpus
     # (docs x 128 x 4 B) + the batch's filter bitmaps (B x docs/8 B)

@@ -131,60 +131,91 @@ __device__ inline uint64_t tail_mask(uint64_t gw, uint64_t doc_num) {
     return valid >= 64 ? ~0ull : ((1ull << valid) - 1);
 }
 
-// Postfix evaluation of one word: the reference's interpretation of the program
-// (kernel_bitmap_text_filter.cpp:52-119). Returns false for a malformed program.
-__device__ inline bool eval_word(const uint32_t* prog, uint32_t plen, const uint64_t* slots, uint32_t slot_stride,
-                                 uint32_t w, uint32_t nop, uint64_t* result) {
-    uint64_t st[kMaxStack];
-    int sp = 0;
-    uint32_t next = 0, pc = 0;
+// Postfix evaluation of W words at once (words w0 + k * step, k < W), the reference's interpretation
+// of the program (kernel_bitmap_text_filter.cpp:52-119): [AND|OR|NOT, postingNum, stackNum] combines
+// the next postingNum operands with stackNum popped results, [CONJUNCTION, parts, n_1..n_parts] ANDs
+// the ORs of consecutive operand groups. Every op is decoded and checked once and applied to all W
+// words, so the per-op decode cost is shared. Returns false for a malformed program.
+template <int W>
+__device__ inline bool eval_words(const uint32_t* prog, uint32_t plen, const uint64_t* slots, uint32_t slot_stride,
+                                  uint32_t w0, uint32_t step, uint32_t nop, uint64_t (&result)[W]) {
+    uint64_t st[kMaxStack][W];
+    uint32_t sp = 0, next = 0, pc = 0;
     while (pc < plen) {
         const uint32_t op = prog[pc];
+        uint64_t acc[W];
         if (op == kOpAnd || op == kOpOr || op == kOpNot) {
             if (pc + 2 >= plen) return false;
             const uint32_t pn = prog[pc + 1], sn = prog[pc + 2];
             pc += 3;
             const bool ok = op == kOpNot ? (pn + sn == 1) : (pn + sn > 0);
-            if (!ok || next + pn > nop || sn > static_cast<uint32_t>(sp)) return false;
-            uint64_t acc;
+            if (!ok || next + pn > nop || sn > sp) return false;
+            const uint64_t* row = slots + static_cast<uint64_t>(next) * slot_stride + w0;
             if (op == kOpNot) {
-                acc = pn ? ~slots[next * slot_stride + w] : ~st[--sp];
-            } else {
-                acc = op == kOpAnd ? ~0ull : 0ull;
-                for (uint32_t k = 0; k < pn; ++k) {
-                    const uint64_t v = slots[(next + k) * slot_stride + w];
-                    acc = op == kOpAnd ? (acc & v) : (acc | v);
+                if (pn) {
+#pragma unroll
+                    for (int k = 0; k < W; ++k) acc[k] = ~row[k * step];
+                } else {
+                    --sp;
+#pragma unroll
+                    for (int k = 0; k < W; ++k) acc[k] = ~st[sp][k];
                 }
-                for (uint32_t k = 0; k < sn; ++k) {
-                    const uint64_t v = st[--sp];
-                    acc = op == kOpAnd ? (acc & v) : (acc | v);
+            } else if (op == kOpAnd) {
+#pragma unroll
+                for (int k = 0; k < W; ++k) acc[k] = ~0ull;
+                for (uint32_t j = 0; j < pn; ++j, row += slot_stride)
+#pragma unroll
+                    for (int k = 0; k < W; ++k) acc[k] &= row[k * step];
+                for (uint32_t j = 0; j < sn; ++j) {
+                    --sp;
+#pragma unroll
+                    for (int k = 0; k < W; ++k) acc[k] &= st[sp][k];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < W; ++k) acc[k] = 0ull;
+                for (uint32_t j = 0; j < pn; ++j, row += slot_stride)
+#pragma unroll
+                    for (int k = 0; k < W; ++k) acc[k] |= row[k * step];
+                for (uint32_t j = 0; j < sn; ++j) {
+                    --sp;
+#pragma unroll
+                    for (int k = 0; k < W; ++k) acc[k] |= st[sp][k];
                 }
             }
             next += pn;
-            if (sp >= kMaxStack) return false;
-            st[sp++] = acc;
         } else if (op == kOpConjunction) {
             if (pc + 1 >= plen) return false;
             const uint32_t parts = prog[pc + 1];
             if (parts == 0 || pc + 2 + parts > plen) return false;
-            uint64_t acc = ~0ull;
+#pragma unroll
+            for (int k = 0; k < W; ++k) acc[k] = ~0ull;
             for (uint32_t p = 0; p < parts; ++p) {
                 const uint32_t pn = prog[pc + 2 + p];
                 if (pn == 0 || next + pn > nop) return false;
-                uint64_t o = 0;
-                for (uint32_t k = 0; k < pn; ++k) o |= slots[(next + k) * slot_stride + w];
-                acc &= o;
+                uint64_t o[W];
+#pragma unroll
+                for (int k = 0; k < W; ++k) o[k] = 0ull;
+                const uint64_t* row = slots + static_cast<uint64_t>(next) * slot_stride + w0;
+                for (uint32_t j = 0; j < pn; ++j, row += slot_stride)
+#pragma unroll
+                    for (int k = 0; k < W; ++k) o[k] |= row[k * step];
+#pragma unroll
+                for (int k = 0; k < W; ++k) acc[k] &= o[k];
                 next += pn;
             }
             pc += 2 + parts;
-            if (sp >= kMaxStack) return false;
-            st[sp++] = acc;
         } else {
             return false;
         }
+        if (sp >= static_cast<uint32_t>(kMaxStack)) return false;
+#pragma unroll
+        for (int k = 0; k < W; ++k) st[sp][k] = acc[k];
+        ++sp;
     }
     if (sp != 1 || next != nop) return false;
-    *result = st[0];
+#pragma unroll
+    for (int k = 0; k < W; ++k) result[k] = st[0][k];
     return true;
 }
 
@@ -310,16 +341,14 @@ __global__ void __launch_bounds__(kTile) filter_batch_kernel(FilterLaunch L) {
     __syncthreads();
 
     const bool bad_posting = s_bad != 0;
-    bool bad = bad_posting;
+    uint64_t res[WPT];
+    const bool bad = bad_posting || !eval_words<WPT>(s_prog, plen, slots, TW, t, kTile, nop, res);
     uint32_t c = 0;
 #pragma unroll
     for (int k = 0; k < WPT; ++k) {
         const uint32_t w = k * kTile + t;
         if (w >= nw) continue;
-        uint64_t r = 0;
-        if (!bad && !eval_word(s_prog, plen, slots, TW, w, nop, &r)) bad = true;
-        if (bad) r = 0;
-        r &= tail_mask(gw0 + w, L.doc_num);
+        const uint64_t r = bad ? 0ull : res[k] & tail_mask(gw0 + w, L.doc_num);
         out_row[gw0 + w] = r;
         c += __popcll(r);
     }
@@ -400,16 +429,14 @@ __global__ void __launch_bounds__(kDenseT) filter_dense_kernel(DenseFilterLaunch
     }
     cp_async_wait_all();
     __syncthreads();
-    bool bad = false;
+    uint64_t res[WPT];
+    const bool bad = !eval_words<WPT>(s_prog, plen, dslots, TW, t, kDenseT, nop, res);
     uint32_t c = 0;
 #pragma unroll
     for (int k = 0; k < WPT; ++k) {
         const uint32_t w = k * kDenseT + t;
         if (w >= nw) continue;
-        uint64_t r = 0;
-        if (!bad && !eval_word(s_prog, plen, dslots, TW, w, nop, &r)) bad = true;
-        if (bad) r = 0;
-        r &= tail_mask(gw0 + w, L.doc_num);
+        const uint64_t r = bad ? 0ull : res[k] & tail_mask(gw0 + w, L.doc_num);
         out_row[gw0 + w] = r;
         c += __popcll(r);
     }
@@ -427,11 +454,10 @@ cudaError_t launch_filter_dense_wpt(const DenseFilterLaunch& L, cudaStream_t str
     const uint64_t gy = static_cast<uint64_t>(L.seg_num) * tiles;
     if (gy > 65535u) return cudaErrorInvalidValue;
     const size_t smem = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * TW * sizeof(uint64_t);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(filter_dense_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem));
-        if (e != cudaSuccess) return e;
-    }
+    // opt in always: static plus dynamic shared memory may pass 48 KB even when the dynamic part does not
+    cudaError_t e = cudaFuncSetAttribute(filter_dense_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
     filter_dense_kernel<WPT><<<dim3(L.nq, static_cast<uint32_t>(gy)), kDenseT, smem, stream>>>(L);
     return cudaGetLastError();
 }
@@ -498,11 +524,10 @@ cudaError_t launch_filter_wpt(const FilterLaunch& L, cudaStream_t stream) {
     const uint64_t gy = static_cast<uint64_t>(L.seg_num) * tiles;
     if (gy > 65535u) return cudaErrorInvalidValue;
     const size_t smem = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * TW * sizeof(uint64_t);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(filter_batch_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem));
-        if (e != cudaSuccess) return e;
-    }
+    // opt in always: static plus dynamic shared memory may pass 48 KB even when the dynamic part does not
+    cudaError_t e = cudaFuncSetAttribute(filter_batch_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
     dim3 grid(L.nq, static_cast<uint32_t>(gy));
     filter_batch_kernel<WPT><<<grid, kTile, smem, stream>>>(L);
     return cudaGetLastError();
@@ -528,13 +553,15 @@ cudaError_t launch_filter_batch(const FilterLaunch& L, cudaStream_t stream) {
     }
 }
 
-// Two words per thread (4 KB of each operand per CTA) while the operand slots fit 48 KB, else one.
+// Four words per thread (8 KB of each operand per CTA) while the operand slots fit 48 KB, then two,
+// then one (an evaluation's decode cost is shared by a thread's words).
 cudaError_t launch_filter_dense(const DenseFilterLaunch& L, cudaStream_t stream) {
     if (L.nq == 0 || L.seg_num == 0) return cudaSuccess;
     if (L.max_opnd > static_cast<uint32_t>(kMaxOperands) || L.rows == 0 || L.seg_words == 0 || (L.seg_words & 1u) ||
         (reinterpret_cast<uintptr_t>(L.dense) & 15u))
         return cudaErrorInvalidValue;
     const size_t per_word = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * sizeof(uint64_t);
+    if (4 * kDenseT * per_word <= 48 * 1024 && L.seg_words >= 2 * kDenseT) return launch_filter_dense_wpt<4>(L, stream);
     if (2 * kDenseT * per_word <= 48 * 1024) return launch_filter_dense_wpt<2>(L, stream);
     return launch_filter_dense_wpt<1>(L, stream);
 }

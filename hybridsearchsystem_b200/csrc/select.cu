@@ -36,19 +36,37 @@ __device__ inline uint32_t pick_digit(SelectSmem& S, uint32_t* krem) {
         S.hist[0][tid] = s;
     }
     __syncthreads();
-    if (tid == 0) {
-        uint32_t cum = 0, chosen = 0, kr = *krem;
-        for (int d = 255; d >= 0; --d) {
-            const uint32_t h = S.hist[0][d];
-            if (cum + h >= kr) {
-                chosen = static_cast<uint32_t>(d);
-                kr -= cum;
-                break;
-            }
-            cum += h;
+    if (tid < 32) {
+        // warp 0 scans the 256 digits from the top: lane l owns digits 255 - 8l .. 248 - 8l
+        const uint32_t lane = tid;
+        const uint32_t kr = *krem;
+        uint32_t h[8], local = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            h[i] = S.hist[0][255 - 8 * lane - i];
+            local += h[i];
         }
-        S.bcast[0] = chosen;
-        S.bcast[1] = kr;
+        uint32_t incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= static_cast<uint32_t>(o)) incl += y;
+        }
+        const uint32_t excl = incl - local;
+        // the first lane whose digits bring the running count to kr holds the k-th largest key
+        const uint32_t hit = __ballot_sync(0xffffffffu, excl < kr && incl >= kr);
+        if (hit && lane == static_cast<uint32_t>(__ffs(hit) - 1)) {
+            uint32_t cum = excl;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (cum + h[i] >= kr) {
+                    S.bcast[0] = 255 - 8 * lane - i;
+                    S.bcast[1] = kr - cum;
+                    break;
+                }
+                cum += h[i];
+            }
+        }
     }
     __syncthreads();
     const uint32_t chosen = S.bcast[0];

@@ -53,6 +53,40 @@ def test_batched_filter_matches_oracle(torch_cuda, layout, in_place):
         assert counts[i] == want.sum(), e
 
 
+@pytest.mark.parametrize("in_place", [False, True], ids=["dense_matrix", "in_place"])
+def test_batched_filter_wide_segments_six_operands(torch_cuda, in_place):
+    # 131072-doc segments and six-operand programs: the widest per-thread word counts and the largest
+    # operand slots in shared memory (48 KB next to the program)
+    torch = torch_cuda
+    mix = data.Mixture(32, 64, (1e-3, 0.5), n_clusters=16, seed=61)
+    vec, bits, _ = mix.corpus(140000, seed=62)
+    table = hss.DataTable.build(vec, bits, 64, device=0, doc_num_per_segment=131072)
+    info = table.info
+    rng = np.random.default_rng(63)
+    exprs = []
+    for i in range(40):
+        t = rng.choice(64, 6, replace=False)
+        ops = rng.choice(["AND", "OR"], 5)
+        e = str(t[0])
+        for o, x in zip(ops, t[1:]):
+            e = f"({e} {o} {'NOT ' if rng.random() < 0.3 else ''}{x})"
+        exprs.append(e)
+    s = hss.FullRecallSearcher(table, max_batch=len(exprs), candidate_cap=4096, decode_in_place=in_place)
+    f = s.compile_filters(exprs)
+    words = info["segment_num"] * info["doc_num_per_segment"] // 64
+    out = torch.zeros((len(exprs), words), dtype=torch.int64, device="cuda")
+    cnt = torch.zeros(len(exprs), dtype=torch.int32, device="cuda")
+    assert s.filter_device(f, len(exprs), out.data_ptr(), words, cnt.data_ptr()) == _lib.HSS_OK
+    got = out.cpu().numpy().view(np.uint64)
+    n = vec.shape[0]
+    for i, e in enumerate(exprs):
+        want = _bits_of(oracle.filter_bits(e, bits), n)
+        row = _bits_of(got[i], words * 64)
+        assert (row[:n] == want).all(), e
+        assert not row[n:].any(), e
+        assert int(cnt.cpu().numpy()[i]) == want.sum(), e
+
+
 def test_filter_operator_both_table_conventions(torch_cuda):
     torch = torch_cuda
     mix, vec, bits, table = _table(torch, "bitmap", seed=5)
