@@ -528,7 +528,7 @@ cudaError_t launch_aggregate(const uint64_t* bits, const float* scores, const ui
 // the process and every call on that device shares it. The count kernel writes every entry a call
 // reads before the scan reads it, so a call never sees an earlier call's contents and nothing has to
 // be cleared; two calls that overlap on the GPU (different streams, no ordering) do race on it.
-__device__ __align__(256) uint32_t g_aggregate_scratch[kAggStaticBlocks];
+static __device__ __align__(256) uint32_t g_aggregate_scratch[kAggStaticBlocks];
 static_assert(kAggStaticMaxDocs == kAggStaticBlocks * static_cast<uint32_t>(kAggT), "one block count per kAggT docs");
 
 cudaError_t aggregate_static_scratch(uint32_t** scratch) {
