@@ -103,6 +103,22 @@ SIGNATURES = [
      [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, vp, ctypes.c_uint64]),
     ("hss_filter_compile", ctypes.c_int,
      [vp, ctypes.c_char_p, vp, ctypes.c_uint32, c_u32p, vp, ctypes.c_uint32, c_u32p, c_u32p, c_i32p]),
+    ("hss_searcher_feature_dim", ctypes.c_uint32, [vp]),
+    ("hss_searcher_features", ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, vp, vp, vp]),
+    ("hss_searcher_set_threshold_model", ctypes.c_int, [vp, vp, ctypes.c_float]),
+    ("hss_searcher_last_thresholds", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32]),
+    ("hss_searcher_last_estimate_counts", ctypes.c_int, [vp, vp, ctypes.c_uint32]),
+    ("hss_model_create", ctypes.c_int, [ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                        ctypes.POINTER(vp)]),
+    ("hss_model_free", None, [vp]),
+    ("hss_model_param_count", ctypes.c_uint64, [vp]),
+    ("hss_model_get_params", ctypes.c_int, [vp, vp]),
+    ("hss_model_set_params", ctypes.c_int, [vp, vp]),
+    ("hss_model_set_output_scale", ctypes.c_int, [vp, ctypes.c_float, ctypes.c_float]),
+    ("hss_model_forward", ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, vp]),
+    ("hss_model_train_step", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32, ctypes.c_float,
+                                            ctypes.POINTER(ctypes.c_float), vp]),
+    ("hss_model_gradients", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32, vp, ctypes.POINTER(ctypes.c_float), vp]),
     ("hss_last_error", ctypes.c_char_p, []),
     ("hss_device_count", ctypes.c_int, []),
 ]

@@ -198,6 +198,33 @@ class FullRecallSearcher:
         k = min(n.value, cap)
         return sc[:k], loc[:k], n.value, th.value, ep.value
 
+    def feature_dim(self):
+        return _lib.load().hss_searcher_feature_dim(self._h)
+
+    def features(self, d_queries, nq, filters, topks, d_x, stream=0):
+        """Feature rows [nq][feature_dim] of a batch into device memory d_x (runs the filter stage and
+        the doc sample)."""
+        t = np.ascontiguousarray(topks, dtype=np.uint32)
+        check(_lib.load().hss_searcher_features(self._h, d_queries, nq, filters._h, _np_ptr(t), d_x, stream))
+
+    def set_threshold_model(self, model, margin):
+        """Learned threshold on (model) or off (None); margin is subtracted from the prediction."""
+        check(_lib.load().hss_searcher_set_threshold_model(self._h, model._h if model else None, margin))
+        self._model = model  # kept alive while the searcher uses it
+
+    def last_thresholds(self, n):
+        """(doc sample's proven thresholds, the model's estimation-pass thresholds) of the last batch."""
+        t1 = np.zeros(max(n, 1), np.float32)
+        ta = np.zeros(max(n, 1), np.float32)
+        check(_lib.load().hss_searcher_last_thresholds(self._h, _np_ptr(t1), _np_ptr(ta), n))
+        return t1[:n], ta[:n]
+
+    def last_estimate_counts(self, n):
+        """Docs each query's threshold-estimation pass kept in the last batch (0 without a model)."""
+        c = np.zeros(max(n, 1), np.uint32)
+        check(_lib.load().hss_searcher_last_estimate_counts(self._h, _np_ptr(c), n))
+        return c[:n]
+
     def set_timing(self, on=True):
         check(_lib.load().hss_searcher_set_timing(self._h, int(on)))
 
@@ -207,6 +234,61 @@ class FullRecallSearcher:
         check(_lib.load().hss_searcher_last_times(self._h, _np_ptr(ms), ctypes.byref(r), ctypes.byref(l)))
         return {"filter_ms": float(ms[0]), "sample_ms": float(ms[1]), "candidates_ms": float(ms[2]),
                 "select_ms": float(ms[3]), "total_ms": float(ms[4]), "retries": r.value, "launches": l.value}
+
+
+class ThresholdModel:
+    """The learned K-th-score predictor (MLP din -> hidden -> hidden -> 1, GELU) on one GPU. Parameters
+    are one flat FP32 vector: W1 [din][hidden], b1, W2 [hidden][hidden], b2, w3 [hidden], b3."""
+
+    def __init__(self, din, hidden=256, device=0, seed=0):
+        h = ctypes.c_void_p()
+        check(_lib.load().hss_model_create(device, din, hidden, seed, ctypes.byref(h)))
+        self._h = h
+        self.din, self.hidden, self.device = din, hidden, device
+        self.scale, self.shift = 1.0, 0.0
+
+    def close(self):
+        if self._h:
+            _lib.load().hss_model_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def param_count(self):
+        return _lib.load().hss_model_param_count(self._h)
+
+    def get_params(self):
+        p = np.zeros(self.param_count, np.float32)
+        check(_lib.load().hss_model_get_params(self._h, _np_ptr(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.param_count
+        check(_lib.load().hss_model_set_params(self._h, _np_ptr(p)))
+
+    def set_output_scale(self, scale, shift):
+        self.scale, self.shift = float(scale), float(shift)
+        check(_lib.load().hss_model_set_output_scale(self._h, self.scale, self.shift))
+
+    def forward(self, d_x, batch, d_y, stream=0):
+        check(_lib.load().hss_model_forward(self._h, d_x, batch, d_y, stream))
+
+    def train_step(self, d_x, d_t, batch, lr, stream=0):
+        loss = ctypes.c_float()
+        check(_lib.load().hss_model_train_step(self._h, d_x, d_t, batch, lr, ctypes.byref(loss), stream))
+        return loss.value
+
+    def gradients(self, d_x, d_t, batch, stream=0):
+        g = np.zeros(self.param_count, np.float32)
+        loss = ctypes.c_float()
+        check(_lib.load().hss_model_gradients(self._h, d_x, d_t, batch, _np_ptr(g), ctypes.byref(loss), stream))
+        return g, loss.value
 
 
 # ---- operator entry points (device pointers as ints) ----

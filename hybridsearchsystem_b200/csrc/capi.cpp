@@ -39,6 +39,10 @@ struct hss_searcher {
     std::vector<std::unique_ptr<hss::QueryNode>> owned;  // trees of the added queries
 };
 
+struct hss_model {
+    std::shared_ptr<hss::ThresholdModel> m;
+};
+
 struct hss_filters {
     std::vector<hss::FilterExpr> exprs;
 };
@@ -390,6 +394,96 @@ int hss_searcher_last_times(const hss_searcher* s, float* ms5, uint32_t* retries
 
 // ---------------------------------------------------------------------------------------------
 // codec
+
+// ---------------------------------------------------------------------------------------------
+// learned threshold predictor
+
+uint32_t hss_searcher_feature_dim(const hss_searcher* s) { return s ? s->s->FeatureDim() : 0; }
+
+int hss_searcher_features(hss_searcher* s, const float* dQueries, uint32_t nq, const hss_filters* filters,
+                          const uint32_t* topks, float* dX, hss_stream_t stream) {
+    if (!s || (nq && (!dQueries || !filters || !topks || !dX)) || (filters && filters->exprs.size() < nq))
+        return SetError(HSS_ERR_INVALID, "hss_searcher_features: bad arguments");
+    std::vector<const hss::FilterExpr*> ptrs(nq);
+    for (uint32_t i = 0; i < nq; ++i) ptrs[i] = &filters->exprs[i];
+    const int rc = s->s->Features(dQueries, nq, ptrs.data(), topks, dX, S(stream));
+    if (rc == -1) return SetError(HSS_ERR_INVALID, s->s->Error());
+    if (rc != 0) return SetError(rc < 0 ? HSS_ERR_CUDA : HSS_ERR_QUERY, s->s->Error());
+    return HSS_OK;
+}
+
+int hss_searcher_set_threshold_model(hss_searcher* s, hss_model* model, float margin) {
+    if (!s) return SetError(HSS_ERR_INVALID, "hss_searcher_set_threshold_model: null searcher");
+    const int rc = s->s->SetThresholdModel(model ? model->m : nullptr, margin);
+    if (rc == -1) return SetError(HSS_ERR_INVALID, s->s->Error());
+    if (rc != 0) return SetError(HSS_ERR_CUDA, s->s->Error());
+    return HSS_OK;
+}
+
+int hss_searcher_last_thresholds(const hss_searcher* s, float* sampleTheta, float* modelTheta, uint32_t n) {
+    if (!s) return SetError(HSS_ERR_INVALID, "hss_searcher_last_thresholds: null searcher");
+    const auto& t1 = s->s->LastSampleThreshold();
+    const auto& ta = s->s->LastModelThreshold();
+    for (uint32_t i = 0; i < n; ++i) {
+        if (sampleTheta) sampleTheta[i] = i < t1.size() ? t1[i] : 0.0f;
+        if (modelTheta) modelTheta[i] = i < ta.size() ? ta[i] : 0.0f;
+    }
+    return HSS_OK;
+}
+
+int hss_searcher_last_estimate_counts(hss_searcher* s, uint32_t* counts, uint32_t n) {
+    if (!s || (n && !counts)) return SetError(HSS_ERR_INVALID, "hss_searcher_last_estimate_counts: bad arguments");
+    const int rc = s->s->LastEstimateCounts(n, counts);
+    if (rc == -1) return SetError(HSS_ERR_INVALID, "hss_searcher_last_estimate_counts: n beyond maxBatch");
+    if (rc != 0) return SetError(HSS_ERR_CUDA, "hss_searcher_last_estimate_counts");
+    return HSS_OK;
+}
+
+int hss_model_create(int32_t deviceId, uint32_t din, uint32_t hidden, uint64_t seed, hss_model** out) {
+    if (!out) return SetError(HSS_ERR_INVALID, "hss_model_create: null output");
+    auto m = std::make_shared<hss::ThresholdModel>(deviceId, din, hidden, seed);
+    if (!m->Ok()) return SetError(HSS_ERR_INVALID, m->Error());
+    *out = new hss_model{m};
+    return HSS_OK;
+}
+
+void hss_model_free(hss_model* m) { delete m; }
+
+uint64_t hss_model_param_count(const hss_model* m) { return m ? m->m->ParamCount() : 0; }
+
+int hss_model_get_params(const hss_model* m, float* params) {
+    if (!m || !params) return SetError(HSS_ERR_INVALID, "hss_model_get_params: bad arguments");
+    return m->m->GetParams(params) == 0 ? HSS_OK : SetError(HSS_ERR_CUDA, "hss_model_get_params");
+}
+
+int hss_model_set_params(hss_model* m, const float* params) {
+    if (!m || !params) return SetError(HSS_ERR_INVALID, "hss_model_set_params: bad arguments");
+    return m->m->SetParams(params) == 0 ? HSS_OK : SetError(HSS_ERR_CUDA, "hss_model_set_params");
+}
+
+int hss_model_set_output_scale(hss_model* m, float scale, float shift) {
+    if (!m) return SetError(HSS_ERR_INVALID, "hss_model_set_output_scale: null model");
+    m->m->scale = scale;
+    m->m->shift = shift;
+    return HSS_OK;
+}
+
+int hss_model_forward(hss_model* m, const float* dX, uint32_t B, float* dY, hss_stream_t stream) {
+    if (!m || (B && (!dX || !dY))) return SetError(HSS_ERR_INVALID, "hss_model_forward: bad arguments");
+    return m->m->Forward(dX, B, dY, S(stream)) == 0 ? HSS_OK : SetError(HSS_ERR_CUDA, m->m->Error());
+}
+
+int hss_model_train_step(hss_model* m, const float* dX, const float* dT, uint32_t B, float lr, float* loss,
+                         hss_stream_t stream) {
+    if (!m || B == 0 || !dX || !dT) return SetError(HSS_ERR_INVALID, "hss_model_train_step: bad arguments");
+    return m->m->TrainStep(dX, dT, B, lr, loss, S(stream)) == 0 ? HSS_OK : SetError(HSS_ERR_CUDA, m->m->Error());
+}
+
+int hss_model_gradients(hss_model* m, const float* dX, const float* dT, uint32_t B, float* grad, float* loss,
+                        hss_stream_t stream) {
+    if (!m || B == 0 || !dX || !dT || !grad) return SetError(HSS_ERR_INVALID, "hss_model_gradients: bad arguments");
+    return m->m->Gradients(dX, dT, B, grad, loss, S(stream)) == 0 ? HSS_OK : SetError(HSS_ERR_CUDA, m->m->Error());
+}
 
 uint64_t hss_hash64(const char* data, uint32_t len) { return hss::Hash64(data, len); }
 

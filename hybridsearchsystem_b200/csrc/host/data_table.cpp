@@ -207,6 +207,8 @@ void DataTable::Release() {
     if (m_dArena) cudaFree(m_dArena);
     if (m_dPostingTable) cudaFree(m_dPostingTable);
     if (m_dGDocIds) cudaFree(m_dGDocIds);
+    if (m_dRowDensity) cudaFree(m_dRowDensity);
+    m_dRowDensity = nullptr;
     m_dVectors = nullptr;
     m_dArena = nullptr;
     m_dPostingTable = nullptr;
@@ -396,6 +398,22 @@ bool DataTable::Upload(std::string* err) {
     if (!CudaOk(cudaMalloc(&m_dGDocIds, m_docNum * sizeof(int64_t)), err, "cudaMalloc gdocids")) return false;
     if (!CudaOk(cudaMemcpy(m_dGDocIds, m_gdocids.data(), m_docNum * sizeof(int64_t), cudaMemcpyHostToDevice), err,
                 "upload gdocids"))
+        return false;
+    // fraction of docs holding each row's token: the hit counts of the posting heads ([layout:4|hits:28])
+    std::vector<float> density(m_rows, 0.0f);
+    for (uint32_t r = 0; r + 1 < m_rows; ++r) {
+        uint64_t hits = 0;
+        for (uint32_t s = 0; s < m_segmentNum; ++s)
+            if (m_rowSegOffset[r][s] >= 0 && m_rowSegLen[r][s] >= 4) {
+                uint32_t head = 0;
+                std::memcpy(&head, m_segPostings[s].data() + m_rowSegOffset[r][s], 4);
+                hits += head & 0x0fffffffu;
+            }
+        density[r] = m_docNum ? static_cast<float>(static_cast<double>(hits) / static_cast<double>(m_docNum)) : 0.0f;
+    }
+    if (!CudaOk(cudaMalloc(&m_dRowDensity, m_rows * sizeof(float)), err, "cudaMalloc row density")) return false;
+    if (!CudaOk(cudaMemcpy(m_dRowDensity, density.data(), m_rows * sizeof(float), cudaMemcpyHostToDevice), err,
+                "upload row density"))
         return false;
     return true;
 }

@@ -236,6 +236,8 @@ class DataTable {
     // posting also leaves it unbuilt, so the in-place path reports it per query.
     bool EnableDensePostings(uint64_t budgetBytes, std::string* err);
     const uint64_t* DeviceDensePostings() const { return m_dDense; }
+    // Fraction of the docs that hold each posting row's token (float [rows], device).
+    const float* DeviceRowDensity() const { return m_dRowDensity; }
     // Host copy of segment s's posting of a token row (for tests / save); null if absent.
     const uint8_t* HostPosting(uint32_t row, uint32_t seg, uint32_t* len) const;
     // Layout code of each posting of a row (PostingFieldData::GetPostingTypes).
@@ -276,6 +278,7 @@ class DataTable {
     uint64_t* m_dPostingTable = nullptr;
     int64_t* m_dGDocIds = nullptr;
     uint64_t* m_dDense = nullptr;  // EnableDensePostings
+    float* m_dRowDensity = nullptr;  // [rows] fraction of docs holding each row's token
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -314,6 +317,58 @@ struct StageTimes {
     uint32_t launches = 0;
 };
 
+// The learned threshold predictor: an MLP (features -> H -> H -> 1, GELU) on one GPU, trained and
+// run by the kernels of mlp.cu. It predicts a standardised K-th filtered score; scale / shift map the
+// output back to a score. Parameters: one flat FP32 vector W1 [din][H], b1, W2 [H][H], b2, w3 [H], b3.
+class ThresholdModel {
+   public:
+    ThresholdModel(int32_t deviceId, uint32_t din, uint32_t hidden, uint64_t seed);
+    ~ThresholdModel();
+    ThresholdModel(const ThresholdModel&) = delete;
+    ThresholdModel& operator=(const ThresholdModel&) = delete;
+
+    bool Ok() const { return m_ok; }
+    const std::string& Error() const { return m_err; }
+    int32_t DeviceId() const { return m_deviceId; }
+    uint32_t Din() const { return m_din; }
+    uint32_t Hidden() const { return m_h; }
+    size_t ParamCount() const { return m_np; }
+
+    // y[B] (standardised) of device features dX [B][din].
+    int Forward(const float* dX, uint32_t B, float* dY, cudaStream_t s);
+    // One Adam step on mean((y - t)^2) over a batch of device features / standardised targets.
+    int TrainStep(const float* dX, const float* dT, uint32_t B, float lr, float* hLoss, cudaStream_t s);
+    // The gradient of mean((y - t)^2) at the current parameters, into a host vector of ParamCount().
+    int Gradients(const float* dX, const float* dT, uint32_t B, float* hGrad, float* hLoss, cudaStream_t s);
+    int GetParams(float* h) const;
+    int SetParams(const float* h);
+
+    float scale = 1.0f, shift = 0.0f;  // score = y * scale + shift
+
+   private:
+    size_t OffW1() const { return 0; }
+    size_t OffB1() const { return static_cast<size_t>(m_din) * m_h; }
+    size_t OffW2() const { return OffB1() + m_h; }
+    size_t OffB2() const { return OffW2() + static_cast<size_t>(m_h) * m_h; }
+    size_t OffW3() const { return OffB2() + m_h; }
+    size_t OffB3() const { return OffW3() + m_h; }
+    bool Reserve(uint32_t batch);
+    cudaError_t ForwardInto(const float* dX, uint32_t B, cudaStream_t s);
+    cudaError_t Backward(const float* dX, const float* dT, uint32_t B, cudaStream_t s);
+    int Finish(cudaError_t e, float* hLoss, uint32_t B, cudaStream_t s);
+
+    int32_t m_deviceId;
+    uint32_t m_din, m_h;
+    size_t m_np = 0;
+    bool m_ok = false;
+    std::string m_err;
+    int m_step = 0;
+    uint32_t m_cap = 0;
+    float *m_dP = nullptr, *m_dG = nullptr, *m_dM = nullptr, *m_dV = nullptr;
+    float *m_dZ1 = nullptr, *m_dA1 = nullptr, *m_dZ2 = nullptr, *m_dA2 = nullptr;
+    float *m_dY = nullptr, *m_dDy = nullptr, *m_dD1 = nullptr, *m_dD2 = nullptr, *m_dSq = nullptr;
+};
+
 class FullRecallSearcher {
    public:
     FullRecallSearcher(int32_t deviceId, std::shared_ptr<DataTable> dataTable, const SearcherConfig& cfg = {});
@@ -347,6 +402,27 @@ class FullRecallSearcher {
     // error bound; for checking the approximate pass against the exact scores.
     int LastCandidates(uint32_t q, float* scores, uint32_t* locs, uint32_t cap, uint32_t* count, float* theta,
                        float* eps);
+
+    // Learned threshold: with a model set, the two-part pass becomes: pass A over every
+    // kLearnedSplit-th tile at max(theta_1, prediction - margin), theta_1 being the doc sample's
+    // proven threshold. Its candidates only estimate theta_2 = max(theta_1, K-th best of pass A -
+    // 2 eps), which is proven because pass A's K-th best exists. A full pass B at theta_2 gives the
+    // candidates of the select step. A bad prediction costs candidates, never exactness, and never
+    // forces a re-run. nullptr switches the model off.
+    int SetThresholdModel(std::shared_ptr<ThresholdModel> model, float margin);
+    // Width of a query's feature row: dim + posting rows + 6.
+    uint32_t FeatureDim() const;
+    // Feature rows [nq][FeatureDim()] of a batch (runs the filter stage and the doc sample).
+    int Features(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks,
+                 float* dX, cudaStream_t stream);
+    // Per query of the last batch: the doc sample's proven threshold theta_1, and the threshold pass A
+    // used (-inf without a model).
+    const std::vector<float>& LastSampleThreshold() const { return m_lastTheta1; }
+    const std::vector<float>& LastModelThreshold() const { return m_lastThetaA; }
+    static constexpr uint32_t kLearnedSplit = 4;
+    // Per query of the last batch with a model: the docs its threshold-estimation pass kept (0
+    // without a model). Reads the device; call before the next batch.
+    int LastEstimateCounts(uint32_t n, uint32_t* counts);
 
     const StageTimes& LastTimes() const { return m_times; }
     void SetTiming(bool on) { m_timing = on; }
@@ -401,6 +477,15 @@ class FullRecallSearcher {
     StageTimes m_times;
     std::vector<int32_t> m_lastStatus;
     std::vector<std::pair<uint32_t, uint32_t>> m_lastSegs;  // per query: (segments, entries per segment)
+    std::shared_ptr<ThresholdModel> m_model;
+    float m_margin = 0.0f;
+    float* m_dX = nullptr;           // [maxBatch][FeatureDim()] model features
+    float* m_dYp = nullptr;          // [maxBatch] model outputs, then pass A's thresholds
+    float* m_dStats = nullptr;       // [maxBatch][4] doc-sample statistics
+    float* m_hThetaA = nullptr;      // pinned copy of pass A's thresholds
+    float* m_featuresOut = nullptr;  // Features(): stop after writing the feature rows here
+    std::vector<float> m_lastTheta1, m_lastThetaA;
+    uint32_t m_lastEstSegs = 0;  // list segments of the last estimation pass (0: none ran)
 };
 
 }  // namespace hss

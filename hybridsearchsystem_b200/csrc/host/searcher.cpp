@@ -85,10 +85,11 @@ FullRecallSearcher::FullRecallSearcher(int32_t deviceId, std::shared_ptr<DataTab
 FullRecallSearcher::~FullRecallSearcher() {
     cudaSetDevice(m_deviceId);
     void* dptrs[] = {m_dBits,    m_dCandScore, m_dCandLoc, m_dWork,     m_dSampScore, m_dSampLoc, m_dStage,
-                     m_dQueries, m_dOutScore,  m_dOutId,   m_dOutCount, m_dStaged,    m_dQScale,  m_dError};
+                     m_dQueries, m_dOutScore,  m_dOutId,   m_dOutCount, m_dStaged,    m_dQScale,  m_dError,
+                     m_dX,       m_dYp,        m_dStats};
     for (void* p : dptrs)
         if (p) cudaFree(p);
-    void* hptrs[] = {m_hStage, m_hOutScore, m_hOutId, m_hOutCount};
+    void* hptrs[] = {m_hStage, m_hOutScore, m_hOutId, m_hOutCount, m_hThetaA};
     for (void* p : hptrs)
         if (p) cudaFreeHost(p);
     for (auto& e : m_ev)
@@ -135,6 +136,8 @@ bool FullRecallSearcher::Allocate() {
     if (!ck(cudaMallocHost(&m_hOutScore, B * kMaxTopK * 4ull), "cudaMallocHost results")) return false;
     if (!ck(cudaMallocHost(&m_hOutId, B * kMaxTopK * 8ull), "cudaMallocHost results")) return false;
     if (!ck(cudaMallocHost(&m_hOutCount, B * 4ull), "cudaMallocHost results")) return false;
+    if (!ck(cudaMalloc(&m_dStats, B * 4ull * sizeof(float)), "cudaMalloc sample statistics")) return false;
+    if (!ck(cudaMallocHost(&m_hThetaA, B * sizeof(float)), "cudaMallocHost thresholds")) return false;
     for (auto& e : m_ev)
         if (!ck(cudaEventCreate(&e), "cudaEventCreate")) return false;
     if (m_cfg.densePostings) {
@@ -305,6 +308,73 @@ int FullRecallSearcher::FilterDevice(uint32_t nq, const FilterExpr* const* exprs
     return bad;
 }
 
+uint32_t FullRecallSearcher::FeatureDim() const {
+    return m_table ? m_table->GetDimension() + m_table->PostingRows() + 6 : 0;
+}
+
+int FullRecallSearcher::SetThresholdModel(std::shared_ptr<ThresholdModel> model, float margin) {
+    if (!m_ok) return -1;
+    if (model && (!model->Ok() || model->Din() != FeatureDim() || model->DeviceId() != m_deviceId)) {
+        m_err = "threshold model does not fit this searcher (feature width or device)";
+        return -1;
+    }
+    if (model && !m_dX) {
+        if (cudaSetDevice(m_deviceId) != cudaSuccess ||
+            cudaMalloc(&m_dX, static_cast<size_t>(m_cfg.maxBatch) * FeatureDim() * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&m_dYp, static_cast<size_t>(m_cfg.maxBatch) * sizeof(float)) != cudaSuccess) {
+            m_err = "cudaMalloc model features";
+            return -2;
+        }
+    }
+    m_model = std::move(model);
+    m_margin = margin;
+    return 0;
+}
+
+// Features of the staged batch (the filter stage and the doc sample have run: pass counts, operands
+// and sample statistics are on the device).
+static cudaError_t LaunchFeatures(const DataTable& T, const uint8_t* D, size_t opndOff, size_t opnd, size_t passCount,
+                                  size_t topk, const float* stats, const float* dQueries, uint32_t nq, uint32_t din,
+                                  float* dX, cudaStream_t stream) {
+    FeatureLaunch F{};
+    F.qry = dQueries;
+    F.stats = stats;
+    F.opnd_row = reinterpret_cast<const uint32_t*>(D + opnd);
+    F.opnd_off = reinterpret_cast<const uint32_t*>(D + opndOff);
+    F.pass_count = reinterpret_cast<const uint32_t*>(D + passCount);
+    F.topk = reinterpret_cast<const uint32_t*>(D + topk);
+    F.row_density = T.DeviceRowDensity();
+    F.x = dX;
+    F.nq = nq;
+    F.dim = T.GetDimension();
+    F.rows = T.PostingRows();
+    F.din = din;
+    F.doc_num = T.GetDocNum();
+    return launch_features(F, stream);
+}
+
+int FullRecallSearcher::LastEstimateCounts(uint32_t n, uint32_t* counts) {
+    if (!m_ok || n > m_cfg.maxBatch) return -1;
+    std::fill(counts, counts + n, 0u);
+    if (m_lastEstSegs == 0 || n == 0) return 0;
+    if (cudaSetDevice(m_deviceId) != cudaSuccess) return -2;
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    std::vector<uint32_t> c(static_cast<size_t>(n) * kMaxCandSegs);
+    if (cudaMemcpy(c.data(), m_dStage + SL.sampCount, c.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+    for (uint32_t q = 0; q < n; ++q)
+        for (uint32_t g = 0; g < m_lastEstSegs; ++g) counts[q] += c[static_cast<size_t>(q) * kMaxCandSegs + g];
+    return 0;
+}
+
+int FullRecallSearcher::Features(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs,
+                                 const uint32_t* topks, float* dX, cudaStream_t stream) {
+    // the batch's own filter, staging and doc sample, stopping at the features
+    m_featuresOut = dX;
+    const int rc = SearchDevice(dQueries, nq, exprs, topks, nullptr, nullptr, nullptr, kMaxTopK, stream);
+    m_featuresOut = nullptr;
+    return rc;
+}
+
 int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs,
                                      const uint32_t* topks, float* dOutScores, int64_t* dOutIds,
                                      uint32_t* dOutCounts, uint32_t outStride, cudaStream_t stream) {
@@ -462,7 +532,8 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     const uint64_t want = std::max<uint64_t>(m_cfg.sampleDocs,
                                              (4ull * std::max<uint32_t>(maxK, 1u) * T.GetDocNum() +
                                               m_cfg.candidateCap - 1) / m_cfg.candidateCap);
-    auto sample = [&](const uint32_t* dList, uint32_t rows, bool simt) {
+    auto sample = [&](const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly = false,
+                      float* stats = nullptr) {
         const uint32_t unit = unitOf(rows, simt);
         const uint64_t tilesU = tilesOf(unit);
         const uint64_t sampTiles = std::min<uint64_t>(tilesU, std::max<uint64_t>(1, (want + unit - 1) / unit));
@@ -478,18 +549,43 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         ST.cap = m_sampCap;
         ST.segs = segs;
         ST.seg_cap = segCap;
-        ST.raise_only = 0;
+        ST.raise_only = raiseOnly ? 1 : 0;
         ST.topk = dTopk;
         ST.eps_sample = dEpsSamp;
         ST.eps_main = dEpsMain;
         ST.theta = dTheta;
         ST.qlist = dList;
         ST.nq_list = rows;
+        ST.stats = stats;
         ck(launch_sample_threshold(ST, stream));
         return count;
     };
-    const uint64_t sampCount = sample(nullptr, nq, false);
+    const bool learned = static_cast<bool>(m_model);
+    const bool wantStats = learned || m_featuresOut != nullptr;
+    m_lastEstSegs = 0;
+    const uint64_t sampCount = sample(nullptr, nq, false, false, wantStats ? m_dStats : nullptr);
     launches += 2;
+    // the sample's proven thresholds (theta_1), read after the batch's first synchronisation
+    ck(cudaMemcpyAsync(H + SL.theta, dTheta, nq * 4ull, cudaMemcpyDeviceToHost, stream));
+    if (m_featuresOut) {
+        ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
+                          m_featuresOut, stream));
+        ck(cudaStreamSynchronize(stream));
+        if (ce != cudaSuccess) {
+            m_err = cudaGetErrorString(ce);
+            return -2;
+        }
+        return 0;
+    }
+    if (learned) {
+        // the model's predicted K-th score minus the margin, never below theta_1
+        ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
+                          m_dX, stream));
+        if (m_model->Forward(m_dX, nq, m_dYp, stream) != 0) ck(cudaErrorUnknown);
+        ck(launch_predict_theta(m_dYp, dTheta, nq, m_model->scale, m_model->shift, m_margin, m_dYp, stream));
+        ck(cudaMemcpyAsync(m_hThetaA, m_dYp, nq * 4ull, cudaMemcpyDeviceToHost, stream));
+        launches += 5;
+    }
     if (m_timing) ck(cudaEventRecord(m_ev[2], stream));
 
     // 2. the full pass, progressively: first every split-th tile (about sqrt(sample / corpus) of it)
@@ -520,7 +616,38 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     SE.status = dStatus;
     SE.qlist = nullptr;
     SE.nq_list = nq;
-    if (split >= 2) {
+    if (learned) {
+        // Pass A, every kLearnedSplit-th tile at the predicted thresholds, only estimates: its
+        // candidates go to the sample buffer. Its K-th best is a proven bound whenever it kept K docs
+        // (they exist), so theta_2 = max(theta_1, K-th best - 2 eps) is safe for the full pass B,
+        // whose candidates alone feed the select step. A prediction that kept fewer than K docs
+        // leaves theta_1 in place; no prediction can make the results inexact or force a re-run.
+        const uint64_t countA = (tilesM + kLearnedSplit - 1) / kLearnedSplit;
+        const uint32_t segsA = segsOf(nq, countA, m_sampCap, false);
+        const uint32_t capA = segCapOf(nq, countA, m_sampCap, segsA, false);
+        m_lastEstSegs = segsA;
+        cand(m_dYp, m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, capA, 0, kLearnedSplit, 0, countA, nullptr, nq,
+             false);
+        SampleThresholdLaunch RT{};
+        RT.score = m_dSampScore;
+        RT.count = dSampCount;
+        RT.cap = m_sampCap;
+        RT.segs = segsA;
+        RT.seg_cap = capA;
+        RT.raise_only = 1;
+        RT.topk = dTopk;
+        RT.eps_sample = dEpsMain;  // t - 2 eps_main
+        RT.eps_main = dEpsMain;
+        RT.theta = dTheta;
+        RT.qlist = nullptr;
+        RT.nq_list = nq;
+        ck(launch_sample_threshold(RT, stream));
+        const uint32_t segs = segsOf(nq, tilesM, C, false);
+        SE.segs = segs;
+        SE.seg_cap = segCapOf(nq, tilesM, C, segs, false);
+        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tilesM, nullptr, nq, false);
+        launches += 3;
+    } else if (split >= 2) {
         const uint64_t countA = (tilesM + split - 1) / split, countB = tilesM - countA;
         const uint32_t segsA = segsOf(nq, countA, C, false), segsB = segsOf(nq, countB, C, false);
         const uint32_t segCap = std::min(segCapOf(nq, countA, C, segsA + segsB, false),
@@ -562,9 +689,19 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     auto* hStatus = reinterpret_cast<int32_t*>(H + SL.status);
     auto* hQlist = reinterpret_cast<uint32_t*>(H + SL.qlist);
     uint32_t retries = 0;
+    bool firstSync = true;
     for (;;) {
         ck(cudaMemcpyAsync(hStatus, dStatus, nq * 4ull, cudaMemcpyDeviceToHost, stream));
         ck(cudaStreamSynchronize(stream));
+        if (firstSync && ce == cudaSuccess) {
+            const float* h1 = reinterpret_cast<const float*>(H + SL.theta);
+            m_lastTheta1.assign(h1, h1 + nq);
+            if (learned)
+                m_lastThetaA.assign(m_hThetaA, m_hThetaA + nq);
+            else
+                m_lastThetaA.assign(nq, -INFINITY);
+            firstSync = false;
+        }
         if (ce != cudaSuccess) break;
         uint32_t nre = 0;
         for (uint32_t q = 0; q < nq; ++q) {

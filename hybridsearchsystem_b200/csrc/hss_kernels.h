@@ -114,6 +114,7 @@ struct SampleThresholdLaunch {
     float* theta;              // [nq] out
     const uint32_t* qlist;
     uint32_t nq_list;
+    float* stats;              // [nq][4] or null: best sample score, K-th best, stored count (-2 when absent)
 };
 
 struct SelectLaunch {
@@ -221,6 +222,34 @@ cudaError_t aggregate_static_scratch(uint32_t** scratch);
 cudaError_t launch_aggregate(const uint64_t* bits, const float* scores, const uint32_t* loc_in, uint32_t n,
                              float* out_scores, uint32_t* out_loc, uint32_t* total, uint32_t* workspace,
                              cudaStream_t stream);
+// Learned threshold predictor (mlp.cu).
+// C = op(A) op(B) (+ C) (+ bias), then act (0 identity, 1 GELU); pre receives the value before act.
+cudaError_t launch_gemm(bool ta, bool tb, const float* A, const float* B, float* C, int M, int N, int K, int lda,
+                        int ldb, int ldc, const float* bias, int act, float* pre, bool accumulate,
+                        cudaStream_t stream);
+cudaError_t launch_gelu_backward(float* dA, const float* Z, int64_t n, cudaStream_t stream);
+cudaError_t launch_colsum(const float* G, int M, int N, int ld, float* out, cudaStream_t stream);
+cudaError_t launch_mse_grad(const float* y, const float* t, int B, float* dy, float* sq, cudaStream_t stream);
+cudaError_t launch_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2,
+                        float eps, int step, cudaStream_t stream);
+struct FeatureLaunch {
+    const float* qry;           // [nq][dim]
+    const float* stats;         // [nq][4] doc-sample statistics (sample_threshold_kernel)
+    const uint32_t* opnd_row;   // concatenated filter operand rows
+    const uint32_t* opnd_off;   // [nq + 1]
+    const uint32_t* pass_count; // [nq] docs the filter lets through
+    const uint32_t* topk;       // [nq]
+    const float* row_density;   // [rows] fraction of docs holding each posting row's token
+    float* x;                   // [nq][din] out
+    uint32_t nq, dim, rows, din;
+    uint64_t doc_num;
+};
+cudaError_t launch_features(const FeatureLaunch& L, cudaStream_t stream);
+// theta_a[q] = max(theta[q], y[q] * scale + shift - margin): the predicted threshold, never below the
+// proven one. theta_a may alias y.
+cudaError_t launch_predict_theta(const float* y, const float* theta, uint32_t nq, float scale, float shift,
+                                 float margin, float* theta_a, cudaStream_t stream);
+
 cudaError_t launch_topk_op(const float* scores, const uint32_t* locs, const uint32_t* count, uint32_t k,
                            float* out_scores, uint32_t* out_locs, uint32_t* out_count, cudaStream_t stream);
 

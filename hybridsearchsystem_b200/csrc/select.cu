@@ -225,6 +225,25 @@ __global__ void __launch_bounds__(kST) sample_threshold_kernel(SampleThresholdLa
     bool lost = false;  // a sample segment that overflowed only lowers the sample's K-th best
     const uint32_t n = load_segments(S, L.count + static_cast<uint64_t>(qi) * kMaxCandSegs, L.segs, L.seg_cap, &lost);
     float theta = L.raise_only ? L.theta[qi] : -INFINITY;
+    if (L.stats) {
+        // the best stored score (one pass), for the threshold predictor's features
+        if (threadIdx.x == 0) S.counter = 0;
+        __syncthreads();
+        const float* sc = L.score + static_cast<uint64_t>(qi) * L.cap;
+        for_each_segment_entry(S, L.segs, L.seg_cap, [&](uint32_t i, bool ok) {
+            uint32_t key = ok ? float_key(sc[i]) : 0u;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) key = max(key, __shfl_xor_sync(0xffffffffu, key, o));
+            if ((threadIdx.x & 31) == 0 && key) atomicMax(&S.counter, key);
+        });
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float* st = L.stats + static_cast<uint64_t>(qi) * 4;
+            st[0] = n ? key_float(S.counter) : -2.0f;
+            st[2] = static_cast<float>(n);
+        }
+        __syncthreads();
+    }
     if (k > 0 && n >= k) {
         const float* sc = L.score + static_cast<uint64_t>(qi) * L.cap;
         const uint32_t kk = kth_largest_u32_visit(
@@ -238,6 +257,9 @@ __global__ void __launch_bounds__(kST) sample_threshold_kernel(SampleThresholdLa
         // a true top-K doc therefore scores >= t - eps_s - eps_m under the main pass's arithmetic.
         const float t = __fsub_rd(__fsub_rd(key_float(kk), L.eps_sample[qi]), L.eps_main[qi]);
         theta = L.raise_only ? fmaxf(theta, t) : t;
+        if (L.stats && threadIdx.x == 0) L.stats[static_cast<uint64_t>(qi) * 4 + 1] = key_float(kk);
+    } else if (L.stats && threadIdx.x == 0) {
+        L.stats[static_cast<uint64_t>(qi) * 4 + 1] = -2.0f;
     }
     __syncthreads();  // every thread has read the old theta
     if (threadIdx.x == 0) L.theta[qi] = theta;

@@ -218,6 +218,55 @@ int hss_searcher_last_candidates(hss_searcher* s, uint32_t query, float* scores,
 int hss_searcher_set_timing(hss_searcher* s, int32_t on);
 int hss_searcher_last_times(const hss_searcher* s, float* ms5, uint32_t* retries, uint32_t* launches);
 
+/* ---- learned threshold predictor ----
+ * An MLP (feature row -> hidden -> hidden -> 1, GELU) that predicts a query's K-th filtered score,
+ * trained and run on the GPU by this library's own kernels. With a model set, a searcher runs a
+ * threshold-estimation pass over every 4th tile at max(doc sample's proven threshold, prediction -
+ * margin), raises each query's threshold to that pass's K-th best minus the error bound (proven), and
+ * takes the select step's candidates from one full pass at that threshold. A bad prediction costs
+ * candidates, never exactness. No counterpart in the reference (whose only threshold is its TOPK
+ * pivot pre-select). */
+typedef struct hss_model hss_model;
+
+/* dim + posting rows + 6: the feature row width a model for this searcher must take. */
+uint32_t hss_searcher_feature_dim(const hss_searcher* s);
+/* Feature rows dX [nq][feature_dim] of a batch (device queries and output): query * sqrt(dim); per
+ * posting row of the query's filter 1 + log10(row density) / 4 (0 elsewhere); log10(filter
+ * selectivity) / 4; log10(K) / 3; 1; the doc sample's best score; its K-th best score (-2 when
+ * absent); log10(filtered sample docs + 1) / 5. Runs the filter stage and the doc sample;
+ * synchronises `stream`. */
+int hss_searcher_features(hss_searcher* s, const float* dQueries, uint32_t nq, const hss_filters* filters,
+                          const uint32_t* topks, float* dX, hss_stream_t stream);
+/* model NULL switches the learned threshold off. margin is subtracted from the prediction. */
+int hss_searcher_set_threshold_model(hss_searcher* s, hss_model* model, float margin);
+/* Per query of the last batch: the doc sample's proven threshold and the threshold the model set for
+ * the estimation pass (-inf without a model); host arrays of n floats, either may be NULL. */
+int hss_searcher_last_thresholds(const hss_searcher* s, float* sampleTheta, float* modelTheta, uint32_t n);
+
+/* Per query of the last batch run with a model: the docs its threshold-estimation pass kept (0 when no
+ * model was set). A count below K means the prediction was too high for that query (its sample
+ * threshold stood). Call before the next batch. */
+int hss_searcher_last_estimate_counts(hss_searcher* s, uint32_t* counts, uint32_t n);
+
+int hss_model_create(int32_t deviceId, uint32_t din, uint32_t hidden, uint64_t seed, hss_model** out);
+void hss_model_free(hss_model* m);
+/* din*hidden + hidden + hidden*hidden + hidden + hidden + 1: W1, b1, W2, b2, w3, b3 in this order. */
+uint64_t hss_model_param_count(const hss_model* m);
+int hss_model_get_params(const hss_model* m, float* params);
+int hss_model_set_params(hss_model* m, const float* params);
+/* The model predicts standardised scores: score = output * scale + shift. */
+int hss_model_set_output_scale(hss_model* m, float scale, float shift);
+/* Outputs dY [B] (standardised) of device features dX [B][din]. */
+int hss_model_forward(hss_model* m, const float* dX, uint32_t B, float* dY, hss_stream_t stream);
+/* One Adam step (b1 0.9, b2 0.999, eps 1e-8) on mean((y - t)^2) over device dX [B][din] and dT [B]
+ * (standardised targets); *loss (may be NULL) = the batch loss before the step. Synchronises. */
+int hss_model_train_step(hss_model* m, const float* dX, const float* dT, uint32_t B, float lr, float* loss,
+                         hss_stream_t stream);
+/* The gradient of mean((y - t)^2) at the current parameters into a host array of param_count floats
+ * (parameter order); *loss (may be NULL) = the loss. Synchronises `stream`. */
+int hss_model_gradients(hss_model* m, const float* dX, const float* dT, uint32_t B, float* grad, float* loss,
+                        hss_stream_t stream);
+
 /* ---- host-side codec (the index format contract) ---- */
 /* Hash64 (src/engine/core/hash/hash.cpp:10-16). */
 uint64_t hss_hash64(const char* data, uint32_t len);

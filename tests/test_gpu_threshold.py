@@ -1,0 +1,130 @@
+"""The learned threshold predictor through the C-ABI.
+
+1. The CUDA forward pass and gradients equal the CPU restatement (oracle/mlp_ref.py, float64) within
+   FP32 tolerance: relative 2e-4 of the gradient's scale, written below.
+2. Training with the library's own kernels lowers the loss.
+3. A searcher using a trained model returns the oracle's results bit for bit; so do models whose
+   thresholds are far too high (the estimation pass keeps nothing and the sample's threshold stands)
+   and far too low.
+4. What the model gains: on held-out queries its threshold-estimation pass keeps far fewer docs than
+   the same pass at the doc sample's threshold, and few queries' predictions were too high.
+"""
+import numpy as np
+import pytest
+
+import hybridsearchsystem_b200 as hss
+import oracle
+from hybridsearchsystem_b200 import data
+from hybridsearchsystem_b200.threshold import fit_threshold_model
+from oracle import mlp_ref
+
+pytestmark = pytest.mark.gpu
+
+GRAD_RTOL = 2e-4  # relative to the largest gradient magnitude (FP32 GEMMs, sums of up to 64 terms)
+
+
+def test_mlp_forward_and_gradients_match_cpu(torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(71)
+    din, h, B = 37, 48, 53
+    m = hss.ThresholdModel(din, h, device=0, seed=3)
+    p = m.get_params().astype(np.float64)
+    X = rng.standard_normal((B, din)).astype(np.float32)
+    t = rng.standard_normal(B).astype(np.float32)
+    dX = torch.tensor(X, device="cuda")
+    dT = torch.tensor(t, device="cuda")
+    dY = torch.zeros(B, dtype=torch.float32, device="cuda")
+    m.forward(dX.data_ptr(), B, dY.data_ptr())
+    torch.cuda.synchronize()
+    y_ref, _ = mlp_ref.forward(p, X, din, h)
+    assert np.allclose(dY.cpu().numpy(), y_ref, rtol=1e-4, atol=1e-4 * np.abs(y_ref).max())
+    g, loss = m.gradients(dX.data_ptr(), dT.data_ptr(), B)
+    loss_ref, g_ref = mlp_ref.loss_and_grad(p, X, t, din, h)
+    assert abs(loss - loss_ref) <= 1e-4 * max(1.0, loss_ref)
+    scale = np.abs(g_ref).max()
+    assert np.abs(g - g_ref).max() <= GRAD_RTOL * scale, np.abs(g - g_ref).max() / scale
+
+
+def test_training_steps_lower_the_loss(torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(72)
+    din, h, B = 24, 32, 256
+    X = rng.standard_normal((B, din)).astype(np.float32)
+    w = rng.standard_normal(din).astype(np.float32)
+    t = np.tanh(X @ w / 4).astype(np.float32)
+    m = hss.ThresholdModel(din, h, device=0, seed=4)
+    dX, dT = torch.tensor(X, device="cuda"), torch.tensor(t, device="cuda")
+    first = m.train_step(dX.data_ptr(), dT.data_ptr(), B, 3e-3)
+    for _ in range(300):
+        last = m.train_step(dX.data_ptr(), dT.data_ptr(), B, 3e-3)
+    assert last < 0.1 * first
+
+
+def _world(seed=81, n=80000, tags=64):
+    mix = data.Mixture(128, tags, (1e-3, 0.6), n_clusters=64, seed=seed)
+    vec, bits, _ = mix.corpus(n, seed=seed + 1)
+    table = hss.DataTable.build(vec, bits, tags, device=0, doc_num_per_segment=16384)
+    return mix, vec, bits, table
+
+
+def _queries(mix, n, seed, k=None):
+    q = mix.queries(n, seed=seed)
+    exprs = data.make_filters(mix, n, n_tags=(1, 4), seed=seed + 1, selectivity_range=(1e-3, 1.0))
+    rng = np.random.default_rng(seed + 2)
+    topks = (rng.choice([10, 100, 1000], n) if k is None else np.full(n, k)).astype(np.uint32)
+    return q, exprs, topks
+
+
+def _search(s, q, exprs, topks):
+    for a, e, k in zip(q, exprs, topks):
+        s.add_query(e, a, int(k))
+    return s.batch_search()
+
+
+def _check_exact(res, want, nq):
+    scores, ids, counts = res
+    ws, wi, wc = want
+    for i in range(nq):
+        c = int(wc[i])
+        assert int(counts[i]) == c, i
+        assert (ids[i][:c] == wi[i][:c]).all(), i
+        assert (scores[i][:c].view(np.uint32) == ws[i][:c].view(np.uint32)).all(), i
+
+
+@pytest.mark.parametrize("method", [2, 1], ids=["bf16", "tf32"])
+def test_learned_threshold_search_is_exact(torch_cuda, method):
+    mix, vec, bits, table = _world()
+    s = hss.FullRecallSearcher(table, max_batch=256, method=method)
+    qt, et, kt = _queries(mix, 3072, 90)
+    model, margin, report = fit_threshold_model(s, qt, et, kt, hidden=128, steps=600, seed=1)
+    assert report["loss_last_epoch"] < report["loss_first_epoch"]
+    qv, ev, kv = _queries(mix, 200, 95)
+    want = oracle.topk(qv, ev, kv, vec, bits, threads=8)
+    for m in (margin, -1.0, 1.5):  # calibrated, far too high a threshold, far too low
+        s.set_threshold_model(model, m)
+        _check_exact(_search(s, qv, ev, kv), want, len(qv))
+        assert (s.last_status(len(qv)) == 0).all()
+
+
+def test_learned_threshold_prunes_the_estimation_pass(torch_cuda):
+    # 400k docs against a 4096-doc sample: the sample's proven threshold is loose, so the estimation
+    # pass at that threshold keeps many docs; the model's threshold should keep far fewer, with few
+    # queries whose prediction was too high (kept fewer than K, so the sample's threshold stood)
+    mix, vec, bits, table = _world(seed=83, n=400000)
+    s = hss.FullRecallSearcher(table, max_batch=256, method=2, sample_docs=4096)
+    qt, et, kt = _queries(mix, 8192, 96)
+    model, margin, report = fit_threshold_model(s, qt, et, kt, hidden=128, steps=3000, seed=2)
+    qv, ev, kv = _queries(mix, 256, 99, k=100)
+    s.set_threshold_model(model, 1e9)  # a threshold of -inf: the estimation pass at the sample's threshold
+    _search(s, qv, ev, kv)
+    at_sample = s.last_estimate_counts(len(qv)).astype(np.int64)
+    s.set_threshold_model(model, margin)
+    _search(s, qv, ev, kv)
+    learned = s.last_estimate_counts(len(qv)).astype(np.int64)
+    assert (learned <= at_sample).all()  # the model can only raise the threshold
+    miss = np.mean(learned < kv)
+    pruned = 1.0 - learned.sum() / max(1, at_sample.sum())
+    print("learned threshold: estimation-pass docs", at_sample.sum(), "->", learned.sum(), "pruned", pruned,
+          "miss rate", miss, report)
+    assert pruned > 0.3, (pruned, miss, report)
+    assert miss < 0.15, (pruned, miss, report)
