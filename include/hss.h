@@ -108,8 +108,9 @@ int hss_aggregator_launch(const uint8_t* filterResult, const float* docScores, c
 /* Allocation-free aggregator. NO COUNTERPART IN THE REFERENCE (whose Aggregator always takes
  * pool-allocated scratch). Same arguments and results as hss_aggregator_launch minus the workspace:
  * for callers that must not allocate device memory per call or hold a workspace of their own --
- * a request handler running under a fixed memory budget, or code between setup and a stream
- * capture that may not call cudaMalloc. Its scratch is a 64 KB array compiled into the library,
+ * a request handler running under a fixed device-memory budget that another allocator owns, or a
+ * latency-critical loop that cannot afford cudaFree, which waits for the whole device to go idle.
+ * Its scratch is a 64 KB array compiled into the library,
  * one per device, so docNumber <= HSS_AGGREGATOR_NOALLOC_MAX_DOCS (else HSS_ERR_LIMIT, nothing
  * launched). It calls no allocator. The first call on each device looks the array's address up
  * (cudaGetSymbolAddress, with that device current), which may load the module: make that first
