@@ -5,11 +5,11 @@ FullRecallSearcher / QueryNode interface.
 """
 from . import data
 from ._lib import HssError, load
-from .api import (DataTable, Filters, FullRecallSearcher, ThresholdModel, aggregator, aggregator_noalloc, aggregator_workspace_size,
+from .api import (DataTable, Filters, FullRecallSearcher, Server, ThresholdModel, aggregator, aggregator_noalloc, aggregator_workspace_size,
                   bitmap_text_filter, device_count, hash64, posting_bitlist_to_set, posting_serialize, topk,
                   vector_score)
 
-__all__ = ["DataTable", "Filters", "FullRecallSearcher", "HssError", "ThresholdModel", "aggregator", "aggregator_noalloc",
+__all__ = ["DataTable", "Filters", "FullRecallSearcher", "HssError", "Server", "ThresholdModel", "aggregator", "aggregator_noalloc",
            "aggregator_workspace_size",
            "bitmap_text_filter", "data", "device_count", "hash64", "load", "posting_bitlist_to_set",
            "posting_serialize", "topk", "vector_score"]

@@ -63,6 +63,18 @@ class SearcherConfig(ctypes.Structure):
                 ("decodeInPlace", ctypes.c_int32)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_uint32), ("maxBatch", ctypes.c_uint32), ("maxWaitUs", ctypes.c_uint32),
+                ("method", ctypes.c_int32), ("memoryBudget", ctypes.c_uint64), ("candidateCap", ctypes.c_uint32),
+                ("sampleDocs", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("slots", ctypes.c_uint32),
+                ("meanBatch", ctypes.c_double), ("p50Ms", ctypes.c_double), ("p99Ms", ctypes.c_double),
+                ("maxMs", ctypes.c_double)]
+
+
 # (name, restype, argtypes) for every symbol include/hss.h declares.
 SIGNATURES = [
     ("hss_vector_score_launch", ctypes.c_int,
@@ -119,6 +131,18 @@ SIGNATURES = [
     ("hss_model_train_step", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32, ctypes.c_float,
                                             ctypes.POINTER(ctypes.c_float), vp]),
     ("hss_model_gradients", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32, vp, ctypes.POINTER(ctypes.c_float), vp]),
+    ("hss_server_create", ctypes.c_int, [vp, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
+    ("hss_server_free", None, [vp]),
+    ("hss_server_submit", ctypes.c_int, [vp, vp, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_uint32,
+                                         ctypes.POINTER(ctypes.c_uint64)]),
+    ("hss_server_wait", ctypes.c_int, [vp, ctypes.c_uint64, vp, vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.c_int32]),
+    ("hss_server_get_stats", ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
+    ("hss_server_reset_stats", ctypes.c_int, [vp]),
+    ("hss_server_set_threshold_model", ctypes.c_int, [vp, vp, ctypes.c_float]),
+    ("hss_server_run_poisson", ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, vp, ctypes.c_double, ctypes.c_uint64, vp,
+                                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("hss_last_error", ctypes.c_char_p, []),
     ("hss_device_count", ctypes.c_int, []),
 ]

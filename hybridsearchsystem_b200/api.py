@@ -236,6 +236,75 @@ class FullRecallSearcher:
                 "select_ms": float(ms[3]), "total_ms": float(ms[4]), "retries": r.value, "launches": l.value}
 
 
+class Server:
+    """The serving loop (continuous batching over one resident table; include/hss.h, hss_server_*)."""
+
+    def __init__(self, table, slots=2, max_batch=256, max_wait_us=200, method=0, memory_budget=0, candidate_cap=0,
+                 sample_docs=0):
+        cfg = _lib.ServerConfig(slots, max_batch, max_wait_us, method, memory_budget, candidate_cap, sample_docs)
+        h = ctypes.c_void_p()
+        check(_lib.load().hss_server_create(table._h, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.table = table
+        self.dim = table.info["dim"]
+
+    def close(self):
+        if self._h:
+            _lib.load().hss_server_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, filter_expr, vector, topk):
+        v = np.ascontiguousarray(vector, dtype=np.float32)
+        rid = ctypes.c_uint64()
+        check(_lib.load().hss_server_submit(self._h, _np_ptr(v), v.size, (filter_expr or "").encode(), topk,
+                                            ctypes.byref(rid)))
+        return rid.value
+
+    def wait(self, rid, cap=_lib.HSS_MAX_TOPK, timeout_ms=-1):
+        """(scores, ids, latency ms, status) of request rid, or None on timeout."""
+        sc = np.zeros(max(cap, 1), np.float32)
+        ids = np.zeros(max(cap, 1), np.int64)
+        n, lat, st = ctypes.c_uint32(), ctypes.c_double(), ctypes.c_int32()
+        rc = _lib.load().hss_server_wait(self._h, rid, _np_ptr(sc), _np_ptr(ids), cap, ctypes.byref(n),
+                                         ctypes.byref(lat), ctypes.byref(st), timeout_ms)
+        if rc == 1:
+            return None
+        check(rc)
+        k = min(n.value, cap)
+        return sc[:k], ids[:k], lat.value, st.value
+
+    def stats(self):
+        st = _lib.ServerStats()
+        check(_lib.load().hss_server_get_stats(self._h, ctypes.byref(st)))
+        return {"completed": st.completed, "batches": st.batches, "slots": st.slots, "mean_batch": st.meanBatch,
+                "p50_ms": st.p50Ms, "p99_ms": st.p99Ms, "max_ms": st.maxMs}
+
+    def reset_stats(self):
+        check(_lib.load().hss_server_reset_stats(self._h))
+
+    def set_threshold_model(self, model, margin):
+        check(_lib.load().hss_server_set_threshold_model(self._h, model._h if model else None, margin))
+        self._model = model
+
+    def run_poisson(self, queries, exprs, topks, rate_qps, seed=0):
+        """Open-loop Poisson arrivals at rate_qps; returns (latencies ms [n], offered QPS, wall seconds)."""
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        n = len(q)
+        arr = (ctypes.c_char_p * max(n, 1))(*[(e or "").encode() for e in exprs])
+        t = np.ascontiguousarray(topks, dtype=np.uint32)
+        lat = np.zeros(max(n, 1), np.float64)
+        offered, wall = ctypes.c_double(), ctypes.c_double()
+        check(_lib.load().hss_server_run_poisson(self._h, _np_ptr(q), n, arr, _np_ptr(t), float(rate_qps), seed,
+                                                 _np_ptr(lat), ctypes.byref(offered), ctypes.byref(wall)))
+        return lat[:n], offered.value, wall.value
+
+
 class ThresholdModel:
     """The learned K-th-score predictor (MLP din -> hidden -> hidden -> 1, GELU) on one GPU. Parameters
     are one flat FP32 vector: W1 [din][hidden], b1, W2 [hidden][hidden], b2, w3 [hidden], b3."""

@@ -43,6 +43,10 @@ struct hss_model {
     std::shared_ptr<hss::ThresholdModel> m;
 };
 
+struct hss_server {
+    std::unique_ptr<hss::ServingLoop> s;
+};
+
 struct hss_filters {
     std::vector<hss::FilterExpr> exprs;
 };
@@ -483,6 +487,85 @@ int hss_model_gradients(hss_model* m, const float* dX, const float* dT, uint32_t
                         hss_stream_t stream) {
     if (!m || B == 0 || !dX || !dT || !grad) return SetError(HSS_ERR_INVALID, "hss_model_gradients: bad arguments");
     return m->m->Gradients(dX, dT, B, grad, loss, S(stream)) == 0 ? HSS_OK : SetError(HSS_ERR_CUDA, m->m->Error());
+}
+
+// ---------------------------------------------------------------------------------------------
+// serving loop
+
+int hss_server_create(hss_table* table, const hss_server_config* cfg, hss_server** out) {
+    if (!table || !out) return SetError(HSS_ERR_INVALID, "hss_server_create: null argument");
+    hss::ServingConfig c;
+    if (cfg) {
+        if (cfg->slots) c.slots = cfg->slots;
+        if (cfg->maxBatch) c.maxBatch = cfg->maxBatch;
+        c.maxWaitUs = cfg->maxWaitUs;
+        c.memoryBudget = cfg->memoryBudget;
+        if (cfg->method < 0 || cfg->method > 3) return SetError(HSS_ERR_INVALID, "unknown scoring method");
+        c.searcher.method = static_cast<hss::ScoreMethod>(cfg->method);
+        if (cfg->candidateCap) c.searcher.candidateCap = cfg->candidateCap;
+        if (cfg->sampleDocs) c.searcher.sampleDocs = cfg->sampleDocs;
+    }
+    auto loop = std::make_unique<hss::ServingLoop>(table->t, c);
+    if (!loop->Ok()) return SetError(HSS_ERR_CUDA, loop->Error());
+    *out = new hss_server{std::move(loop)};
+    return HSS_OK;
+}
+
+void hss_server_free(hss_server* s) { delete s; }
+
+int hss_server_submit(hss_server* s, const float* vector, uint32_t dim, const char* filterExpr, uint32_t topK,
+                      uint64_t* id) {
+    if (!s) return SetError(HSS_ERR_INVALID, "hss_server_submit: null server");
+    const int rc = s->s->Submit(vector, dim, filterExpr, topK, id);
+    if (rc == -3) return SetError(HSS_ERR_PARSE, std::string("filter does not parse: ") + (filterExpr ? filterExpr : ""));
+    if (rc == -4) return SetError(HSS_ERR_PROGRAM, "filter program rejected");
+    if (rc != 0) return SetError(HSS_ERR_INVALID, "hss_server_submit: bad arguments");
+    return HSS_OK;
+}
+
+int hss_server_wait(hss_server* s, uint64_t id, float* scores, int64_t* ids, uint32_t cap, uint32_t* count,
+                    double* latencyMs, int32_t* status, int32_t timeoutMs) {
+    if (!s) return SetError(HSS_ERR_INVALID, "hss_server_wait: null server");
+    const int rc = s->s->Wait(id, scores, ids, cap, count, latencyMs, status, timeoutMs);
+    if (rc < 0) return SetError(HSS_ERR_INVALID, "hss_server_wait: unknown request id");
+    return rc;
+}
+
+int hss_server_get_stats(const hss_server* s, hss_server_stats* out) {
+    if (!s || !out) return SetError(HSS_ERR_INVALID, "hss_server_get_stats: null argument");
+    const hss::ServingStats st = s->s->Stats();
+    out->completed = st.completed;
+    out->batches = st.batches;
+    out->slots = st.slots;
+    out->meanBatch = st.meanBatch;
+    out->p50Ms = st.p50Ms;
+    out->p99Ms = st.p99Ms;
+    out->maxMs = st.maxMs;
+    return HSS_OK;
+}
+
+int hss_server_reset_stats(hss_server* s) {
+    if (!s) return SetError(HSS_ERR_INVALID, "hss_server_reset_stats: null server");
+    s->s->ResetStats();
+    return HSS_OK;
+}
+
+int hss_server_set_threshold_model(hss_server* s, hss_model* model, float margin) {
+    if (!s) return SetError(HSS_ERR_INVALID, "hss_server_set_threshold_model: null server");
+    if (s->s->SetThresholdModel(model ? model->m : nullptr, margin) != 0)
+        return SetError(HSS_ERR_INVALID, "threshold model does not fit this server's searchers");
+    return HSS_OK;
+}
+
+int hss_server_run_poisson(hss_server* s, const float* queries, uint32_t n, const char* const* filterExprs,
+                           const uint32_t* topks, double rateQps, uint64_t seed, double* latencyMs,
+                           double* offeredQps, double* wallSeconds) {
+    if (!s || !queries || !filterExprs || !topks || rateQps <= 0)
+        return SetError(HSS_ERR_INVALID, "hss_server_run_poisson: bad arguments");
+    const int bad = s->s->RunPoisson(queries, n, filterExprs, topks, rateQps, seed, latencyMs, offeredQps, wallSeconds);
+    if (bad < 0) return SetError(HSS_ERR_INVALID, "hss_server_run_poisson: bad arguments");
+    if (bad > 0) return SetError(HSS_ERR_QUERY, std::to_string(bad) + " queries failed");
+    return HSS_OK;
 }
 
 uint64_t hss_hash64(const char* data, uint32_t len) { return hss::Hash64(data, len); }

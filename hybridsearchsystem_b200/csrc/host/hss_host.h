@@ -14,8 +14,13 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <cstdint>
+#include <deque>
 #include <memory>
+#include <mutex>
+#include <thread>
 #include <string>
 #include <unordered_map>
 #include <unordered_set>
@@ -486,6 +491,105 @@ class FullRecallSearcher {
     float* m_featuresOut = nullptr;  // Features(): stop after writing the feature rows here
     std::vector<float> m_lastTheta1, m_lastThetaA;
     uint32_t m_lastEstSegs = 0;  // list segments of the last estimation pass (0: none ran)
+};
+
+// ---------------------------------------------------------------------------------------------
+// Serving loop: continuous batching of single queries over one resident table.
+//
+// Clients submit (vector, filter text, K) at any time; the filter is compiled on the submitting
+// thread. `slots` workers each own a FullRecallSearcher (its whole device arena) and a CUDA stream.
+// A free worker takes every queued request up to maxBatch -- waiting at most maxWaitUs for more when
+// fewer are queued -- and runs them as one batch, so requests that arrive while other batches are on
+// the GPU join the next batch of the next free slot, and the slots' batches overlap on the device.
+// The slot count is admitted by device memory: at most what `memoryBudget` bytes of searcher arenas
+// allow. Each request's latency runs from its submission to its result being on the host.
+struct ServingConfig {
+    uint32_t slots = 2;
+    uint32_t maxBatch = 256;
+    uint32_t maxWaitUs = 200;
+    uint64_t memoryBudget = 0;  // bytes for the slots' arenas; 0 = half of the free device memory
+    SearcherConfig searcher;    // maxBatch is taken from above
+};
+
+struct ServingStats {
+    uint64_t completed = 0, batches = 0;
+    uint32_t slots = 0;
+    double meanBatch = 0, p50Ms = 0, p99Ms = 0, maxMs = 0;
+};
+
+class ServingLoop {
+   public:
+    ServingLoop(std::shared_ptr<DataTable> table, const ServingConfig& cfg);
+    ~ServingLoop();
+    ServingLoop(const ServingLoop&) = delete;
+    ServingLoop& operator=(const ServingLoop&) = delete;
+    bool Ok() const { return m_ok; }
+    const std::string& Error() const { return m_err; }
+
+    // 0 and *id on success; HSS-style negative codes: -3 the filter does not parse, -4 bad program,
+    // -1 bad arguments.
+    int Submit(const float* vec, uint32_t dim, const char* filter, uint32_t topK, uint64_t* id);
+    // Blocks (up to timeoutMs, < 0 = forever) for request `id`, copies its results (scores desc,
+    // global ids) into cap-entry arrays and forgets it. 0 done, 1 timed out, -1 unknown id. *status
+    // gets the query's status bits (HSS_QSTATUS_*), or -2 when its batch failed on the device.
+    int Wait(uint64_t id, float* scores, int64_t* ids, uint32_t cap, uint32_t* count, double* latencyMs,
+             int32_t* status, int timeoutMs);
+    ServingStats Stats() const;
+    void ResetStats();
+    // Open-loop load: n queries (row i of queries [n][dim], filters[i], topks[i]) submitted at Poisson
+    // arrival times of rate rateQps, each waited for; per-request latency into latencyMs[n]. Returns
+    // the number of failed requests; *offeredQps = the arrival rate actually achieved.
+    int RunPoisson(const float* queries, uint32_t n, const char* const* filters, const uint32_t* topks, double rateQps,
+                   uint64_t seed, double* latencyMs, double* offeredQps, double* wallSeconds);
+    int SetThresholdModel(std::shared_ptr<ThresholdModel> model, float margin);
+    uint32_t Slots() const { return static_cast<uint32_t>(m_slots.size()); }
+
+   private:
+    struct Request {
+        uint64_t id = 0;
+        std::vector<float> vec;
+        FilterExpr expr;
+        uint32_t topK = 0;
+        std::chrono::steady_clock::time_point arrival, done;
+        std::vector<float> scores;
+        std::vector<int64_t> ids;
+        uint32_t count = 0;
+        int32_t status = 0;
+        bool finished = false;
+    };
+    struct Slot {
+        std::unique_ptr<FullRecallSearcher> searcher;
+        cudaStream_t stream = nullptr;
+        float* hQ = nullptr;  // pinned [maxBatch][dim]
+        float* dQ = nullptr;
+        float *hSc = nullptr, *dSc = nullptr;  // [maxBatch][kMaxTopK]
+        int64_t *hId = nullptr, *dId = nullptr;
+        uint32_t *hCnt = nullptr, *dCnt = nullptr;
+        uint64_t modelGen = 0;
+        std::thread worker;
+    };
+    void Worker(Slot* slot);
+    void RunBatch(Slot* slot, std::vector<std::shared_ptr<Request>>& batch);
+
+    std::shared_ptr<DataTable> m_table;
+    ServingConfig m_cfg;
+    bool m_ok = false;
+    std::string m_err;
+    uint32_t m_dim = 0;
+    std::vector<std::unique_ptr<Slot>> m_slots;
+    mutable std::mutex m_mu;
+    std::condition_variable m_cvQueue, m_cvDone;
+    std::deque<std::shared_ptr<Request>> m_queue;
+    std::unordered_map<uint64_t, std::shared_ptr<Request>> m_live;
+    uint64_t m_nextId = 1;
+    bool m_stop = false;
+    // threshold model: each slot picks up a new one before its next batch
+    std::shared_ptr<ThresholdModel> m_model;
+    float m_margin = 0.0f;
+    uint64_t m_modelGen = 0;
+    // stats
+    std::vector<double> m_lat;
+    uint64_t m_batches = 0, m_batched = 0;
 };
 
 }  // namespace hss

@@ -268,6 +268,50 @@ int hss_model_train_step(hss_model* m, const float* dX, const float* dT, uint32_
 int hss_model_gradients(hss_model* m, const float* dX, const float* dT, uint32_t B, float* grad, float* loss,
                         hss_stream_t stream);
 
+/* ---- serving loop ----
+ * Continuous batching of single queries over one resident table: clients submit (vector, filter text,
+ * K) at any time; `slots` workers, each with its own searcher arena and CUDA stream, take every
+ * queued request (up to maxBatch, waiting at most maxWaitUs for more) as one batch, so batches of
+ * different slots overlap on the GPU and requests arriving meanwhile join the next free slot's batch.
+ * Slots are admitted by device memory (memoryBudget bytes of arenas). Replaces the reference's
+ * RunContext / schedule_* drivers (run_context.cpp:121-274), which run pre-formed batches. */
+typedef struct hss_server hss_server;
+typedef struct hss_server_config {
+    uint32_t slots;        /* concurrent batches on the GPU (default 2) */
+    uint32_t maxBatch;     /* queries per batch (default 256) */
+    uint32_t maxWaitUs;    /* longest wait for a fuller batch (default 200) */
+    int32_t method;        /* as hss_searcher_config.method */
+    uint64_t memoryBudget; /* bytes for the slots' arenas; 0 = half the free device memory */
+    uint32_t candidateCap; /* as in hss_searcher_config; 0 = default */
+    uint32_t sampleDocs;
+} hss_server_config;
+typedef struct hss_server_stats {
+    uint64_t completed, batches;
+    uint32_t slots;
+    double meanBatch, p50Ms, p99Ms, maxMs; /* latency from submission to results on the host */
+} hss_server_stats;
+
+int hss_server_create(hss_table* table, const hss_server_config* cfg, hss_server** out);
+void hss_server_free(hss_server* s);
+/* Compiles the filter on the calling thread and queues the query; *id identifies it. */
+int hss_server_submit(hss_server* s, const float* vector, uint32_t dim, const char* filterExpr, uint32_t topK,
+                      uint64_t* id);
+/* Blocks up to timeoutMs (< 0: no limit) for query id; copies up to cap results (scores descending,
+ * global doc ids), *count = its result count, *latencyMs, *status (HSS_QSTATUS_* bits, -2 when its
+ * batch failed on the device). HSS_OK, 1 on timeout (the query stays pending), HSS_ERR_INVALID for an
+ * unknown id. Each id is returned once. */
+int hss_server_wait(hss_server* s, uint64_t id, float* scores, int64_t* ids, uint32_t cap, uint32_t* count,
+                    double* latencyMs, int32_t* status, int32_t timeoutMs);
+int hss_server_get_stats(const hss_server* s, hss_server_stats* out);
+int hss_server_reset_stats(hss_server* s);
+int hss_server_set_threshold_model(hss_server* s, hss_model* model, float margin);
+/* Open-loop load test: query i (queries [n][dim], filterExprs[i], topks[i]) arrives at Poisson times
+ * of rate rateQps; per-request latencies into latencyMs[n]. Returns HSS_OK, or HSS_ERR_QUERY when
+ * some queries failed; *offeredQps = the arrival rate achieved, *wallSeconds = the whole run. */
+int hss_server_run_poisson(hss_server* s, const float* queries, uint32_t n, const char* const* filterExprs,
+                           const uint32_t* topks, double rateQps, uint64_t seed, double* latencyMs,
+                           double* offeredQps, double* wallSeconds);
+
 /* ---- host-side codec (the index format contract) ---- */
 /* Hash64 (src/engine/core/hash/hash.cpp:10-16). */
 uint64_t hss_hash64(const char* data, uint32_t len);
