@@ -48,8 +48,16 @@ def parse_args():
     ap.add_argument("--cpu-queries", type=int, default=0, help="CPU baseline sample size (0: 2 per thread)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cand-cap", type=int, default=1 << 18, help="per-query candidate capacity")
-    ap.add_argument("--method", default="tf32", choices=list(METHODS),
-                    help="candidate pass: simt (FP32 FFMA), tf32 (tensor cores over the FP32 rows), bf16, e4m3")
+    ap.add_argument("--method", default="bf16", choices=list(METHODS),
+                    help="the chosen form's candidate pass: simt (FP32 FFMA), tf32 (tensor cores over the FP32 "
+                         "rows), bf16, e4m3")
+    ap.add_argument("--learned", action="store_true", help="the chosen form uses the learned threshold")
+    ap.add_argument("--train-queries", type=int, default=8192, help="training queries of the learned threshold")
+    ap.add_argument("--no-plain", dest="plain", action="store_false",
+                    help="skip measuring the plain FP32 (TF32) form beside the chosen one")
+    ap.add_argument("--no-serve", dest="serve", action="store_false", help="skip the serving-loop latency sweep")
+    ap.add_argument("--serve-requests", type=int, default=40000)
+    ap.add_argument("--serve-wait-us", type=int, default=300)
     return ap.parse_args()
 
 
@@ -208,24 +216,38 @@ def config_of(args, world):
             "docs": args.docs, "dim": 128, "tags": 256, "batch": args.batch, "topk": args.topk,
             "doc_num_per_segment": 131072, "filters": "1-6 tags AND/OR/NOT, est. selectivity 1e-4..1",
             "parallelism": f"replica x{world}",
-            "l2": "inputs larger than L2: every step reads the 5.1 GB corpus"}
+            "l2": "inputs larger than L2: every step reads the whole corpus copy (FP32 5.1 GB, BF16 2.6 GB, "
+                  "E4M3 1.3 GB)"}
 
 
-def run_ours(args):
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def measure_form(args, ctx, method, learned=False):
+    """One form of the path (candidate-pass method, with or without the learned threshold) over the
+    workload: device-resident QPS (CUDA events, max over ranks), end-to-end QPS through the C-ABI,
+    stage times and the candidate stage's roofline."""
     import torch
-    import torch.distributed as dist
 
     import hybridsearchsystem_b200 as hss
-    rank, local, world = dist_env()
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-    dev = f"cuda:{local}"
-    _, vec, bits, queries, exprs = workload(args, dev)
-    table = hss.DataTable.build(vec, bits, 256, device=local, doc_num_per_segment=131072)
+    from hybridsearchsystem_b200.threshold import fit_threshold_model
+    rank, world, dev, table = ctx["rank"], ctx["world"], ctx["dev"], ctx["table"]
+    queries, exprs, barrier = ctx["queries"], ctx["exprs"], ctx["barrier"]
     B, K = args.batch, args.topk
-    searcher = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[args.method])
+    searcher = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[method])
+    report = None
+    if learned:
+        # trained on its own queries (seeded apart from the measured ones), labels from the exact path
+        tq = ctx["mix"].queries(args.train_queries, seed=20)
+        te = data_filters(ctx["mix"], args.train_queries, 21)
+        tk = np.random.default_rng(22).choice([10, 100, 1000], args.train_queries).astype(np.uint32)
+        model, margin, report = fit_threshold_model(searcher, tq, te, tk, hidden=256, steps=2000, seed=3)
+        searcher.set_threshold_model(model, margin)
     searcher.set_timing(True)
     nb = max(1, len(queries) // B)
     filters = [searcher.compile_filters(exprs[i * B:(i + 1) * B]) for i in range(nb)]
@@ -244,15 +266,11 @@ def run_ours(args):
         assert rc == 0, searcher.last_status(B)
         return searcher.last_times()
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
     # device-resident leg
-    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
     cand_ms, launches, stage_ms = [], 0, []
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(gpu_id) as clk:
@@ -267,9 +285,8 @@ def run_ours(args):
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
-    t_ms = ev0.elapsed_time(ev1)
     clocks = clk.summary()
-    t_max = max_over_ranks(t_ms, dev)
+    t_max = max_over_ranks(ev0.elapsed_time(ev1), dev)
     value = whole_job_qps(world, args.steps, B, t_max)
 
     # end-to-end leg through the C-ABI: pinned host queries in, results out, every step
@@ -298,45 +315,126 @@ def run_ours(args):
     barrier()
     e2e = whole_job_qps(world, args.steps, B, max_over_ranks(e0.elapsed_time(e1), dev))
 
-    # roofline of the dominant kernel (the candidate pass): algorithmic bytes per launch = the corpus
-    # (docs x 128 x 4 B) + the batch's filter bitmaps (B x docs/8 B)
+    # roofline of the dominant stage, the candidate passes: algorithmic bytes per batch = the corpus
+    # rows the passes read (docs x 128 x element bytes, +4 B scale for E4M3; a learned form's
+    # estimation pass re-reads a quarter) + the batch's filter bitmaps (B x docs/8 B)
     info = table.info
     words = info["segment_num"] * info["doc_num_per_segment"] // 64
-    elem = {"simt": 4, "tf32": 4, "bf16": 2, "e4m3": 1}[args.method]
-    alg_bytes = args.docs * 128 * elem + B * words * 8 + (args.docs * 4 if args.method == "e4m3" else 0)
-    cand_avg = float(np.mean(cand_ms)) if cand_ms else float("nan")
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
+    elem = {"simt": 4, "tf32": 4, "bf16": 2, "e4m3": 1}[method]
+    reads = 1.25 if learned else 1.0
+    alg_bytes = reads * args.docs * (128 * elem + (4 if method == "e4m3" else 0)) + B * words * 8
+    cand_avg = float(np.mean(cand_ms))
+    peaks = _peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg_bytes / (cand_avg / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "cand_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("bytes_per_launch_full_workload")
+            traffic = json.load(f).get(method)
+    kernel = "cand_simt_kernel" if method == "simt" else ("tc2_cand_kernel" if B > 128 else "tc_cand_kernel")
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": traffic, "kernel": "cand_simt_kernel" if args.method == "simt" else "tc_cand_kernel",
-            "avg_ms": cand_avg,
+            "traffic": traffic, "kernel": kernel, "avg_ms": cand_avg,
             "peak_source": "measured" if peaks else "fallback"}
-
-    rec = {"metric": METRIC, "value": value, "unit": "QPS", "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded cluster mixture, HYDSET2 shapes)",
-           "config": dict(config_of(args, world), form=FORMS[args.method], method=args.method),
-           "e2e": {"value": e2e, "unit": "QPS", "h2d_bytes_per_step": B * 128 * 4,
-                   "d2h_bytes_per_step": B * K * (4 + 8) + B * 4},
-           "roofline": roof, "clocks": clocks, "gpu_launches": launches,
+    out = {"value": value, "t_max_ms": t_max, "e2e": e2e, "roofline": roof, "clocks": clocks, "launches": launches,
            "stages_ms": dict(zip(["filter", "sample", "candidates", "select", "total"],
-                                 [round(float(x), 4) for x in np.mean(np.array(stage_ms), axis=0)]))}
+                                 [round(float(x), 4) for x in np.mean(np.array(stage_ms), axis=0)])),
+           "form": FORMS[method] + (" + learned threshold" if learned else ""), "method": method,
+           "learned": learned, "searcher": searcher, "filters": filters, "d_q": d_q,
+           "out": (o_sc, o_id, o_n, topks, sh)}
+    if report:
+        out["learned_report"] = {k: (round(v, 5) if isinstance(v, float) else v) for k, v in report.items()}
+    return out
+
+
+def data_filters(mix, n, seed):
+    from hybridsearchsystem_b200 import data
+    return data.make_filters(mix, n, n_tags=(1, 6), seed=seed, selectivity_range=(1e-4, 1.0))
+
+
+def measure_serving(args, ctx, method, rates):
+    """p50/p99 latency of single queries through the serving loop (continuous batching) at
+    open-loop Poisson arrival rates."""
+    import hybridsearchsystem_b200 as hss
+    srv = hss.Server(ctx["table"], slots=2, max_batch=args.batch, max_wait_us=args.serve_wait_us,
+                     method=METHODS[method], candidate_cap=args.cand_cap)
+    q, ex = ctx["queries"], ctx["exprs"]
+    out = []
+    for rate in rates:
+        n = int(min(args.serve_requests, max(2000, rate * 0.6)))
+        idx = np.arange(n) % len(q)
+        srv.reset_stats()
+        lat, offered, wall = srv.run_poisson(q[idx], [ex[i] for i in idx], np.full(n, args.topk, np.uint32), rate,
+                                             seed=int(rate))
+        st = srv.stats()
+        out.append({"offered_qps": round(offered), "completed_qps": round(n / wall), "p50_ms": round(st["p50_ms"], 3),
+                    "p99_ms": round(st["p99_ms"], 3), "mean_batch": round(st["mean_batch"], 1)})
+    srv.close()
+    return {"form": FORMS[method], "slots": 2, "max_wait_us": args.serve_wait_us, "topk": args.topk,
+            "rates": out}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import hybridsearchsystem_b200 as hss
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    dev = f"cuda:{local}"
+    mix, vec, bits, queries, exprs = workload(args, dev)
+    table = hss.DataTable.build(vec, bits, 256, device=local, doc_num_per_segment=131072)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    ctx = {"rank": rank, "world": world, "dev": dev, "table": table, "queries": queries, "exprs": exprs,
+           "barrier": barrier, "mix": mix}
+    B, K = args.batch, args.topk
+    chosen = measure_form(args, ctx, args.method, learned=args.learned)
+    forms = {"chosen": chosen}
+    if args.plain:
+        # the two plain FP32 forms (both read the FP32 rows): TF32 tensor cores, and SIMT FFMA
+        if not (args.method == "tf32" and not args.learned):
+            forms["plain_fp32"] = measure_form(args, ctx, "tf32")
+        forms["plain_fp32_simt"] = measure_form(args, ctx, "simt")
+    serving = None
+    if rank == 0 and world == 1 and args.serve:
+        rates = [r * chosen["value"] for r in (0.25, 0.5, 0.75)]
+        serving = measure_serving(args, ctx, args.method, rates)
+
+    def summary(f):
+        d = {"value": f["value"], "e2e_qps": f["e2e"], "ms_per_step": f["t_max_ms"] / args.steps,
+             "stages_ms": f["stages_ms"], "roofline_frac": f["roofline"]["frac"], "form": f["form"]}
+        if "learned_report" in f:
+            d["learned_report"] = f["learned_report"]
+        return d
+
+    rec = {"metric": METRIC, "value": chosen["value"], "unit": "QPS", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": chosen["t_max_ms"] / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": {"simt": "f32", "tf32": "f32", "bf16": "bf16",
+                                                             "e4m3": "e4m3"}[args.method] + "+f32 rescore",
+           "data": "synthetic (seeded cluster mixture, HYDSET2 shapes)",
+           "config": dict(config_of(args, world), form=chosen["form"], method=args.method, learned=args.learned),
+           "e2e": {"value": chosen["e2e"], "unit": "QPS", "h2d_bytes_per_step": B * 128 * 4,
+                   "d2h_bytes_per_step": B * K * (4 + 8) + B * 4},
+           "roofline": chosen["roofline"], "clocks": chosen["clocks"], "gpu_launches": chosen["launches"],
+           "stages_ms": chosen["stages_ms"], "forms": {k: summary(v) for k, v in forms.items()}}
+    if "plain_fp32" in forms:
+        rec["chosen_over_plain"] = chosen["value"] / forms["plain_fp32"]["value"]
+    if serving:
+        rec["serving"] = serving
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, ref_ids, ref_counts = cpu_baseline(vec, bits, queries, exprs, K, args.cpu_queries)
         rec["cpu_baseline"] = cb
-        # parity at full scale: the GPU's ids for the CPU sample's queries (first batches)
+        # parity at full scale: the chosen form's ids for the CPU sample's queries, in order
+        searcher, filters, d_q = chosen["searcher"], chosen["filters"], chosen["d_q"]
+        o_sc, o_id, o_n, topks, sh = chosen["out"]
         nq = len(ref_counts)
         ok = True
         for j in range((nq + B - 1) // B):
@@ -349,9 +447,9 @@ def run_ours(args):
                 if qi >= nq:
                     break
                 c = int(ref_counts[qi])
-                if int(g_n[i]) != c or set(g_id[i][:c].tolist()) != set(ref_ids[qi][:c].tolist()):
+                if int(g_n[i]) != c or not (g_id[i][:c] == ref_ids[qi][:c]).all():
                     ok = False
-        rec["parity_full_scale"] = {"queries": nq, "ids_match_cpu_ground_truth": ok, "against": cb["kind"]}
+        rec["parity_full_scale"] = {"queries": nq, "ids_match_cpu_ground_truth_in_order": ok, "against": cb["kind"]}
     if rank == 0:
         print(json.dumps(rec))
     if world > 1:

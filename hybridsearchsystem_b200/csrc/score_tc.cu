@@ -274,11 +274,52 @@ __device__ inline float max3(float a, float b, float c) {
     return d;
 }
 
+// Maximum of a lane's 32 scores as a tree of three-input maxima (four dependent steps, not sixteen:
+// the epilogue warps have little else to hide the latency behind).
 __device__ inline float max32(const uint32_t (&r)[32]) {
-    float m = __uint_as_float(r[0]);
+    float a[11];
 #pragma unroll
-    for (int i = 1; i < 31; i += 2) m = max3(m, __uint_as_float(r[i]), __uint_as_float(r[i + 1]));
-    return fmaxf(m, __uint_as_float(r[31]));
+    for (int i = 0; i < 10; ++i)
+        a[i] = max3(__uint_as_float(r[3 * i]), __uint_as_float(r[3 * i + 1]), __uint_as_float(r[3 * i + 2]));
+    a[10] = fmaxf(__uint_as_float(r[30]), __uint_as_float(r[31]));
+    const float b0 = max3(a[0], a[1], a[2]), b1 = max3(a[3], a[4], a[5]), b2 = max3(a[6], a[7], a[8]);
+    const float b3 = fmaxf(a[9], a[10]);
+    return fmaxf(max3(b0, b1, b2), b3);
+}
+
+// v[j] for a lane-varying j, as a five-level select tree over registers (no local-memory array).
+__device__ __forceinline__ uint32_t pick32(const uint32_t (&v)[32], uint32_t j) {
+    uint32_t a[16], b[8], c[4], d[2];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a[i] = (j & 16u) ? v[i + 16] : v[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) b[i] = (j & 8u) ? a[i + 8] : a[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) c[i] = (j & 4u) ? b[i + 4] : b[i];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) d[i] = (j & 2u) ? c[i + 2] : c[i];
+    return (j & 1u) ? d[1] : d[0];
+}
+
+// One 32-doc chunk of a thread's TF32 / BF16 scores (its query): the docs whose filter bit (m) is set
+// and whose approximate score clears the threshold t go to the thread's list segment, in doc order.
+// The loop runs once per kept doc (typically zero or one per chunk), so the code stays small.
+__device__ __forceinline__ void emit_lane(uint32_t m, const uint32_t (&v)[32], float t, uint64_t doc0,
+                                          float* out_score, uint32_t* out_loc, uint32_t seg_cap, uint32_t& ncand) {
+    if (m == 0u || !(max32(v) >= t)) return;
+    uint32_t pass = 0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) pass |= (__uint_as_float(v[j]) >= t ? 1u : 0u) << j;
+    pass &= m;
+    while (pass != 0u) {
+        const uint32_t j = static_cast<uint32_t>(__ffs(pass) - 1);
+        pass &= pass - 1u;
+        if (ncand < seg_cap) {
+            out_score[ncand] = __uint_as_float(pick32(v, j));
+            out_loc[ncand] = static_cast<uint32_t>(doc0 + j);
+        }
+        ++ncand;
+    }
 }
 
 // One 32-doc chunk of a thread's E4M3 scores (its query, raw accumulators v): the docs whose filter
@@ -488,23 +529,8 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
                 if constexpr (F == kTcE4M3) {
                     emit_chunk<F>(live[c], m[c], v[c], t, theta, qs, L.doc_scale, doc0, out_score, out_loc, seg_cap,
                                   ncand);
-                } else {
-                    if (!live[c] || m[c] == 0u) continue;
-                    if (!(max32(v[c]) >= t)) continue;
-                    uint32_t pass = 0;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) pass |= (__uint_as_float(v[c][j]) >= t ? 1u : 0u) << j;
-                    pass &= m[c];
-                    if (pass == 0u) continue;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        if (!((pass >> j) & 1u)) continue;
-                        if (ncand < seg_cap) {
-                            out_score[ncand] = __uint_as_float(v[c][j]);
-                            out_loc[ncand] = static_cast<uint32_t>(doc0 + j);
-                        }
-                        ++ncand;
-                    }
+                } else if (live[c]) {
+                    emit_lane(m[c], v[c], t, doc0, out_score, out_loc, seg_cap, ncand);
                 }
             }
         }
@@ -751,23 +777,8 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
                 if constexpr (F == kTcE4M3) {
                     emit_chunk<F>(live[c], m[c], v[c], t, theta, qs, L.doc_scale, doc0, out_score, out_loc, seg_cap,
                                   ncand);
-                } else {
-                    if (!live[c] || m[c] == 0u) continue;
-                    if (!(max32(v[c]) >= t)) continue;
-                    uint32_t pass = 0;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) pass |= (__uint_as_float(v[c][j]) >= t ? 1u : 0u) << j;
-                    pass &= m[c];
-                    if (pass == 0u) continue;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        if (!((pass >> j) & 1u)) continue;
-                        if (ncand < seg_cap) {
-                            out_score[ncand] = __uint_as_float(v[c][j]);
-                            out_loc[ncand] = static_cast<uint32_t>(doc0 + j);
-                        }
-                        ++ncand;
-                    }
+                } else if (live[c]) {
+                    emit_lane(m[c], v[c], t, doc0, out_score, out_loc, seg_cap, ncand);
                 }
             }
         }
