@@ -52,7 +52,11 @@ def parse_args():
                     help="the chosen form's candidate pass: simt (FP32 FFMA), tf32 (tensor cores over the FP32 "
                          "rows), bf16, e4m3")
     ap.add_argument("--learned", action="store_true", help="the chosen form uses the learned threshold")
-    ap.add_argument("--train-queries", type=int, default=8192, help="training queries of the learned threshold")
+    ap.add_argument("--train-queries", type=int, default=32768, help="training queries of the learned threshold")
+    ap.add_argument("--no-learned-form", dest="learned_form", action="store_false",
+                    help="skip measuring the chosen format with the learned threshold beside it")
+    ap.add_argument("--e2e-workers", type=int, default=1,
+                    help="host threads (each with its own searcher and stream) in the end-to-end leg")
     ap.add_argument("--no-plain", dest="plain", action="store_false",
                     help="skip measuring the plain FP32 (TF32) form beside the chosen one")
     ap.add_argument("--no-serve", dest="serve", action="store_false", help="skip the serving-loop latency sweep")
@@ -289,30 +293,65 @@ def measure_form(args, ctx, method, learned=False):
     t_max = max_over_ranks(ev0.elapsed_time(ev1), dev)
     value = whole_job_qps(world, args.steps, B, t_max)
 
-    # end-to-end leg through the C-ABI: pinned host queries in, results out, every step
+    # end-to-end leg through the C-ABI: pinned host queries in, results out, every step. Each step
+    # is one batch through hss_filters_compile + hss_searcher_search_device with its host->device query
+    # copy and device->host result copy; args.e2e_workers host threads each drive their own searcher
+    # on their own stream and take every e2e_workers-th step, so one batch's host work (filter
+    # compilation, the per-batch status read, copies) overlaps another's GPU work.
+    import threading
     h_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1)).pin_memory()
-    h_sc = torch.zeros((B, K), dtype=torch.float32).pin_memory()
-    h_id = torch.zeros((B, K), dtype=torch.int64).pin_memory()
-    h_n = torch.zeros(B, dtype=torch.int32).pin_memory()
-    d_stage = torch.zeros((B, 128), dtype=torch.float32, device=dev)
+
+    def make_worker(sr):
+        return {"searcher": sr, "stream": torch.cuda.Stream(device=dev),
+                "h_sc": torch.zeros((B, K), dtype=torch.float32).pin_memory(),
+                "h_id": torch.zeros((B, K), dtype=torch.int64).pin_memory(),
+                "h_n": torch.zeros(B, dtype=torch.int32).pin_memory(),
+                "d_q": torch.zeros((B, 128), dtype=torch.float32, device=dev),
+                "o_sc": torch.zeros((B, K), dtype=torch.float32, device=dev),
+                "o_id": torch.zeros((B, K), dtype=torch.int64, device=dev),
+                "o_n": torch.zeros(B, dtype=torch.int32, device=dev), "rc": 0}
+
+    workers = [make_worker(searcher)]
+    for _ in range(1, max(1, args.e2e_workers)):
+        sr = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[method])
+        if learned:
+            sr.set_threshold_model(model, margin)
+        workers.append(make_worker(sr))
+
+    def run_steps(w, wi, steps):
+        st = w["stream"]
+        with torch.cuda.stream(st):
+            for i in range(wi, steps, len(workers)):
+                j = (rank * 7919 + args.warmup + i) % nb
+                w["d_q"].copy_(h_q[j], non_blocking=True)
+                f = w["searcher"].compile_filters(exprs[j * B:(j + 1) * B])
+                rc = w["searcher"].search_device(w["d_q"].data_ptr(), B, f, topks, w["o_sc"].data_ptr(),
+                                                 w["o_id"].data_ptr(), w["o_n"].data_ptr(), K, st.cuda_stream)
+                w["rc"] |= rc
+                w["h_sc"].copy_(w["o_sc"], non_blocking=True)
+                w["h_id"].copy_(w["o_id"], non_blocking=True)
+                w["h_n"].copy_(w["o_n"], non_blocking=True)
+                st.synchronize()
+                f.close()
+
+    def e2e_run(steps):
+        threads = [threading.Thread(target=run_steps, args=(w, wi, steps)) for wi, w in enumerate(workers)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+
+    e2e_run(len(workers) * 2)  # warm-up of the extra searchers
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
     e0.record(stream)
-    for i in range(args.steps):
-        j = (rank * 7919 + args.warmup + i) % nb
-        d_stage.copy_(h_q[j], non_blocking=True)
-        f = searcher.compile_filters(exprs[j * B:(j + 1) * B])
-        rc = searcher.search_device(d_stage.data_ptr(), B, f, topks, o_sc.data_ptr(), o_id.data_ptr(),
-                                    o_n.data_ptr(), K, sh)
-        assert rc == 0
-        h_sc.copy_(o_sc, non_blocking=True)
-        h_id.copy_(o_id, non_blocking=True)
-        h_n.copy_(o_n, non_blocking=True)
-        stream.synchronize()
+    e2e_run(args.steps)
+    torch.cuda.synchronize()
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
+    assert all(w["rc"] == 0 for w in workers)
     e2e = whole_job_qps(world, args.steps, B, max_over_ranks(e0.elapsed_time(e1), dev))
 
     # roofline of the dominant stage, the candidate passes: algorithmic bytes per batch = the corpus
@@ -336,7 +375,7 @@ def measure_form(args, ctx, method, learned=False):
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "traffic": traffic, "kernel": kernel, "avg_ms": cand_avg,
             "peak_source": "measured" if peaks else "fallback"}
-    out = {"value": value, "t_max_ms": t_max, "e2e": e2e, "roofline": roof, "clocks": clocks, "launches": launches,
+    out = {"value": value, "t_max_ms": t_max, "e2e": e2e, "e2e_workers": len(workers), "roofline": roof, "clocks": clocks, "launches": launches,
            "stages_ms": dict(zip(["filter", "sample", "candidates", "select", "total"],
                                  [round(float(x), 4) for x in np.mean(np.array(stage_ms), axis=0)])),
            "form": FORMS[method] + (" + learned threshold" if learned else ""), "method": method,
@@ -344,6 +383,24 @@ def measure_form(args, ctx, method, learned=False):
            "out": (o_sc, o_id, o_n, topks, sh)}
     if report:
         out["learned_report"] = {k: (round(v, 5) if isinstance(v, float) else v) for k, v in report.items()}
+        # what the model does on this workload: its estimation pass against the same pass at the doc
+        # sample's proven threshold (margin 1e9 turns the prediction into -inf), over the measured batches
+        at_sample, at_model, kk = [], [], []
+        for j in range(min(nb, 8)):
+            for m, sink in ((1e9, at_sample), (margin, at_model)):
+                searcher.set_threshold_model(model, m)
+                rc = searcher.search_device(d_q[j].data_ptr(), B, filters[j], topks, o_sc.data_ptr(), o_id.data_ptr(),
+                                            o_n.data_ptr(), K, sh)
+                assert rc == 0
+                sink.append(searcher.last_estimate_counts(B).astype(np.int64))
+            kk.append(topks.astype(np.int64))
+        at_sample, at_model, kk = np.concatenate(at_sample), np.concatenate(at_model), np.concatenate(kk)
+        searcher.set_threshold_model(model, margin)
+        out["learned_report"].update({
+            "estimation_pass_docs_at_sample_threshold": int(at_sample.sum()),
+            "estimation_pass_docs_at_model_threshold": int(at_model.sum()),
+            "pruned_fraction": round(1.0 - at_model.sum() / max(1, at_sample.sum()), 4),
+            "miss_rate": round(float(np.mean(at_model < kk)), 4), "queries": int(len(kk))})
     return out
 
 
@@ -397,6 +454,9 @@ def run_ours(args):
     B, K = args.batch, args.topk
     chosen = measure_form(args, ctx, args.method, learned=args.learned)
     forms = {"chosen": chosen}
+    if args.learned_form and not args.learned:
+        # the chosen format with the learned threshold, measured beside it
+        forms["chosen_learned"] = measure_form(args, ctx, args.method, learned=True)
     if args.plain:
         # the two plain FP32 forms (both read the FP32 rows): TF32 tensor cores, and SIMT FFMA
         if not (args.method == "tf32" and not args.learned):
@@ -421,7 +481,9 @@ def run_ours(args):
            "data": "synthetic (seeded cluster mixture, HYDSET2 shapes)",
            "config": dict(config_of(args, world), form=chosen["form"], method=args.method, learned=args.learned),
            "e2e": {"value": chosen["e2e"], "unit": "QPS", "h2d_bytes_per_step": B * 128 * 4,
-                   "d2h_bytes_per_step": B * K * (4 + 8) + B * 4},
+                   "d2h_bytes_per_step": B * K * (4 + 8) + B * 4, "host_threads": chosen["e2e_workers"],
+                   "path": "hss_filters_compile + hss_searcher_search_device per batch, pinned host "
+                           "queries in and results out"},
            "roofline": chosen["roofline"], "clocks": chosen["clocks"], "gpu_launches": chosen["launches"],
            "stages_ms": chosen["stages_ms"], "forms": {k: summary(v) for k, v in forms.items()}}
     if "plain_fp32" in forms:

@@ -148,8 +148,10 @@ __device__ inline bool eval_words(const uint32_t* prog, uint32_t plen, const uin
             if (pc + 2 >= plen) return false;
             const uint32_t pn = prog[pc + 1], sn = prog[pc + 2];
             pc += 3;
-            const bool ok = op == kOpNot ? (pn + sn == 1) : (pn + sn > 0);
-            if (!ok || next + pn > nop || sn > sp) return false;
+            // comparisons written so that no u32 sum can wrap (the program may come straight from a
+            // caller's device buffer): next <= nop always holds
+            const bool ok = op == kOpNot ? ((pn == 1 && sn == 0) || (pn == 0 && sn == 1)) : (pn != 0 || sn != 0);
+            if (!ok || pn > nop - next || sn > sp) return false;
             const uint64_t* row = slots + static_cast<uint64_t>(next) * slot_stride + w0;
             if (op == kOpNot) {
                 if (pn) {
@@ -187,12 +189,12 @@ __device__ inline bool eval_words(const uint32_t* prog, uint32_t plen, const uin
         } else if (op == kOpConjunction) {
             if (pc + 1 >= plen) return false;
             const uint32_t parts = prog[pc + 1];
-            if (parts == 0 || pc + 2 + parts > plen) return false;
+            if (parts == 0 || parts > plen - pc - 2) return false;
 #pragma unroll
             for (int k = 0; k < W; ++k) acc[k] = ~0ull;
             for (uint32_t p = 0; p < parts; ++p) {
                 const uint32_t pn = prog[pc + 2 + p];
-                if (pn == 0 || next + pn > nop) return false;
+                if (pn == 0 || pn > nop - next) return false;
                 uint64_t o[W];
 #pragma unroll
                 for (int k = 0; k < W; ++k) o[k] = 0ull;
@@ -462,6 +464,219 @@ cudaError_t launch_filter_dense_wpt(const DenseFilterLaunch& L, cudaStream_t str
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------------------------
+// The dense filter for programs of at most kWideMaxOpnd operands. A CTA takes up to
+// kWideTilesPerCta word tiles of one segment for one query; 128 threads each own 8 of a tile's 1024
+// words (2 adjacent words in each of 4 groups of 256), so the per-op decode is shared by 8 words.
+// Operands are read straight from the dense posting matrix as 16-byte read-only loads:
+// the batch's queries share rows, so most reads hit L2, and without staging buffers sized for the
+// batch's largest program the SM holds as many CTAs as registers allow. One thread checks the program
+// (check_program: eval_words' acceptance rules), so the evaluation carries no checks. The top of the
+// evaluation stack stays in registers; only entries under it (a sibling subtree still waiting for its
+// parent) go to a local array.
+constexpr int kWideT = 128;
+constexpr int kWideW = 8;
+constexpr uint32_t kWideTW = kWideT * kWideW;  // words per tile
+constexpr uint32_t kWideGS = 2 * kWideT;       // words between a thread's word pairs
+constexpr uint32_t kWideTilesPerCta = 4;       // word tiles of one segment per CTA
+constexpr uint32_t kWideMaxOpnd = 8;          // operand rows held in shared memory
+
+// True exactly when eval_words would accept the program (same rules, no evaluation).
+__device__ inline bool check_program(const uint32_t* prog, uint32_t plen, uint32_t nop) {
+    uint32_t sp = 0, next = 0, pc = 0;
+    while (pc < plen) {
+        const uint32_t op = prog[pc];
+        if (op == kOpAnd || op == kOpOr || op == kOpNot) {
+            if (pc + 2 >= plen) return false;
+            const uint32_t pn = prog[pc + 1], sn = prog[pc + 2];
+            pc += 3;
+            const bool ok = op == kOpNot ? ((pn == 1 && sn == 0) || (pn == 0 && sn == 1)) : (pn != 0 || sn != 0);
+            if (!ok || pn > nop - next || sn > sp) return false;
+            sp -= sn;
+            next += pn;
+        } else if (op == kOpConjunction) {
+            if (pc + 1 >= plen) return false;
+            const uint32_t parts = prog[pc + 1];
+            if (parts == 0 || parts > plen - pc - 2) return false;
+            for (uint32_t p = 0; p < parts; ++p) {
+                const uint32_t pn = prog[pc + 2 + p];
+                if (pn == 0 || pn > nop - next) return false;
+                next += pn;
+            }
+            pc += 2 + parts;
+        } else {
+            return false;
+        }
+        if (sp >= static_cast<uint32_t>(kMaxStack)) return false;
+        ++sp;
+    }
+    return sp == 1 && next == nop;
+}
+
+// This thread's kWideW words of operand i: words off[g] + {0, 1} of the operand's row in the segment.
+__device__ __forceinline__ void wide_load(const uint64_t* const* base, uint32_t i, const uint32_t (&off)[kWideW / 2],
+                                          uint64_t (&o)[kWideW]) {
+    const uint64_t* p = base[i];
+#pragma unroll
+    for (int g = 0; g < kWideW / 2; ++g) {
+        const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p + off[g]));
+        o[2 * g] = v.x;
+        o[2 * g + 1] = v.y;
+    }
+}
+
+// Evaluates a checked program (check_program) over this thread's kWideW words of the operand rows
+// at base[i] + off[g] into res.
+__device__ __forceinline__ void eval_wide(const uint32_t* s_prog, uint32_t plen, const uint64_t* const* s_base,
+                                          const uint32_t (&off)[kWideW / 2], uint64_t (&res)[kWideW]) {
+    uint64_t top[kWideW];
+    uint64_t deep[kMaxStack][kWideW];  // entries under the top
+    uint32_t depth = 0, next = 0, pc = 0;
+    bool has_top = false;
+    auto pop_into = [&](uint64_t (&acc)[kWideW], bool is_and) {
+        if (has_top) {
+            has_top = false;
+#pragma unroll
+            for (int k = 0; k < kWideW; ++k) acc[k] = is_and ? (acc[k] & top[k]) : (acc[k] | top[k]);
+        } else {
+            --depth;
+#pragma unroll
+            for (int k = 0; k < kWideW; ++k)
+                acc[k] = is_and ? (acc[k] & deep[depth][k]) : (acc[k] | deep[depth][k]);
+        }
+    };
+    while (pc < plen) {
+        const uint32_t op = s_prog[pc];
+        uint64_t acc[kWideW], o[kWideW];
+        if (op == kOpConjunction) {
+            const uint32_t parts = s_prog[pc + 1];
+#pragma unroll
+            for (int k = 0; k < kWideW; ++k) acc[k] = ~0ull;
+            for (uint32_t p = 0; p < parts; ++p) {
+                const uint32_t pn = s_prog[pc + 2 + p];
+                uint64_t u[kWideW];
+                wide_load(s_base, next, off, u);
+                for (uint32_t j = 1; j < pn; ++j) {
+                    wide_load(s_base, next + j, off, o);
+#pragma unroll
+                    for (int k = 0; k < kWideW; ++k) u[k] |= o[k];
+                }
+#pragma unroll
+                for (int k = 0; k < kWideW; ++k) acc[k] &= u[k];
+                next += pn;
+            }
+            pc += 2 + parts;
+        } else {
+            const uint32_t pn = s_prog[pc + 1], sn = s_prog[pc + 2];
+            pc += 3;
+            if (op == kOpNot) {
+                if (pn) {
+                    wide_load(s_base, next, off, acc);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < kWideW; ++k) acc[k] = 0ull;
+                    pop_into(acc, false);
+                }
+#pragma unroll
+                for (int k = 0; k < kWideW; ++k) acc[k] = ~acc[k];
+            } else {
+                const bool is_and = op == kOpAnd;
+#pragma unroll
+                for (int k = 0; k < kWideW; ++k) acc[k] = is_and ? ~0ull : 0ull;
+                for (uint32_t j = 0; j < pn; ++j) {
+                    wide_load(s_base, next + j, off, o);
+#pragma unroll
+                    for (int k = 0; k < kWideW; ++k) acc[k] = is_and ? (acc[k] & o[k]) : (acc[k] | o[k]);
+                }
+                for (uint32_t j = 0; j < sn; ++j) pop_into(acc, is_and);
+            }
+            next += pn;
+        }
+        // push: the old top (if any) moves under the new one
+        if (has_top) {
+#pragma unroll
+            for (int k = 0; k < kWideW; ++k) deep[depth][k] = top[k];
+            ++depth;
+        }
+#pragma unroll
+        for (int k = 0; k < kWideW; ++k) top[k] = acc[k];
+        has_top = true;
+    }
+#pragma unroll
+#pragma unroll
+    for (int k = 0; k < kWideW; ++k) res[k] = top[k];
+}
+
+__global__ void __launch_bounds__(kWideT, 5) filter_dense_wide_kernel(DenseFilterLaunch L) {
+    __shared__ uint32_t s_prog[kMaxProgram];
+    __shared__ const uint64_t* s_base[kWideMaxOpnd];
+    __shared__ int s_ok;
+
+    const uint32_t q = blockIdx.x;
+    const uint32_t t = threadIdx.x;
+    const uint32_t seg_words = L.seg_words;
+    const uint32_t tiles = (seg_words + kWideTW - 1) / kWideTW;  // word tiles of a segment
+    const uint32_t groups = (tiles + kWideTilesPerCta - 1) / kWideTilesPerCta;
+    const uint32_t seg = blockIdx.y / groups;
+    const uint32_t tile0 = (blockIdx.y % groups) * kWideTilesPerCta;
+    const uint32_t tile1 = min(tiles, tile0 + kWideTilesPerCta);
+    const uint64_t seg_w0 = static_cast<uint64_t>(seg) * seg_words;
+    uint64_t* out_row = L.out + static_cast<uint64_t>(q) * L.out_stride + seg_w0;
+
+    const uint32_t p0 = L.prog_off[q], p1 = L.prog_off[q + 1];
+    const uint32_t o0 = L.opnd_off[q], o1 = L.opnd_off[q + 1];
+    const uint32_t nop = o1 - o0;
+    const uint32_t plen = p1 - p0;
+    const bool empty = plen == 0;  // match all (text_filter.cpp:553-559)
+    const bool fits = nop <= L.max_opnd && nop <= kWideMaxOpnd && plen <= static_cast<uint32_t>(kMaxProgram);
+    if (!empty && fits) {
+        for (uint32_t i = t; i < plen; i += kWideT) s_prog[i] = L.prog[p0 + i];
+        if (t < nop) {
+            uint32_t r = L.opnd_row[o0 + t];
+            r = r < L.rows ? r : L.rows - 1;  // a row past the table reads the all-zero row
+            s_base[t] = L.dense + (static_cast<uint64_t>(r) * L.seg_num + seg) * seg_words;
+        }
+        __syncthreads();
+        if (t == 0) s_ok = check_program(s_prog, plen, nop);
+    } else if (t == 0) {
+        s_ok = empty;
+    }
+    __syncthreads();
+    const bool ok = s_ok != 0;
+    uint32_t c = 0;
+    // the program's setup (load, check) is shared by the CTA's word tiles of this segment
+    for (uint32_t tile = tile0; tile < tile1; ++tile) {
+        const uint32_t w0 = tile * kWideTW;
+        const uint32_t nw = min(kWideTW, seg_words - w0);  // even
+        // word offsets (from the segment's start) of this thread's pairs; a pair past a partial tile
+        // reads the tile's first pair instead (in bounds; not stored)
+        uint32_t off[kWideW / 2];
+#pragma unroll
+        for (int g = 0; g < kWideW / 2; ++g) off[g] = w0 + (kWideGS * g + 2u * t < nw ? kWideGS * g + 2u * t : 0u);
+        uint64_t res[kWideW];
+        if (empty || !ok) {
+#pragma unroll
+            for (int k = 0; k < kWideW; ++k) res[k] = empty ? ~0ull : 0ull;
+        } else {
+            eval_wide(s_prog, plen, s_base, off, res);
+        }
+#pragma unroll
+        for (int g = 0; g < kWideW / 2; ++g) {
+            const uint32_t w = kWideGS * g + 2u * t;
+            if (w >= nw) continue;
+            const uint64_t a = res[2 * g] & tail_mask(seg_w0 + w0 + w, L.doc_num);
+            const uint64_t b = res[2 * g + 1] & tail_mask(seg_w0 + w0 + w + 1, L.doc_num);
+            *reinterpret_cast<ulonglong2*>(out_row + w0 + w) = make_ulonglong2(a, b);
+            c += __popcll(a) + __popcll(b);
+        }
+    }
+    if (L.pass_count) {
+        c = warp_sum(c);
+        if ((t & 31) == 0 && c) atomicAdd(L.pass_count + q, c);
+    }
+    if (t == 0 && L.status && !empty && !ok) atomicOr(L.status + q, kStatusBadProgram);
+}
+
 // One CTA per posting: expand `src[i]` (any layout) into the dense bitset `dst[i]` of
 // byte_size bytes (the PostingBitListToSet operator, bitlist_to_set.h:6-155).
 __global__ void __launch_bounds__(256) posting_expand_kernel(const uint64_t* src, const uint64_t* dst, uint32_t count,
@@ -560,6 +775,14 @@ cudaError_t launch_filter_dense(const DenseFilterLaunch& L, cudaStream_t stream)
     if (L.max_opnd > static_cast<uint32_t>(kMaxOperands) || L.rows == 0 || L.seg_words == 0 || (L.seg_words & 1u) ||
         (reinterpret_cast<uintptr_t>(L.dense) & 15u))
         return cudaErrorInvalidValue;
+    if (L.max_opnd <= kWideMaxOpnd && (L.out_stride & 1u) == 0 && (reinterpret_cast<uintptr_t>(L.out) & 15u) == 0) {
+        const uint32_t tiles = (L.seg_words + kWideTW - 1) / kWideTW;
+        const uint64_t gy = static_cast<uint64_t>(L.seg_num) * ((tiles + kWideTilesPerCta - 1) / kWideTilesPerCta);
+        if (gy <= 65535u) {
+            filter_dense_wide_kernel<<<dim3(L.nq, static_cast<uint32_t>(gy)), kWideT, 0, stream>>>(L);
+            return cudaGetLastError();
+        }
+    }
     const size_t per_word = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * sizeof(uint64_t);
     if (4 * kDenseT * per_word <= 48 * 1024 && L.seg_words >= 2 * kDenseT) return launch_filter_dense_wpt<4>(L, stream);
     if (2 * kDenseT * per_word <= 48 * 1024) return launch_filter_dense_wpt<2>(L, stream);

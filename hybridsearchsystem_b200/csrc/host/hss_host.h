@@ -415,7 +415,7 @@ class FullRecallSearcher {
     // candidates of the select step. A bad prediction costs candidates, never exactness, and never
     // forces a re-run. nullptr switches the model off.
     int SetThresholdModel(std::shared_ptr<ThresholdModel> model, float margin);
-    // Width of a query's feature row: dim + posting rows + 6.
+    // Width of a query's feature row: dim + posting rows + 12.
     uint32_t FeatureDim() const;
     // Feature rows [nq][FeatureDim()] of a batch (runs the filter stage and the doc sample).
     int Features(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks,

@@ -136,7 +136,7 @@ bool FullRecallSearcher::Allocate() {
     if (!ck(cudaMallocHost(&m_hOutScore, B * kMaxTopK * 4ull), "cudaMallocHost results")) return false;
     if (!ck(cudaMallocHost(&m_hOutId, B * kMaxTopK * 8ull), "cudaMallocHost results")) return false;
     if (!ck(cudaMallocHost(&m_hOutCount, B * 4ull), "cudaMallocHost results")) return false;
-    if (!ck(cudaMalloc(&m_dStats, B * 4ull * sizeof(float)), "cudaMalloc sample statistics")) return false;
+    if (!ck(cudaMalloc(&m_dStats, B * static_cast<uint64_t>(kSampleStats) * sizeof(float)), "cudaMalloc sample statistics")) return false;
     if (!ck(cudaMallocHost(&m_hThetaA, B * sizeof(float)), "cudaMallocHost thresholds")) return false;
     for (auto& e : m_ev)
         if (!ck(cudaEventCreate(&e), "cudaEventCreate")) return false;
@@ -309,7 +309,7 @@ int FullRecallSearcher::FilterDevice(uint32_t nq, const FilterExpr* const* exprs
 }
 
 uint32_t FullRecallSearcher::FeatureDim() const {
-    return m_table ? m_table->GetDimension() + m_table->PostingRows() + 6 : 0;
+    return m_table ? m_table->GetDimension() + m_table->PostingRows() + kFeatureTail : 0;
 }
 
 int FullRecallSearcher::SetThresholdModel(std::shared_ptr<ThresholdModel> model, float margin) {

@@ -93,4 +93,45 @@ __host__ __device__ inline uint64_t pass_tile(uint64_t begin, uint64_t step, uin
     return skip >= 2 ? it + it / (skip - 1) + 1 : begin + it * step;
 }
 
+// Launch-side guard for TileWalk: every `it` a CTA reaches (below count + stride) and every tile index
+// of the pass fit in 32 bits.
+__host__ __device__ inline bool tile_walk_fits(uint64_t begin, uint64_t step, uint32_t skip, uint64_t count,
+                                               uint64_t stride) {
+    if (count == 0) return true;
+    if (count + stride >= (1ull << 32) || begin >= (1ull << 32) || step >= (1ull << 32)) return false;
+    return pass_tile(begin, step, skip, count - 1) < (1ull << 32);
+}
+
+// pass_tile over it = it0, it0 + stride, it0 + 2 stride, ... without a division per step: the quotient
+// and remainder of it / (skip - 1) are carried along (a division by a runtime divisor costs tens of
+// instructions, and the candidate kernels step once per tile in every thread). 32-bit state: a pass
+// has far fewer than 2^32 tiles (launchers check tile_walk_fits).
+struct TileWalk {
+    uint32_t begin, step, it, stride, q, dq, d, r, dr;  // d = skip - 1 (0: strided), it = q d + r, stride = dq d + dr
+    __device__ TileWalk(uint64_t b, uint64_t s, uint32_t skip, uint64_t it0, uint64_t strd)
+        : begin(static_cast<uint32_t>(b)), step(static_cast<uint32_t>(s)), it(static_cast<uint32_t>(it0)),
+          stride(static_cast<uint32_t>(strd)), q(0), dq(0), d(skip >= 2 ? skip - 1 : 0), r(0), dr(0) {
+        if (d) {
+            q = it / d;
+            r = it - q * d;
+            dq = stride / d;
+            dr = stride - dq * d;
+        }
+    }
+    __device__ uint64_t tile() const {
+        return d ? static_cast<uint64_t>(it) + q + 1 : static_cast<uint64_t>(begin) + static_cast<uint64_t>(it) * step;
+    }
+    __device__ void advance() {
+        it += stride;
+        if (d) {
+            q += dq;
+            r += dr;  // r, dr < d: one correction suffices
+            if (r >= d) {
+                r -= d;
+                ++q;
+            }
+        }
+    }
+};
+
 }  // namespace hss

@@ -102,6 +102,16 @@ uint32_t cand_simt_segments(uint64_t tile_count, int num_sms, uint32_t cap);
 // Threshold from the K-th best approximate score of a segmented list (segments [0, segs)):
 // theta = kth - eps_sample - eps_main. With raise_only the result is max(old theta, that), and a list
 // with fewer than K entries keeps the old theta.
+// Doc-sample statistics for the threshold predictor's features, floats per query: [0, kSampleRanks)
+// the sample's best approximate scores at ranks 1, 2, 4, ..., 64 (-2 past the sample's size), then
+// the K-th best (-2 when the sample holds fewer than K), then the number of filtered sample docs,
+// then zeros.
+constexpr uint32_t kSampleRanks = 7;
+constexpr uint32_t kSampleStats = 12;
+// Features past the query vector and the per-row block: log selectivity, log K, a constant, the
+// sample's rank scores, its K-th best and its log size.
+constexpr uint32_t kFeatureTail = 3 + kSampleRanks + 2;
+
 struct SampleThresholdLaunch {
     const float* score;        // [nq][cap] sample scores, segmented
     const uint32_t* count;     // [nq][kMaxCandSegs]
@@ -114,7 +124,7 @@ struct SampleThresholdLaunch {
     float* theta;              // [nq] out
     const uint32_t* qlist;
     uint32_t nq_list;
-    float* stats;              // [nq][4] or null: best sample score, K-th best, stored count (-2 when absent)
+    float* stats;              // [nq][kSampleStats] or null (layout at kSampleStats)
 };
 
 struct SelectLaunch {
@@ -234,7 +244,7 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, int64_t n,
                         float eps, int step, cudaStream_t stream);
 struct FeatureLaunch {
     const float* qry;           // [nq][dim]
-    const float* stats;         // [nq][4] doc-sample statistics (sample_threshold_kernel)
+    const float* stats;         // [nq][kSampleStats] doc-sample statistics (sample_threshold_kernel)
     const uint32_t* opnd_row;   // concatenated filter operand rows
     const uint32_t* opnd_off;   // [nq + 1]
     const uint32_t* pass_count; // [nq] docs the filter lets through

@@ -147,14 +147,14 @@ __global__ void features_kernel(FeatureLaunch L) {
     }
     if (threadIdx.x == 0) {
         const float sel = fmaxf(static_cast<float>(L.pass_count[q]), 1.0f) / static_cast<float>(L.doc_num);
-        const float* st = L.stats + static_cast<uint64_t>(q) * 4;
+        const float* st = L.stats + static_cast<uint64_t>(q) * kSampleStats;
         float* t = x + L.dim + L.rows;
         t[0] = log10f(sel) * 0.25f;
         t[1] = log10f(fmaxf(static_cast<float>(L.topk[q]), 1.0f)) / 3.0f;
         t[2] = 1.0f;
-        t[3] = st[0];
-        t[4] = st[1];
-        t[5] = log10f(st[2] + 1.0f) * 0.2f;
+        for (uint32_t j = 0; j < kSampleRanks; ++j) t[3 + j] = st[j];
+        t[3 + kSampleRanks] = st[kSampleRanks];
+        t[4 + kSampleRanks] = log10f(st[kSampleRanks + 1] + 1.0f) * 0.2f;
     }
 }
 
@@ -216,7 +216,7 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, int64_t n,
 
 cudaError_t launch_features(const FeatureLaunch& L, cudaStream_t stream) {
     if (L.nq == 0) return cudaSuccess;
-    if (L.din < L.dim + L.rows + 6 || !L.stats) return cudaErrorInvalidValue;
+    if (L.din < L.dim + L.rows + kFeatureTail || !L.stats) return cudaErrorInvalidValue;
     features_kernel<<<L.nq, 128, 0, stream>>>(L);
     return cudaGetLastError();
 }

@@ -61,8 +61,9 @@ __global__ void __launch_bounds__(kCT) cand_simt_kernel(CandLaunch L) {
     const uint32_t kchunks = (L.dim + kCK - 1) / kCK;
     for (uint32_t i = tid; i < L.nq_list; i += kCT) sCount[i] = 0;
 
-    for (uint64_t it = blockIdx.x; it < L.tile_count; it += gridDim.x) {
-        const uint64_t tile = pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it);
+    TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, blockIdx.x, gridDim.x);
+    for (uint64_t it = blockIdx.x; it < L.tile_count; it += gridDim.x, walk.advance()) {
+        const uint64_t tile = walk.tile();
         const uint64_t doc0 = tile * kDocTile;
         for (uint32_t chunk = 0; chunk < nchunks; ++chunk) {
             float acc[4][8];
@@ -203,7 +204,8 @@ cudaError_t launch_cand_simt(const CandLaunch& L, int num_sms, cudaStream_t stre
     if (L.tile_count == 0 || L.nq_list == 0) return cudaSuccess;
     const uint64_t seg_end = static_cast<uint64_t>(L.seg_base) + L.segs;
     if (L.segs != cand_simt_segments(L.tile_count, num_sms, L.cap) || L.seg_cap == 0 || seg_end > kMaxCandSegs ||
-        seg_end * L.seg_cap > L.cap || L.nq_list > kMaxSimtBatch)
+        seg_end * L.seg_cap > L.cap || L.nq_list > kMaxSimtBatch ||
+        !tile_walk_fits(L.tile_begin, L.tile_step, L.tile_skip, L.tile_count, L.segs))
         return cudaErrorInvalidValue;
     const size_t smem = static_cast<size_t>(L.nq_list) * sizeof(uint32_t);
     cand_simt_kernel<<<L.segs, kCT, smem, stream>>>(L);

@@ -287,38 +287,52 @@ __device__ inline float max32(const uint32_t (&r)[32]) {
     return fmaxf(max3(b0, b1, b2), b3);
 }
 
-// v[j] for a lane-varying j, as a five-level select tree over registers (no local-memory array).
-__device__ __forceinline__ uint32_t pick32(const uint32_t (&v)[32], uint32_t j) {
-    uint32_t a[16], b[8], c[4], d[2];
+// Maximum of the 8 scores v[8k .. 8k + 7] (three steps).
+__device__ __forceinline__ float max8(const uint32_t (&v)[32], int k) {
+    const float a = max3(__uint_as_float(v[8 * k]), __uint_as_float(v[8 * k + 1]), __uint_as_float(v[8 * k + 2]));
+    const float b = max3(__uint_as_float(v[8 * k + 3]), __uint_as_float(v[8 * k + 4]), __uint_as_float(v[8 * k + 5]));
+    return max3(a, b, fmaxf(__uint_as_float(v[8 * k + 6]), __uint_as_float(v[8 * k + 7])));
+}
+
+// v[8k + j] for a lane-varying j < 8, as a three-level select tree over registers (no local array).
+__device__ __forceinline__ uint32_t pick8(const uint32_t (&v)[32], int k, uint32_t j) {
+    uint32_t a[4], b[2];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) a[i] = (j & 16u) ? v[i + 16] : v[i];
+    for (int i = 0; i < 4; ++i) a[i] = (j & 4u) ? v[8 * k + 4 + i] : v[8 * k + i];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) b[i] = (j & 8u) ? a[i + 8] : a[i];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) c[i] = (j & 4u) ? b[i + 4] : b[i];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) d[i] = (j & 2u) ? c[i + 2] : c[i];
-    return (j & 1u) ? d[1] : d[0];
+    for (int i = 0; i < 2; ++i) b[i] = (j & 2u) ? a[2 + i] : a[i];
+    return (j & 1u) ? b[1] : b[0];
 }
 
 // One 32-doc chunk of a thread's TF32 / BF16 scores (its query): the docs whose filter bit (m) is set
 // and whose approximate score clears the threshold t go to the thread's list segment, in doc order.
-// The loop runs once per kept doc (typically zero or one per chunk), so the code stays small.
+// The epilogue runs on the ALU pipe (compares, maxima, selects), so the chunk is tested as four 8-doc
+// groups: only a group whose maximum clears t builds a keep mask, and a kept doc is picked from its
+// group's 8 registers. The loop runs once per kept doc (typically zero or one per chunk).
 __device__ __forceinline__ void emit_lane(uint32_t m, const uint32_t (&v)[32], float t, uint64_t doc0,
                                           float* out_score, uint32_t* out_loc, uint32_t seg_cap, uint32_t& ncand) {
-    if (m == 0u || !(max32(v) >= t)) return;
-    uint32_t pass = 0;
+    if (m == 0u) return;
+    float g[4];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) pass |= (__uint_as_float(v[j]) >= t ? 1u : 0u) << j;
-    pass &= m;
-    while (pass != 0u) {
-        const uint32_t j = static_cast<uint32_t>(__ffs(pass) - 1);
-        pass &= pass - 1u;
-        if (ncand < seg_cap) {
-            out_score[ncand] = __uint_as_float(pick32(v, j));
-            out_loc[ncand] = static_cast<uint32_t>(doc0 + j);
+    for (int k = 0; k < 4; ++k) g[k] = max8(v, k);
+    if (!(fmaxf(max3(g[0], g[1], g[2]), g[3]) >= t)) return;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t mk = (m >> (8 * k)) & 0xffu;
+        if (mk == 0u || !(g[k] >= t)) continue;
+        uint32_t pass = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) pass |= (__uint_as_float(v[8 * k + j]) >= t ? 1u : 0u) << j;
+        pass &= mk;
+        while (pass != 0u) {
+            const uint32_t j = static_cast<uint32_t>(__ffs(pass) - 1);
+            pass &= pass - 1u;
+            if (ncand < seg_cap) {
+                out_score[ncand] = __uint_as_float(pick8(v, k, j));
+                out_loc[ncand] = static_cast<uint32_t>(doc0 + 8u * k + j);
+            }
+            ++ncand;
         }
-        ++ncand;
     }
 }
 
@@ -411,8 +425,9 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
                     tma_load_2d(qsm + (static_cast<size_t>(h) * kb_n + kb) * kStageBytes, &qry_map,
                                 static_cast<int>(kb * (128 / Fmt<F>::elem)), h * kRows, &S.qbar);
             uint32_t n = 0;
-            for (uint64_t it = blockIdx.x; it < ntiles && !S.abort; it += gridDim.x) {
-                const int y = static_cast<int>(pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it) * kRows);
+            TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, blockIdx.x, gridDim.x);
+            for (uint64_t it = blockIdx.x; it < ntiles && !S.abort; it += gridDim.x, walk.advance()) {
+                const int y = static_cast<int>(walk.tile() * kRows);
                 for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
                     if (!mbar_wait(&S.empty[s], ph ^ 1u, S, L.error, 1)) break;
@@ -484,14 +499,17 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
         uint32_t iter = 0;
         // the query's filter bits of this thread's 64 docs, loaded one tile ahead so the (uncoalesced)
         // load is in flight during the previous tile's work
+        TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, blockIdx.x, gridDim.x);
+        uint64_t tile_next = walk.tile();
         uint64_t fw_next = 0;
-        if (valid && blockIdx.x < ntiles) fw_next = brow[pass_tile(L.tile_begin, L.tile_step, L.tile_skip, blockIdx.x) * 2 + colh];
+        if (valid && blockIdx.x < ntiles) fw_next = brow[tile_next * 2 + colh];
         for (uint64_t it = blockIdx.x; it < ntiles; it += gridDim.x, ++iter) {
             const uint32_t buf = iter & 1u;
-            const uint64_t tile = pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it);
+            const uint64_t tile = tile_next;
             const uint64_t fw = fw_next;
-            if (valid && it + gridDim.x < ntiles)
-                fw_next = brow[pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it + gridDim.x) * 2 + colh];
+            walk.advance();
+            tile_next = walk.tile();
+            if (valid && it + gridDim.x < ntiles) fw_next = brow[tile_next * 2 + colh];
             // threshold on the raw accumulator: acc * qs * ds >= theta
             float t = theta;
             if (F == kTcE4M3) {
@@ -646,9 +664,9 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
                 tma_load_2d(qsm + static_cast<size_t>(kb) * kStageBytes, &qry_map,
                             static_cast<int>(kb * (128 / Fmt<F>::elem)), static_cast<int>(rank * kRows), &S.qbar);
             uint32_t n = 0;
-            for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs) {
-                const int y = static_cast<int>(pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it) * 2 * kRows +
-                                               rank * kRows);
+            TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, pair, npairs);
+            for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs, walk.advance()) {
+                const int y = static_cast<int>(walk.tile() * 2 * kRows + rank * kRows);
                 for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
                     if (!pair_wait<F>(&S.empty[s], ph ^ 1u, S, L.error, 1, false)) break;
@@ -733,16 +751,22 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
         uint32_t ncand = 0;
         uint32_t iter = 0;
         // filter word of this thread's 64 docs of a tile (past the bitmap: none pass)
-        auto word_of = [&](uint64_t it) -> uint64_t {
-            const uint64_t w = pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it) * 4 + g;
+        auto word_of = [&](uint64_t tile) -> uint64_t {
+            const uint64_t w = tile * 4 + g;
             return (valid && w < L.bits_stride) ? brow[w] : 0ull;
         };
-        uint64_t fw_next = pair < ntiles ? word_of(pair) : 0ull;
-        for (uint64_t it = pair; it < ntiles; it += npairs, ++iter) {
+        // 32-bit tile counters (the launcher checks tile_walk_fits): registers are tight at 576 threads
+        TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, pair, npairs);
+        const uint32_t nt = static_cast<uint32_t>(ntiles);
+        uint32_t tile_next = static_cast<uint32_t>(walk.tile());
+        uint64_t fw_next = pair < nt ? word_of(tile_next) : 0ull;
+        for (uint32_t it = pair; it < nt; it += npairs, ++iter) {
             const uint32_t buf = iter & 1u;
-            const uint64_t tile = pass_tile(L.tile_begin, L.tile_step, L.tile_skip, it);
+            const uint64_t tile = tile_next;
             const uint64_t fw = fw_next;
-            if (it + npairs < ntiles) fw_next = word_of(it + npairs);
+            walk.advance();
+            tile_next = static_cast<uint32_t>(walk.tile());
+            if (it + npairs < nt) fw_next = word_of(tile_next);
             float t = theta;
             if (F == kTcE4M3) {
                 uint64_t ts = tile * 2 + g / 2;  // 128-doc tile holding this thread's docs
@@ -867,7 +891,9 @@ size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages) {
 cudaError_t launch_tc_cand(const TcCandLaunch& Lin, const CUtensorMap& doc_map, const CUtensorMap& qry_map, int sms,
                            cudaStream_t stream) {
     if (Lin.tile_count == 0 || Lin.nq_rows == 0) return cudaSuccess;
-    if (Lin.kblocks == 0 || Lin.nq_rows > 256 || Lin.tiles128 == 0) return cudaErrorInvalidValue;
+    if (Lin.kblocks == 0 || Lin.nq_rows > 256 || Lin.tiles128 == 0 ||
+        !tile_walk_fits(Lin.tile_begin, Lin.tile_step, Lin.tile_skip, Lin.tile_count, Lin.ctas))
+        return cudaErrorInvalidValue;
     TcCandLaunch L = Lin;
     const bool pair = L.nq_rows > 128;
     // as many stages as shared memory holds next to the resident queries

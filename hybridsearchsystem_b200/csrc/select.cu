@@ -16,23 +16,27 @@ namespace hss {
 namespace {
 
 constexpr int kST = 1024;             // threads of the selection CTAs
-constexpr int kWarps = kST / 32;
+constexpr int kHist = 16;             // radix histograms per CTA (warp w adds to hist[w % kHist])
+constexpr uint32_t kSelFast = 6144;   // candidates a select CTA holds in shared memory
 
 struct SelectSmem {
-    uint32_t hist[kWarps][256];                 // per-warp radix histograms
+    uint32_t hist[kHist][256];                  // radix histograms
     unsigned long long sortbuf[kMaxTopK];       // bitonic sort buffer
     uint32_t segn[kMaxCandSegs];                // stored entries of each candidate segment
+    uint32_t segoff[kMaxCandSegs];              // their exclusive prefix sum (scan_segments)
     uint32_t bcast[4];
     uint32_t counter;
+    uint32_t total;                             // stored entries (load_segments)
+    uint32_t wsum[kST / 32];
 };
 
-// Merges the per-warp histograms into hist[0] and picks, from the top, the digit holding the k-th
+// Merges the histograms into hist[0] and picks, from the top, the digit holding the k-th
 // largest key. Returns the digit and updates *krem to the rank inside that digit.
 __device__ inline uint32_t pick_digit(SelectSmem& S, uint32_t* krem) {
     const uint32_t tid = threadIdx.x;
     if (tid < 256) {
         uint32_t s = 0;
-        for (int w = 0; w < kWarps; ++w) s += S.hist[w][tid];
+        for (int w = 0; w < kHist; ++w) s += S.hist[w][tid];
         S.hist[0][tid] = s;
     }
     __syncthreads();
@@ -75,8 +79,19 @@ __device__ inline uint32_t pick_digit(SelectSmem& S, uint32_t* krem) {
     return chosen;
 }
 
+// Counts digit d (< 256; 256 = nothing) of each calling lane into hist_row. Lanes holding the same
+// digit add once, together: candidate scores cluster (a query's nearest cluster scores within a few
+// hundredths), so most of a warp's keys share their leading digits and 32 increments of one
+// shared-memory word would serialise.
+__device__ __forceinline__ void hist_add(uint32_t* hist_row, uint32_t d) {
+    const uint32_t active = __activemask();
+    const uint32_t grp = __match_any_sync(active, d);
+    if (d < 256u && (threadIdx.x & 31u) == static_cast<uint32_t>(__ffs(grp) - 1))
+        atomicAdd(&hist_row[d], static_cast<uint32_t>(__popc(grp)));
+}
+
 __device__ inline void clear_hist(SelectSmem& S) {
-    for (uint32_t i = threadIdx.x; i < kWarps * 256; i += blockDim.x) (&S.hist[0][0])[i] = 0;
+    for (uint32_t i = threadIdx.x; i < kHist * 256; i += blockDim.x) (&S.hist[0][0])[i] = 0;
     __syncthreads();
 }
 
@@ -88,12 +103,97 @@ __device__ uint32_t kth_largest_u32_visit(Visit visit, uint32_t k, SelectSmem& S
     for (int shift = 24; shift >= 0; shift -= 8) {
         clear_hist(S);
         visit([&](uint32_t v) {
-            if ((v & mask) == prefix) atomicAdd(&S.hist[warp][(v >> shift) & 255u], 1u);
+            hist_add(S.hist[warp % kHist], (v & mask) == prefix ? ((v >> shift) & 255u) : 256u);
         });
         __syncthreads();
         const uint32_t d = pick_digit(S, &krem);
         prefix |= d << shift;
         mask |= 255u << shift;
+    }
+    return prefix;
+}
+
+// Picks, from the top of a 4096-bin histogram, the bin holding the k-th largest key (blockDim.x ==
+// kST: thread t owns bins 4095 - 4t .. 4092 - 4t). Returns the bin; *krem becomes the rank inside it.
+__device__ inline uint32_t pick_digit4096(const uint32_t* hist, uint32_t* krem, SelectSmem& S) {
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t kr = *krem;
+    uint32_t h[4], local = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        h[j] = hist[4095 - 4 * t - j];
+        local += h[j];
+    }
+    uint32_t x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= static_cast<uint32_t>(o)) x += y;
+    }
+    if (lane == 31) S.wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = S.wsum[lane];
+        uint32_t z = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= static_cast<uint32_t>(o)) z += y;
+        }
+        S.wsum[lane] = z - w;  // exclusive over warps
+    }
+    __syncthreads();
+    const uint32_t incl = S.wsum[warp] + x, excl = incl - local;
+    if (excl < kr && incl >= kr) {  // exactly one thread
+        uint32_t cum = excl;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (cum + h[j] >= kr) {
+                S.bcast[0] = 4095 - 4 * t - j;
+                S.bcast[1] = kr - cum;
+                break;
+            }
+            cum += h[j];
+        }
+    }
+    __syncthreads();
+    const uint32_t d = S.bcast[0];
+    *krem = S.bcast[1];
+    __syncthreads();
+    return d;
+}
+
+// A lower bound of the k-th largest (1-based, k <= the number of keys) of the u32 keys that visit(fn)
+// hands to fn: the k-th largest key's top 24 bits with the low 8 bits cleared. Every key sharing that
+// prefix is >= the result, so at least k keys are >= it -- all a proven threshold or a rescoring cut
+// needs -- and as an order-preserving float key it is at most 2^-15 (relative) below the k-th
+// largest. Two passes of 12-bit digits over one 4096-bin histogram; each thread merges runs of equal
+// digits before adding them (keys of one query cluster, so consecutive keys mostly share a digit).
+template <class Visit>
+__device__ uint32_t kth_lower_bound_u32_visit(Visit visit, uint32_t k, SelectSmem& S) {
+    uint32_t* hist = &S.hist[0][0];
+    static_assert(sizeof(S.hist) / sizeof(uint32_t) >= 4096, "4096-bin histogram");
+    uint32_t prefix = 0, mask = 0, krem = k;
+    for (int pass = 0; pass < 2; ++pass) {
+        const int shift = pass == 0 ? 20 : 8;
+        for (uint32_t i = threadIdx.x; i < 4096; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        uint32_t cur = 0, cnt = 0;
+        visit([&](uint32_t v) {
+            if ((v & mask) != prefix) return;
+            const uint32_t d = (v >> shift) & 4095u;
+            if (d != cur) {
+                if (cnt) atomicAdd(&hist[cur], cnt);
+                cur = d;
+                cnt = 0;
+            }
+            ++cnt;
+        });
+        if (cnt) atomicAdd(&hist[cur], cnt);
+        __syncthreads();
+        const uint32_t d = pick_digit4096(hist, &krem, S);
+        prefix |= d << shift;
+        mask |= 4095u << shift;
     }
     return prefix;
 }
@@ -108,8 +208,37 @@ __device__ uint32_t kth_largest_u32(KeyFn key, uint32_t n, uint32_t k, SelectSme
         k, S);
 }
 
+// S.segoff[g] = entries stored in segments before g (exclusive prefix sum of S.segn[0..segs)).
+// segs <= kMaxCandSegs = blockDim.x.
+__device__ inline void scan_segments(SelectSmem& S, uint32_t segs) {
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t v = t < segs ? S.segn[t] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= static_cast<uint32_t>(o)) x += y;
+    }
+    if (lane == 31) S.wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = lane < (blockDim.x >> 5) ? S.wsum[lane] : 0u;
+        uint32_t z = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= static_cast<uint32_t>(o)) z += y;
+        }
+        S.wsum[lane] = z - w;  // exclusive over warps
+    }
+    __syncthreads();
+    if (t < segs) S.segoff[t] = S.wsum[warp] + x - v;
+    __syncthreads();
+}
+
 // Loads the per-segment counts of one query's segmented candidate list (kMaxCandSegs layout) into
-// S.segn (clamped to seg_cap). Returns the stored total; *overflow = some segment lost entries.
+// S.segn (clamped to seg_cap) and their prefix sums into S.segoff. Returns the stored total (also in
+// S.total); *overflow = some segment lost entries. segs <= blockDim.x.
 __device__ uint32_t load_segments(SelectSmem& S, const uint32_t* counts, uint32_t segs, uint32_t seg_cap,
                                   bool* overflow) {
     if (threadIdx.x == 0) {
@@ -127,19 +256,48 @@ __device__ uint32_t load_segments(SelectSmem& S, const uint32_t* counts, uint32_
     __syncthreads();
     const uint32_t n = S.bcast[2];
     *overflow = S.bcast[3] != 0;
-    __syncthreads();
+    if (threadIdx.x == 0) S.total = n;
+    scan_segments(S, segs);  // synchronises
     return n;
 }
 
-// Calls fn(index, valid) for every stored entry of a segmented list: warp w walks segments w,
-// w + 32, ..., its lanes 32 consecutive entries at a time, so every call is made by a full warp
-// (valid = false for the lanes past a segment's end) and fn may use warp collectives.
+// Storage index of the idx-th stored entry (idx < S.total) of a segmented list: the last segment
+// starting at or before idx, by binary search over S.segoff (empty segments share their successor's
+// start, so the last such segment is the non-empty one holding idx).
+__device__ __forceinline__ uint64_t segment_entry(const SelectSmem& S, uint32_t segs, uint32_t seg_cap, uint32_t idx) {
+    uint32_t lo = 0, hi = segs;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (S.segoff[mid] <= idx) lo = mid;
+        else hi = mid;
+    }
+    return static_cast<uint64_t>(lo) * seg_cap + (idx - S.segoff[lo]);
+}
+
+// Calls fn(index, valid, score) for every stored entry of a segmented list of scores src (after
+// load_segments). A warp takes 4 x 32 consecutive entries of the flattened list per round: lanes
+// read consecutive entries (coalesced within a segment), and each lane's 4 segment lookups and loads
+// are independent, so a thread keeps 4 loads in flight instead of one dependent chain per entry.
+// Every call is made by a full warp (valid = false past the end), so fn may use warp collectives.
 template <class Fn>
-__device__ inline void for_each_segment_entry(const SelectSmem& S, uint32_t segs, uint32_t seg_cap, Fn fn) {
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (uint32_t g = warp; g < segs; g += blockDim.x >> 5) {
-        const uint32_t n = S.segn[g];
-        for (uint32_t o0 = 0; o0 < n; o0 += 32) fn(g * seg_cap + o0 + lane, o0 + lane < n);
+__device__ inline void for_each_segment_entry(const SelectSmem& S, uint32_t segs, uint32_t seg_cap,
+                                              const float* src, Fn fn) {
+    constexpr uint32_t U = 4;
+    const uint32_t n = S.total, lane = threadIdx.x & 31;
+    for (uint32_t b = (threadIdx.x >> 5) * 32u * U; b < n; b += blockDim.x * U) {
+        uint64_t i[U];
+        bool ok[U];
+        float v[U];
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u) {
+            const uint32_t idx = b + 32u * u + lane;
+            ok[u] = idx < n;
+            i[u] = ok[u] ? segment_entry(S, segs, seg_cap, idx) : 0ull;
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u) v[u] = ok[u] ? src[i[u]] : 0.0f;
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u) fn(static_cast<uint32_t>(i[u]), ok[u], v[u]);
     }
 }
 
@@ -152,7 +310,7 @@ __device__ uint64_t kth_largest_u64(KeyFn key, uint32_t n, uint32_t k, SelectSme
         clear_hist(S);
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
             const uint64_t v = key(i);
-            if ((v & mask) == prefix) atomicAdd(&S.hist[warp][(v >> shift) & 255u], 1u);
+            hist_add(S.hist[warp % kHist], (v & mask) == prefix ? static_cast<uint32_t>((v >> shift) & 255u) : 256u);
         }
         __syncthreads();
         const uint64_t d = pick_digit(S, &krem);
@@ -226,30 +384,61 @@ __global__ void __launch_bounds__(kST) sample_threshold_kernel(SampleThresholdLa
     const uint32_t n = load_segments(S, L.count + static_cast<uint64_t>(qi) * kMaxCandSegs, L.segs, L.seg_cap, &lost);
     float theta = L.raise_only ? L.theta[qi] : -INFINITY;
     if (L.stats) {
-        // the best stored score (one pass), for the threshold predictor's features
+        // the sample's best scores at ranks 1, 2, 4, ..., 64: the key at rank r = min(64, n), then the
+        // (fewer than r) keys above it, each placed by counting the keys that precede it
+        float* st = L.stats + static_cast<uint64_t>(qi) * kSampleStats;
+        const float* sc = L.score + static_cast<uint64_t>(qi) * L.cap;
+        const uint32_t r = min(n, 64u);
+        uint32_t key_r = 0;
+        if (r > 0)
+            key_r = kth_largest_u32_visit(
+                [&](auto fn) {
+                    for_each_segment_entry(S, L.segs, L.seg_cap, sc, [&](uint32_t, bool ok, float v) {
+                        if (ok) fn(float_key(v));
+                    });
+                },
+                r, S);
         if (threadIdx.x == 0) S.counter = 0;
         __syncthreads();
-        const float* sc = L.score + static_cast<uint64_t>(qi) * L.cap;
-        for_each_segment_entry(S, L.segs, L.seg_cap, [&](uint32_t i, bool ok) {
-            uint32_t key = ok ? float_key(sc[i]) : 0u;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) key = max(key, __shfl_xor_sync(0xffffffffu, key, o));
-            if ((threadIdx.x & 31) == 0 && key) atomicMax(&S.counter, key);
-        });
+        if (r > 0)
+            for_each_segment_entry(S, L.segs, L.seg_cap, sc, [&](uint32_t, bool ok, float v) {
+                const uint32_t key = ok ? float_key(v) : 0u;
+                if (ok && key > key_r) {
+                    const uint32_t slot = atomicAdd(&S.counter, 1u);
+                    if (slot < 64u) S.sortbuf[slot] = key;
+                }
+            });
         __syncthreads();
-        if (threadIdx.x == 0) {
-            float* st = L.stats + static_cast<uint64_t>(qi) * 4;
-            st[0] = n ? key_float(S.counter) : -2.0f;
-            st[2] = static_cast<float>(n);
+        const uint32_t c = min(S.counter, 64u);  // < r unless keys were lost
+        if (threadIdx.x < c) {
+            const unsigned long long key = S.sortbuf[threadIdx.x];
+            uint32_t rank = 0;
+            for (uint32_t j = 0; j < c; ++j) {
+                const unsigned long long o = S.sortbuf[j];
+                rank += (o > key || (o == key && j < threadIdx.x)) ? 1u : 0u;
+            }
+            S.sortbuf[64 + rank] = key;
+        }
+        __syncthreads();
+        if (threadIdx.x < kSampleRanks) {
+            const uint32_t rho = 1u << threadIdx.x;
+            float v = -2.0f;
+            if (rho <= r) v = key_float(rho <= c ? static_cast<uint32_t>(S.sortbuf[64 + rho - 1]) : key_r);
+            st[threadIdx.x] = v;
+        } else if (threadIdx.x == kSampleRanks) {
+            st[kSampleRanks] = -2.0f;  // the K-th best, set below when the sample holds K docs
+            st[kSampleRanks + 1] = static_cast<float>(n);
+            for (uint32_t j = kSampleRanks + 2; j < kSampleStats; ++j) st[j] = 0.0f;
         }
         __syncthreads();
     }
     if (k > 0 && n >= k) {
         const float* sc = L.score + static_cast<uint64_t>(qi) * L.cap;
-        const uint32_t kk = kth_largest_u32_visit(
+        // a lower bound of the K-th best serves the proof below as well as the K-th best itself
+        const uint32_t kk = kth_lower_bound_u32_visit(
             [&](auto fn) {
-                for_each_segment_entry(S, L.segs, L.seg_cap, [&](uint32_t i, bool ok) {
-                    if (ok) fn(float_key(sc[i]));
+                for_each_segment_entry(S, L.segs, L.seg_cap, sc, [&](uint32_t, bool ok, float v) {
+                    if (ok) fn(float_key(v));
                 });
             },
             k, S);
@@ -257,12 +446,16 @@ __global__ void __launch_bounds__(kST) sample_threshold_kernel(SampleThresholdLa
         // a true top-K doc therefore scores >= t - eps_s - eps_m under the main pass's arithmetic.
         const float t = __fsub_rd(__fsub_rd(key_float(kk), L.eps_sample[qi]), L.eps_main[qi]);
         theta = L.raise_only ? fmaxf(theta, t) : t;
-        if (L.stats && threadIdx.x == 0) L.stats[static_cast<uint64_t>(qi) * 4 + 1] = key_float(kk);
-    } else if (L.stats && threadIdx.x == 0) {
-        L.stats[static_cast<uint64_t>(qi) * 4 + 1] = -2.0f;
+        if (L.stats && threadIdx.x == 0) L.stats[static_cast<uint64_t>(qi) * kSampleStats + kSampleRanks] = key_float(kk);
     }
     __syncthreads();  // every thread has read the old theta
     if (threadIdx.x == 0) L.theta[qi] = theta;
+}
+
+// Byte offset of the shared-memory candidate arrays of select_topk_kernel: after SelectSmem and the
+// query (dim floats), 16-byte aligned.
+__host__ __device__ inline size_t select_cand_offset(uint32_t dim) {
+    return (sizeof(SelectSmem) + static_cast<size_t>(dim) * sizeof(float) + 15) & ~static_cast<size_t>(15);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -288,8 +481,8 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
     const uint32_t* lc = L.cand_loc + row;
     const float eps = L.eps_main[qi];
     auto visit_scores = [&](auto fn) {
-        for_each_segment_entry(S, L.segs, L.seg_cap, [&](uint32_t i, bool ok) {
-            if (ok) fn(float_key(sc[i]));
+        for_each_segment_entry(S, L.segs, L.seg_cap, sc, [&](uint32_t, bool ok, float v) {
+            if (ok) fn(float_key(v));
         });
     };
     if (overflow) {
@@ -297,7 +490,7 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
         // the true K-th best from below: raise the threshold and let the host re-run this query.
         float theta = L.theta[qi];
         if (n >= k && k > 0) {
-            const uint32_t kk = kth_largest_u32_visit(visit_scores, k, S);
+            const uint32_t kk = kth_lower_bound_u32_visit(visit_scores, k, S);
             theta = fmaxf(theta, __fsub_rd(key_float(kk), 2.0f * eps));
         }
         if (tid == 0) {
@@ -313,19 +506,38 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
     }
     const uint32_t kq = min(k, n);
     for (uint32_t i = tid; i < L.dim; i += blockDim.x) sq[i] = L.qry[static_cast<uint64_t>(qi) * L.dim + i];
+    // A list that fits is gathered into shared memory once; the selection and rescoring passes then
+    // read shared memory instead of walking the segments again.
+    const bool fast = n <= kSelFast;
+    float* cs = reinterpret_cast<float*>(smem_raw + select_cand_offset(L.dim));
+    uint32_t* cl = reinterpret_cast<uint32_t*>(cs + kSelFast);
+    if (fast) {
+        for (uint32_t idx = tid; idx < n; idx += blockDim.x) {
+            const uint64_t i = segment_entry(S, L.segs, L.seg_cap, idx);
+            cs[idx] = sc[i];
+            cl[idx] = lc[i];
+        }
+        __syncthreads();
+    }
     float thr = -INFINITY;
     if (n > kq) {
-        const uint32_t kk = kth_largest_u32_visit(visit_scores, kq, S);
+        // a lower bound of the K-th best approximate score only widens the rescoring cut
+        const uint32_t kk = fast ? kth_lower_bound_u32_visit(
+                                       [&](auto fn) {
+                                           for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) fn(float_key(cs[i]));
+                                       },
+                                       kq, S)
+                                 : kth_lower_bound_u32_visit(visit_scores, kq, S);
         thr = __fsub_rd(key_float(kk), 2.0f * eps);
     }
     if (tid == 0) S.counter = 0;
     __syncthreads();
     unsigned long long* ws = L.work + row;
-    for_each_segment_entry(S, L.segs, L.seg_cap, [&](uint32_t i, bool ok) {
+    // rescoring of one entry (score s, location loc; warp-collective): kept entries are appended to ws
+    auto rescore = [&](bool ok, float s, uint32_t loc) {
         bool take = false;
         unsigned long long key = 0;
-        if (ok && sc[i] >= thr) {
-            const uint32_t loc = lc[i];
+        if (ok && s >= thr) {
             const float e = exact_dot(sq, L.vec + static_cast<uint64_t>(loc) * L.dim, L.dim);
             key = result_key(e, loc);
             take = true;
@@ -339,7 +551,18 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
             base = __shfl_sync(0xffffffffu, base, leader);
             if (take) ws[base + __popc(mask & ((1u << lane) - 1u))] = key;
         }
-    });
+    };
+    if (fast) {
+        for (uint32_t b = tid & ~31u; b < n; b += blockDim.x) {  // warp-uniform bounds
+            const uint32_t idx = b + (tid & 31);
+            const bool ok = idx < n;
+            rescore(ok, ok ? cs[idx] : 0.0f, ok ? cl[idx] : 0u);
+        }
+    } else {
+        for_each_segment_entry(S, L.segs, L.seg_cap, sc, [&](uint32_t i, bool ok, float v) {
+            rescore(ok, v, ok && v >= thr ? lc[i] : 0u);
+        });
+    }
     __syncthreads();
     const uint32_t nf = S.counter;
     __syncthreads();
@@ -514,8 +737,8 @@ cudaError_t launch_sample_threshold(const SampleThresholdLaunch& L, cudaStream_t
 
 cudaError_t launch_select_topk(const SelectLaunch& L, cudaStream_t stream) {
     if (L.nq_list == 0) return cudaSuccess;
-    if (bad_segments(L.segs, L.seg_cap, L.cap)) return cudaErrorInvalidValue;
-    const size_t smem = sizeof(SelectSmem) + static_cast<size_t>(L.dim) * sizeof(float);
+    if (bad_segments(L.segs, L.seg_cap, L.cap) || L.segs > static_cast<uint32_t>(kST)) return cudaErrorInvalidValue;
+    const size_t smem = select_cand_offset(L.dim) + kSelFast * (sizeof(float) + sizeof(uint32_t));
     cudaError_t e = set_smem(select_topk_kernel, smem);
     if (e != cudaSuccess) return e;
     select_topk_kernel<<<L.nq_list, kST, smem, stream>>>(L);

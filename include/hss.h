@@ -110,13 +110,12 @@ int hss_aggregator_launch(const uint8_t* filterResult, const float* docScores, c
  * for callers that must not allocate device memory per call or hold a workspace of their own --
  * a request handler running under a fixed device-memory budget that another allocator owns, or a
  * latency-critical loop that cannot afford cudaFree, which waits for the whole device to go idle.
- * Its scratch is a 64 KB array compiled into the library,
- * one per device, so docNumber <= HSS_AGGREGATOR_NOALLOC_MAX_DOCS (else HSS_ERR_LIMIT, nothing
- * launched). It calls no allocator. The first call on each device looks the array's address up
- * (cudaGetSymbolAddress, with that device current), which may load the module: make that first
- * call before any stream capture. Every call on a device shares the one array: calls that can
- * overlap on the GPU (different streams without ordering between them) race and must not be made;
- * calls ordered on one stream are safe, since each call rewrites all the scratch it reads. */
+ * Its scratch is a 64 KB array compiled into the library, one per device, so docNumber <=
+ * HSS_AGGREGATOR_NOALLOC_MAX_DOCS (else HSS_ERR_LIMIT, nothing launched). It calls no allocator.
+ * The first call on each device looks the array's address up (cudaGetSymbolAddress, with that
+ * device current). Every call on a device shares the one array: calls that can overlap on the GPU
+ * (different streams without ordering between them) race and must not be made; calls ordered on
+ * one stream are safe, since each call rewrites all the scratch it reads. */
 #define HSS_AGGREGATOR_NOALLOC_MAX_DOCS 16777216u
 int hss_aggregator_launch_noalloc(const uint8_t* filterResult, const float* docScores,
                                   const uint32_t* docLocationConst, float* outScores, uint32_t* outLocations,
@@ -229,13 +228,13 @@ int hss_searcher_last_times(const hss_searcher* s, float* ms5, uint32_t* retries
  * pivot pre-select). */
 typedef struct hss_model hss_model;
 
-/* dim + posting rows + 6: the feature row width a model for this searcher must take. */
+/* dim + posting rows + 12: the feature row width a model for this searcher must take. */
 uint32_t hss_searcher_feature_dim(const hss_searcher* s);
 /* Feature rows dX [nq][feature_dim] of a batch (device queries and output): query * sqrt(dim); per
  * posting row of the query's filter 1 + log10(row density) / 4 (0 elsewhere); log10(filter
- * selectivity) / 4; log10(K) / 3; 1; the doc sample's best score; its K-th best score (-2 when
- * absent); log10(filtered sample docs + 1) / 5. Runs the filter stage and the doc sample;
- * synchronises `stream`. */
+ * selectivity) / 4; log10(K) / 3; 1; the doc sample's best scores at ranks 1, 2, 4, ..., 64 (-2
+ * past the sample's size); its K-th best score (-2 when absent); log10(filtered sample docs + 1) / 5.
+ * Runs the filter stage and the doc sample; synchronises `stream`. */
 int hss_searcher_features(hss_searcher* s, const float* dQueries, uint32_t nq, const hss_filters* filters,
                           const uint32_t* topks, float* dX, hss_stream_t stream);
 /* model NULL switches the learned threshold off. margin is subtracted from the prediction. */

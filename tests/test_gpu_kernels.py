@@ -135,6 +135,34 @@ def test_filter_operator_both_table_conventions(torch_cuda):
             assert (got == want).all(), (e, convention)
 
 
+def test_filter_operator_rejects_programs_whose_counts_would_wrap(torch_cuda):
+    # Raw programs reach the operator as a device buffer, so the kernel's own program check is the
+    # only guard. Operand and part counts near 2^32 would wrap a u32 sum (next + pn, pc + 2 + parts);
+    # the check compares against the remaining room instead and reports the program as bad.
+    torch = torch_cuda
+    mix, vec, bits, table = _table(torch, "bitmap", seed=7)
+    info = table.info
+    S, P = info["segment_num"], info["doc_num_per_segment"]
+    _, ptab, _ = table.device_ptrs()
+    heads = torch.empty(info["posting_rows"] * S, dtype=torch.int64, device="cuda")
+    _copy_device(ptab, heads.data_ptr(), heads.numel() * 8)
+    _, rows, _, _ = table.compile_filter("5")
+    tab = heads.view(info["posting_rows"], S)[int(rows[0])].contiguous()  # [segments], one operand
+    big = 0xFFFFFFFF
+    AND, OR, NOT, CONJ = 1, 2, 3, 0
+    words = S * P // 64
+    for prog in ([AND, 1, 0, AND, big, 1], [AND, 1, 0, CONJ, big], [NOT, big, 2], [OR, 1, 0, OR, big, 0],
+                 [CONJ, 1, 1, AND, big, 1]):
+        d_prog = torch.tensor(np.array(prog, np.uint32).view(np.int32), device="cuda")
+        d_out = torch.full((words,), -1, dtype=torch.int64, device="cuda")
+        d_status = torch.zeros(1, dtype=torch.int32, device="cuda")
+        ctx = _lib.FilterContext(1, S, P // 16, 1, len(prog), 1, _lib.HSS_FILTER_HEAD_ADDRESSES)
+        hss.bitmap_text_filter(tab.data_ptr(), d_prog.data_ptr(), ctx, d_out.data_ptr(), d_status.data_ptr())
+        torch.cuda.synchronize()
+        assert int(d_status.item()) & _lib.QSTATUS_BAD_PROGRAM, prog
+        assert not d_out.cpu().numpy().any(), prog
+
+
 _ROW_CACHE = {}
 
 

@@ -91,6 +91,37 @@ def _check_exact(res, want, nq):
         assert (scores[i][:c].view(np.uint32) == ws[i][:c].view(np.uint32)).all(), i
 
 
+def test_feature_rows_hold_the_sample_order_statistics(torch_cuda):
+    # tail of a feature row: log selectivity, log K, 1, the sample's scores at ranks 1, 2, 4, ..., 64
+    # (-2 past the sample's size), its K-th best (-2 when absent), log10(sample docs + 1) / 5
+    torch = torch_cuda
+    mix, vec, bits, table = _world(seed=85, n=60000)
+    s = hss.FullRecallSearcher(table, max_batch=64, method=2)
+    q, ex, k = _queries(mix, 64, 97)
+    din = s.feature_dim()
+    assert din == 128 + table.info["posting_rows"] + 12
+    X = torch.zeros((64, din), dtype=torch.float32, device="cuda")
+    dq = torch.tensor(q, device="cuda")
+    f = s.compile_filters(ex)
+    s.features(dq.data_ptr(), 64, f, k, X.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    tail = X.cpu().numpy()[:, din - 12:]
+    assert np.isfinite(tail).all()
+    assert (tail[:, 2] == 1.0).all()
+    ranks, kth, logn = tail[:, 3:10], tail[:, 10], tail[:, 11]
+    n = np.rint(10 ** (logn * 5) - 1).astype(np.int64)
+    for i in range(64):
+        have = (1 << np.arange(7)) <= n[i]
+        assert (ranks[i][~have] == -2.0).all(), i
+        r = ranks[i][have]
+        assert (np.diff(r) <= 0).all(), (i, r)  # best first
+        if n[i] >= k[i]:
+            assert kth[i] <= r[0], i
+            if k[i] <= 64:
+                assert kth[i] <= r[int(np.log2(k[i]))], i
+        else:
+            assert kth[i] == -2.0, i
+
+
 @pytest.mark.parametrize("method", [2, 1], ids=["bf16", "tf32"])
 def test_learned_threshold_search_is_exact(torch_cuda, method):
     mix, vec, bits, table = _world()
