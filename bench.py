@@ -354,9 +354,19 @@ def measure_form(args, ctx, method, learned=False):
         with open(tpath) as f:
             traffic = json.load(f).get(method)
     kernel = "cand_simt_kernel" if method == "simt" else ("tc2_cand_kernel" if B > 128 else "tc_cand_kernel")
+    # the tensor side of the same stage: 2 d flops per (query, doc) pair of every pass, against the
+    # pipe's peak (measured BF16 GEMM rate; TF32 and E4M3 by the nominal dense ratios 1/2 and 2)
+    flops = reads * 2.0 * 128 * args.docs * B
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    tpeak = {"simt": None, "tf32": bf16_peak / 2, "bf16": bf16_peak, "e4m3": bf16_peak * 2}[method]
+    t_s = cand_avg / 1e3
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "traffic": traffic, "kernel": kernel, "avg_ms": cand_avg,
-            "peak_source": "measured" if peaks else "fallback"}
+            "peak_source": "measured" if peaks else "fallback",
+            "tensor": None if tpeak is None else {
+                "achieved_tflops": flops / t_s / 1e12, "peak_tflops": tpeak, "frac": flops / t_s / 1e12 / tpeak,
+                "peak_note": "measured BF16 GEMM" + ("" if method == "bf16" else " x nominal dense ratio")},
+            "bound_frac": (max(alg_bytes / (hbm * 1e9), 0.0 if tpeak is None else flops / (tpeak * 1e12)) / t_s)}
     out = {"value": value, "t_max_ms": t_max, "e2e": e2e, "roofline": roof, "clocks": clocks, "launches": launches,
            "stages_ms": dict(zip(["filter", "sample", "candidates", "select", "total"],
                                  [round(float(x), 4) for x in np.mean(np.array(stage_ms), axis=0)])),
@@ -485,6 +495,7 @@ def run_ours(args):
         o_sc, o_id, o_n, topks, sh = chosen["out"]
         nq = len(ref_counts)
         set_ok = order_ok = score_ok = True
+        err_abs, err_rel = [], []
         for j in range((nq + B - 1) // B):
             rc = searcher.search_device(d_q[j].data_ptr(), B, filters[j], topks, o_sc.data_ptr(), o_id.data_ptr(),
                                         o_n.data_ptr(), K, sh)
@@ -506,11 +517,20 @@ def run_ours(args):
                     acc = (acc + (qv[d] * dv[:, d]).astype(np.float32)).astype(np.float32)
                 if not (acc.view(np.uint32) == sc.view(np.uint32)).all():
                     score_ok = False
+                exact64 = dv.astype(np.float64) @ qv.astype(np.float64)
+                err_abs.append(np.abs(sc.astype(np.float64) - exact64))
+                err_rel.append(np.abs(sc.astype(np.float64) - exact64) / np.maximum(np.abs(exact64), 1e-30))
                 if c > 1 and not all(sc[r] > sc[r + 1] or (sc[r] == sc[r + 1] and ids[r] < ids[r + 1])
                                      for r in range(c - 1)):
                     order_ok = False
         rec["parity_full_scale"] = {"queries": nq, "against": cb["kind"], "id_sets_match": set_ok,
                                     "scores_bit_exact": score_ok, "order_score_desc_id_asc": order_ok}
+        if err_abs:
+            ea, er = np.concatenate(err_abs), np.concatenate(err_rel)
+            # the returned FP32 scores against an FP64 dot product of the same vectors
+            rec["parity_full_scale"]["score_error_vs_fp64"] = {
+                "max_abs": float(ea.max()), "median_abs": float(np.median(ea)),
+                "max_rel": float(er.max()), "median_rel": float(np.median(er))}
     if rank == 0:
         print(json.dumps(rec))
     if world > 1:

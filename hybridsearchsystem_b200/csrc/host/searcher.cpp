@@ -160,11 +160,6 @@ bool FullRecallSearcher::Allocate() {
             m_err = "cuTensorMapEncodeTiled failed";
             return false;
         }
-        // the resident queries (128 rows per SM) and at least two k-block stages fit shared memory
-        if (tc_pair_smem_bytes(m_tcKblocks, 2) > 232448 || tc_smem_bytes(1, m_tcKblocks, 2) > 232448) {
-            m_err = "vector dimension too large for the tensor-core pass";
-            return false;
-        }
     }
     return true;
 }
@@ -454,11 +449,11 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     // segments [segBase, segBase + its segments) of segCap entries each. Tiles hold unitOf() docs:
     // 128 for the SIMT pass and the single-SM tensor-core pass, 256 for the SM-pair pass.
     auto useSimt = [&](bool simt) { return !tc || simt; };
-    auto unitOf = [&](uint32_t rows, bool simt) { return useSimt(simt) ? 128u : tc_tile_docs(rows); };
+    auto unitOf = [&](uint32_t rows, bool simt) { return useSimt(simt) ? 128u : tc_tile_docs(rows, m_tcKblocks); };
     auto tilesOf = [&](uint32_t unit) { return (T.GetDocNum() + unit - 1) / unit; };
     auto ctasOf = [&](uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) {
         return useSimt(simt) ? cand_simt_segments(countTiles, m_numSms, cap)
-                             : tc_cand_ctas(rows, countTiles, m_numSms, cap);
+                             : tc_cand_ctas(rows, m_tcKblocks, countTiles, m_numSms, cap);
     };
     auto segsOf = [&](uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) {
         const uint32_t g = ctasOf(rows, countTiles, cap, simt);

@@ -172,18 +172,22 @@ struct TcCandLaunch {
     uint32_t cap;
     uint32_t ctas, seg_cap;    // CTAs of the launch (tc_cand_ctas); entries per list segment
     uint32_t seg_base;         // first segment this pass writes (it writes 2 per CTA)
-    uint64_t tile_begin, tile_step, tile_count;  // tiles of tc_tile_docs(nq_rows) docs
+    uint64_t tile_begin, tile_step, tile_count;  // tiles of tc_tile_docs(nq_rows, kblocks) docs
     uint32_t tile_skip;
     uint64_t tiles128;         // 128-doc tiles of the corpus (rows of the tensor map / 128)
     int32_t* error;            // device error bits (bounded waits that expired)
 };
 
+// Whether a tensor-core pass over rows of `kblocks` 128-byte k-blocks streams the queries' k-blocks
+// through its stage ring with the docs' (an SM pair per tile, any batch size) instead of keeping them
+// resident: when fewer than four stages would fit next to the resident queries (long vectors).
+bool tc_stream_queries(uint32_t kblocks);
 // Docs per tile of a tensor-core pass over `rows` staged queries: 128 (one SM per tile, rows <= 128)
-// or 256 (an SM pair per tile, cta_group::2, rows 129..256).
-uint32_t tc_tile_docs(uint32_t rows);
+// or 256 (an SM pair per tile, cta_group::2: rows 129..256, or streamed queries).
+uint32_t tc_tile_docs(uint32_t rows, uint32_t kblocks);
 // CTAs of a tensor-core pass over tile_count such tiles into lists of `cap` entries; it writes two
 // list segments per CTA.
-uint32_t tc_cand_ctas(uint32_t rows, uint64_t tile_count, int num_sms, uint32_t cap);
+uint32_t tc_cand_ctas(uint32_t rows, uint32_t kblocks, uint64_t tile_count, int num_sms, uint32_t cap);
 size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages);
 size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages);
 cudaError_t launch_tc_cand(const TcCandLaunch& L, const CUtensorMap& doc_map, const CUtensorMap& qry_map, int sms,

@@ -612,16 +612,19 @@ __device__ inline bool pair_wait(unsigned long long* bar, uint32_t parity, PairS
     return true;
 }
 
-template <int F>
+// SQ (streamed queries, long vectors): no resident query tile; each stage holds the query k-block
+// (16 KB, from the L2-resident staged queries) followed by the doc k-block, loaded together.
+template <int F, bool SQ>
 __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_constant__ CUtensorMap doc_map,
                                                                   const __grid_constant__ CUtensorMap qry_map,
                                                                   TcCandLaunch L) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t kb_n = L.kblocks;
+    constexpr size_t kStage = SQ ? 2 * kStageBytes : kStageBytes;  // bytes of one ring stage
     unsigned char* qsm = base;
-    unsigned char* ring = base + static_cast<size_t>(kb_n) * kStageBytes;
-    PairShared& S = *reinterpret_cast<PairShared*>(ring + static_cast<size_t>(L.stages) * kStageBytes);
+    unsigned char* ring = base + (SQ ? 0 : static_cast<size_t>(kb_n) * kStageBytes);
+    PairShared& S = *reinterpret_cast<PairShared*>(ring + static_cast<size_t>(L.stages) * kStage);
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t stages = L.stages;
@@ -659,10 +662,12 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
 
     if (warp == 0) {
         if (lane == 0) {
-            mbar_expect_tx(&S.qbar, kb_n * kStageBytes);
-            for (uint32_t kb = 0; kb < kb_n; ++kb)
-                tma_load_2d(qsm + static_cast<size_t>(kb) * kStageBytes, &qry_map,
-                            static_cast<int>(kb * (128 / Fmt<F>::elem)), static_cast<int>(rank * kRows), &S.qbar);
+            if (!SQ) {
+                mbar_expect_tx(&S.qbar, kb_n * kStageBytes);
+                for (uint32_t kb = 0; kb < kb_n; ++kb)
+                    tma_load_2d(qsm + static_cast<size_t>(kb) * kStageBytes, &qry_map,
+                                static_cast<int>(kb * (128 / Fmt<F>::elem)), static_cast<int>(rank * kRows), &S.qbar);
+            }
             uint32_t n = 0;
             TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, pair, npairs);
             for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs, walk.advance()) {
@@ -670,9 +675,13 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
                 for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
                     if (!pair_wait<F>(&S.empty[s], ph ^ 1u, S, L.error, 1, false)) break;
-                    mbar_expect_tx(&S.full[s], kStageBytes);
-                    tma_load_2d(ring + static_cast<size_t>(s) * kStageBytes, &doc_map,
-                                static_cast<int>(kb * (128 / Fmt<F>::elem)), y, &S.full[s]);
+                    unsigned char* st = ring + static_cast<size_t>(s) * kStage;
+                    mbar_expect_tx(&S.full[s], static_cast<uint32_t>(kStage));
+                    if (SQ)
+                        tma_load_2d(st, &qry_map, static_cast<int>(kb * (128 / Fmt<F>::elem)),
+                                    static_cast<int>(rank * kRows), &S.full[s]);
+                    tma_load_2d(st + (SQ ? kStageBytes : 0), &doc_map, static_cast<int>(kb * (128 / Fmt<F>::elem)), y,
+                                &S.full[s]);
                 }
             }
             S.n_issued = n;
@@ -681,8 +690,8 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
         if (lane == 0 && rank == 1) {
             // forwarder: the even CTA's MMAs read this CTA's queries and stages; tell it when they land
             uint32_t n = 0;
-            if (pair_wait<F>(&S.qbar, 0, S, L.error, 2, false)) {
-                mbar_arrive_cluster(peer_addr(&S.pqbar, 0));
+            if (SQ || pair_wait<F>(&S.qbar, 0, S, L.error, 2, false)) {
+                if (!SQ) mbar_arrive_cluster(peer_addr(&S.pqbar, 0));
                 for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs) {
                     bool ok = true;
                     for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
@@ -702,7 +711,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
             constexpr uint32_t idesc =
                 (1u << 4) | (Fmt<F>::ab << 7) | (Fmt<F>::ab << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
             uint32_t n = 0, iter = 0;
-            bool ok = pair_wait<F>(&S.qbar, 0, S, L.error, 2, false) && pair_wait<F>(&S.pqbar, 0, S, L.error, 2, true);
+            bool ok = SQ || (pair_wait<F>(&S.qbar, 0, S, L.error, 2, false) && pair_wait<F>(&S.pqbar, 0, S, L.error, 2, true));
             for (uint64_t it = pair; ok && it < ntiles && !S.abort; it += npairs, ++iter) {
                 const uint32_t buf = iter & 1u;
                 if (!pair_wait<F>(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4, true)) break;
@@ -715,8 +724,9 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
                         break;
                     }
                     fence_after();
-                    const uint64_t adesc = smem_desc(smem_u32(qsm + static_cast<size_t>(kb) * kStageBytes));
-                    const uint64_t bdesc = smem_desc(smem_u32(ring + static_cast<size_t>(s) * kStageBytes));
+                    unsigned char* st = ring + static_cast<size_t>(s) * kStage;
+                    const uint64_t adesc = smem_desc(smem_u32(SQ ? st : qsm + static_cast<size_t>(kb) * kStageBytes));
+                    const uint64_t bdesc = smem_desc(smem_u32(st + (SQ ? kStageBytes : 0)));
 #pragma unroll
                     for (uint32_t ks = 0; ks < 4; ++ks)  // 32 bytes of K per instruction
                         mma_pair<F>(tmem + buf * 256u, adesc + ks * 2u, bdesc + ks * 2u, idesc, (kb | ks) != 0);
@@ -814,7 +824,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
         for (uint32_t k = S.n_consumed; k < S.n_issued; ++k)
             if (!mbar_wait_drain(&S.full[k % stages], (k / stages) & 1u)) break;
     }
-    if (threadIdx.x == 0 && !mbar_try(&S.qbar, 0)) mbar_wait_drain(&S.qbar, 0);
+    if (!SQ && threadIdx.x == 0 && !mbar_try(&S.qbar, 0)) mbar_wait_drain(&S.qbar, 0);
     __syncthreads();
     // neither CTA leaves (or frees TMEM) while the pair's MMAs or the other CTA's remote arrives may
     // still touch its shared memory
@@ -825,11 +835,11 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
     }
 }
 
-template <int F>
+template <int F, bool SQ>
 cudaError_t launch_tc2_typed(const TcCandLaunch& L, const CUtensorMap& dmap, const CUtensorMap& qmap,
                              cudaStream_t stream) {
     const size_t smem = tc_pair_smem_bytes(L.kblocks, L.stages);
-    cudaError_t e = cudaFuncSetAttribute(tc2_cand_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(tc2_cand_kernel<F, SQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg{};
@@ -844,7 +854,7 @@ cudaError_t launch_tc2_typed(const TcCandLaunch& L, const CUtensorMap& dmap, con
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, tc2_cand_kernel<F>, dmap, qmap, L);
+    return cudaLaunchKernelEx(&cfg, tc2_cand_kernel<F, SQ>, dmap, qmap, L);
 }
 
 template <int F>
@@ -862,12 +872,18 @@ constexpr size_t kSmemBudget = 232448;  // dynamic shared memory of one CTA
 
 }  // namespace
 
-uint32_t tc_tile_docs(uint32_t rows) { return rows > 128 ? 256u : 128u; }
+bool tc_stream_queries(uint32_t kblocks) {
+    return 1024 + (static_cast<size_t>(kblocks) + 4) * kStageBytes + sizeof(PairShared) > kSmemBudget;
+}
 
-uint32_t tc_cand_ctas(uint32_t rows, uint64_t tile_count, int num_sms, uint32_t cap) {
+uint32_t tc_tile_docs(uint32_t rows, uint32_t kblocks) {
+    return rows > 128 || tc_stream_queries(kblocks) ? 256u : 128u;
+}
+
+uint32_t tc_cand_ctas(uint32_t rows, uint32_t kblocks, uint64_t tile_count, int num_sms, uint32_t cap) {
     // every CTA fills two list segments; two passes' segments must fit kMaxCandSegs with at least
     // kMinSegCap entries each
-    const uint64_t unit = rows > 128 ? 2 : 1;  // CTAs per tile group
+    const uint64_t unit = tc_tile_docs(rows, kblocks) == 256u ? 2 : 1;  // CTAs per tile group
     uint64_t g = static_cast<uint64_t>(num_sms) / unit;
     g = tile_count < g ? tile_count : g;
     const uint64_t by_segs = kMaxCandSegs / (4 * unit);
@@ -884,6 +900,8 @@ size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages) {
 }
 
 size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages) {
+    if (tc_stream_queries(kblocks))  // no resident queries; a stage holds a query and a doc k-block
+        return 1024 + static_cast<size_t>(stages) * 2 * kStageBytes + sizeof(PairShared);
     return 1024 + static_cast<size_t>(kblocks) * kStageBytes + static_cast<size_t>(stages) * kStageBytes +
            sizeof(PairShared);
 }
@@ -895,24 +913,30 @@ cudaError_t launch_tc_cand(const TcCandLaunch& Lin, const CUtensorMap& doc_map, 
         !tile_walk_fits(Lin.tile_begin, Lin.tile_step, Lin.tile_skip, Lin.tile_count, Lin.ctas))
         return cudaErrorInvalidValue;
     TcCandLaunch L = Lin;
-    const bool pair = L.nq_rows > 128;
-    // as many stages as shared memory holds next to the resident queries
+    const bool sq = tc_stream_queries(L.kblocks);
+    const bool pair = tc_tile_docs(L.nq_rows, L.kblocks) == 256u;
+    // as many stages as shared memory holds next to the resident queries (or, streamed, as many
+    // query + doc stage pairs as it holds)
+    const size_t stage = sq ? 2 * kStageBytes : kStageBytes;
     const size_t fixed = pair ? tc_pair_smem_bytes(L.kblocks, 0) : tc_smem_bytes(1, L.kblocks, 0);
-    if (fixed + 2 * kStageBytes > kSmemBudget) return cudaErrorInvalidValue;
-    const size_t st = (kSmemBudget - fixed) / kStageBytes;
+    if (fixed + 2 * stage > kSmemBudget) return cudaErrorInvalidValue;
+    const size_t st = (kSmemBudget - fixed) / stage;
     L.stages = static_cast<uint32_t>(st < static_cast<size_t>(kMaxTcStages) ? st : kMaxTcStages);
     // every CTA writes segments seg_base + 2 b and seg_base + 2 b + 1 (pair: 4 per pair)
     const uint64_t seg_end = static_cast<uint64_t>(L.seg_base) + 2ull * L.ctas;
-    if (L.ctas != tc_cand_ctas(L.nq_rows, L.tile_count, sms, L.cap) || L.seg_cap == 0 || seg_end > kMaxCandSegs ||
+    if (L.ctas != tc_cand_ctas(L.nq_rows, L.kblocks, L.tile_count, sms, L.cap) || L.seg_cap == 0 || seg_end > kMaxCandSegs ||
         seg_end * L.seg_cap > L.cap)
         return cudaErrorInvalidValue;
     switch (L.format) {
-        case kTcTF32: return pair ? launch_tc2_typed<kTcTF32>(L, doc_map, qry_map, stream)
-                                  : launch_tc1_typed<kTcTF32>(L, doc_map, qry_map, stream);
-        case kTcBF16: return pair ? launch_tc2_typed<kTcBF16>(L, doc_map, qry_map, stream)
-                                  : launch_tc1_typed<kTcBF16>(L, doc_map, qry_map, stream);
-        case kTcE4M3: return pair ? launch_tc2_typed<kTcE4M3>(L, doc_map, qry_map, stream)
-                                  : launch_tc1_typed<kTcE4M3>(L, doc_map, qry_map, stream);
+        case kTcTF32: return sq ? launch_tc2_typed<kTcTF32, true>(L, doc_map, qry_map, stream)
+                                : pair ? launch_tc2_typed<kTcTF32, false>(L, doc_map, qry_map, stream)
+                                       : launch_tc1_typed<kTcTF32>(L, doc_map, qry_map, stream);
+        case kTcBF16: return sq ? launch_tc2_typed<kTcBF16, true>(L, doc_map, qry_map, stream)
+                                : pair ? launch_tc2_typed<kTcBF16, false>(L, doc_map, qry_map, stream)
+                                       : launch_tc1_typed<kTcBF16>(L, doc_map, qry_map, stream);
+        case kTcE4M3: return sq ? launch_tc2_typed<kTcE4M3, true>(L, doc_map, qry_map, stream)
+                                : pair ? launch_tc2_typed<kTcE4M3, false>(L, doc_map, qry_map, stream)
+                                       : launch_tc1_typed<kTcE4M3>(L, doc_map, qry_map, stream);
     }
     return cudaErrorInvalidValue;
 }

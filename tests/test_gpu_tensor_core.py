@@ -101,3 +101,28 @@ def test_tensor_core_overflow_reruns_are_exact(torch_cuda, method, nq):
         assert int(counts[i]) == c
         assert (ids[i][:c] == wi[i][:c]).all(), (method, i)
         assert (scores[i][:c].view(np.uint32) == ws[i][:c].view(np.uint32)).all(), (method, i)
+
+
+@pytest.mark.parametrize("nq", [64, 256], ids=["few_queries", "sm_pair"])
+@pytest.mark.parametrize("method", list(METHODS))
+def test_long_vectors_are_exact(torch_cuda, method, nq):
+    # 768-dim vectors (the precision-form configuration's width): the query tile no longer fits next
+    # to a deep stage ring for TF32 (24 k-blocks) and BF16 (12), so those passes stream each query
+    # k-block with the doc k-block through the ring on SM pairs, also for a batch of 64; E4M3 (6
+    # k-blocks) keeps its queries resident
+    mix = data.Mixture(768, 64, (1e-3, 0.6), n_clusters=32, seed=61)
+    vec, bits, _ = mix.corpus(30000, seed=62)
+    table = hss.DataTable.build(vec, bits, 64, device=0, doc_num_per_segment=8192)
+    q = mix.queries(nq, seed=63)
+    exprs = data.make_filters(mix, nq, n_tags=(1, 4), seed=64, selectivity_range=(1e-3, 1.0))
+    topks = np.array([1, 10, 100, 500] * (nq // 4))
+    s = hss.FullRecallSearcher(table, max_batch=nq, method=METHODS[method])
+    for a, e, k in zip(q, exprs, topks):
+        s.add_query(e, a, int(k))
+    scores, ids, counts = s.batch_search()
+    ws, wi, wc = oracle.topk(q, exprs, topks, vec, bits, threads=8)
+    for i in range(nq):
+        c = int(wc[i])
+        assert int(counts[i]) == c, (method, i)
+        assert (ids[i][:c] == wi[i][:c]).all(), (method, i)
+        assert (scores[i][:c].view(np.uint32) == ws[i][:c].view(np.uint32)).all(), (method, i)
