@@ -59,6 +59,8 @@ def parse_args():
                     help="skip measuring the plain FP32 (TF32) form beside the chosen one")
     ap.add_argument("--no-serve", dest="serve", action="store_false", help="skip the serving-loop latency sweep")
     ap.add_argument("--serve-requests", type=int, default=40000)
+    ap.add_argument("--serve-rates", default="1000,10000,50000,100000,150000,200000",
+                    help="offered Poisson rates (QPS) of the serving sweep")
     ap.add_argument("--serve-wait-us", type=int, default=300)
     return ap.parse_args()
 
@@ -374,6 +376,7 @@ def measure_form(args, ctx, method, learned=False):
            "learned": learned, "searcher": searcher, "filters": filters, "d_q": d_q,
            "out": (o_sc, o_id, o_n, topks, sh)}
     if report:
+        out["model"], out["margin"] = model, margin
         out["learned_report"] = {k: (round(v, 5) if isinstance(v, float) else v) for k, v in report.items()}
         # what the model does on this workload: its estimation pass against the same pass at the doc
         # sample's proven threshold (margin 1e9 turns the prediction into -inf), over the measured batches
@@ -401,26 +404,30 @@ def data_filters(mix, n, seed):
     return data.make_filters(mix, n, n_tags=(1, 6), seed=seed, selectivity_range=(1e-4, 1.0))
 
 
-def measure_serving(args, ctx, method, rates):
-    """p50/p99 latency of single queries through the serving loop (continuous batching) at
-    open-loop Poisson arrival rates."""
+def measure_serving(args, ctx, method, rates, model=None, margin=0.0):
+    """p50/p99 latency of single queries through the serving loop (continuous batching) at open-loop
+    Poisson arrival rates. Requests mix the workload's filters (selectivity log-uniform in
+    [1e-4, 1]) with per-request K log-uniform in [1, 1000]."""
     import hybridsearchsystem_b200 as hss
     srv = hss.Server(ctx["table"], slots=2, max_batch=args.batch, max_wait_us=args.serve_wait_us,
                      method=METHODS[method], candidate_cap=args.cand_cap)
+    if model is not None:
+        srv.set_threshold_model(model, margin)
     q, ex = ctx["queries"], ctx["exprs"]
+    kk = np.exp(np.random.default_rng(77).uniform(0.0, np.log(1000.0), len(q))).astype(np.uint32) + 1
+    kk = np.minimum(kk, 1000)
     out = []
     for rate in rates:
-        n = int(min(args.serve_requests, max(2000, rate * 0.6)))
+        n = int(min(args.serve_requests, max(2000, rate * 0.5)))
         idx = np.arange(n) % len(q)
         srv.reset_stats()
-        lat, offered, wall = srv.run_poisson(q[idx], [ex[i] for i in idx], np.full(n, args.topk, np.uint32), rate,
-                                             seed=int(rate))
+        lat, offered, wall = srv.run_poisson(q[idx], [ex[i] for i in idx], kk[idx], rate, seed=int(rate))
         st = srv.stats()
         out.append({"offered_qps": round(offered), "completed_qps": round(n / wall), "p50_ms": round(st["p50_ms"], 3),
                     "p99_ms": round(st["p99_ms"], 3), "mean_batch": round(st["mean_batch"], 1)})
     srv.close()
-    return {"form": FORMS[method], "slots": 2, "max_wait_us": args.serve_wait_us, "topk": args.topk,
-            "rates": out}
+    return {"form": FORMS[method] + (" + learned threshold" if model is not None else ""), "slots": 2,
+            "max_wait_us": args.serve_wait_us, "topk": "log-uniform in [1, 1000] per request", "rates": out}
 
 
 def run_ours(args):
@@ -456,8 +463,14 @@ def run_ours(args):
         forms["plain_fp32_simt"] = measure_form(args, ctx, "simt")
     serving = None
     if rank == 0 and world == 1 and args.serve:
-        rates = [r * chosen["value"] for r in (0.25, 0.5, 0.75)]
-        serving = measure_serving(args, ctx, args.method, rates)
+        rates = [float(r) for r in args.serve_rates.split(",")]
+        serving = {"chosen": measure_serving(args, ctx, args.method, rates, chosen.get("model"),
+                                             chosen.get("margin", 0.0))}
+        if "chosen_learned" in forms:
+            serving["chosen_learned"] = measure_serving(args, ctx, args.method, rates, forms["chosen_learned"]["model"],
+                                                        forms["chosen_learned"]["margin"])
+        if args.plain:
+            serving["plain_fp32"] = measure_serving(args, ctx, "tf32", rates)
 
     def summary(f):
         d = {"value": f["value"], "e2e_qps": f["e2e"], "ms_per_step": f["t_max_ms"] / args.steps,
