@@ -714,12 +714,14 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
             bool ok = SQ || (pair_wait<F>(&S.qbar, 0, S, L.error, 2, false) && pair_wait<F>(&S.pqbar, 0, S, L.error, 2, true));
             for (uint64_t it = pair; ok && it < ntiles && !S.abort; it += npairs, ++iter) {
                 const uint32_t buf = iter & 1u;
-                if (!pair_wait<F>(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4, true)) break;
+                // CTA-scope waits on the barriers the odd CTA arrives on remotely (as its arrives are
+                // CTA-scope): a cluster-scope acquire on every stage cost the TF32 pass about 4 %
+                if (!pair_wait<F>(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4, false)) break;
                 fence_after();
                 for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
                     if (!pair_wait<F>(&S.full[s], ph, S, L.error, 8, false) ||
-                        !pair_wait<F>(&S.pfull[s], ph, S, L.error, 8, true)) {
+                        !pair_wait<F>(&S.pfull[s], ph, S, L.error, 8, false)) {
                         ok = false;
                         break;
                     }
