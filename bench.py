@@ -48,6 +48,7 @@ def parse_args():
     ap.add_argument("--cpu-queries", type=int, default=0, help="CPU baseline sample size (0: 2 per thread)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cand-cap", type=int, default=1 << 18, help="per-query candidate capacity")
+    ap.add_argument("--sample-docs", type=int, default=32768, help="docs of the threshold sample per batch")
     ap.add_argument("--method", default="bf16", choices=list(METHODS),
                     help="the chosen form's candidate pass: simt (FP32 FFMA), tf32 (tensor cores over the FP32 "
                          "rows), bf16, e4m3")
@@ -243,7 +244,8 @@ def measure_form(args, ctx, method, learned=False):
     rank, world, dev, table = ctx["rank"], ctx["world"], ctx["dev"], ctx["table"]
     queries, exprs, barrier = ctx["queries"], ctx["exprs"], ctx["barrier"]
     B, K = args.batch, args.topk
-    searcher = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[method])
+    searcher = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[method],
+                                      sample_docs=args.sample_docs)
     report = None
     if learned:
         # trained on its own queries (seeded apart from the measured ones), labels from the exact path
