@@ -17,7 +17,7 @@ namespace {
 
 constexpr int kST = 1024;             // threads of the selection CTAs
 constexpr int kHist = 16;             // radix histograms per CTA (warp w adds to hist[w % kHist])
-constexpr uint32_t kSelFast = 6144;   // candidates a select CTA holds in shared memory
+constexpr uint32_t kSelFast = 12288;  // candidate scores a select CTA holds in shared memory
 
 struct SelectSmem {
     uint32_t hist[kHist][256];                  // radix histograms
@@ -506,17 +506,13 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
     }
     const uint32_t kq = min(k, n);
     for (uint32_t i = tid; i < L.dim; i += blockDim.x) sq[i] = L.qry[static_cast<uint64_t>(qi) * L.dim + i];
-    // A list that fits is gathered into shared memory once; the selection and rescoring passes then
-    // read shared memory instead of walking the segments again.
+    // A list that fits is gathered into shared memory once (scores only: the few rescored entries
+    // look their location up again); the selection and rescoring passes then read shared memory
+    // instead of walking the segments again.
     const bool fast = n <= kSelFast;
     float* cs = reinterpret_cast<float*>(smem_raw + select_cand_offset(L.dim));
-    uint32_t* cl = reinterpret_cast<uint32_t*>(cs + kSelFast);
     if (fast) {
-        for (uint32_t idx = tid; idx < n; idx += blockDim.x) {
-            const uint64_t i = segment_entry(S, L.segs, L.seg_cap, idx);
-            cs[idx] = sc[i];
-            cl[idx] = lc[i];
-        }
+        for (uint32_t idx = tid; idx < n; idx += blockDim.x) cs[idx] = sc[segment_entry(S, L.segs, L.seg_cap, idx)];
         __syncthreads();
     }
     float thr = -INFINITY;
@@ -556,7 +552,8 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
         for (uint32_t b = tid & ~31u; b < n; b += blockDim.x) {  // warp-uniform bounds
             const uint32_t idx = b + (tid & 31);
             const bool ok = idx < n;
-            rescore(ok, ok ? cs[idx] : 0.0f, ok ? cl[idx] : 0u);
+            const float v = ok ? cs[idx] : 0.0f;
+            rescore(ok, v, ok && v >= thr ? lc[segment_entry(S, L.segs, L.seg_cap, idx)] : 0u);
         }
     } else {
         for_each_segment_entry(S, L.segs, L.seg_cap, sc, [&](uint32_t i, bool ok, float v) {
@@ -738,7 +735,7 @@ cudaError_t launch_sample_threshold(const SampleThresholdLaunch& L, cudaStream_t
 cudaError_t launch_select_topk(const SelectLaunch& L, cudaStream_t stream) {
     if (L.nq_list == 0) return cudaSuccess;
     if (bad_segments(L.segs, L.seg_cap, L.cap) || L.segs > static_cast<uint32_t>(kST)) return cudaErrorInvalidValue;
-    const size_t smem = select_cand_offset(L.dim) + kSelFast * (sizeof(float) + sizeof(uint32_t));
+    const size_t smem = select_cand_offset(L.dim) + kSelFast * sizeof(float);
     cudaError_t e = set_smem(select_topk_kernel, smem);
     if (e != cudaSuccess) return e;
     select_topk_kernel<<<L.nq_list, kST, smem, stream>>>(L);
