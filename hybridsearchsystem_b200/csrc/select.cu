@@ -349,6 +349,29 @@ __device__ inline uint32_t pow2_at_least(uint32_t x) {
 // Top `kq` (<= kMaxTopK) of n distinct u64 keys key(i), sorted descending into S.sortbuf[0..kq).
 template <class KeyFn>
 __device__ void top_keys(KeyFn key, uint32_t n, uint32_t kq, SelectSmem& S) {
+    if (n <= static_cast<uint32_t>(kMaxTopK) && n > 2 * kq) {
+        // keep only keys whose score half is at least a lower bound of the kq-th best score (it keeps
+        // the top kq and at most the few keys sharing the kq-th's 24-bit prefix beyond them), then
+        // sort those: a bitonic sort over about kq keys instead of n
+        const uint32_t lb = kth_lower_bound_u32_visit(
+            [&](auto fn) {
+                for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) fn(static_cast<uint32_t>(key(i) >> 32));
+            },
+            kq, S);
+        if (threadIdx.x == 0) S.counter = 0;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint64_t v = key(i);
+            if (static_cast<uint32_t>(v >> 32) >= lb) S.sortbuf[atomicAdd(&S.counter, 1u)] = v;
+        }
+        __syncthreads();
+        const uint32_t got = S.counter;  // >= kq, <= n
+        const uint32_t m = pow2_at_least(got);
+        for (uint32_t i = got + threadIdx.x; i < m; i += blockDim.x) S.sortbuf[i] = 0ull;
+        __syncthreads();
+        bitonic_desc(S, m);
+        return;
+    }
     if (n <= static_cast<uint32_t>(kMaxTopK)) {
         const uint32_t m = pow2_at_least(n);
         for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) S.sortbuf[i] = i < n ? key(i) : 0ull;
