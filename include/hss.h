@@ -113,9 +113,10 @@ int hss_aggregator_launch(const uint8_t* filterResult, const float* docScores, c
  * Its scratch is a 64 KB array compiled into the library, one per device, so docNumber <=
  * HSS_AGGREGATOR_NOALLOC_MAX_DOCS (else HSS_ERR_LIMIT, nothing launched). It calls no allocator.
  * The first call on each device looks the array's address up (cudaGetSymbolAddress, with that
- * device current). Every call on a device shares the one array: calls that can overlap on the GPU
- * (different streams without ordering between them) race and must not be made; calls ordered on
- * one stream are safe, since each call rewrites all the scratch it reads. */
+ * device current); make that first call before any stream capture. Every call on a device shares
+ * the one array: calls that can overlap on the GPU (different streams without ordering between
+ * them) race and must not be made; calls ordered on one stream are safe, since each call rewrites
+ * all the scratch it reads. */
 #define HSS_AGGREGATOR_NOALLOC_MAX_DOCS 16777216u
 int hss_aggregator_launch_noalloc(const uint8_t* filterResult, const float* docScores,
                                   const uint32_t* docLocationConst, float* outScores, uint32_t* outLocations,
