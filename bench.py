@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--no-plain", dest="plain", action="store_false",
                     help="skip measuring the plain FP32 (TF32) form beside the chosen one")
     ap.add_argument("--no-serve", dest="serve", action="store_false", help="skip the serving-loop latency sweep")
+    ap.add_argument("--no-batch64", dest="batch64", action="store_false",
+                    help="skip measuring the chosen (and plain) form at batches of 64 queries")
     ap.add_argument("--serve-requests", type=int, default=40000)
     ap.add_argument("--serve-rates", default="1000,10000,50000,100000,150000,200000",
                     help="offered Poisson rates (QPS) of the serving sweep")
@@ -371,7 +373,7 @@ def measure_form(args, ctx, method, learned=False):
                 "achieved_tflops": flops / t_s / 1e12, "peak_tflops": tpeak, "frac": flops / t_s / 1e12 / tpeak,
                 "peak_note": "measured BF16 GEMM" + ("" if method == "bf16" else " x nominal dense ratio")},
             "bound_frac": (max(alg_bytes / (hbm * 1e9), 0.0 if tpeak is None else flops / (tpeak * 1e12)) / t_s)}
-    out = {"value": value, "t_max_ms": t_max, "e2e": e2e, "roofline": roof, "clocks": clocks, "launches": launches,
+    out = {"value": value, "t_max_ms": t_max, "e2e": e2e, "batch": B, "roofline": roof, "clocks": clocks, "launches": launches,
            "stages_ms": dict(zip(["filter", "sample", "candidates", "select", "total"],
                                  [round(float(x), 4) for x in np.mean(np.array(stage_ms), axis=0)])),
            "form": FORMS[method] + (" + learned threshold" if learned else ""), "method": method,
@@ -463,6 +465,14 @@ def run_ours(args):
         if not (args.method == "tf32" and not args.learned):
             forms["plain_fp32"] = measure_form(args, ctx, "tf32")
         forms["plain_fp32_simt"] = measure_form(args, ctx, "simt")
+    if args.batch64 and args.batch != 64:
+        # the configuration's other batch size: 64 queries per batch (one SM per 128-doc tile)
+        import copy
+        a64 = copy.copy(args)
+        a64.batch = 64
+        forms["chosen_batch64"] = measure_form(a64, ctx, args.method)
+        if args.plain:
+            forms["plain_fp32_batch64"] = measure_form(a64, ctx, "tf32")
     serving = None
     if rank == 0 and world == 1 and args.serve:
         rates = [float(r) for r in args.serve_rates.split(",")]
@@ -476,7 +486,8 @@ def run_ours(args):
 
     def summary(f):
         d = {"value": f["value"], "e2e_qps": f["e2e"], "ms_per_step": f["t_max_ms"] / args.steps,
-             "stages_ms": f["stages_ms"], "roofline_frac": f["roofline"]["frac"], "form": f["form"]}
+             "stages_ms": f["stages_ms"], "roofline_frac": f["roofline"]["frac"], "form": f["form"],
+             "batch": f["batch"]}
         if "learned_report" in f:
             d["learned_report"] = f["learned_report"]
         return d
