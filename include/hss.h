@@ -171,7 +171,10 @@ typedef struct hss_searcher_config {
     uint32_t maxRetries;   /* re-runs of a query whose candidates overflowed (default 4) */
     int32_t method;        /* candidate pass: 0 FP32 SIMT, 1 tensor cores TF32 over the FP32 rows,
                               2 tensor cores over a BF16 copy, 3 tensor cores over an FP8 E4M3 copy
-                              with per-vector scales (every method returns the exact FP32 results) */
+                              with per-vector scales (every method returns the exact FP32 results).
+                              The tensor-core methods need dim a multiple of 32 (TF32), 64 (BF16)
+                              or 128 (E4M3), else hss_searcher_create fails; any dim up to 4096
+                              otherwise (long vectors stream through the pass) */
     int32_t decodeInPlace; /* 0: filter over a dense bitmap of every posting, decoded once when the
                               searcher is created if it takes at most 40% of free device memory;
                               1: always decode the postings in place (no extra memory) */
