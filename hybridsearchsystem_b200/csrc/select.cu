@@ -275,15 +275,37 @@ __device__ __forceinline__ uint64_t segment_entry(const SelectSmem& S, uint32_t 
 }
 
 // Calls fn(index, valid, score) for every stored entry of a segmented list of scores src (after
-// load_segments). A warp takes 4 x 32 consecutive entries of the flattened list per round: lanes
-// read consecutive entries (coalesced within a segment), and each lane's 4 segment lookups and loads
-// are independent, so a thread keeps 4 loads in flight instead of one dependent chain per entry.
+// load_segments). Short segments (a candidate list's: a few entries each): a warp takes 4 x 32
+// consecutive entries of the flattened list per round: lanes read consecutive entries (coalesced
+// within a segment), and each lane's 4 segment lookups and loads are independent, so a thread keeps 4
+// loads in flight instead of one dependent chain per entry. Long segments: walked segment by segment.
 // Every call is made by a full warp (valid = false past the end), so fn may use warp collectives.
 template <class Fn>
 __device__ inline void for_each_segment_entry(const SelectSmem& S, uint32_t segs, uint32_t seg_cap,
                                               const float* src, Fn fn) {
     constexpr uint32_t U = 4;
     const uint32_t n = S.total, lane = threadIdx.x & 31;
+    if (n >= 32u * segs) {
+        // long segments (a doc sample's lists): warp w walks segments w, w + 32, ..., 4 x 32 entries
+        // a round, with no per-entry segment lookup
+        for (uint32_t g = threadIdx.x >> 5; g < segs; g += blockDim.x >> 5) {
+            const uint32_t cnt = S.segn[g];
+            const uint64_t base = static_cast<uint64_t>(g) * seg_cap;
+            for (uint32_t o = 0; o < cnt; o += 32u * U) {
+                bool ok[U];
+                float v[U];
+#pragma unroll
+                for (uint32_t u = 0; u < U; ++u) {
+                    const uint32_t e = o + 32u * u + lane;
+                    ok[u] = e < cnt;
+                    v[u] = ok[u] ? src[base + e] : 0.0f;
+                }
+#pragma unroll
+                for (uint32_t u = 0; u < U; ++u) fn(static_cast<uint32_t>(base + o + 32u * u + lane), ok[u], v[u]);
+            }
+        }
+        return;
+    }
     for (uint32_t b = (threadIdx.x >> 5) * 32u * U; b < n; b += blockDim.x * U) {
         uint64_t i[U];
         bool ok[U];
