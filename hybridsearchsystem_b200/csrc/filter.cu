@@ -466,7 +466,7 @@ cudaError_t launch_filter_dense_wpt(const DenseFilterLaunch& L, cudaStream_t str
 
 // ---------------------------------------------------------------------------------------------
 // The dense filter for programs of at most kWideMaxOpnd operands. A CTA takes up to
-// kWideTilesPerCta word tiles of one segment for one query; 128 threads each own 8 of a tile's 1024
+// kWideTilesPerCta consecutive word tiles (across segment boundaries) of one query; 128 threads each own 8 of a tile's 1024
 // words (2 adjacent words in each of 4 groups of 256), so the per-op decode is shared by 8 words.
 // Operands are read straight from the dense posting matrix as 16-byte read-only loads:
 // the batch's queries share rows, so most reads hit L2, and without staging buffers sized for the
@@ -478,7 +478,7 @@ constexpr int kWideT = 128;
 constexpr int kWideW = 8;
 constexpr uint32_t kWideTW = kWideT * kWideW;  // words per tile
 constexpr uint32_t kWideGS = 2 * kWideT;       // words between a thread's word pairs
-constexpr uint32_t kWideTilesPerCta = 4;       // word tiles of one segment per CTA
+constexpr uint32_t kWideTilesPerCta = 4;       // word tiles per CTA (consecutive, across segments)
 constexpr uint32_t kWideMaxOpnd = 8;          // operand rows held in shared memory
 
 // True exactly when eval_words would accept the program (same rules, no evaluation).
@@ -616,12 +616,10 @@ __global__ void __launch_bounds__(kWideT, 5) filter_dense_wide_kernel(DenseFilte
     const uint32_t t = threadIdx.x;
     const uint32_t seg_words = L.seg_words;
     const uint32_t tiles = (seg_words + kWideTW - 1) / kWideTW;  // word tiles of a segment
-    const uint32_t groups = (tiles + kWideTilesPerCta - 1) / kWideTilesPerCta;
-    const uint32_t seg = blockIdx.y / groups;
-    const uint32_t tile0 = (blockIdx.y % groups) * kWideTilesPerCta;
-    const uint32_t tile1 = min(tiles, tile0 + kWideTilesPerCta);
-    const uint64_t seg_w0 = static_cast<uint64_t>(seg) * seg_words;
-    uint64_t* out_row = L.out + static_cast<uint64_t>(q) * L.out_stride + seg_w0;
+    const uint32_t total = L.seg_num * tiles;                    // word tiles of a query's bitmap
+    const uint32_t tile0 = blockIdx.y * kWideTilesPerCta;
+    const uint32_t tile1 = min(total, tile0 + kWideTilesPerCta);
+    uint64_t* out_row = L.out + static_cast<uint64_t>(q) * L.out_stride;
 
     const uint32_t p0 = L.prog_off[q], p1 = L.prog_off[q + 1];
     const uint32_t o0 = L.opnd_off[q], o1 = L.opnd_off[q + 1];
@@ -634,7 +632,7 @@ __global__ void __launch_bounds__(kWideT, 5) filter_dense_wide_kernel(DenseFilte
         if (t < nop) {
             uint32_t r = L.opnd_row[o0 + t];
             r = r < L.rows ? r : L.rows - 1;  // a row past the table reads the all-zero row
-            s_base[t] = L.dense + (static_cast<uint64_t>(r) * L.seg_num + seg) * seg_words;
+            s_base[t] = L.dense + static_cast<uint64_t>(r) * L.seg_num * seg_words;  // the row's first segment
         }
         __syncthreads();
         if (t == 0) s_ok = check_program(s_prog, plen, nop);
@@ -644,15 +642,18 @@ __global__ void __launch_bounds__(kWideT, 5) filter_dense_wide_kernel(DenseFilte
     __syncthreads();
     const bool ok = s_ok != 0;
     uint32_t c = 0;
-    // the program's setup (load, check) is shared by the CTA's word tiles of this segment
-    for (uint32_t tile = tile0; tile < tile1; ++tile) {
-        const uint32_t w0 = tile * kWideTW;
+    // the program's setup (load, check) is shared by the CTA's word tiles, which may span segments
+    for (uint32_t gt = tile0; gt < tile1; ++gt) {
+        const uint32_t seg = gt / tiles;
+        const uint32_t w0 = (gt % tiles) * kWideTW;
         const uint32_t nw = min(kWideTW, seg_words - w0);  // even
-        // word offsets (from the segment's start) of this thread's pairs; a pair past a partial tile
-        // reads the tile's first pair instead (in bounds; not stored)
+        const uint32_t seg_w0 = seg * seg_words;           // < 2^32: a row's words
+        // word offsets (from the row's start) of this thread's pairs; a pair past a partial tile reads
+        // the tile's first pair instead (in bounds; not stored)
         uint32_t off[kWideW / 2];
 #pragma unroll
-        for (int g = 0; g < kWideW / 2; ++g) off[g] = w0 + (kWideGS * g + 2u * t < nw ? kWideGS * g + 2u * t : 0u);
+        for (int g = 0; g < kWideW / 2; ++g)
+            off[g] = seg_w0 + w0 + (kWideGS * g + 2u * t < nw ? kWideGS * g + 2u * t : 0u);
         uint64_t res[kWideW];
         if (empty || !ok) {
 #pragma unroll
@@ -660,13 +661,19 @@ __global__ void __launch_bounds__(kWideT, 5) filter_dense_wide_kernel(DenseFilte
         } else {
             eval_wide(s_prog, plen, s_base, off, res);
         }
+        // only a tile reaching past the last doc needs the per-word tail mask (uniform per CTA)
+        const bool tail = (static_cast<uint64_t>(seg_w0) + w0 + nw) * 64 > L.doc_num;
 #pragma unroll
         for (int g = 0; g < kWideW / 2; ++g) {
             const uint32_t w = kWideGS * g + 2u * t;
             if (w >= nw) continue;
-            const uint64_t a = res[2 * g] & tail_mask(seg_w0 + w0 + w, L.doc_num);
-            const uint64_t b = res[2 * g + 1] & tail_mask(seg_w0 + w0 + w + 1, L.doc_num);
-            *reinterpret_cast<ulonglong2*>(out_row + w0 + w) = make_ulonglong2(a, b);
+            const uint64_t gw = static_cast<uint64_t>(seg_w0) + w0 + w;
+            uint64_t a = res[2 * g], b = res[2 * g + 1];
+            if (tail) {
+                a &= tail_mask(gw, L.doc_num);
+                b &= tail_mask(gw + 1, L.doc_num);
+            }
+            *reinterpret_cast<ulonglong2*>(out_row + gw) = make_ulonglong2(a, b);
             c += __popcll(a) + __popcll(b);
         }
     }
@@ -777,8 +784,9 @@ cudaError_t launch_filter_dense(const DenseFilterLaunch& L, cudaStream_t stream)
         return cudaErrorInvalidValue;
     if (L.max_opnd <= kWideMaxOpnd && (L.out_stride & 1u) == 0 && (reinterpret_cast<uintptr_t>(L.out) & 15u) == 0) {
         const uint32_t tiles = (L.seg_words + kWideTW - 1) / kWideTW;
-        const uint64_t gy = static_cast<uint64_t>(L.seg_num) * ((tiles + kWideTilesPerCta - 1) / kWideTilesPerCta);
-        if (gy <= 65535u) {
+        const uint64_t total = static_cast<uint64_t>(L.seg_num) * tiles;
+        const uint64_t gy = (total + kWideTilesPerCta - 1) / kWideTilesPerCta;
+        if (gy <= 65535u && static_cast<uint64_t>(L.seg_num) * L.seg_words < (1ull << 32)) {
             filter_dense_wide_kernel<<<dim3(L.nq, static_cast<uint32_t>(gy)), kWideT, 0, stream>>>(L);
             return cudaGetLastError();
         }
