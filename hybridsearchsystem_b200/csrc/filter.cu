@@ -556,6 +556,8 @@ __device__ __forceinline__ void eval_wide(const uint32_t* s_prog, uint32_t plen,
                 const uint32_t pn = s_prog[pc + 2 + p];
                 uint64_t u[kWideW];
                 wide_load(s_base, next, off, u);
+                // two operands' loads in flight at a time (the pass waits on L2 latency)
+#pragma unroll 2
                 for (uint32_t j = 1; j < pn; ++j) {
                     wide_load(s_base, next + j, off, o);
 #pragma unroll
@@ -583,6 +585,7 @@ __device__ __forceinline__ void eval_wide(const uint32_t* s_prog, uint32_t plen,
                 const bool is_and = op == kOpAnd;
 #pragma unroll
                 for (int k = 0; k < kWideW; ++k) acc[k] = is_and ? ~0ull : 0ull;
+#pragma unroll 2  // two operands' loads in flight, as above
                 for (uint32_t j = 0; j < pn; ++j) {
                     wide_load(s_base, next + j, off, o);
 #pragma unroll
