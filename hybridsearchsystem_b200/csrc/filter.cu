@@ -466,7 +466,7 @@ cudaError_t launch_filter_dense_wpt(const DenseFilterLaunch& L, cudaStream_t str
 
 // ---------------------------------------------------------------------------------------------
 // The dense filter for programs of at most kWideMaxOpnd operands. A CTA takes up to
-// kWideTilesPerCta consecutive word tiles (across segment boundaries) of one query; 128 threads each own 8 of a tile's 1024
+// tiles_per_cta (1, 2 or 4) consecutive word tiles (across segment boundaries) of one query; 128 threads each own 8 of a tile's 1024
 // words (2 adjacent words in each of 4 groups of 256), so the per-op decode is shared by 8 words.
 // Operands are read straight from the dense posting matrix as 16-byte read-only loads:
 // the batch's queries share rows, so most reads hit L2, and without staging buffers sized for the
@@ -478,7 +478,8 @@ constexpr int kWideT = 128;
 constexpr int kWideW = 8;
 constexpr uint32_t kWideTW = kWideT * kWideW;  // words per tile
 constexpr uint32_t kWideGS = 2 * kWideT;       // words between a thread's word pairs
-constexpr uint32_t kWideTilesPerCta = 4;       // word tiles per CTA (consecutive, across segments)
+constexpr uint32_t kWideMaxTilesPerCta = 4;    // word tiles per CTA at most (consecutive, across segments)
+constexpr uint32_t kWideCtasPerSm = 5;         // resident CTAs per SM (__launch_bounds__ below)
 constexpr uint32_t kWideMaxOpnd = 8;          // operand rows held in shared memory
 
 // True exactly when eval_words would accept the program (same rules, no evaluation).
@@ -610,7 +611,8 @@ __device__ __forceinline__ void eval_wide(const uint32_t* s_prog, uint32_t plen,
     for (int k = 0; k < kWideW; ++k) res[k] = top[k];
 }
 
-__global__ void __launch_bounds__(kWideT, 5) filter_dense_wide_kernel(DenseFilterLaunch L) {
+__global__ void __launch_bounds__(kWideT, kWideCtasPerSm) filter_dense_wide_kernel(DenseFilterLaunch L,
+                                                                                    uint32_t tiles_per_cta) {
     __shared__ uint32_t s_prog[kMaxProgram];
     __shared__ const uint64_t* s_base[kWideMaxOpnd];
     __shared__ int s_ok;
@@ -620,8 +622,8 @@ __global__ void __launch_bounds__(kWideT, 5) filter_dense_wide_kernel(DenseFilte
     const uint32_t seg_words = L.seg_words;
     const uint32_t tiles = (seg_words + kWideTW - 1) / kWideTW;  // word tiles of a segment
     const uint32_t total = L.seg_num * tiles;                    // word tiles of a query's bitmap
-    const uint32_t tile0 = blockIdx.y * kWideTilesPerCta;
-    const uint32_t tile1 = min(total, tile0 + kWideTilesPerCta);
+    const uint32_t tile0 = blockIdx.y * tiles_per_cta;
+    const uint32_t tile1 = min(total, tile0 + tiles_per_cta);
     uint64_t* out_row = L.out + static_cast<uint64_t>(q) * L.out_stride;
 
     const uint32_t p0 = L.prog_off[q], p1 = L.prog_off[q + 1];
@@ -788,9 +790,17 @@ cudaError_t launch_filter_dense(const DenseFilterLaunch& L, cudaStream_t stream)
     if (L.max_opnd <= kWideMaxOpnd && (L.out_stride & 1u) == 0 && (reinterpret_cast<uintptr_t>(L.out) & 15u) == 0) {
         const uint32_t tiles = (L.seg_words + kWideTW - 1) / kWideTW;
         const uint64_t total = static_cast<uint64_t>(L.seg_num) * tiles;
-        const uint64_t gy = (total + kWideTilesPerCta - 1) / kWideTilesPerCta;
+        // More tiles per CTA share its program setup over more words, fewer leave more CTAs: take the
+        // most (4, 2, 1) that still leaves 4 waves of resident CTAs (small batches and tables take 1),
+        // but no fewer than the grid's height limit needs.
+        const uint64_t want = 4ull * kWideCtasPerSm * (L.sm_count ? L.sm_count : 148u);
+        uint32_t tpc = kWideMaxTilesPerCta;
+        while (tpc > 1 && static_cast<uint64_t>(L.nq) * ((total + tpc - 1) / tpc) < want &&
+               (total + tpc / 2 - 1) / (tpc / 2) <= 65535u)
+            tpc >>= 1;
+        const uint64_t gy = (total + tpc - 1) / tpc;
         if (gy <= 65535u && static_cast<uint64_t>(L.seg_num) * L.seg_words < (1ull << 32)) {
-            filter_dense_wide_kernel<<<dim3(L.nq, static_cast<uint32_t>(gy)), kWideT, 0, stream>>>(L);
+            filter_dense_wide_kernel<<<dim3(L.nq, static_cast<uint32_t>(gy)), kWideT, 0, stream>>>(L, tpc);
             return cudaGetLastError();
         }
     }

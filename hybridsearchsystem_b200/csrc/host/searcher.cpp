@@ -247,6 +247,7 @@ int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exp
         F.seg_num = T.GetSegmentNum();
         F.doc_num = T.GetDocNum();
         F.max_opnd = maxOpnd;
+        F.sm_count = m_numSms;
         ck(launch_filter_dense(F, stream));
         return ce == cudaSuccess ? 0 : static_cast<int>(ce);
     }

@@ -57,6 +57,7 @@ struct DenseFilterLaunch {
     uint32_t seg_num;
     uint64_t doc_num;
     uint32_t max_opnd;         // largest operand count of any query in the batch (<= 64)
+    uint32_t sm_count;         // SMs of the device (sizes the grid; 0: 148)
 };
 cudaError_t launch_filter_dense(const DenseFilterLaunch& L, cudaStream_t stream);
 

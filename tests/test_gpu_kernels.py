@@ -87,6 +87,39 @@ def test_batched_filter_wide_segments_six_operands(torch_cuda, in_place):
         assert int(cnt.cpu().numpy()[i]) == want.sum(), e
 
 
+# The dense filter's CTAs take 4, 2 or 1 consecutive word tiles (1024 words each) of a query's bitmap,
+# across segment boundaries: the most that still leaves 4 waves of 5 CTAs per SM. On 148 SMs:
+# - 4096-doc segments (one 64-word tile each), 47 of them: 256 queries take 4, 128 take 2, 8 take 1;
+# - 135168-doc segments (tiles of 1024, 1024 and 64 words), 16 of them, 256 queries: 4 tiles per CTA,
+#   so CTAs start inside segments, and the last segment's last tiles lie past the last doc.
+@pytest.mark.parametrize("seg_docs,n_docs,nq,check", [(4096, 190000, 256, 256), (4096, 190000, 128, 128),
+                                                      (4096, 190000, 8, 8), (135168, 2030000, 256, 48)],
+                         ids=["4_tiles", "2_tiles", "1_tile", "4_tiles_mid_segment"])
+def test_batched_filter_tiles_across_segments(torch_cuda, seg_docs, n_docs, nq, check):
+    torch = torch_cuda
+    mix = data.Mixture(32, 64, (1e-3, 0.5), n_clusters=16, seed=91)
+    vec, bits, _ = mix.corpus(n_docs, seed=92)
+    table = hss.DataTable.build(vec, bits, 64, device=0, doc_num_per_segment=seg_docs)
+    info = table.info
+    exprs = data.make_filters(mix, nq, n_tags=(1, 6), seed=93)
+    s = hss.FullRecallSearcher(table, max_batch=nq, candidate_cap=4096)
+    f = s.compile_filters(exprs)
+    words = info["segment_num"] * info["doc_num_per_segment"] // 64
+    out = torch.zeros((nq, words), dtype=torch.int64, device="cuda")
+    cnt = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    assert s.filter_device(f, nq, out.data_ptr(), words, cnt.data_ptr()) == _lib.HSS_OK
+    got = out.cpu().numpy().view(np.uint64)
+    counts = cnt.cpu().numpy()
+    # every row, or rows spread over the batch (the oracle takes ~65 ms a filter at 2M docs)
+    for i in np.linspace(0, nq - 1, check).astype(int):
+        e = exprs[i]
+        want = _bits_of(oracle.filter_bits(e, bits), n_docs)
+        row = _bits_of(got[i], words * 64)
+        assert (row[:n_docs] == want).all(), (i, e)
+        assert not row[n_docs:].any(), (i, e)
+        assert counts[i] == want.sum(), (i, e)
+
+
 def test_filter_operator_both_table_conventions(torch_cuda):
     torch = torch_cuda
     mix, vec, bits, table = _table(torch, "bitmap", seed=5)
