@@ -465,9 +465,10 @@ cudaError_t launch_filter_dense_wpt(const DenseFilterLaunch& L, cudaStream_t str
 }
 
 // ---------------------------------------------------------------------------------------------
-// The dense filter for programs of at most kWideMaxOpnd operands. A CTA takes up to
-// tiles_per_cta (1, 2 or 4) consecutive word tiles (across segment boundaries) of one query; 128 threads each own 8 of a tile's 1024
-// words (2 adjacent words in each of 4 groups of 256), so the per-op decode is shared by 8 words.
+// The dense filter for programs of at most kWideMaxOpnd operands. A CTA takes tiles_per_cta (1, 2 or
+// 4) consecutive word tiles of one query's bitmap, across segment boundaries; 128 threads each own 8
+// of a tile's 1024 words (2 adjacent words in each of 4 groups of 256), so the per-op decode is
+// shared by 8 words.
 // Operands are read straight from the dense posting matrix as 16-byte read-only loads:
 // the batch's queries share rows, so most reads hit L2, and without staging buffers sized for the
 // batch's largest program the SM holds as many CTAs as registers allow. One thread checks the program
