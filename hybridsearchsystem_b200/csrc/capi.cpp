@@ -1,4 +1,6 @@
 // capi.cpp -- extern "C" entry points of libhss.so (declared in include/hss.h).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -131,11 +133,43 @@ int hss_aggregator_launch(const uint8_t* filterResult, const float* docScores, c
 }
 
 namespace {
-// Address of the aggregator's module-scope scratch on each device, looked up once per device (with
-// that device current) on the first allocation-free call made there.
+static_assert(HSS_AGGREGATOR_NOALLOC_MAX_DOCS == hss::kAggStaticMaxDocs,
+              "the public allocation-free aggregator limit must equal the size of its scratch array");
+
+// Address of the aggregator's module-scope scratch on each device, looked up (with that device
+// current) on the first allocation-free call made there, and again whenever the device's CUDA context
+// has changed since (cudaDeviceReset destroys the primary context; the module, and with it the array,
+// is loaded anew in the next one, possibly at another address). The context is identified by its
+// process-unique id (cuCtxGetId), not by its handle, which a new context may reuse.
 constexpr int kMaxDevices = 64;
 std::mutex g_staticScratchMu;
-uint32_t* g_staticScratch[kMaxDevices] = {};
+struct ScratchEntry {
+    unsigned long long ctxId;
+    uint32_t* ptr;
+};
+ScratchEntry g_staticScratch[kMaxDevices] = {};
+
+// Id of the calling thread's current context; false when no context is current or the driver
+// entry points are unavailable.
+bool CurrentContextId(unsigned long long* id) {
+    static PFN_cuCtxGetCurrent_v4000 getCurrent = nullptr;
+    static PFN_cuCtxGetId_v12000 getId = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            getCurrent = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            getId = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+    });
+    CUcontext ctx = nullptr;
+    if (!getCurrent || !getId || getCurrent(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return getId(ctx, id) == CUDA_SUCCESS;
+}
 
 int StaticAggregateScratch(uint32_t** out) {
     int dev = 0;
@@ -143,14 +177,24 @@ int StaticAggregateScratch(uint32_t** out) {
     if (e != cudaSuccess) return FromCuda(e);
     if (dev < 0 || dev >= kMaxDevices) return SetError(HSS_ERR_LIMIT, "hss_aggregator_launch_noalloc: device index");
     std::lock_guard<std::mutex> lock(g_staticScratchMu);
-    if (!g_staticScratch[dev]) {
+    ScratchEntry& ent = g_staticScratch[dev];
+    unsigned long long ctx = 0;
+    const bool known = CurrentContextId(&ctx);
+    if (!ent.ptr || !known || ent.ctxId != ctx) {
+        // the lookup also makes the device's primary context current if it was not yet
         uint32_t* p = nullptr;
         e = hss::aggregate_static_scratch(&p);
         if (e != cudaSuccess) return FromCuda(e);
         if (!p) return SetError(HSS_ERR_CUDA, "hss_aggregator_launch_noalloc: scratch symbol has no address");
-        g_staticScratch[dev] = p;
+        if (!CurrentContextId(&ctx)) {
+            // without a context id the address cannot be cached safely: use it for this call only
+            *out = p;
+            ent = ScratchEntry{};
+            return HSS_OK;
+        }
+        ent = ScratchEntry{ctx, p};
     }
-    *out = g_staticScratch[dev];
+    *out = ent.ptr;
     return HSS_OK;
 }
 }  // namespace

@@ -608,7 +608,6 @@ __device__ __forceinline__ void eval_wide(const uint32_t* s_prog, uint32_t plen,
         has_top = true;
     }
 #pragma unroll
-#pragma unroll
     for (int k = 0; k < kWideW; ++k) res[k] = top[k];
 }
 

@@ -422,7 +422,7 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     auto stage = [&](const uint32_t* dList, uint32_t rows) {
         if (!tc) {
             const double rel = SimtRelBound(dim);
-            ck(launch_query_eps(dQueries, nq, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
+            ck(launch_query_eps(dQueries, dList, rows, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
             return;
         }
         StageQueriesLaunch Q{};
@@ -718,9 +718,10 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         // thresholds stay valid (every bound derived so far was at least the SIMT one).
         const bool simt = tc && retries >= 2;
         if (simt) {
-            // the plain path for these queries: SIMT bounds, a SIMT doc sample for a fresh threshold
+            // the plain path for these queries: SIMT bounds (for the re-run queries only, so every other
+            // query keeps the bound its own pass used), a SIMT doc sample for a fresh threshold
             const double rel = SimtRelBound(dim);
-            ck(launch_query_eps(dQueries, nq, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
+            ck(launch_query_eps(dQueries, dQlist, nre, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
             (void)sample(dQlist, nre, true);
             launches += 3;
         } else if (tc) {

@@ -225,8 +225,9 @@ cudaError_t launch_exact_score(const float* qry, const float* docs, float* out, 
 cudaError_t launch_cand_simt(const CandLaunch& L, int num_sms, cudaStream_t stream);
 cudaError_t launch_sample_threshold(const SampleThresholdLaunch& L, cudaStream_t stream);
 cudaError_t launch_select_topk(const SelectLaunch& L, cudaStream_t stream);
-cudaError_t launch_query_eps(const float* qry, uint32_t nq, uint32_t dim, float max_norm, double c_main,
-                             double c_sample, float* eps_main, float* eps_sample, cudaStream_t stream);
+// Error bounds of the SIMT pass for queries qlist[0..nq) (all of 0..nq-1 when qlist is null).
+cudaError_t launch_query_eps(const float* qry, const uint32_t* qlist, uint32_t nq, uint32_t dim, float max_norm,
+                             double c_main, double c_sample, float* eps_main, float* eps_sample, cudaStream_t stream);
 size_t aggregate_workspace_bytes(uint32_t n);
 // Allocation-free aggregator scratch: kAggStaticBlocks block counts in a module-scope device array;
 // aggregate_static_scratch returns its address on the current device (the runtime may load the

@@ -336,6 +336,17 @@ __device__ __forceinline__ void emit_lane(uint32_t m, const uint32_t (&v)[32], f
     }
 }
 
+// Threshold on a tile's raw E4M3 accumulators: every doc of the tile whose dequantised score
+// acc * qs * ds (ds in [mm.x, mm.y], both positive) reaches theta has acc >= the returned value.
+// The two divisions round to nearest; the result is then lowered by a relative 2^-20 (plus a tiny
+// absolute step) whatever its sign, so it stays below the exact quotient. NaN (no query) gives -inf.
+__device__ __forceinline__ float e4m3_tile_threshold(float theta, float qs, float2 mm) {
+    const float tq = theta / qs;
+    float t = tq > 0.0f ? tq / mm.y : tq / mm.x;
+    if (!(t == t)) return -INFINITY;
+    return __fsub_rd(t, __fmaf_ru(fabsf(t), 0x1p-20f, 1e-30f));
+}
+
 // One 32-doc chunk of a thread's E4M3 scores (its query, raw accumulators v): the docs whose filter
 // bit (m) is set and whose dequantised score clears the threshold go to the thread's list segment.
 // Warp-collective: the warp leaves at once when no lane's chunk clears its tile threshold t, and the
@@ -511,14 +522,7 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
             tile_next = walk.tile();
             if (valid && it + gridDim.x < ntiles) fw_next = brow[tile_next * 2 + colh];
             // threshold on the raw accumulator: acc * qs * ds >= theta
-            float t = theta;
-            if (F == kTcE4M3) {
-                const float2 mm = L.tile_scale[tile];  // (min, max) doc scale of the tile
-                const float tq = theta / qs;
-                t = tq > 0.0f ? tq / mm.y : tq / mm.x;
-                t = t == t ? t : -INFINITY;
-                t = __fmul_rd(t, 1.0f - 1e-6f) - 1e-30f;  // stay on the safe side of the rounding
-            }
+            const float t = F == kTcE4M3 ? e4m3_tile_threshold(theta, qs, L.tile_scale[tile]) : theta;
             const uint32_t m[2] = {static_cast<uint32_t>(fw), static_cast<uint32_t>(fw >> 32)};
             // 32-doc chunks that no query of the warp lets through are not read from TMEM at all
             bool live[2];
@@ -783,11 +787,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
             if (F == kTcE4M3) {
                 uint64_t ts = tile * 2 + g / 2;  // 128-doc tile holding this thread's docs
                 ts = ts < L.tiles128 ? ts : L.tiles128 - 1;
-                const float2 mm = L.tile_scale[ts];
-                const float tq = theta / qs;
-                t = tq > 0.0f ? tq / mm.y : tq / mm.x;
-                t = t == t ? t : -INFINITY;
-                t = __fmul_rd(t, 1.0f - 1e-6f) - 1e-30f;
+                t = e4m3_tile_threshold(theta, qs, L.tile_scale[ts]);
             }
             const uint32_t m[2] = {static_cast<uint32_t>(fw), static_cast<uint32_t>(fw >> 32)};
             bool live[2];

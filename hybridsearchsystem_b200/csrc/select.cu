@@ -733,12 +733,14 @@ __global__ void __launch_bounds__(kST) topk_op_kernel(const float* __restrict__ 
 
 // Per-query error bounds: eps = c * ||q||_2 * max_doc ||v||_2 (Cauchy-Schwarz on sum |q_i v_i|),
 // computed in double and rounded up to float.
-__global__ void query_eps_kernel(const float* __restrict__ qry, uint32_t nq, uint32_t dim, float max_norm,
-                                 double c_main, double c_sample, float* __restrict__ eps_main,
-                                 float* __restrict__ eps_sample) {
-    const uint32_t q = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+// Bounds of queries qlist[0..nq) (or 0..nq-1 when qlist is null), written at the query's own index.
+__global__ void query_eps_kernel(const float* __restrict__ qry, const uint32_t* __restrict__ qlist, uint32_t nq,
+                                 uint32_t dim, float max_norm, double c_main, double c_sample,
+                                 float* __restrict__ eps_main, float* __restrict__ eps_sample) {
+    const uint32_t r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     const uint32_t lane = threadIdx.x & 31;
-    if (q >= nq) return;
+    if (r >= nq) return;
+    const uint32_t q = qlist ? qlist[r] : r;
     double s = 0.0;
     for (uint32_t d = lane; d < dim; d += 32) {
         const double x = qry[static_cast<uint64_t>(q) * dim + d];
@@ -787,10 +789,11 @@ cudaError_t launch_select_topk(const SelectLaunch& L, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_query_eps(const float* qry, uint32_t nq, uint32_t dim, float max_norm, double c_main,
-                             double c_sample, float* eps_main, float* eps_sample, cudaStream_t stream) {
+cudaError_t launch_query_eps(const float* qry, const uint32_t* qlist, uint32_t nq, uint32_t dim, float max_norm,
+                             double c_main, double c_sample, float* eps_main, float* eps_sample, cudaStream_t stream) {
     if (nq == 0) return cudaSuccess;
-    query_eps_kernel<<<(nq + 7) / 8, 256, 0, stream>>>(qry, nq, dim, max_norm, c_main, c_sample, eps_main, eps_sample);
+    query_eps_kernel<<<(nq + 7) / 8, 256, 0, stream>>>(qry, qlist, nq, dim, max_norm, c_main, c_sample, eps_main,
+                                                       eps_sample);
     return cudaGetLastError();
 }
 

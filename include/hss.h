@@ -113,7 +113,9 @@ int hss_aggregator_launch(const uint8_t* filterResult, const float* docScores, c
  * Its scratch is a 64 KB array compiled into the library, one per device, so docNumber <=
  * HSS_AGGREGATOR_NOALLOC_MAX_DOCS (else HSS_ERR_LIMIT, nothing launched). It calls no allocator.
  * The first call on each device looks the array's address up (cudaGetSymbolAddress, with that
- * device current); make that first call before any stream capture. Every call on a device shares
+ * device current); make that first call before any stream capture. The address is cached per device
+ * together with the id of the CUDA context it belongs to, so the first call after the device's
+ * context was replaced (cudaDeviceReset) looks it up again. Every call on a device shares
  * the one array: calls that can overlap on the GPU (different streams without ordering between
  * them) race and must not be made; calls ordered on one stream are safe, since each call rewrites
  * all the scratch it reads. */
