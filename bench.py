@@ -11,8 +11,20 @@ max over ranks); `e2e` is the same through the public C-ABI with the batch's que
 host memory and its results copied back inside the timed region. Under torchrun every rank holds a
 full replica and serves its own batches (weak scaling, no data-path collective).
 
+Besides the headline form, one run measures (keys of the JSON line):
+  forms              the chosen form with the learned threshold, the plain FP32 forms (TF32 tensor
+                     cores, SIMT FFMA), the E4M3 form, batches of 64, and per-query K drawn from
+                     {10, 100, 1000};
+  parity_full_scale  every form's results for 256 queries at K = 10, 100 and 1000 against the
+                     reference's own CpuTopKBatch (id sets, bit-exact FP32 scores, order);
+  configs.cfg1       the one-segment configuration (131,072 docs, 64 tags, batches of 32) with its
+                     parity against the reference;
+  configs.cfg3       the precision form at 20M x 768 (FP32 + BF16 + E4M3 copies resident), recall and
+                     score error against an FP64 dot product;
+  serving            p50/p99 latency of the serving loop at open-loop Poisson rates.
+
 --impl reference times the reference's own CPU ground-truth scan (CpuTopKBatch, compiled from the
-reference sources into oracle/_ref) on this host's cores for the same workload.
+reference sources into oracle/_ref) on this host's cores, on the same batch of queries per step.
 """
 import argparse
 import json
@@ -20,6 +32,7 @@ import os
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -33,9 +46,10 @@ FORMS = {"simt": "plain FP32 (SIMT FFMA candidate pass + exact FP32 rescoring)",
          "tf32": "plain FP32 (TF32 tensor-core candidate pass over the FP32 rows + exact FP32 rescoring)",
          "bf16": "BF16 copy (tensor-core candidate pass + exact FP32 rescoring)",
          "e4m3": "FP8 E4M3 copy with per-vector scales (tensor-core candidate pass + exact FP32 rescoring)"}
+PARITY_KS = (10, 100, 1000)
 
 
-def parse_args():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
@@ -45,7 +59,9 @@ def parse_args():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--topk", type=int, default=100)
     ap.add_argument("--queries", type=int, default=2048, help="query pool the steps cycle through")
-    ap.add_argument("--cpu-queries", type=int, default=0, help="CPU baseline sample size (0: 2 per thread)")
+    ap.add_argument("--cpu-queries", type=int, default=0,
+                    help="queries per reference step (0: one batch, fewer only if the run would exceed ~4 min)")
+    ap.add_argument("--parity-queries", type=int, default=256, help="full-scale parity sample per K")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cand-cap", type=int, default=1 << 18, help="per-query candidate capacity")
     ap.add_argument("--sample-docs", type=int, default=32768, help="docs of the threshold sample per batch")
@@ -58,14 +74,21 @@ def parse_args():
                     help="skip measuring the chosen format with the learned threshold beside it")
     ap.add_argument("--no-plain", dest="plain", action="store_false",
                     help="skip measuring the plain FP32 (TF32) form beside the chosen one")
+    ap.add_argument("--no-e4m3", dest="e4m3", action="store_false", help="skip measuring the E4M3 form")
     ap.add_argument("--no-serve", dest="serve", action="store_false", help="skip the serving-loop latency sweep")
     ap.add_argument("--no-batch64", dest="batch64", action="store_false",
                     help="skip measuring the chosen (and plain) form at batches of 64 queries")
+    ap.add_argument("--no-kmix", dest="kmix", action="store_false",
+                    help="skip measuring batches whose per-query K is drawn from {10, 100, 1000}")
+    ap.add_argument("--no-cfg1", dest="cfg1", action="store_false", help="skip the one-segment configuration")
+    ap.add_argument("--no-precision", dest="precision", action="store_false",
+                    help="skip the 20M x 768 precision-form configuration")
+    ap.add_argument("--precision-docs", type=int, default=20_000_000)
     ap.add_argument("--serve-requests", type=int, default=40000)
     ap.add_argument("--serve-rates", default="1000,10000,50000,100000,150000,200000",
                     help="offered Poisson rates (QPS) of the serving sweep")
     ap.add_argument("--serve-wait-us", type=int, default=300)
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def dist_env():
@@ -101,78 +124,130 @@ def workload(args, device):
     return mix, vec, bits, queries, exprs
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 50 ms while running. Entering waits until
-    the first sample has been written (nvidia-smi takes a while to start); that sample predates the
-    timed region and is dropped from the summary."""
+    """SM clocks and clock-event reasons sampled in-process through NVML every 0.5 ms while running
+    (the timed regions last tens of ms); nvidia-smi every 50 ms when NVML is unavailable. Only
+    reads the GPU's state."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_id):
-        self.gpu_id = gpu_id
-        self.proc = None
-        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    def __init__(self, gpu_uuid):
+        self.uuid = gpu_uuid
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.source = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._proc = None
+        self._out = None
+
+    def _nvml_loop(self, nv, h):
+        names = {nv.nvmlClocksEventReasonHwSlowdown: "hw_slowdown",
+                 nv.nvmlClocksEventReasonHwThermalSlowdown: "hw_thermal_slowdown",
+                 nv.nvmlClocksEventReasonSwThermalSlowdown: "sw_thermal_slowdown",
+                 nv.nvmlClocksEventReasonSwPowerCap: "sw_power_cap"}
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for bit, n in names.items():
+                    if r & bit:
+                        self.reasons.add(n)
+            except Exception:
+                break
+            time.sleep(0.0005)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "50", "-i", self.gpu_id], stdout=self.out,
-                                         stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByUUID(self.uuid)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self._thread.start()
+            self.source = "nvml 0.5 ms"
+            while not self.samples and self._thread.is_alive():
+                time.sleep(0.0005)
+            self.samples.clear()  # the first sample predates the timed region
+            self.reasons.clear()
+            return self
+        except Exception:
+            self._thread = None
+        self._out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                           "-lms", "50", "-i", self.uuid], stdout=self._out,
+                                          stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi 50 ms"
         except OSError:
-            self.proc = None
+            self._proc = None
         t0 = time.time()
-        while self.proc and time.time() - t0 < 10 and os.path.getsize(self.out.name) == 0:
+        while self._proc and time.time() - t0 < 10 and os.path.getsize(self._out.name) == 0:
             time.sleep(0.01)
         return self
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=2)
+        if self._proc:
+            self._proc.terminate()
             try:
-                self.proc.wait(timeout=5)
+                self._proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
-                self.proc.kill()
+                self._proc.kill()
 
     def summary(self):
-        self.out.flush()
-        self.out.seek(0)
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.out.read().splitlines()[1:]:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        os.unlink(self.out.name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self._out is not None:
+            self._out.flush()
+            self._out.seek(0)
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for line in self._out.read().splitlines()[1:]:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    self.samples.append(float(parts[1]))
+                    self.max_mhz = max(self.max_mhz or 0.0, float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        self.reasons.add(n)
+            os.unlink(self._out.name)
+            self._out = None
+        return {"sm_mhz": float(np.median(self.samples)) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": self.source}
 
 
-def cpu_baseline(vec, bits, queries, exprs, topk, nq_sample):
+def reference_topk(vec, bits, queries, exprs, topk, threads=None):
     """The reference's CpuTopKBatch (oracle/_ref, compiled from its sources) on all host threads, or the
-    oracle's restatement of it when the reference build is absent. Returns (record, ids, counts)."""
+    oracle's restatement of it when the reference build is absent. Returns (ids [nq][topk] as sets in
+    id order, counts, seconds, kind)."""
     import ctypes
 
     import oracle
-    threads = os.cpu_count() or 1
-    nq = nq_sample or 2 * threads
-    nq = min(nq, len(queries))
-    q = np.ascontiguousarray(queries[:nq], np.float32)
-    ex = exprs[:nq]
+    threads = threads or os.cpu_count() or 1
+    nq = len(queries)
+    q = np.ascontiguousarray(queries, np.float32)
     topks = np.full(nq, topk, np.int32)
     t0 = time.perf_counter()
     if oracle.ref_available():
         r = oracle.ref()
-        arr = (ctypes.c_char_p * nq)(*[e.encode() for e in ex])
+        arr = (ctypes.c_char_p * nq)(*[e.encode() for e in exprs])
         ids = np.full((nq, topk), -1, np.int64)
         counts = np.zeros(nq, np.int32)
         rc = r.ref_cpu_topk_batch(q.ctypes.data, nq, q.shape[1], arr, topks.ctypes.data, vec.ctypes.data,
@@ -181,13 +256,53 @@ def cpu_baseline(vec, bits, queries, exprs, topk, nq_sample):
         assert rc == 0
         kind = "reference"
     else:
-        _, ids, counts = oracle.topk(q, ex, topks, vec, bits, threads=threads, out_stride=topk)
+        _, ids, counts = oracle.topk(q, list(exprs), topks, vec, bits, threads=threads, out_stride=topk)
         kind = "port"
-    dt = time.perf_counter() - t0
-    rec = {"value": nq / dt, "unit": "QPS", "cores": threads, "kind": kind,
-           "sample": f"{nq} queries (filtered top-{topk}) over the full {vec.shape[0]}-doc corpus, "
-                     f"CpuTopKBatch in {threads} query slices, fp32 mode"}
-    return rec, ids, counts
+    return ids, counts, time.perf_counter() - t0, kind
+
+
+def cpu_record(nq, dt, kind, threads, topk, docs, batch_note=""):
+    return {"value": nq / dt, "unit": "QPS", "cores": threads, "kind": kind, "cpu_model": cpu_model(),
+            "sample": f"{nq} queries{batch_note} (filtered top-{topk}) over the full {docs}-doc corpus, "
+                      f"CpuTopKBatch in {threads} query slices, fp32 mode"}
+
+
+def ordered_truth(vec, queries, ids, counts):
+    """The ground truth's ordered results from its id sets: each id's FP32 score in the ground truth's
+    own arithmetic (sum over d ascending, every product and sum rounded to FP32, no contraction),
+    sorted by (score desc, id asc). Returns a list of (scores, ids) per query."""
+    out = []
+    for i in range(len(counts)):
+        c = int(counts[i])
+        idv = np.sort(ids[i][:c].astype(np.int64))
+        acc = np.zeros(c, np.float32)
+        qv, dv = queries[i].astype(np.float32), vec[idv].astype(np.float32)
+        for d in range(qv.shape[0]):
+            acc = (acc + (qv[d] * dv[:, d]).astype(np.float32)).astype(np.float32)
+        order = np.lexsort((idv, -acc.astype(np.float64)))
+        out.append((acc[order], idv[order]))
+    return out
+
+
+def check_against(truth, scores, ids, counts):
+    """Compares a form's results with the ordered ground truth: (id sets equal, scores bit-exact,
+    order identical, queries that differ)."""
+    sets = bits = order = True
+    bad = 0
+    for i, (ts, ti) in enumerate(truth):
+        c = len(ti)
+        if int(counts[i]) != c or set(ids[i][:c].tolist()) != set(ti.tolist()):
+            sets = False
+            bad += 1
+            continue
+        if not (ids[i][:c] == ti).all():
+            order = False
+            bad += 1
+            continue
+        if not (scores[i][:c].view(np.uint32) == ts.view(np.uint32)).all():
+            bits = False
+            bad += 1
+    return sets, bits, order, bad
 
 
 def run_reference(args):
@@ -198,18 +313,28 @@ def run_reference(args):
     device = "cuda" if torch.cuda.is_available() else None
     _, vec, bits, queries, exprs = workload(args, device)
     threads = os.cpu_count() or 1
-    nq = args.cpu_queries or 2 * threads
-    for _ in range(args.warmup):
-        cpu_baseline(vec, bits, queries, exprs, args.topk, max(1, nq // 4))
-    total_q, total_t = 0, 0.0
-    rec = None
+    nq_pool = len(queries)
+    # one batch of queries per step, as the GPU arm; fewer only when the run would take over ~4 min
+    per_step = min(args.cpu_queries or args.batch, nq_pool)
+    warm_n = max(1, min(per_step, 2 * threads))
+    _, _, dt, _ = reference_topk(vec, bits, queries[:warm_n], exprs[:warm_n], args.topk, threads)
+    rate = warm_n / dt
+    if not args.cpu_queries and args.steps * per_step / rate > 240.0:
+        per_step = max(threads, int(240.0 * rate / max(1, args.steps)))
+    for w in range(max(0, args.warmup - 1)):
+        reference_topk(vec, bits, queries[:warm_n], exprs[:warm_n], args.topk, threads)
+    total_q, total_t, kind = 0, 0.0, "reference"
     for s in range(args.steps):
-        t0 = time.perf_counter()
-        rec, _, _ = cpu_baseline(vec, bits, queries, exprs, args.topk, nq)
-        total_t += time.perf_counter() - t0
-        total_q += min(nq, len(queries))
+        a = (s * per_step) % max(1, nq_pool - per_step + 1)
+        _, _, dt, kind = reference_topk(vec, bits, queries[a:a + per_step], exprs[a:a + per_step], args.topk,
+                                        threads)
+        total_t += dt
+        total_q += per_step
     v = total_q / total_t
-    rec = dict(rec, value=v)
+    note = f" per step (one batch of {args.batch})" if per_step == args.batch else \
+        f" per step (batch {args.batch} cut to fit the run's time)"
+    rec = cpu_record(per_step, total_t / args.steps, kind, threads, args.topk, args.docs, note)
+    rec["value"] = v
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "QPS", "n_gpus": world,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps,
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -218,13 +343,18 @@ def run_reference(args):
                       "e2e": {"value": v, "unit": "QPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def form_name(method, learned):
+    return FORMS[method] + (" + learned threshold" if learned else "")
+
+
 def config_of(args, world):
     return {"workload": f"filtered top-{args.topk}, {args.docs} docs x 128 FP32, 256 tags, batch {args.batch}",
             "docs": args.docs, "dim": 128, "tags": 256, "batch": args.batch, "topk": args.topk,
             "doc_num_per_segment": 131072, "filters": "1-6 tags AND/OR/NOT, est. selectivity 1e-4..1",
             "parallelism": f"replica x{world}",
             "l2": "inputs larger than L2: every step reads the whole corpus copy (FP32 5.1 GB, BF16 2.6 GB, "
-                  "E4M3 1.3 GB)"}
+                  "E4M3 1.3 GB)",
+            "form": form_name(args.method, args.learned), "method": args.method, "learned": args.learned}
 
 
 def _peaks():
@@ -235,17 +365,29 @@ def _peaks():
         return {}
 
 
-def measure_form(args, ctx, method, learned=False):
+def _topks(args, B, nb, kmix):
+    """Per-batch K arrays: the headline K, or K drawn from {10, 100, 1000} per query."""
+    if not kmix:
+        return [np.full(B, args.topk, np.uint32) for _ in range(nb)]
+    rng = np.random.default_rng(99)
+    return [rng.choice(np.array(PARITY_KS, np.uint32), B) for _ in range(nb)]
+
+
+def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=128, flush_l2=False):
     """One form of the path (candidate-pass method, with or without the learned threshold) over the
-    workload: device-resident QPS (CUDA events, max over ranks), end-to-end QPS through the C-ABI,
-    stage times and the candidate stage's roofline."""
+    context's workload: device-resident QPS (CUDA events, max over ranks), end-to-end QPS through the
+    C-ABI, stage times and the candidate stage's roofline. With flush_l2 (a corpus that fits in L2),
+    every step is timed on its own, after a 256 MB write that evicts L2 outside its events. Returns
+    the record with the live searcher under "searcher" (for parity checks; the caller closes it)."""
     import torch
 
     import hybridsearchsystem_b200 as hss
     from hybridsearchsystem_b200.threshold import fit_threshold_model
     rank, world, dev, table = ctx["rank"], ctx["world"], ctx["dev"], ctx["table"]
     queries, exprs, barrier = ctx["queries"], ctx["exprs"], ctx["barrier"]
-    B, K = args.batch, args.topk
+    docs = docs or args.docs
+    B = args.batch
+    kmax = max(PARITY_KS) if kmix else args.topk
     searcher = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[method],
                                       sample_docs=args.sample_docs)
     report = None
@@ -259,34 +401,42 @@ def measure_form(args, ctx, method, learned=False):
     searcher.set_timing(True)
     nb = max(1, len(queries) // B)
     filters = [searcher.compile_filters(exprs[i * B:(i + 1) * B]) for i in range(nb)]
-    topks = np.full(B, K, np.uint32)
+    topks = _topks(args, B, nb, kmix)
     d_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1), device=dev)
-    o_sc = torch.zeros((B, K), dtype=torch.float32, device=dev)
-    o_id = torch.zeros((B, K), dtype=torch.int64, device=dev)
+    o_sc = torch.zeros((B, kmax), dtype=torch.float32, device=dev)
+    o_id = torch.zeros((B, kmax), dtype=torch.int64, device=dev)
     o_n = torch.zeros(B, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
 
     def step(i):
         j = (rank * 7919 + i) % nb
-        rc = searcher.search_device(d_q[j].data_ptr(), B, filters[j], topks, o_sc.data_ptr(), o_id.data_ptr(),
-                                    o_n.data_ptr(), K, sh)
+        rc = searcher.search_device(d_q[j].data_ptr(), B, filters[j], topks[j], o_sc.data_ptr(), o_id.data_ptr(),
+                                    o_n.data_ptr(), kmax, sh)
         assert rc == 0, searcher.last_status(B)
         return searcher.last_times()
 
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev) if flush_l2 else None
+    pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+             for _ in range(args.steps)] if flush_l2 else None
     # device-resident leg
-    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
     cand_ms, launches, stage_ms = [], 0, []
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(gpu_id) as clk:
+    with ClockSampler(gpu_uuid) as clk:
         barrier()
         torch.cuda.synchronize()
         ev0.record(stream)
         for i in range(args.steps):
+            if flush_l2:
+                flush.fill_(float(i))
+                pairs[i][0].record(stream)
             t = step(args.warmup + i)
+            if flush_l2:
+                pairs[i][1].record(stream)
             cand_ms.append(t["candidates_ms"])
             stage_ms.append([t["filter_ms"], t["sample_ms"], t["candidates_ms"], t["select_ms"], t["total_ms"]])
             launches += t["launches"]
@@ -294,7 +444,8 @@ def measure_form(args, ctx, method, learned=False):
         torch.cuda.synchronize()
         barrier()
     clocks = clk.summary()
-    t_max = max_over_ranks(ev0.elapsed_time(ev1), dev)
+    own_ms = sum(a.elapsed_time(b) for a, b in pairs) if flush_l2 else ev0.elapsed_time(ev1)
+    t_max = max_over_ranks(own_ms, dev)
     value = whole_job_qps(world, args.steps, B, t_max)
 
     # end-to-end leg through the C-ABI: pinned host queries in, results out, every step. Each step
@@ -304,15 +455,15 @@ def measure_form(args, ctx, method, learned=False):
     # GPU; the ctypes calls release the interpreter lock.
     from concurrent.futures import ThreadPoolExecutor
     h_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1)).pin_memory()
-    h_sc = torch.zeros((B, K), dtype=torch.float32).pin_memory()
-    h_id = torch.zeros((B, K), dtype=torch.int64).pin_memory()
+    h_sc = torch.zeros((B, kmax), dtype=torch.float32).pin_memory()
+    h_id = torch.zeros((B, kmax), dtype=torch.int64).pin_memory()
     h_n = torch.zeros(B, dtype=torch.int32).pin_memory()
-    d_stage = torch.zeros((B, 128), dtype=torch.float32, device=dev)
+    d_stage = torch.zeros((B, dim), dtype=torch.float32, device=dev)
 
     def batch_of(i):
         return (rank * 7919 + args.warmup + i) % nb
 
-    def e2e_run(steps, pool):
+    def e2e_run(steps, pool, ev=None):
         fut = pool.submit(lambda: searcher.compile_filters(exprs[batch_of(0) * B:(batch_of(0) + 1) * B]))
         for i in range(steps):
             j = batch_of(i)
@@ -320,13 +471,18 @@ def measure_form(args, ctx, method, learned=False):
             if i + 1 < steps:
                 jn = batch_of(i + 1)
                 fut = pool.submit(lambda jn=jn: searcher.compile_filters(exprs[jn * B:(jn + 1) * B]))
+            if ev is not None:
+                flush.fill_(float(i))
+                ev[i][0].record(stream)
             d_stage.copy_(h_q[j], non_blocking=True)
-            rc = searcher.search_device(d_stage.data_ptr(), B, f, topks, o_sc.data_ptr(), o_id.data_ptr(),
-                                        o_n.data_ptr(), K, sh)
+            rc = searcher.search_device(d_stage.data_ptr(), B, f, topks[j], o_sc.data_ptr(), o_id.data_ptr(),
+                                        o_n.data_ptr(), kmax, sh)
             assert rc == 0
             h_sc.copy_(o_sc, non_blocking=True)
             h_id.copy_(o_id, non_blocking=True)
             h_n.copy_(o_n, non_blocking=True)
+            if ev is not None:
+                ev[i][1].record(stream)
             stream.synchronize()
             f.close()
 
@@ -336,33 +492,34 @@ def measure_form(args, ctx, method, learned=False):
         barrier()
         torch.cuda.synchronize()
         e0.record(stream)
-        e2e_run(args.steps, pool)
+        e2e_run(args.steps, pool, pairs)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-    e2e = whole_job_qps(world, args.steps, B, max_over_ranks(e0.elapsed_time(e1), dev))
+    own_e2e = sum(a.elapsed_time(b) for a, b in pairs) if flush_l2 else e0.elapsed_time(e1)
+    e2e = whole_job_qps(world, args.steps, B, max_over_ranks(own_e2e, dev))
 
     # roofline of the dominant stage, the candidate passes: algorithmic bytes per batch = the corpus
-    # rows the passes read (docs x 128 x element bytes, +4 B scale for E4M3; a learned form's
+    # rows the passes read (docs x dim x element bytes, +4 B scale for E4M3; a learned form's
     # estimation pass re-reads a quarter) + the batch's filter bitmaps (B x docs/8 B)
     info = table.info
     words = info["segment_num"] * info["doc_num_per_segment"] // 64
     elem = {"simt": 4, "tf32": 4, "bf16": 2, "e4m3": 1}[method]
     reads = 1.25 if learned else 1.0
-    alg_bytes = reads * args.docs * (128 * elem + (4 if method == "e4m3" else 0)) + B * words * 8
+    alg_bytes = reads * docs * (dim * elem + (4 if method == "e4m3" else 0)) + B * words * 8
     cand_avg = float(np.mean(cand_ms))
     peaks = _peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg_bytes / (cand_avg / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "cand_traffic.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and dim == 128:
         with open(tpath) as f:
             traffic = json.load(f).get(method)
     kernel = "cand_simt_kernel" if method == "simt" else ("tc2_cand_kernel" if B > 128 else "tc_cand_kernel")
     # the tensor side of the same stage: 2 d flops per (query, doc) pair of every pass, against the
     # pipe's peak (measured BF16 GEMM rate; TF32 and E4M3 by the nominal dense ratios 1/2 and 2)
-    flops = reads * 2.0 * 128 * args.docs * B
+    flops = reads * 2.0 * dim * docs * B
     bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
     tpeak = {"simt": None, "tf32": bf16_peak / 2, "bf16": bf16_peak, "e4m3": bf16_peak * 2}[method]
     t_s = cand_avg / 1e3
@@ -373,12 +530,16 @@ def measure_form(args, ctx, method, learned=False):
                 "achieved_tflops": flops / t_s / 1e12, "peak_tflops": tpeak, "frac": flops / t_s / 1e12 / tpeak,
                 "peak_note": "measured BF16 GEMM" + ("" if method == "bf16" else " x nominal dense ratio")},
             "bound_frac": (max(alg_bytes / (hbm * 1e9), 0.0 if tpeak is None else flops / (tpeak * 1e12)) / t_s)}
-    out = {"value": value, "t_max_ms": t_max, "e2e": e2e, "batch": B, "roofline": roof, "clocks": clocks, "launches": launches,
+    out = {"value": value, "t_max_ms": t_max, "e2e": e2e, "batch": B, "roofline": roof, "clocks": clocks,
+           "launches": launches,
            "stages_ms": dict(zip(["filter", "sample", "candidates", "select", "total"],
                                  [round(float(x), 4) for x in np.mean(np.array(stage_ms), axis=0)])),
-           "form": FORMS[method] + (" + learned threshold" if learned else ""), "method": method,
-           "learned": learned, "searcher": searcher, "filters": filters, "d_q": d_q,
-           "out": (o_sc, o_id, o_n, topks, sh)}
+           "form": form_name(method, learned) + (", K from {10, 100, 1000} per query" if kmix else ""),
+           "l2": "flushed between steps (256 MB write outside the step's events)" if flush_l2 else
+                 "inputs larger than L2",
+           "method": method, "learned": learned, "searcher": searcher, "dev": dev}
+    for f in filters:
+        f.close()
     if report:
         out["model"], out["margin"] = model, margin
         out["learned_report"] = {k: (round(v, 5) if isinstance(v, float) else v) for k, v in report.items()}
@@ -386,13 +547,15 @@ def measure_form(args, ctx, method, learned=False):
         # sample's proven threshold (margin 1e9 turns the prediction into -inf), over the measured batches
         at_sample, at_model, kk = [], [], []
         for j in range(min(nb, 8)):
+            f = searcher.compile_filters(exprs[j * B:(j + 1) * B])
             for m, sink in ((1e9, at_sample), (margin, at_model)):
                 searcher.set_threshold_model(model, m)
-                rc = searcher.search_device(d_q[j].data_ptr(), B, filters[j], topks, o_sc.data_ptr(), o_id.data_ptr(),
-                                            o_n.data_ptr(), K, sh)
+                rc = searcher.search_device(d_q[j].data_ptr(), B, f, topks[j], o_sc.data_ptr(), o_id.data_ptr(),
+                                            o_n.data_ptr(), kmax, sh)
                 assert rc == 0
                 sink.append(searcher.last_estimate_counts(B).astype(np.int64))
-            kk.append(topks.astype(np.int64))
+            f.close()
+            kk.append(topks[j].astype(np.int64))
         at_sample, at_model, kk = np.concatenate(at_sample), np.concatenate(at_model), np.concatenate(kk)
         searcher.set_threshold_model(model, margin)
         out["learned_report"].update({
@@ -401,6 +564,58 @@ def measure_form(args, ctx, method, learned=False):
             "pruned_fraction": round(1.0 - at_model.sum() / max(1, at_sample.sum()), 4),
             "miss_rate": round(float(np.mean(at_model < kk)), 4), "queries": int(len(kk))})
     return out
+
+
+def parity_of_form(searcher, dev, B, pq, pe, truth_by_k):
+    """Runs a form's searcher over the parity queries at every K (batches of B) and checks each K's
+    results against the reference's ordered ground truth."""
+    import torch
+    res = {}
+    n = len(pq)
+    for k, truth in truth_by_k.items():
+        d_q = torch.tensor(np.ascontiguousarray(pq), device=dev)
+        o_sc = torch.zeros((B, k), dtype=torch.float32, device=dev)
+        o_id = torch.zeros((B, k), dtype=torch.int64, device=dev)
+        o_n = torch.zeros(B, dtype=torch.int32, device=dev)
+        sc_all = np.zeros((n, k), np.float32)
+        id_all = np.zeros((n, k), np.int64)
+        n_all = np.zeros(n, np.int64)
+        sh = torch.cuda.current_stream().cuda_stream
+        for a in range(0, n, B):
+            b = min(n, a + B)
+            f = searcher.compile_filters(pe[a:b])
+            rc = searcher.search_device(d_q[a].data_ptr(), b - a, f, np.full(b - a, k, np.uint32), o_sc.data_ptr(),
+                                        o_id.data_ptr(), o_n.data_ptr(), k, sh)
+            torch.cuda.synchronize()
+            f.close()
+            assert rc == 0, searcher.last_status(b - a)
+            sc_all[a:b] = o_sc.cpu().numpy()[:b - a]
+            id_all[a:b] = o_id.cpu().numpy()[:b - a]
+            n_all[a:b] = o_n.cpu().numpy()[:b - a]
+        sets, bits, order, bad = check_against(truth, sc_all, id_all, n_all)
+        res[f"K{k}"] = {"id_sets_match": sets, "scores_bit_exact": bits, "order_score_desc_id_asc": order,
+                        "queries_differing": bad}
+        res.setdefault("_last", (sc_all, id_all, n_all))
+    last = res.pop("_last")
+    return res, last
+
+
+def fp64_error(vec, queries, scores, ids, counts):
+    """Max and median |returned FP32 score - FP64 dot product of the same vectors|."""
+    ea, er = [], []
+    for i in range(len(counts)):
+        c = int(counts[i])
+        if c == 0:
+            continue
+        ex = vec[ids[i][:c]].astype(np.float64) @ queries[i].astype(np.float64)
+        e = np.abs(scores[i][:c].astype(np.float64) - ex)
+        ea.append(e)
+        er.append(e / np.maximum(np.abs(ex), 1e-30))
+    if not ea:
+        return None
+    ea, er = np.concatenate(ea), np.concatenate(er)
+    return {"max_abs": float(ea.max()), "median_abs": float(np.median(ea)), "max_rel": float(er.max()),
+            "median_rel": float(np.median(er))}
 
 
 def data_filters(mix, n, seed):
@@ -430,8 +645,138 @@ def measure_serving(args, ctx, method, rates, model=None, margin=0.0):
         out.append({"offered_qps": round(offered), "completed_qps": round(n / wall), "p50_ms": round(st["p50_ms"], 3),
                     "p99_ms": round(st["p99_ms"], 3), "mean_batch": round(st["mean_batch"], 1)})
     srv.close()
-    return {"form": FORMS[method] + (" + learned threshold" if model is not None else ""), "slots": 2,
+    return {"form": form_name(method, model is not None), "slots": 2,
             "max_wait_us": args.serve_wait_us, "topk": "log-uniform in [1, 1000] per request", "rates": out}
+
+
+def summary(f, steps):
+    d = {"value": f["value"], "e2e_qps": f["e2e"], "ms_per_step": f["t_max_ms"] / steps,
+         "stages_ms": f["stages_ms"], "roofline_frac": f["roofline"]["frac"], "form": f["form"],
+         "batch": f["batch"], "l2": f["l2"], "clocks": {k: f["clocks"][k] for k in ("sm_mhz", "reasons", "samples")}}
+    if "learned_report" in f:
+        d["learned_report"] = f["learned_report"]
+    if "parity" in f:
+        d["parity"] = f["parity"]
+    return d
+
+
+def run_cfg1(args, dev, local):
+    """The one-segment configuration: 131,072 docs x 128, 64 tags (densities in [1e-3, 0.5]), filters
+    of 1-4 tags, 1,000 queries in batches of 32, top-100; chosen and plain forms, each checked against
+    the reference on all 1,000 queries."""
+    import copy
+
+    import hybridsearchsystem_b200 as hss
+    from hybridsearchsystem_b200 import data
+    c = data.CONFIGS["cfg1"]
+    mix = data.Mixture(c["dim"], c["tag_num"], c["p_range"], n_clusters=1024, sigma=0.3, n_corr=16, seed=5)
+    vec, bits, _ = mix.corpus(c["n"], seed=51)
+    queries = mix.queries(c["nq"], seed=52)
+    exprs = data.make_filters(mix, c["nq"], n_tags=c["n_tags"], seed=53)
+    table = hss.DataTable.build(vec, bits, c["tag_num"], device=local, doc_num_per_segment=c["doc_num_per_segment"])
+    threads = os.cpu_count() or 1
+    ids, counts, dt, kind = reference_topk(vec, bits, queries, exprs, 100, threads)
+    truth = {100: ordered_truth(vec, queries, ids, counts)}
+    a = copy.copy(args)
+    a.batch, a.topk, a.docs = c["batch"], 100, c["n"]
+    a.steps = max(args.steps, 31)
+    ctx = {"rank": 0, "world": 1, "dev": dev, "table": table, "queries": queries, "exprs": exprs,
+           "barrier": lambda: None}
+    out = {"workload": "filtered top-100, 131072 docs x 128 FP32 (one segment), 64 tags, batch 32",
+           "cpu_baseline": cpu_record(len(queries), dt, kind, threads, 100, c["n"])}
+    for key, method in (("chosen", args.method), ("plain_fp32", "tf32"), ("plain_fp32_simt", "simt")):
+        f = measure_form(a, ctx, method, flush_l2=True)
+        f["parity"], _ = parity_of_form(f["searcher"], dev, a.batch, queries, exprs, truth)
+        f["searcher"].close()
+        out[key] = summary(f, a.steps)
+    table.close()
+    return out
+
+
+def run_cfg3(args, dev, local):
+    """The precision form at 20M x 768: FP32 rows (61 GB) with BF16 and E4M3 copies resident together
+    (108 GB), 64 tags, batches of 256, top-100. Each form's QPS, recall against the reference's
+    CpuTopKBatch (run over the corpus in 1M-doc chunks copied to the host, merged by (score desc, id
+    asc)) for a query sample, and the returned scores' error against an FP64 dot product."""
+    import copy
+
+    import torch
+
+    import hybridsearchsystem_b200 as hss
+    from hybridsearchsystem_b200 import data
+    n, dim, tags = args.precision_docs, 768, 64
+    mix = data.Mixture(dim, tags, (1e-3, 0.5), n_clusters=1024, sigma=0.3, n_corr=16, seed=7)
+    t0 = time.perf_counter()
+    d_vec, bits = mix.corpus_device(n, device=dev, seed=71)
+    table = hss.DataTable.build_device(d_vec.data_ptr(), n, dim, bits, tags, device=local,
+                                       doc_num_per_segment=131072)
+    queries = mix.queries(2048, seed=72)
+    exprs = data.make_filters(mix, 2048, n_tags=(1, 4), seed=73)
+    # reference ground truth for a sample, in chunks of the corpus copied to the host
+    npar = 32
+    threads = os.cpu_count() or 1
+    chunk = 1 << 20
+    best = [[] for _ in range(npar)]
+    t_ref = 0.0
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        hv = d_vec[a:b].cpu().numpy()
+        ids, counts, dt, kind = reference_topk(hv, bits[a:b], queries[:npar], exprs[:npar], 100, threads)
+        t_ref += dt
+        for i in range(npar):
+            c = int(counts[i])
+            loc = np.sort(ids[i][:c])
+            acc = np.zeros(c, np.float32)
+            for d in range(dim):
+                acc = (acc + (queries[i][d] * hv[loc, d]).astype(np.float32)).astype(np.float32)
+            best[i].extend(zip((-acc.astype(np.float64)).tolist(), (loc + a).tolist(), acc.tolist()))
+        del hv
+    truth = []
+    for i in range(npar):
+        top = sorted(best[i])[:100]
+        truth.append((np.array([t[2] for t in top], np.float32), np.array([t[1] for t in top], np.int64)))
+    # the truth's rows on the host, for the FP64 error of the returned scores
+    want = np.unique(np.concatenate([t[1] for t in truth]))
+    rows64 = d_vec[torch.tensor(want, device=dev)].cpu().numpy().astype(np.float64)
+    del d_vec
+    torch.cuda.empty_cache()
+    build_s = time.perf_counter() - t0
+    a = copy.copy(args)
+    a.docs, a.topk, a.batch = n, 100, 256
+    a.steps = min(args.steps, 10)
+    ctx = {"rank": 0, "world": 1, "dev": dev, "table": table, "queries": queries, "exprs": exprs,
+           "barrier": lambda: None}
+    out = {"workload": f"filtered top-100, {n} docs x {dim} FP32 + BF16 + E4M3 copies, {tags} tags, batch 256",
+           "setup_s": round(build_s, 1),
+           "cpu_baseline": {"value": npar / t_ref, "unit": "QPS", "cores": threads, "kind": kind,
+                            "cpu_model": cpu_model(),
+                            "sample": f"{npar} queries over the corpus in 1M-doc chunks"}}
+    pos = {int(g): j for j, g in enumerate(want)}
+    for method in ("tf32", "bf16", "e4m3"):
+        f = measure_form(a, ctx, method, docs=n, dim=dim)
+        par, (sc, ids, cnt) = parity_of_form(f["searcher"], dev, a.batch, queries[:npar], exprs[:npar],
+                                             {100: truth})
+        f["parity"] = par
+        f["searcher"].close()
+        s = summary(f, a.steps)
+        # recall of the reference's ids and the FP64 error of the returned scores
+        rec = [len(set(ids[i][:len(truth[i][1])].tolist()) & set(truth[i][1].tolist())) / max(1, len(truth[i][1]))
+               for i in range(npar)]
+        s["recall"] = float(np.mean(rec))
+        ea = []
+        for i in range(npar):
+            c = int(cnt[i])
+            rows = np.array([pos.get(int(g), -1) for g in ids[i][:c]])
+            if c == 0 or (rows < 0).any():
+                continue
+            ex = rows64[rows] @ queries[i].astype(np.float64)
+            ea.append(np.abs(sc[i][:c].astype(np.float64) - ex))
+        if ea:
+            ea = np.concatenate(ea)
+            s["score_error_vs_fp64"] = {"max_abs": float(ea.max()), "median_abs": float(np.median(ea))}
+        out[method] = s
+    table.close()
+    return out
 
 
 def run_ours(args):
@@ -455,26 +800,61 @@ def run_ours(args):
     ctx = {"rank": rank, "world": world, "dev": dev, "table": table, "queries": queries, "exprs": exprs,
            "barrier": barrier, "mix": mix}
     B, K = args.batch, args.topk
-    chosen = measure_form(args, ctx, args.method, learned=args.learned)
-    forms = {"chosen": chosen}
+    solo = rank == 0 and world == 1
+    # the reference's ground truth for the parity sample (K = 10, 100, 1000); the K = 100 run is the
+    # timed CPU baseline
+    truth, cb = None, None
+    if solo and not args.no_cpu_baseline:
+        npq = min(args.parity_queries, len(queries))
+        pq, pe = queries[:npq], exprs[:npq]
+        threads = os.cpu_count() or 1
+        truth = {}
+        for k in PARITY_KS:
+            ids, counts, dt, kind = reference_topk(vec, bits, pq, pe, k, threads)
+            truth[k] = ordered_truth(vec, pq, ids, counts)
+            if k == K:
+                cb = cpu_record(npq, dt, kind, threads, K, args.docs)
+
+    forms = {}
+
+    def run_form(key, method, learned=False, batch=None, kmix=False):
+        import copy
+        a = args
+        if batch and batch != args.batch:
+            a = copy.copy(args)
+            a.batch = batch
+        f = measure_form(a, ctx, method, learned=learned, kmix=kmix)
+        if truth is not None and not kmix:
+            f["parity"], last = parity_of_form(f["searcher"], dev, a.batch, pq, pe, truth)
+            if key == "chosen":
+                f["fp64"] = fp64_error(vec, pq, *last)
+        if key != "chosen":
+            f["searcher"].close()
+            f.pop("searcher")
+        forms[key] = f
+        return f
+
+    chosen = run_form("chosen", args.method, learned=args.learned)
     if args.learned_form and not args.learned:
-        # the chosen format with the learned threshold, measured beside it
-        forms["chosen_learned"] = measure_form(args, ctx, args.method, learned=True)
+        run_form("chosen_learned", args.method, learned=True)
     if args.plain:
         # the two plain FP32 forms (both read the FP32 rows): TF32 tensor cores, and SIMT FFMA
         if not (args.method == "tf32" and not args.learned):
-            forms["plain_fp32"] = measure_form(args, ctx, "tf32")
-        forms["plain_fp32_simt"] = measure_form(args, ctx, "simt")
+            run_form("plain_fp32", "tf32")
+        run_form("plain_fp32_simt", "simt")
+    if args.e4m3 and args.method != "e4m3":
+        run_form("e4m3", "e4m3")
     if args.batch64 and args.batch != 64:
         # the configuration's other batch size: 64 queries per batch (one SM per 128-doc tile)
-        import copy
-        a64 = copy.copy(args)
-        a64.batch = 64
-        forms["chosen_batch64"] = measure_form(a64, ctx, args.method)
+        run_form("chosen_batch64", args.method, batch=64)
         if args.plain:
-            forms["plain_fp32_batch64"] = measure_form(a64, ctx, "tf32")
+            run_form("plain_fp32_batch64", "tf32", batch=64)
+    if args.kmix:
+        run_form("chosen_kmix", args.method, kmix=True)
+        if args.plain:
+            run_form("plain_fp32_kmix", "tf32", kmix=True)
     serving = None
-    if rank == 0 and world == 1 and args.serve:
+    if solo and args.serve:
         rates = [float(r) for r in args.serve_rates.split(",")]
         serving = {"chosen": measure_serving(args, ctx, args.method, rates, chosen.get("model"),
                                              chosen.get("margin", 0.0))}
@@ -484,79 +864,44 @@ def run_ours(args):
         if args.plain:
             serving["plain_fp32"] = measure_serving(args, ctx, "tf32", rates)
 
-    def summary(f):
-        d = {"value": f["value"], "e2e_qps": f["e2e"], "ms_per_step": f["t_max_ms"] / args.steps,
-             "stages_ms": f["stages_ms"], "roofline_frac": f["roofline"]["frac"], "form": f["form"],
-             "batch": f["batch"]}
-        if "learned_report" in f:
-            d["learned_report"] = f["learned_report"]
-        return d
-
     rec = {"metric": METRIC, "value": chosen["value"], "unit": "QPS", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": chosen["t_max_ms"] / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": {"simt": "f32", "tf32": "f32", "bf16": "bf16",
                                                              "e4m3": "e4m3"}[args.method] + "+f32 rescore",
            "data": "synthetic (seeded cluster mixture, HYDSET2 shapes)",
-           "config": dict(config_of(args, world), form=chosen["form"], method=args.method, learned=args.learned),
+           "config": config_of(args, world),
            "e2e": {"value": chosen["e2e"], "unit": "QPS", "h2d_bytes_per_step": B * 128 * 4,
                    "d2h_bytes_per_step": B * K * (4 + 8) + B * 4,
                    "path": "hss_filters_compile (next batch, compile thread) + hss_searcher_search_device "
                            "per batch, pinned host queries in and results out"},
            "roofline": chosen["roofline"], "clocks": chosen["clocks"], "gpu_launches": chosen["launches"],
-           "stages_ms": chosen["stages_ms"], "forms": {k: summary(v) for k, v in forms.items()}}
+           "stages_ms": chosen["stages_ms"], "forms": {k: summary(v, args.steps) for k, v in forms.items()}}
     if "plain_fp32" in forms:
         rec["chosen_over_plain"] = chosen["value"] / forms["plain_fp32"]["value"]
     if serving:
         rec["serving"] = serving
-
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb, ref_ids, ref_counts = cpu_baseline(vec, bits, queries, exprs, K, args.cpu_queries)
+    if cb is not None:
         rec["cpu_baseline"] = cb
-        # parity at full scale, for the CPU sample's queries. The reference's ground truth is a set
-        # (CpuTopK returns an unordered_set, recall_ref.cpp:18-48; the reference build hands it back
-        # sorted by id), so ids are compared as sets; the order (score desc, id asc) and the scores are
-        # checked against the ground truth's own arithmetic: an FP32 sum over d ascending, each product
-        # and sum rounded to FP32.
-        searcher, filters, d_q = chosen["searcher"], chosen["filters"], chosen["d_q"]
-        o_sc, o_id, o_n, topks, sh = chosen["out"]
-        nq = len(ref_counts)
-        set_ok = order_ok = score_ok = True
-        err_abs, err_rel = [], []
-        for j in range((nq + B - 1) // B):
-            rc = searcher.search_device(d_q[j].data_ptr(), B, filters[j], topks, o_sc.data_ptr(), o_id.data_ptr(),
-                                        o_n.data_ptr(), K, sh)
-            torch.cuda.synchronize()
-            assert rc == 0
-            g_id, g_n, g_sc = o_id.cpu().numpy(), o_n.cpu().numpy(), o_sc.cpu().numpy()
-            for i in range(B):
-                qi = j * B + i
-                if qi >= nq:
-                    break
-                c = int(ref_counts[qi])
-                if int(g_n[i]) != c or set(g_id[i][:c].tolist()) != set(ref_ids[qi][:c].tolist()):
-                    set_ok = False
-                    continue
-                ids, sc = g_id[i][:c], g_sc[i][:c]
-                acc = np.zeros(c, np.float32)
-                qv, dv = queries[qi].astype(np.float32), vec[ids].astype(np.float32)
-                for d in range(qv.shape[0]):
-                    acc = (acc + (qv[d] * dv[:, d]).astype(np.float32)).astype(np.float32)
-                if not (acc.view(np.uint32) == sc.view(np.uint32)).all():
-                    score_ok = False
-                exact64 = dv.astype(np.float64) @ qv.astype(np.float64)
-                err_abs.append(np.abs(sc.astype(np.float64) - exact64))
-                err_rel.append(np.abs(sc.astype(np.float64) - exact64) / np.maximum(np.abs(exact64), 1e-30))
-                if c > 1 and not all(sc[r] > sc[r + 1] or (sc[r] == sc[r + 1] and ids[r] < ids[r + 1])
-                                     for r in range(c - 1)):
-                    order_ok = False
-        rec["parity_full_scale"] = {"queries": nq, "against": cb["kind"], "id_sets_match": set_ok,
-                                    "scores_bit_exact": score_ok, "order_score_desc_id_asc": order_ok}
-        if err_abs:
-            ea, er = np.concatenate(err_abs), np.concatenate(err_rel)
-            # the returned FP32 scores against an FP64 dot product of the same vectors
-            rec["parity_full_scale"]["score_error_vs_fp64"] = {
-                "max_abs": float(ea.max()), "median_abs": float(np.median(ea)),
-                "max_rel": float(er.max()), "median_rel": float(np.median(er))}
+        per = {k: v["parity"] for k, v in forms.items() if "parity" in v}
+        ok = all(all(x["id_sets_match"] and x["scores_bit_exact"] and x["order_score_desc_id_asc"]
+                     for x in p.values()) for p in per.values())
+        rec["parity_full_scale"] = {"queries": len(pq), "k": list(PARITY_KS), "against": cb["kind"],
+                                    "all_forms_exact": ok, "forms": per,
+                                    "score_error_vs_fp64": chosen.get("fp64")}
+    chosen["searcher"].close()
+    for f in forms.values():
+        for key in ("searcher", "model"):
+            f.pop(key, None)
+    configs = {}
+    if solo and args.cfg1:
+        configs["cfg1"] = run_cfg1(args, dev, local)
+    if solo and args.precision:
+        table.close()
+        del vec, bits
+        torch.cuda.empty_cache()
+        configs["cfg3"] = run_cfg3(args, dev, local)
+    if configs:
+        rec["configs"] = configs
     if rank == 0:
         print(json.dumps(rec))
     if world > 1:

@@ -43,6 +43,21 @@ class DataTable:
         return cls(h.value, device)
 
     @classmethod
+    def build_device(cls, d_vectors, doc_num, dim, tag_bits, tag_num, device=0, doc_num_per_segment=131072,
+                     density_threshold=1.0 / 64, matrix_posting=False, sparse_packed=False, doc_offset=0):
+        """The same build from vectors already on `device` (d_vectors: device pointer of [doc_num][dim]
+        float32, copied by the table; the caller may free it afterwards). tag_bits is a host array."""
+        lib = _lib.load()
+        tag_bits = np.ascontiguousarray(tag_bits, dtype=np.uint64)
+        assert tag_bits.shape[0] == doc_num and tag_bits.shape[1] == (tag_num + 63) // 64
+        cfg = _lib.IndexConfig(doc_num_per_segment, density_threshold, int(matrix_posting), int(sparse_packed),
+                               doc_offset)
+        h = ctypes.c_void_p()
+        check(lib.hss_table_build_device(device, ctypes.c_void_p(d_vectors), _np_ptr(tag_bits), doc_num, dim, tag_num,
+                                         ctypes.byref(cfg), ctypes.byref(h)))
+        return cls(h.value, device)
+
+    @classmethod
     def load(cls, directory, device=0):
         lib = _lib.load()
         h = ctypes.c_void_p()
@@ -97,6 +112,18 @@ class DataTable:
                                              _np_ptr(rows), rows.size, ctypes.byref(rl), ctypes.byref(opn),
                                              ctypes.byref(empty)))
         return prog[:pl.value].copy(), rows[:rl.value].copy(), opn.value, bool(empty.value)
+
+    def compile_filter_accumulator(self, expr):
+        """(accumulator ops, posting row of each slot, empty_tree) the range filter runs for one filter
+        text (include/hss.h, hss_filter_compile_accumulator)."""
+        ops = np.zeros(_lib.HSS_MAX_PROGRAM + _lib.HSS_MAX_OPERANDS, np.uint32)
+        rows = np.zeros(_lib.HSS_MAX_OPERANDS, np.uint32)
+        ol, rl = ctypes.c_uint32(), ctypes.c_uint32()
+        empty = ctypes.c_int32()
+        check(_lib.load().hss_filter_compile_accumulator(self._h, expr.encode(), _np_ptr(ops), ops.size,
+                                                         ctypes.byref(ol), _np_ptr(rows), rows.size, ctypes.byref(rl),
+                                                         ctypes.byref(empty)))
+        return ops[:ol.value].copy(), rows[:rl.value].copy(), bool(empty.value)
 
 
 class Filters:

@@ -246,6 +246,25 @@ int hss_table_build(int32_t deviceId, const float* vectors, const uint64_t* tagB
     return HSS_OK;
 }
 
+int hss_table_build_device(int32_t deviceId, const float* dVectors, const uint64_t* tagBits, uint64_t docNum,
+                           uint32_t dim, uint32_t tagNum, const hss_index_config* cfg, hss_table** out) {
+    if (!dVectors || !tagBits || !out) return SetError(HSS_ERR_INVALID, "hss_table_build_device: null argument");
+    hss::IndexConfig c;
+    if (cfg) {
+        c.docNumPerSegment = cfg->docNumPerSegment;
+        c.densityThreshold = cfg->densityThreshold;
+        c.matrixPosting = cfg->matrixPosting != 0;
+        c.sparsePacked = cfg->sparsePacked != 0;
+        c.docOffset = cfg->docOffset;
+    }
+    auto t = std::make_shared<hss::DataTable>();
+    std::string err;
+    if (!t->BuildFromDevice(deviceId, dVectors, tagBits, docNum, dim, tagNum, c, &err))
+        return SetError(HSS_ERR_INDEX, err);
+    *out = new hss_table{t};
+    return HSS_OK;
+}
+
 int hss_table_load(int32_t deviceId, const char* dir, hss_table** out) {
     if (!dir || !out) return SetError(HSS_ERR_INVALID, "hss_table_load: null argument");
     auto t = std::make_shared<hss::DataTable>();
@@ -646,6 +665,40 @@ int hss_filter_compile(const hss_table* table, const char* filterExpr, uint32_t*
     if (*progLen > progCap || *rowLen > rowCap) return SetError(HSS_ERR_LIMIT, "output buffers too small");
     if (prog) std::copy(e.postExpr.begin(), e.postExpr.end(), prog);
     if (rows) std::copy(e.postingRows.begin(), e.postingRows.end(), rows);
+    return HSS_OK;
+}
+
+int hss_filter_compile_accumulator(const hss_table* table, const char* filterExpr, uint32_t* ops, uint32_t opCap,
+                                   uint32_t* opLen, uint32_t* slotRows, uint32_t slotCap, uint32_t* slotLen,
+                                   int32_t* emptyTree) {
+    if (!table || !opLen || !slotLen) return SetError(HSS_ERR_INVALID, "null argument");
+    bool ok = true;
+    auto ast = hss::ParseFilter(filterExpr ? filterExpr : "", ok);
+    if (!ok) return SetError(HSS_ERR_PARSE, "filter does not parse");
+    auto tree = hss::BuildQueryNode(ast.get(), table->t->GetConfig().postingField);
+    hss::FilterExpr e;
+    std::string err;
+    if (!hss::PrepareExpr(tree.get(), *table->t, e, &err)) return SetError(HSS_ERR_PROGRAM, err);
+    if (emptyTree) *emptyTree = e.emptyTree ? 1 : 0;
+    // slots in first-use order over the operand list, as the searcher assigns them within a batch
+    std::vector<uint32_t> rows, slots(e.postingRows.size());
+    for (size_t j = 0; j < e.postingRows.size(); ++j) {
+        const uint32_t r = std::min(e.postingRows[j], table->t->PostingRows() - 1);
+        const auto it = std::find(rows.begin(), rows.end(), r);
+        slots[j] = static_cast<uint32_t>(it - rows.begin());
+        if (it == rows.end()) rows.push_back(r);
+    }
+    std::vector<uint32_t> code;
+    bool fits = true;
+    if (!e.emptyTree && !hss::CompileMicro(e.postExpr.data(), static_cast<uint32_t>(e.postExpr.size()), slots.data(),
+                                           static_cast<uint32_t>(slots.size()), code, &fits))
+        return SetError(HSS_ERR_PROGRAM, "malformed filter program");
+    if (!fits) return SetError(HSS_ERR_LIMIT, "filter program deeper than the range filter's register stack");
+    *opLen = static_cast<uint32_t>(code.size());
+    *slotLen = static_cast<uint32_t>(rows.size());
+    if (*opLen > opCap || *slotLen > slotCap) return SetError(HSS_ERR_LIMIT, "output buffers too small");
+    if (ops) std::copy(code.begin(), code.end(), ops);
+    if (slotRows) std::copy(rows.begin(), rows.end(), slotRows);
     return HSS_OK;
 }
 

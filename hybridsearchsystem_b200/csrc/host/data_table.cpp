@@ -240,6 +240,23 @@ std::vector<uint8_t> DataTable::PostingTypes(uint32_t row) const {
 
 bool DataTable::Build(int32_t deviceId, const float* vectors, const uint64_t* tagBits, uint64_t docNum, uint32_t dim,
                       uint32_t tagNum, const IndexConfig& cfg, std::string* err) {
+    return BuildImpl(deviceId, vectors, false, tagBits, docNum, dim, tagNum, cfg, err);
+}
+
+bool DataTable::BuildFromDevice(int32_t deviceId, const float* dVectors, const uint64_t* tagBits, uint64_t docNum,
+                                uint32_t dim, uint32_t tagNum, const IndexConfig& cfg, std::string* err) {
+    if (deviceId < 0) return Fail(err, "a build from device vectors needs a device");
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, dVectors) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+        at.device != deviceId) {
+        cudaGetLastError();
+        return Fail(err, "vectors are not device memory of the table's device");
+    }
+    return BuildImpl(deviceId, dVectors, true, tagBits, docNum, dim, tagNum, cfg, err);
+}
+
+bool DataTable::BuildImpl(int32_t deviceId, const float* vectors, bool onDevice, const uint64_t* tagBits,
+                          uint64_t docNum, uint32_t dim, uint32_t tagNum, const IndexConfig& cfg, std::string* err) {
     Release();
     if (docNum == 0 || docNum >= 0xffffffffull) return Fail(err, "docNum must be in [1, 2^32-1)");
     if (dim == 0 || dim % 4 != 0 || dim > 4096) return Fail(err, "dim must be a multiple of 4 in [4, 4096]");
@@ -256,10 +273,10 @@ bool DataTable::Build(int32_t deviceId, const float* vectors, const uint64_t* ta
     m_postingFields = {cfg.postingField};
     const uint32_t words = (tagNum + 63) / 64;
 
-    // gdocids and the corpus norm bound
+    // gdocids and the corpus norm bound (device vectors: after the upload, on the device)
     m_gdocids.resize(docNum);
     for (uint64_t i = 0; i < docNum; ++i) m_gdocids[i] = static_cast<int64_t>(cfg.docOffset + i);
-    {
+    if (!onDevice) {
         const unsigned t = HostThreads();
         std::vector<double> mx(t, 0.0);
         const uint64_t per = (docNum + t - 1) / t;
@@ -346,13 +363,30 @@ bool DataTable::Build(int32_t deviceId, const float* vectors, const uint64_t* ta
     if (!CudaOk(cudaSetDevice(deviceId), err, "cudaSetDevice")) return false;
     const uint64_t rowsAlloc = GetTileNum() * 128;
     if (!CudaOk(cudaMalloc(&m_dVectors, rowsAlloc * dim * sizeof(float)), err, "cudaMalloc vectors")) return false;
-    if (!CudaOk(cudaMemcpy(m_dVectors, vectors, docNum * dim * sizeof(float), cudaMemcpyHostToDevice), err,
-                "upload vectors"))
+    if (!CudaOk(cudaMemcpy(m_dVectors, vectors, docNum * dim * sizeof(float),
+                           onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice),
+                err, "upload vectors"))
         return false;
     if (rowsAlloc > docNum &&
         !CudaOk(cudaMemset(m_dVectors + docNum * dim, 0, (rowsAlloc - docNum) * dim * sizeof(float)), err,
                 "memset vectors"))
         return false;
+    if (onDevice) {
+        // per-row norms (FP64 sums, rounded up) by the quantiser's FP32 mode, maximum on the host
+        float* norm = nullptr;
+        bool ok = CudaOk(cudaMalloc(&norm, rowsAlloc * sizeof(float)), err, "cudaMalloc norms") &&
+                  CudaOk(launch_quantize_docs(m_dVectors, rowsAlloc, docNum, dim, kTcTF32, nullptr, nullptr, norm,
+                                              nullptr, nullptr),
+                         err, "row norms");
+        std::vector<float> hn(rowsAlloc, 0.0f);
+        if (ok) ok = CudaOk(cudaMemcpy(hn.data(), norm, rowsAlloc * sizeof(float), cudaMemcpyDeviceToHost), err,
+                            "download norms");
+        if (norm) cudaFree(norm);
+        if (!ok) return false;
+        float m = 0.0f;
+        for (float x : hn) m = std::max(m, x);
+        m_maxNorm = m;
+    }
     return Upload(err);
 }
 

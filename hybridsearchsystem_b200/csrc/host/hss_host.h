@@ -80,6 +80,12 @@ struct FilterExpr {
     bool emptyTree = false;  // match all
 };
 
+// The range filter's accumulator form (MicroOp) of a postfix program whose operand j reads row slot
+// slots[j]; false for a malformed program (the stack-machine kernels' rules), *fits false when the
+// program needs more stack than the range filter's registers hold (query_node.cpp).
+bool CompileMicro(const uint32_t* prog, uint32_t plen, const uint32_t* slots, uint32_t nop, std::vector<uint32_t>& out,
+                  bool* fits);
+
 class QueryNode {
    public:
     virtual ~QueryNode() = default;
@@ -200,6 +206,11 @@ class DataTable {
     // deviceId < 0 keeps the table on the host only (index build, filter compilation, Save).
     bool Build(int32_t deviceId, const float* vectors, const uint64_t* tagBits, uint64_t docNum, uint32_t dim,
                uint32_t tagNum, const IndexConfig& cfg, std::string* err);
+    // The same build from vectors already resident on deviceId (dVectors, [docNum][dim] device
+    // memory, copied into the table's own allocation): corpora too large to stage through the host.
+    // The tag bitmaps are host arrays (the postings are built on the host).
+    bool BuildFromDevice(int32_t deviceId, const float* dVectors, const uint64_t* tagBits, uint64_t docNum,
+                         uint32_t dim, uint32_t tagNum, const IndexConfig& cfg, std::string* err);
     // DataTable::LoadData (data_table.cpp:35-124) over the index directory Save() writes.
     bool LoadData(int32_t deviceId, const std::string& dataDir, std::string* err);
     bool Save(const std::string& dataDir, std::string* err) const;
@@ -250,6 +261,8 @@ class DataTable {
 
    private:
     bool Upload(std::string* err);
+    bool BuildImpl(int32_t deviceId, const float* vectors, bool onDevice, const uint64_t* tagBits, uint64_t docNum,
+                   uint32_t dim, uint32_t tagNum, const IndexConfig& cfg, std::string* err);
     void Release();
 
     int32_t m_deviceId = -1;
@@ -481,6 +494,7 @@ class FullRecallSearcher {
     bool m_timing = false;
     StageTimes m_times;
     std::vector<int32_t> m_lastStatus;
+    std::vector<uint32_t> m_slotOfRow;  // range filter: shared-memory slot of each posting row in a batch
     std::vector<std::pair<uint32_t, uint32_t>> m_lastSegs;  // per query: (segments, entries per segment)
     std::shared_ptr<ThresholdModel> m_model;
     float m_margin = 0.0f;

@@ -32,11 +32,42 @@ double SimtRelBound(uint32_t d) {
 
 size_t AlignUp(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Accumulation error of one tensor-core dot product, relative to |q~||v~| (the quantised vectors'
+// norms), for d terms in the pass's format.
+//
+// Model: every MMA instruction adds its k products (k = 32 bytes of K: 8 TF32, 16 BF16, 32 E4M3
+// terms) to the FP32 accumulator as one fused sum. The products are exact; the k + 1 addends are
+// aligned to the largest of them and cut to p bits (truncation, no rounding), and the sum is
+// normalised to p bits by truncation again. That is the behaviour Fasi, Higham, Mikaitis and Pranesh
+// measured on the V100, T4 and A100 tensor cores ("Numerical behavior of NVIDIA tensor cores", PeerJ
+// Computer Science 7:e330, 2021), where the FP32-accumulating modes kept no fewer bits than the FP32
+// significand. For FP8, the DeepSeek-V3 technical report (arXiv:2412.19437, section 3.3.2) measured
+// Hopper's FP8 MMA keeping only about 14 bits of the accumulation.
+//
+// Each addend loses less than one unit in the p-th bit of the largest addend, and the normalisation
+// less than one of the sum, so one instruction's error is below (k + 2) 2^(1-p) M, where M bounds
+// every partial sum and product: M <= sum_i |q~_i v~_i| <= |q~||v~| (Cauchy-Schwarz). Over ceil(d/k)
+// instructions: (d + 2 ceil(d/k)) 2^(1-p) |q~||v~|, with p one bit below what was measured (23 for
+// TF32 and BF16, 13 for E4M3) and a factor (1 + 2^-10) for the second-order growth of M. The 2^-21
+// covers the E4M3 dequantising multiplies (acc * q scale * doc scale, two roundings). The GPU test
+// test_accumulation_bound_under_cancellation drives the passes with high-cancellation,
+// wide-dynamic-range rows and reports the measured fraction of this bound.
+double TcAccumulationBound(int format, uint32_t d) {
+    const uint32_t k = format == kTcTF32 ? 8u : (format == kTcBF16 ? 16u : 32u);
+    const int p = format == kTcE4M3 ? 13 : 23;
+    const double steps = static_cast<double>((d + k - 1) / k);
+    return (static_cast<double>(d) + 2.0 * steps) * std::ldexp(1.0, 1 - p) * (1.0 + std::ldexp(1.0, -10)) +
+           std::ldexp(1.0, -21);
+}
+
 // Offsets of the packed per-batch staging buffer.
 struct StageLayout {
-    size_t progOff, opndOff, topk, epsMain, epsSamp, negInf, theta, qlist, counters, passCount, candCount, sampCount,
-        status, prog, opnd, total;
+    size_t progOff, opndOff, microOff, rowList, topk, epsMain, epsSamp, negInf, theta, qlist, counters, passCount,
+        candCount, sampCount, status, prog, opnd, micro, total;
 };
+
+// u32 words of one query's accumulator program at most: one op per operand plus one per program word.
+constexpr uint32_t kMaxMicro = kMaxProgram + kMaxOperands;
 
 StageLayout MakeLayout(uint32_t B) {
     StageLayout L{};
@@ -48,6 +79,8 @@ StageLayout MakeLayout(uint32_t B) {
     };
     L.progOff = take((B + 1) * 4ull);
     L.opndOff = take((B + 1) * 4ull);
+    L.microOff = take((B + 1) * 4ull);
+    L.rowList = take(kRangeMaxRows * 4ull);
     L.topk = take(B * 4ull);
     L.epsMain = take(B * 4ull);
     L.epsSamp = take(B * 4ull);
@@ -59,6 +92,7 @@ StageLayout MakeLayout(uint32_t B) {
     L.status = take(B * 4ull);
     L.prog = take(static_cast<size_t>(B) * kMaxProgram * 4ull);
     L.opnd = take(static_cast<size_t>(B) * kMaxOperands * 4ull);
+    L.micro = take(static_cast<size_t>(B) * kMaxMicro * 4ull);
     // per-segment candidate counts: every producing CTA writes its own, no clearing
     L.candCount = take(static_cast<size_t>(B) * kMaxCandSegs * 4ull);
     L.sampCount = take(static_cast<size_t>(B) * kMaxCandSegs * 4ull);
@@ -219,6 +253,52 @@ int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exp
         if (topk[q] > static_cast<uint32_t>(kMaxTopK)) m_lastStatus[q] |= kStatusTopKTooLarge;
     *maxKOut = maxK;
 
+    // The range filter when every program compiles into the accumulator form and the batch's
+    // distinct rows fit its shared-memory table; else the stack-machine kernel.
+    const DataTable& T = *m_table;
+    const bool dense = m_cfg.densePostings && T.DeviceDensePostings() != nullptr;
+    uint32_t nrows = 0, nm = 0;
+    bool range = dense;
+    if (dense) {
+        auto* microOff = reinterpret_cast<uint32_t*>(H + SL.microOff);
+        auto* rowList = reinterpret_cast<uint32_t*>(H + SL.rowList);
+        auto* micro = reinterpret_cast<uint32_t*>(H + SL.micro);
+        m_slotOfRow.assign(T.PostingRows(), 0xffffffffu);
+        std::vector<uint32_t> slots, code;
+        for (uint32_t q = 0; q < nq && range; ++q) {
+            microOff[q] = nm;
+            const uint32_t o0 = opndOff[q], o1 = opndOff[q + 1];
+            const uint32_t pl = progOff[q + 1] - progOff[q];
+            if (pl == 0) continue;  // match all
+            slots.resize(o1 - o0);
+            for (uint32_t j = o0; j < o1 && range; ++j) {
+                const uint32_t r = std::min(opnd[j], T.PostingRows() - 1);
+                if (m_slotOfRow[r] == 0xffffffffu) {
+                    if (nrows == kRangeMaxRows) {
+                        range = false;
+                        break;
+                    }
+                    m_slotOfRow[r] = nrows;
+                    rowList[nrows++] = r;
+                }
+                slots[j - o0] = m_slotOfRow[r];
+            }
+            if (!range) break;
+            code.clear();
+            bool fits = true;
+            if (!CompileMicro(prog + progOff[q], pl, slots.data(), o1 - o0, code, &fits)) {
+                m_lastStatus[q] |= kStatusBadProgram;  // as the stack machine reports it: match nothing
+                code.assign(1, kMicroZero);
+            } else if (!fits) {
+                range = false;
+                break;
+            }
+            std::memcpy(micro + nm, code.data(), code.size() * 4);
+            nm += static_cast<uint32_t>(code.size());
+        }
+        if (range) microOff[nq] = nm;
+    }
+
     cudaError_t ce = cudaSuccess;
     auto ck = [&](cudaError_t e) {
         if (ce == cudaSuccess && e != cudaSuccess) ce = e;
@@ -229,8 +309,27 @@ int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exp
     ck(cudaMemcpyAsync(D + SL.opnd, H + SL.opnd, no * 4ull, cudaMemcpyHostToDevice, stream));
     ck(cudaMemsetAsync(D + SL.counters, 0, SL.prog - SL.counters, stream));
 
-    const DataTable& T = *m_table;
-    if (m_cfg.densePostings && T.DeviceDensePostings()) {
+    if (dense) {
+        if (range) {
+            // (the offsets and the row list went with the bulk copy above)
+            if (nm) ck(cudaMemcpyAsync(D + SL.micro, H + SL.micro, nm * 4ull, cudaMemcpyHostToDevice, stream));
+            RangeFilterLaunch R{};
+            R.micro = reinterpret_cast<const uint32_t*>(D + SL.micro);
+            R.micro_off = reinterpret_cast<const uint32_t*>(D + SL.microOff);
+            R.row_list = reinterpret_cast<const uint32_t*>(D + SL.rowList);
+            R.nrows = nrows;
+            R.dense = T.DeviceDensePostings();
+            R.rows = T.PostingRows();
+            R.row_words = T.GetBitmapWords();
+            R.out = dBits;
+            R.out_stride = bitsStride;
+            R.pass_count = reinterpret_cast<uint32_t*>(D + SL.passCount);
+            R.nq = nq;
+            R.doc_num = T.GetDocNum();
+            R.sm_count = m_numSms;
+            ck(launch_filter_range(R, stream));
+            return ce == cudaSuccess ? 0 : static_cast<int>(ce);
+        }
         DenseFilterLaunch F{};
         F.prog = reinterpret_cast<const uint32_t*>(D + SL.prog);
         F.prog_off = reinterpret_cast<const uint32_t*>(D + SL.progOff);
@@ -438,7 +537,7 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         Q.eps_sample = dEpsSamp;
         Q.doc_norm_max = T.NormMax(m_tcFormat);
         Q.doc_err_max = T.ErrMax(m_tcFormat);
-        Q.acc_rel = dim * std::ldexp(1.0, -22) + std::ldexp(1.0, -21);
+        Q.acc_rel = TcAccumulationBound(m_tcFormat, dim);
         ck(launch_stage_queries(Q, stream));
     };
     stage(nullptr, nq);

@@ -101,12 +101,32 @@ class Mixture:
     def corpus_torch(self, n, device="cuda", seed=None, chunk=1 << 21):
         """The same model drawn with torch on a GPU (fast for 10M-doc corpora; a different stream of
         random numbers than corpus()). Returns host numpy arrays (vectors, tag bits)."""
+        vec = np.empty((n, self.dim), np.float32)
+
+        def sink(a, b, x):
+            vec[a:b] = x.float().cpu().numpy()
+
+        bits = self._draw_torch(n, device, seed, chunk, sink)
+        return vec, bits
+
+    def corpus_device(self, n, device="cuda", seed=None, chunk=1 << 20):
+        """As corpus_torch, but the vectors stay on the device: (torch tensor [n, dim] float32 on
+        `device`, host tag bits). For corpora larger than host memory should hold twice."""
+        import torch
+        vec = torch.empty((n, self.dim), dtype=torch.float32, device=device)
+
+        def sink(a, b, x):
+            vec[a:b] = x
+
+        bits = self._draw_torch(n, device, seed, chunk, sink)
+        return vec, bits
+
+    def _draw_torch(self, n, device, seed, chunk, sink):
         import torch
         g = torch.Generator(device=device)
         g.manual_seed(self.seed * 1000003 + 29 if seed is None else seed)
         words = (self.tag_num + 63) // 64
         centres = torch.tensor(self.centres, device=device)
-        vec = np.empty((n, self.dim), np.float32)
         bits = np.zeros((n, words), np.uint64)
         p = torch.tensor(self.p, device=device, dtype=torch.float32)
         corr_mask = torch.zeros(self.tag_num, self.n_clusters, dtype=torch.bool, device=device)
@@ -123,7 +143,8 @@ class Mixture:
             cid = torch.randint(0, self.n_clusters, (m,), generator=g, device=device)
             x = centres[cid] + self.sigma * torch.randn((m, self.dim), generator=g, device=device)
             x = x / torch.linalg.norm(x, dim=1, keepdim=True)
-            vec[a:b] = x.float().cpu().numpy()
+            sink(a, b, x)
+            del x
             u = torch.rand((m, self.tag_num), generator=g, device=device)
             prob = p.expand(m, -1)
             inside = corr_mask[:, cid].T  # [m, tag_num]
@@ -134,7 +155,7 @@ class Mixture:
                 hit = torch.nn.functional.pad(hit, (0, pad))
             w = (hit.view(m, words, 64) << shifts).sum(dim=2)  # bits are disjoint: sum == or
             bits[a:b] = w.cpu().numpy().view(np.uint64)
-        return vec, bits
+        return bits
 
     def queries(self, nq, seed=2):
         rng = np.random.default_rng(seed)

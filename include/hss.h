@@ -148,6 +148,12 @@ typedef struct hss_index_config {
  * Hash64(decimal string of t). The result is resident on deviceId. */
 int hss_table_build(int32_t deviceId, const float* vectors, const uint64_t* tagBits, uint64_t docNum, uint32_t dim,
                     uint32_t tagNum, const hss_index_config* cfg, hss_table** out);
+/* The same build from vectors already resident on deviceId: dVectors is device memory of that
+ * device ([docNum][dim] float32, copied into the table's own allocation, so the caller may free it
+ * afterwards); tagBits stays a host array. For corpora too large to stage through host memory (the
+ * reference's builder writes its .vector files from host records, vector_builder.cpp:34-176). */
+int hss_table_build_device(int32_t deviceId, const float* dVectors, const uint64_t* tagBits, uint64_t docNum,
+                           uint32_t dim, uint32_t tagNum, const hss_index_config* cfg, hss_table** out);
 /* DataTable::LoadData(deviceId, dir) (data_table.cpp:35-124) over a directory hss_table_save wrote. */
 int hss_table_load(int32_t deviceId, const char* dir, hss_table** out);
 int hss_table_save(const hss_table* table, const char* dir);
@@ -329,6 +335,17 @@ int64_t hss_posting_serialize(const uint32_t* ids, uint32_t n, uint32_t docNum, 
 int hss_filter_compile(const hss_table* table, const char* filterExpr, uint32_t* prog, uint32_t progCap,
                        uint32_t* progLen, uint32_t* rows, uint32_t rowCap, uint32_t* rowLen, uint32_t* opNum,
                        int32_t* emptyTree);
+
+/* Inspection of the accumulator form the searcher's range filter runs for one filter text: ops
+ * (one u32 each: bits 0-3 the op -- 0 push row, 1 AND row, 2 OR row, 3 AND pop, 4 OR pop, 5 NOT,
+ * 6 push zero; bit 4 complements the row; bits 16-31 the row slot) and, per slot, the posting row it
+ * reads. An accumulator holds the newest value; "push" moves it onto a stack. No counterpart in the
+ * reference, which interprets the postfix program with a stack in global memory
+ * (kernel_bitmap_text_filter.cpp:52-119); this form is the same program compiled for registers.
+ * HSS_ERR_LIMIT when the program needs a deeper stack (the searcher then runs the postfix form). */
+int hss_filter_compile_accumulator(const hss_table* table, const char* filterExpr, uint32_t* ops, uint32_t opCap,
+                                   uint32_t* opLen, uint32_t* slotRows, uint32_t slotCap, uint32_t* slotLen,
+                                   int32_t* emptyTree);
 
 /* Last error message of this thread ("" when none). */
 const char* hss_last_error(void);
