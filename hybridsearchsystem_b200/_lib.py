@@ -94,6 +94,9 @@ SIGNATURES = [
       ctypes.POINTER(IndexConfig), ctypes.POINTER(vp)]),
     ("hss_table_load", ctypes.c_int, [ctypes.c_int32, ctypes.c_char_p, ctypes.POINTER(vp)]),
     ("hss_table_save", ctypes.c_int, [vp, ctypes.c_char_p]),
+    ("hss_table_load_reference", ctypes.c_int, [ctypes.c_int32, ctypes.c_char_p, ctypes.POINTER(vp)]),
+    ("hss_table_save_reference", ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_uint32]),
+    ("hss_table_load_times", ctypes.c_int, [vp, vp, c_u64p, c_u64p, c_u32p]),
     ("hss_table_free", None, [vp]),
     ("hss_table_info", ctypes.c_int, [vp, c_u64p, c_u32p, c_u32p, c_u32p, c_u32p, c_f32p]),
     ("hss_table_posting", ctypes.c_int,

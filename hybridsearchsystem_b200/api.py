@@ -67,6 +67,30 @@ class DataTable:
     def save(self, directory):
         check(_lib.load().hss_table_save(self._h, str(directory).encode()))
 
+    @classmethod
+    def load_reference(cls, directory, device=0):
+        """An index directory in the reference's own layout (its fr_builder's output)."""
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        check(lib.hss_table_load_reference(device, str(directory).encode(), ctypes.byref(h)))
+        return cls(h.value, device)
+
+    def save_reference(self, directory, split_doc_num_zn=16):
+        """Writes the table in the reference's index layout (FP16 vectors in Zn blocks)."""
+        check(_lib.load().hss_table_save_reference(self._h, str(directory).encode(), split_doc_num_zn))
+
+    @property
+    def load_times(self):
+        """Where the last load spent its time (ms) and the bytes it moved."""
+        ms = np.zeros(6, np.float64)
+        vb, pb = ctypes.c_uint64(), ctypes.c_uint64()
+        th = ctypes.c_uint32()
+        check(_lib.load().hss_table_load_times(self._h, _np_ptr(ms), ctypes.byref(vb), ctypes.byref(pb),
+                                               ctypes.byref(th)))
+        return {"meta_ms": ms[0], "postings_read_ms": ms[1], "vectors_read_ms": ms[2], "vectors_h2d_ms": ms[3],
+                "postings_h2d_ms": ms[4], "total_ms": ms[5], "vector_bytes": vb.value, "posting_bytes": pb.value,
+                "threads": th.value}
+
     def close(self):
         if self._h:
             _lib.load().hss_table_free(self._h)

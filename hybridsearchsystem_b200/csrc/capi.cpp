@@ -274,6 +274,40 @@ int hss_table_load(int32_t deviceId, const char* dir, hss_table** out) {
     return HSS_OK;
 }
 
+int hss_table_load_reference(int32_t deviceId, const char* dir, hss_table** out) {
+    if (!dir || !out) return SetError(HSS_ERR_INVALID, "hss_table_load_reference: null argument");
+    auto t = std::make_shared<hss::DataTable>();
+    std::string err;
+    if (!t->LoadReferenceIndex(deviceId, dir, &err)) return SetError(HSS_ERR_INDEX, err);
+    *out = new hss_table{t};
+    return HSS_OK;
+}
+
+int hss_table_save_reference(const hss_table* table, const char* dir, uint32_t splitDocNumZn) {
+    if (!table || !dir) return SetError(HSS_ERR_INVALID, "hss_table_save_reference: null argument");
+    std::string err;
+    if (!table->t->SaveReferenceIndex(dir, splitDocNumZn, &err)) return SetError(HSS_ERR_INDEX, err);
+    return HSS_OK;
+}
+
+int hss_table_load_times(const hss_table* table, double* ms6, uint64_t* vectorBytes, uint64_t* postingBytes,
+                         uint32_t* threads) {
+    if (!table) return SetError(HSS_ERR_INVALID, "null table");
+    const auto& t = table->t->GetLoadTimes();
+    if (ms6) {
+        ms6[0] = t.meta;
+        ms6[1] = t.postingsRead;
+        ms6[2] = t.vectorsRead;
+        ms6[3] = t.vectorsH2D;
+        ms6[4] = t.postingsH2D;
+        ms6[5] = t.total;
+    }
+    if (vectorBytes) *vectorBytes = t.vectorBytes;
+    if (postingBytes) *postingBytes = t.postingBytes;
+    if (threads) *threads = t.threads;
+    return HSS_OK;
+}
+
 int hss_table_save(const hss_table* table, const char* dir) {
     if (!table || !dir) return SetError(HSS_ERR_INVALID, "hss_table_save: null argument");
     std::string err;

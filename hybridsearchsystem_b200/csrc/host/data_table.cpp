@@ -11,13 +11,19 @@
 //        token dict tokenNum x {u64 Hash64(token), u32 postingOffset, u32 tokenOffset} (offsets from
 //        the file start), the postings (each padded to 4 bytes), then the token literals {u32 len, bytes}.
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <dirent.h>
 #include <fstream>
 #include <sstream>
+#include <chrono>
+#include <fcntl.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
 #include <thread>
+#include <unistd.h>
 
 #include "../hss_kernels.h"
 #include "hss_host.h"
@@ -62,8 +68,200 @@ float RoundUp(double x) {
     return f;
 }
 
-std::string PostingFileName(uint32_t seg, const std::string& field) {
-    return "poissonengine_" + std::to_string(kIndexVersion) + "_" + std::to_string(seg) + "_" + field + ".posting";
+std::string PostingFileName(uint32_t seg, const std::string& field, uint32_t ver = kIndexVersion) {
+    return "poissonengine_" + std::to_string(ver) + "_" + std::to_string(seg) + "_" + field + ".posting";
+}
+
+using Clock = std::chrono::steady_clock;
+double MsSince(Clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+// A read-only mapping of a whole file.
+struct MappedFile {
+    const uint8_t* data = nullptr;
+    size_t size = 0;
+    bool Open(const std::string& path) {
+        const int fd = ::open(path.c_str(), O_RDONLY);
+        if (fd < 0) return false;
+        struct stat st {};
+        if (::fstat(fd, &st) != 0) {
+            ::close(fd);
+            return false;
+        }
+        size = static_cast<size_t>(st.st_size);
+        void* p = size ? ::mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fd, 0) : nullptr;
+        ::close(fd);
+        if (size && p == MAP_FAILED) return false;
+        data = static_cast<const uint8_t*>(p);
+        return true;
+    }
+    ~MappedFile() {
+        if (data) ::munmap(const_cast<uint8_t*>(data), size);
+    }
+};
+
+// The reference's file head (file_writer.cpp:4-26, file_header.cpp:20-38):
+// [version:1][reserved:5][extendedLen:2][extended:extendedLen].
+std::string FileHead(uint8_t ver, const std::string& ext) {
+    std::string h(1, static_cast<char>(ver));
+    h.append(5, '\0');
+    const uint16_t n = static_cast<uint16_t>(ext.size());
+    h.append(reinterpret_cast<const char*>(&n), 2);
+    h.append(ext);
+    return h;
+}
+bool ParseHead(const uint8_t* p, size_t size, uint8_t* ver, std::string* ext, size_t* bodyAt) {
+    if (size < 8) return false;
+    uint16_t n;
+    std::memcpy(&n, p + 6, 2);
+    if (size < 8ull + n) return false;
+    *ver = p[0];
+    ext->assign(reinterpret_cast<const char*>(p) + 8, n);
+    *bodyAt = 8ull + n;
+    return true;
+}
+
+// IEEE binary16 <-> binary32 as the reference's Float32ToFloat16 / Float16ToFloat32 convert
+// (trans_number.cpp:38-105): round to nearest even; inputs and results below the normal range of
+// binary16 become signed zero; overflow becomes infinity; NaN stays NaN.
+uint16_t HalfFromFloat(float f) {
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+    const uint32_t sign = (b >> 16) & 0x8000u, e = (b >> 23) & 0xffu, m = b & 0x7fffffu;
+    if (e == 0) return static_cast<uint16_t>(sign);
+    // (an infinity, whose payload is zero, becomes the NaN 0x7c01 as well, as the reference's does)
+    if (e == 0xff) return static_cast<uint16_t>(sign | 0x7c00u | std::max<uint32_t>(1u, (m >> 13) & 0x3ffu));
+    int32_t he = static_cast<int32_t>(e) - 112;  // rebias 127 -> 15
+    if (he >= 31) return static_cast<uint16_t>(sign | 0x7c00u);
+    if (he <= 0) return static_cast<uint16_t>(sign);
+    uint32_t hm = m >> 13;
+    const uint32_t rest = m & 0x1fffu;  // the 13 dropped bits: half-way is 0x1000
+    if (rest > 0x1000u || (rest == 0x1000u && (hm & 1u))) {
+        if (++hm == 0x400u) {
+            hm = 0;
+            if (++he >= 31) return static_cast<uint16_t>(sign | 0x7c00u);
+        }
+    }
+    return static_cast<uint16_t>(sign | (static_cast<uint32_t>(he) << 10) | hm);
+}
+float FloatFromHalf(uint16_t h) {
+    const uint32_t sign = (h & 0x8000u) << 16, e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+    uint32_t b;
+    if (e == 0)
+        b = sign;  // subnormal halves read as signed zero
+    else if (e == 31)
+        b = sign | 0x7f800000u | (m << 13);
+    else
+        b = sign | ((e + 112) << 23) | (m << 13);
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+
+// A small JSON reader for the reference's meta file (protobuf's JSON form of IndexMeta: objects,
+// arrays, strings and numbers).
+struct Json {
+    enum Kind { kNull, kNum, kStr, kArr, kObj } kind = kNull;
+    double num = 0;
+    std::string str;
+    std::vector<Json> arr;
+    std::vector<std::pair<std::string, Json>> obj;
+    const Json* Get(const std::string& a, const std::string& b = "") const {
+        for (const auto& kv : obj)
+            if (kv.first == a || (!b.empty() && kv.first == b)) return &kv.second;
+        return nullptr;
+    }
+};
+bool ParseJson(const std::string& s, size_t& i, Json& out, int depth = 0) {
+    auto ws = [&]() {
+        while (i < s.size() && std::isspace(static_cast<unsigned char>(s[i]))) ++i;
+    };
+    auto str = [&](std::string& o) {
+        if (i >= s.size() || s[i] != '"') return false;
+        for (++i; i < s.size() && s[i] != '"'; ++i) {
+            if (s[i] == '\\' && i + 1 < s.size()) ++i;
+            o.push_back(s[i]);
+        }
+        if (i >= s.size()) return false;
+        ++i;
+        return true;
+    };
+    if (depth > 16) return false;
+    ws();
+    if (i >= s.size()) return false;
+    if (s[i] == '{') {
+        out.kind = Json::kObj;
+        ++i;
+        ws();
+        if (i < s.size() && s[i] == '}') return ++i, true;
+        for (;;) {
+            ws();
+            std::string k;
+            if (!str(k)) return false;
+            ws();
+            if (i >= s.size() || s[i] != ':') return false;
+            ++i;
+            Json v;
+            if (!ParseJson(s, i, v, depth + 1)) return false;
+            out.obj.emplace_back(std::move(k), std::move(v));
+            ws();
+            if (i < s.size() && s[i] == ',') {
+                ++i;
+                continue;
+            }
+            if (i < s.size() && s[i] == '}') return ++i, true;
+            return false;
+        }
+    }
+    if (s[i] == '[') {
+        out.kind = Json::kArr;
+        ++i;
+        ws();
+        if (i < s.size() && s[i] == ']') return ++i, true;
+        for (;;) {
+            Json v;
+            if (!ParseJson(s, i, v, depth + 1)) return false;
+            out.arr.push_back(std::move(v));
+            ws();
+            if (i < s.size() && s[i] == ',') {
+                ++i;
+                continue;
+            }
+            if (i < s.size() && s[i] == ']') return ++i, true;
+            return false;
+        }
+    }
+    if (s[i] == '"') {
+        out.kind = Json::kStr;
+        return str(out.str);
+    }
+    size_t e = i;
+    while (e < s.size() && (std::isalnum(static_cast<unsigned char>(s[e])) || s[e] == '-' || s[e] == '+' || s[e] == '.'))
+        ++e;
+    const std::string tok = s.substr(i, e - i);
+    i = e;
+    if (tok == "null" || tok == "true" || tok == "false") return true;
+    try {
+        out.num = std::stod(tok);
+    } catch (...) {
+        return false;
+    }
+    out.kind = Json::kNum;
+    return true;
+}
+// A uint32 field of IndexMeta's JSON form: the number, or its decimal string (protobuf's printer
+// writes 64-bit integers as strings), 0 when absent (proto3 JSON omits zero values).
+uint64_t JsonUint(const Json* v) {
+    if (!v) return 0;
+    if (v->kind == Json::kNum) return v->num < 0 ? 0 : static_cast<uint64_t>(v->num);
+    if (v->kind == Json::kStr) {
+        try {
+            return std::stoull(v->str);
+        } catch (...) {
+        }
+    }
+    return 0;
 }
 
 // Minimal flat JSON object writer/reader for the meta file (string and number values only).
@@ -484,6 +682,13 @@ bool DataTable::Save(const std::string& dir, std::string* err) const {
                 static_cast<std::streamsize>(m_gdocids.size() * sizeof(int64_t)));
         if (!f || !g) return Fail(err, "write vectors / gdocids");
     }
+    return WritePostingFiles(dir, err);
+}
+
+// The posting files of the table's posting field (inverted_builder.cpp:178-250, file_writer.cpp:4-26).
+bool DataTable::WritePostingFiles(const std::string& dir, std::string* err) const {
+    const std::string pdir = dir + "/" + m_cfg.postingField;
+    ::mkdir(pdir.c_str(), 0755);
     for (uint32_t s = 0; s < m_segmentNum; ++s) {
         std::vector<uint32_t> rows;
         for (uint32_t r = 0; r + 1 < m_rows; ++r)
@@ -530,6 +735,8 @@ bool DataTable::Save(const std::string& dir, std::string* err) const {
 
 bool DataTable::LoadData(int32_t deviceId, const std::string& dir, std::string* err) {
     Release();
+    m_loadTimes = LoadTimes{};
+    const auto t0 = Clock::now();
     std::ifstream mf(dir + "/hss_meta.json");
     if (!mf) return Fail(err, "meta file not found in " + dir);
     std::stringstream ss;
@@ -556,18 +763,43 @@ bool DataTable::LoadData(int32_t deviceId, const std::string& dir, std::string* 
     m_cfg = cfg;
     m_deviceId = deviceId;
     m_postingFields = {cfg.postingField};
-    const uint32_t P = cfg.docNumPerSegment;
+    m_loadTimes.meta = MsSince(t0);
+    if (!ReadPostingFiles(dir, cfg.postingField, kIndexVersion, err)) return false;
+    m_gdocids.resize(m_docNum);
+    {
+        std::ifstream g(dir + "/gdocid.i64", std::ios::binary);
+        g.read(reinterpret_cast<char*>(m_gdocids.data()), static_cast<std::streamsize>(m_docNum * sizeof(int64_t)));
+        if (!g) return Fail(err, "gdocid.i64 missing or short");
+    }
+    MappedFile vf;
+    if (!vf.Open(dir + "/vectors.f32") || vf.size < m_docNum * m_dim * sizeof(float))
+        return Fail(err, "vectors.f32 missing or short");
+    const uint32_t dim = m_dim;
+    const bool ok = FinishRows(
+        deviceId,
+        [&](uint64_t r0, uint64_t r1, float* dst) {
+            std::memcpy(dst, vf.data + r0 * dim * sizeof(float), (r1 - r0) * dim * sizeof(float));
+        },
+        err);
+    m_loadTimes.total = MsSince(t0);
+    return ok;
+}
 
-    // postings (PostingFieldData::AddSegment / ParseTokenDict / FinishAdd)
+bool DataTable::ReadPostingFiles(const std::string& dir, const std::string& field, uint32_t ver, std::string* err) {
+    // PostingFieldData::AddSegment / ParseTokenDict / FinishAdd
+    const auto t0 = Clock::now();
+    const uint32_t P = m_cfg.docNumPerSegment;
     m_tokens.clear();
     m_tokenText.clear();
     m_tokenRow.clear();
     m_segPostings.assign(m_segmentNum, {});
     std::vector<std::vector<std::pair<uint32_t, std::pair<int64_t, uint32_t>>>> segEntries(m_segmentNum);
+    uint64_t bytes = 0;
     for (uint32_t s = 0; s < m_segmentNum; ++s) {
-        std::ifstream f(dir + "/" + cfg.postingField + "/" + PostingFileName(s, cfg.postingField), std::ios::binary);
+        std::ifstream f(dir + "/" + field + "/" + PostingFileName(s, field, ver), std::ios::binary);
         if (!f) return Fail(err, "posting file missing for segment " + std::to_string(s));
         std::string file((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+        bytes += file.size();
         if (file.size() < 13) return Fail(err, "posting file too short");
         uint16_t extLen;
         std::memcpy(&extLen, file.data() + 6, 2);
@@ -640,37 +872,312 @@ bool DataTable::LoadData(int32_t deviceId, const std::string& dir, std::string* 
             m_rowSegOffset[rowOf[e.first]][s] = e.second.first;
             m_rowSegLen[rowOf[e.first]][s] = e.second.second;
         }
+    m_loadTimes.postingsRead = MsSince(t0);
+    m_loadTimes.postingBytes = bytes;
+    return true;
+}
 
-    // vectors, doc ids, norm bound
-    std::vector<float> v(m_docNum * m_dim);
-    {
-        std::ifstream f(dir + "/vectors.f32", std::ios::binary);
-        f.read(reinterpret_cast<char*>(v.data()), static_cast<std::streamsize>(v.size() * sizeof(float)));
-        if (!f) return Fail(err, "vectors.f32 missing or short");
-        m_gdocids.resize(m_docNum);
-        std::ifstream g(dir + "/gdocid.i64", std::ios::binary);
-        g.read(reinterpret_cast<char*>(m_gdocids.data()), static_cast<std::streamsize>(m_docNum * sizeof(int64_t)));
-        if (!g) return Fail(err, "gdocid.i64 missing or short");
-    }
-    double mx = 0;
-    for (uint64_t r = 0; r < m_docNum; ++r) {
-        double s = 0;
-        for (uint32_t d = 0; d < m_dim; ++d) s += static_cast<double>(v[r * m_dim + d]) * v[r * m_dim + d];
-        mx = std::max(mx, s);
-    }
-    m_maxNorm = RoundUp(std::sqrt(mx) * (1.0 + 1e-12));
-    if (deviceId < 0) {
-        m_vectors = std::move(v);
+bool DataTable::FinishRows(int32_t deviceId, const std::function<void(uint64_t, uint64_t, float*)>& fill,
+                           std::string* err) {
+    const auto t0 = Clock::now();
+    const uint32_t dim = m_dim;
+    const unsigned T = HostThreads();
+    m_loadTimes.threads = T;
+    m_loadTimes.vectorBytes = m_docNum * dim * sizeof(float);
+    // rows [r0, r1) into dst on T threads
+    auto parallelFill = [&](uint64_t r0, uint64_t r1, float* dst) {
+        const uint64_t n = r1 - r0, per = (n + T - 1) / T;
+        std::vector<std::thread> pool;
+        for (unsigned i = 0; i < T; ++i) {
+            const uint64_t a = std::min(n, i * per), b = std::min(n, a + per);
+            if (a < b) pool.emplace_back([&, a, b]() { fill(r0 + a, r0 + b, dst + a * dim); });
+        }
+        for (auto& th : pool) th.join();
+    };
+    if (deviceId < 0) {  // host-only table
+        m_vectors.assign(m_docNum * dim, 0.0f);
+        parallelFill(0, m_docNum, m_vectors.data());
+        double mx = 0;
+        for (uint64_t r = 0; r < m_docNum; ++r) {
+            double s2 = 0;
+            for (uint32_t d = 0; d < dim; ++d) s2 += static_cast<double>(m_vectors[r * dim + d]) * m_vectors[r * dim + d];
+            mx = std::max(mx, s2);
+        }
+        m_maxNorm = RoundUp(std::sqrt(mx) * (1.0 + 1e-12));
+        m_loadTimes.vectorsRead = MsSince(t0);
         return true;
     }
     if (!CudaOk(cudaSetDevice(deviceId), err, "cudaSetDevice")) return false;
     const uint64_t rowsAlloc = GetTileNum() * 128;
-    if (!CudaOk(cudaMalloc(&m_dVectors, rowsAlloc * m_dim * sizeof(float)), err, "cudaMalloc vectors")) return false;
-    if (!CudaOk(cudaMemset(m_dVectors, 0, rowsAlloc * m_dim * sizeof(float)), err, "memset vectors")) return false;
-    if (!CudaOk(cudaMemcpy(m_dVectors, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice), err,
-                "upload vectors"))
+    if (!CudaOk(cudaMalloc(&m_dVectors, rowsAlloc * dim * sizeof(float)), err, "cudaMalloc vectors")) return false;
+    if (rowsAlloc > m_docNum &&
+        !CudaOk(cudaMemset(m_dVectors + m_docNum * dim, 0, (rowsAlloc - m_docNum) * dim * sizeof(float)), err,
+                "memset vectors"))
         return false;
-    return Upload(err);
+    // two pinned staging chunks of ~64 MB: host threads fill one while the other is copied
+    const uint64_t chunkRows = std::max<uint64_t>(1, (64ull << 20) / (dim * sizeof(float)));
+    float* pin[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    bool ok = CudaOk(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), err, "cudaStreamCreate");
+    for (int b = 0; b < 2 && ok; ++b)
+        ok = CudaOk(cudaMallocHost(&pin[b], chunkRows * dim * sizeof(float)), err, "cudaMallocHost staging") &&
+             CudaOk(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming), err, "cudaEventCreate");
+    double fillMs = 0;
+    for (uint64_t r0 = 0, c = 0; ok && r0 < m_docNum; r0 += chunkRows, ++c) {
+        const uint64_t r1 = std::min(m_docNum, r0 + chunkRows);
+        const int b = static_cast<int>(c & 1);
+        if (c >= 2) ok = CudaOk(cudaEventSynchronize(ev[b]), err, "staging copy");
+        if (!ok) break;
+        const auto f0 = Clock::now();
+        parallelFill(r0, r1, pin[b]);
+        fillMs += MsSince(f0);
+        ok = CudaOk(cudaMemcpyAsync(m_dVectors + r0 * dim, pin[b], (r1 - r0) * dim * sizeof(float),
+                                    cudaMemcpyHostToDevice, st),
+                    err, "upload vectors") &&
+             CudaOk(cudaEventRecord(ev[b], st), err, "cudaEventRecord");
+    }
+    if (ok) ok = CudaOk(cudaStreamSynchronize(st), err, "upload vectors");
+    for (int b = 0; b < 2; ++b) {
+        if (pin[b]) cudaFreeHost(pin[b]);
+        if (ev[b]) cudaEventDestroy(ev[b]);
+    }
+    if (st) cudaStreamDestroy(st);
+    if (!ok) return false;
+    m_loadTimes.vectorsRead = fillMs;
+    m_loadTimes.vectorsH2D = MsSince(t0);
+    // the corpus norm bound: per-row FP64 norms rounded up (the quantiser's FP32 mode), maximum here
+    {
+        float* norm = nullptr;
+        bool nok = CudaOk(cudaMalloc(&norm, rowsAlloc * sizeof(float)), err, "cudaMalloc norms") &&
+                   CudaOk(launch_quantize_docs(m_dVectors, rowsAlloc, m_docNum, dim, kTcTF32, nullptr, nullptr, norm,
+                                               nullptr, nullptr),
+                          err, "row norms");
+        std::vector<float> hn(rowsAlloc, 0.0f);
+        if (nok) nok = CudaOk(cudaMemcpy(hn.data(), norm, rowsAlloc * sizeof(float), cudaMemcpyDeviceToHost), err,
+                              "download norms");
+        if (norm) cudaFree(norm);
+        if (!nok) return false;
+        float m = 0.0f;
+        for (float x : hn) m = std::max(m, x);
+        m_maxNorm = m;
+    }
+    const auto u0 = Clock::now();
+    const bool up = Upload(err);
+    m_loadTimes.postingsH2D = MsSince(u0);
+    return up;
+}
+
+bool DataTable::LoadReferenceIndex(int32_t deviceId, const std::string& dir, std::string* err) {
+    Release();
+    m_loadTimes = LoadTimes{};
+    const auto t0 = Clock::now();
+    // the meta file: the first *.meta of the directory (by name); its version is the name's 2nd field
+    std::string metaName;
+    {
+        struct stat st {};
+        if (::stat(dir.c_str(), &st) != 0 || !S_ISDIR(st.st_mode)) return Fail(err, "index directory not found: " + dir);
+        std::vector<std::string> names;
+        if (DIR* d = ::opendir(dir.c_str())) {
+            while (dirent* e = ::readdir(d)) {
+                const std::string n = e->d_name;
+                if (n.size() > 5 && n.compare(n.size() - 5, 5, ".meta") == 0) names.push_back(n);
+            }
+            ::closedir(d);
+        }
+        if (names.empty()) return Fail(err, "meta file not exist in " + dir);
+        std::sort(names.begin(), names.end());
+        metaName = names[0];
+    }
+    uint32_t ver = 0;
+    {
+        const std::string stem = metaName.substr(0, metaName.size() - 5);
+        const size_t a = stem.find('_');
+        const size_t b = a == std::string::npos ? a : stem.find('_', a + 1);
+        try {
+            if (a == std::string::npos) throw 0;
+            ver = static_cast<uint32_t>(std::stoul(stem.substr(a + 1, b == std::string::npos ? b : b - a - 1)));
+        } catch (...) {
+            return Fail(err, "meta filename invalid: " + metaName);
+        }
+        if (ver > 255) return Fail(err, "meta filename invalid: " + metaName);
+    }
+    Json meta;
+    {
+        std::ifstream mf(dir + "/" + metaName);
+        std::stringstream ss;
+        ss << mf.rdbuf();
+        size_t i = 0;
+        if (!mf || !ParseJson(ss.str(), i, meta) || meta.kind != Json::kObj) return Fail(err, "malformed meta file");
+    }
+    const Json* config = meta.Get("config");
+    const Json* schema = meta.Get("schema");
+    const Json* stats = meta.Get("statistics");
+    if (!config || !schema || !stats) return Fail(err, "meta file lacks config / schema / statistics");
+    const uint64_t P = JsonUint(config->Get("docNumPerSegment", "doc_num_per_segment"));
+    const uint64_t zn = JsonUint(config->Get("splitDocNumZn", "split_doc_num_zn"));
+    m_docNum = JsonUint(stats->Get("docNum", "doc_num"));
+    m_segmentNum = static_cast<uint32_t>(JsonUint(stats->Get("segmentNum", "segment_num")));
+    const Json* pf = schema->Get("posting");
+    const Json* vfs = schema->Get("vector");
+    if (!pf || pf->kind != Json::kArr || pf->arr.empty() || pf->arr[0].kind != Json::kStr || !vfs ||
+        vfs->kind != Json::kArr || vfs->arr.empty() || vfs->arr[0].kind != Json::kStr)
+        return Fail(err, "meta schema needs a posting and a vector field");
+    if (m_docNum == 0 || m_docNum >= 0xffffffffull || P == 0 || zn == 0 ||
+        m_segmentNum != (m_docNum + P - 1) / P)
+        return Fail(err, "inconsistent meta file");
+    if (P % 128 != 0)
+        return Fail(err, "doc_num_per_segment " + std::to_string(P) +
+                             " is not a multiple of 128 (this library's segment geometry; the reference needs 8)");
+    IndexConfig cfg;
+    cfg.docNumPerSegment = static_cast<uint32_t>(P);
+    cfg.postingField = pf->arr[0].str;
+    cfg.vectorField = vfs->arr[0].str;
+    m_cfg = cfg;
+    m_deviceId = deviceId;
+    m_postingFields = {cfg.postingField};
+    m_loadTimes.meta = MsSince(t0);
+    if (!ReadPostingFiles(dir, cfg.postingField, ver, err)) return false;
+
+    // doc ids (DocIdMapping::Load, doc_id_mapping.cpp:38-114): the global-id form only
+    m_gdocids.clear();
+    m_gdocids.reserve(m_docNum);
+    for (uint32_t s = 0; s < m_segmentNum; ++s) {
+        const uint64_t segDocs = std::min<uint64_t>(P, m_docNum - s * P);
+        MappedFile f;
+        const std::string path = dir + "/id/poissonengine_" + std::to_string(ver) + "_" + std::to_string(s) + ".idm";
+        uint8_t fv;
+        std::string ext;
+        size_t at;
+        if (!f.Open(path) || !ParseHead(f.data, f.size, &fv, &ext, &at)) return Fail(err, "id mapping file: " + path);
+        if (fv != ver) return Fail(err, "id mapping version differs from the meta file's: " + path);
+        if (ext == "1")
+            return Fail(err, "string doc ids (sdocid) are not supported: results carry 64-bit global ids");
+        if (f.size - at < segDocs * 8) return Fail(err, "id mapping file short: " + path);
+        for (uint64_t l = 0; l < segDocs; ++l) {
+            uint64_t g;
+            std::memcpy(&g, f.data + at + 8 * l, 8);
+            m_gdocids.push_back(static_cast<int64_t>(g));
+        }
+    }
+    // vectors (VectorFieldData::AddSegment, vector_field_data.cpp:10-47): FP16, per segment in blocks of
+    // Zn docs; inside a block, for each group of 16 dims, the block's docs' 16 halves in doc order
+    std::vector<MappedFile> vf(m_segmentNum);
+    std::vector<size_t> bodyAt(m_segmentNum);
+    uint32_t dim = 0;
+    for (uint32_t s = 0; s < m_segmentNum; ++s) {
+        const std::string path = dir + "/" + cfg.vectorField + "/poissonengine_" + std::to_string(ver) + "_" +
+                                 std::to_string(s) + "_" + cfg.vectorField + ".vector";
+        uint8_t fv;
+        std::string ext;
+        if (!vf[s].Open(path) || !ParseHead(vf[s].data, vf[s].size, &fv, &ext, &bodyAt[s]) || ext.size() != 2)
+            return Fail(err, "vector file: " + path);
+        uint16_t d;
+        std::memcpy(&d, ext.data(), 2);
+        if (d == 0 || (dim && d != dim)) return Fail(err, "vector dimension invalid or differs between segments");
+        dim = d;
+        const uint64_t segDocs = std::min<uint64_t>(P, m_docNum - s * P);
+        const uint64_t groups = (dim + 15) / 16;
+        // the last doc's last 16-dim group must lie inside the body
+        const uint64_t l = segDocs - 1;
+        const uint64_t end = ((l / zn) * zn * groups + (zn * (groups - 1) + l % zn)) * 32 + 32;
+        if (vf[s].size - bodyAt[s] < end) return Fail(err, "vector file short: " + path);
+    }
+    if (dim % 4 != 0 || dim > 4096) return Fail(err, "vector dimension must be a multiple of 4 up to 4096");
+    m_dim = dim;
+    const uint64_t groups = (dim + 15) / 16;
+    const bool ok = FinishRows(
+        deviceId,
+        [&](uint64_t r0, uint64_t r1, float* dst) {
+            for (uint64_t g = r0; g < r1; ++g, dst += dim) {
+                const uint64_t s = g / P, l = g % P;
+                const uint8_t* body = vf[s].data + bodyAt[s];
+                const uint64_t blockAt = (l / zn) * zn * groups * 16, slot = l % zn;
+                for (uint64_t j = 0; j < groups; ++j) {
+                    const uint8_t* h = body + (blockAt + (zn * j + slot) * 16) * 2;
+                    for (uint32_t k = 0; k < 16 && j * 16 + k < dim; ++k) {
+                        uint16_t v;
+                        std::memcpy(&v, h + 2 * k, 2);
+                        dst[j * 16 + k] = FloatFromHalf(v);
+                    }
+                }
+            }
+        },
+        err);
+    m_loadTimes.total = MsSince(t0);
+    return ok;
+}
+
+bool DataTable::SaveReferenceIndex(const std::string& dir, uint32_t zn, std::string* err) const {
+    if (m_dVectors == nullptr && m_vectors.size() != m_docNum * m_dim) return Fail(err, "table not loaded");
+    if (zn == 0) return Fail(err, "splitDocNumZn must be positive");
+    if (m_dim > 0xffff) return Fail(err, "dimension does not fit the vector file's 16-bit field");
+    const uint32_t P = m_cfg.docNumPerSegment;
+    const uint8_t ver = static_cast<uint8_t>(kIndexVersion);
+    const std::string& vfield = m_cfg.vectorField;
+    const std::string& pfield = m_cfg.postingField;
+    ::mkdir(dir.c_str(), 0755);
+    ::mkdir((dir + "/id").c_str(), 0755);
+    ::mkdir((dir + "/" + vfield).c_str(), 0755);
+    // meta: IndexMeta in protobuf's JSON form (MetaBuilder::WriteMeta, meta_builder.cpp:8-27)
+    {
+        std::ofstream m(dir + "/poissonengine_" + std::to_string(kIndexVersion) + ".meta");
+        m << "{\"config\":{\"docNumPerSegment\":" << P << ",\"splitDocNumZn\":" << zn << "},\"schema\":{\"posting\":[\""
+          << pfield << "\"],\"vector\":[\"" << vfield << "\"]},\"statistics\":{\"docNum\":" << m_docNum
+          << ",\"segmentNum\":" << m_segmentNum << "}}";
+        if (!m) return Fail(err, "write meta");
+    }
+    std::vector<float> v;
+    const float* rows = m_vectors.data();
+    if (m_dVectors) {
+        v.resize(m_docNum * m_dim);
+        if (!CudaOk(cudaSetDevice(m_deviceId), err, "cudaSetDevice") ||
+            !CudaOk(cudaMemcpy(v.data(), m_dVectors, v.size() * sizeof(float), cudaMemcpyDeviceToHost), err,
+                    "download vectors"))
+            return false;
+        rows = v.data();
+    }
+    const uint32_t groups = (m_dim + 15) / 16;
+    for (uint32_t s = 0; s < m_segmentNum; ++s) {
+        const uint64_t d0 = static_cast<uint64_t>(s) * P;
+        const uint64_t segDocs = std::min<uint64_t>(P, m_docNum - d0);
+        // id mapping (IDMappingBuilder, idmapping_builder.cpp:11-70): head extension '0' (global ids)
+        {
+            std::ofstream f(dir + "/id/poissonengine_" + std::to_string(kIndexVersion) + "_" + std::to_string(s) + ".idm",
+                            std::ios::binary);
+            const std::string h = FileHead(ver, "0");
+            f.write(h.data(), static_cast<std::streamsize>(h.size()));
+            for (uint64_t l = 0; l < segDocs; ++l) {
+                const uint64_t g = static_cast<uint64_t>(m_gdocids[d0 + l]);
+                f.write(reinterpret_cast<const char*>(&g), 8);
+            }
+            if (!f) return Fail(err, "write id mapping");
+        }
+        // vectors (VectorBuilder::WriteDocVectorBlocks, vector_builder.cpp:34-72): FP16, blocks of zn
+        // docs, 16-dim groups, the tail group zero-padded; the last segment padded to whole blocks
+        {
+            const uint64_t padded = (segDocs + zn - 1) / zn * zn;
+            std::vector<uint16_t> body(padded * groups * 16, 0);
+            for (uint64_t l = 0; l < segDocs; ++l) {
+                const float* x = rows + (d0 + l) * m_dim;
+                const uint64_t blockAt = (l / zn) * zn * groups * 16, slot = l % zn;
+                for (uint32_t j = 0; j < groups; ++j)
+                    for (uint32_t k = 0; k < 16 && j * 16 + k < m_dim; ++k)
+                        body[blockAt + (zn * j + slot) * 16 + k] = HalfFromFloat(x[j * 16 + k]);
+            }
+            std::string ext(2, '\0');
+            const uint16_t d = static_cast<uint16_t>(m_dim);
+            std::memcpy(&ext[0], &d, 2);
+            std::ofstream f(dir + "/" + vfield + "/poissonengine_" + std::to_string(kIndexVersion) + "_" +
+                                std::to_string(s) + "_" + vfield + ".vector",
+                            std::ios::binary);
+            const std::string h = FileHead(ver, ext);
+            f.write(h.data(), static_cast<std::streamsize>(h.size()));
+            f.write(reinterpret_cast<const char*>(body.data()), static_cast<std::streamsize>(body.size() * 2));
+            if (!f) return Fail(err, "write vector file");
+        }
+    }
+    return WritePostingFiles(dir, err);
 }
 
 }  // namespace hss

@@ -18,6 +18,7 @@
 #include <condition_variable>
 #include <cstdint>
 #include <deque>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -214,6 +215,23 @@ class DataTable {
     // DataTable::LoadData (data_table.cpp:35-124) over the index directory Save() writes.
     bool LoadData(int32_t deviceId, const std::string& dataDir, std::string* err);
     bool Save(const std::string& dataDir, std::string* err) const;
+    // The reference's own index directory (what its fr_builder writes, read as its
+    // DataTable::LoadData does, data_table.cpp:35-124,147-186): poissonengine_<ver>.meta (IndexMeta
+    // as protobuf JSON), id/poissonengine_<ver>_<seg>.idm (u64 global ids), per vector field
+    // <field>/poissonengine_<ver>_<seg>_<field>.vector (FP16 in Zn blocks, vector_builder.cpp:34-176)
+    // and per posting field the posting files. The first vector and posting fields of the schema are
+    // loaded; the FP16 vectors become FP32 rows (exactly).
+    bool LoadReferenceIndex(int32_t deviceId, const std::string& dataDir, std::string* err);
+    // Writes that directory (the reference's builder output format; vectors rounded to FP16 as its
+    // Float32ToFloat16 rounds them, Zn = splitDocNumZn docs per block).
+    bool SaveReferenceIndex(const std::string& dataDir, uint32_t splitDocNumZn, std::string* err) const;
+    // Where the last LoadData / LoadReferenceIndex spent its time (ms) and moved its bytes.
+    struct LoadTimes {
+        double meta = 0, postingsRead = 0, vectorsRead = 0, vectorsH2D = 0, postingsH2D = 0, total = 0;
+        uint64_t vectorBytes = 0, postingBytes = 0;
+        uint32_t threads = 0;
+    };
+    const LoadTimes& GetLoadTimes() const { return m_loadTimes; }
 
     int32_t GetDeviceId() const { return m_deviceId; }
     uint64_t GetDocNum() const { return m_docNum; }
@@ -261,6 +279,14 @@ class DataTable {
 
    private:
     bool Upload(std::string* err);
+    bool WritePostingFiles(const std::string& dir, std::string* err) const;
+    // Posting files of one field (version `ver` in their names) into the host posting tables.
+    bool ReadPostingFiles(const std::string& dir, const std::string& field, uint32_t ver, std::string* err);
+    // The table's FP32 rows, produced by fill(r0, r1, dst) (rows [r0, r1) into dst, called from
+    // several threads on disjoint ranges), to the device through two pinned staging chunks (filling
+    // one while the other is copied), then the norm bound, the postings and the doc ids. With
+    // deviceId < 0 the rows are kept on the host.
+    bool FinishRows(int32_t deviceId, const std::function<void(uint64_t, uint64_t, float*)>& fill, std::string* err);
     bool BuildImpl(int32_t deviceId, const float* vectors, bool onDevice, const uint64_t* tagBits, uint64_t docNum,
                    uint32_t dim, uint32_t tagNum, const IndexConfig& cfg, std::string* err);
     void Release();
@@ -273,6 +299,7 @@ class DataTable {
     uint32_t m_rows = 0;  // token rows + 1 (the all-zero row)
     float m_maxNorm = 0.0f;
     std::unordered_set<std::string> m_postingFields;
+    LoadTimes m_loadTimes;
 
     // host side
     std::vector<float> m_vectors;            // [docNum][dim]

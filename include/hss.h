@@ -157,6 +157,23 @@ int hss_table_build_device(int32_t deviceId, const float* dVectors, const uint64
 /* DataTable::LoadData(deviceId, dir) (data_table.cpp:35-124) over a directory hss_table_save wrote. */
 int hss_table_load(int32_t deviceId, const char* dir, hss_table** out);
 int hss_table_save(const hss_table* table, const char* dir);
+/* DataTable::LoadData over the REFERENCE's own index directory, as its fr_builder writes it
+ * (data_table.cpp:35-124,147-186): poissonengine_<ver>.meta (IndexMeta, protobuf JSON form),
+ * id/poissonengine_<ver>_<seg>.idm (64-bit global ids; string ids are rejected),
+ * <vectorField>/poissonengine_<ver>_<seg>_<vectorField>.vector (FP16 in blocks of splitDocNumZn docs,
+ * vector_builder.cpp:34-176; loaded as the exact FP32 values) and the posting files of the first
+ * posting field. docNumPerSegment must be a multiple of 128 here. */
+int hss_table_load_reference(int32_t deviceId, const char* dir, hss_table** out);
+/* Writes a table in that layout (meta, id mapping, FP16 vectors rounded as the reference's
+ * Float32ToFloat16 rounds, trans_number.cpp:38-83, and the posting files); splitDocNumZn docs per
+ * vector block (the reference's loader needs dim * splitDocNumZn <= 16384). */
+int hss_table_save_reference(const hss_table* table, const char* dir, uint32_t splitDocNumZn);
+/* Where the table's load spent its time, ms: meta, posting files read, vector rows read / decoded
+ * (host, on `threads` threads), vectors to the device (reading and pinned, double-buffered copies
+ * overlapped; the whole phase), postings to the device, total; bytes of vectors and posting files.
+ * Zero for a built table. Replaces the reference's [Load] line (data_table.cpp:105-112). */
+int hss_table_load_times(const hss_table* table, double* ms6, uint64_t* vectorBytes, uint64_t* postingBytes,
+                         uint32_t* threads);
 void hss_table_free(hss_table* table);
 int hss_table_info(const hss_table* table, uint64_t* docNum, uint32_t* dim, uint32_t* segmentNum,
                    uint32_t* docNumPerSegment, uint32_t* postingRows, float* maxNorm);

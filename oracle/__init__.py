@@ -82,6 +82,10 @@ def ref():
                                          vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int32, vp, vp]
         r.ref_cpu_topk_batch.restype = ctypes.c_int
+        r.ref_f32_to_f16.argtypes = [ctypes.c_float]
+        r.ref_f32_to_f16.restype = ctypes.c_uint16
+        r.ref_f16_to_f32.argtypes = [ctypes.c_uint16]
+        r.ref_f16_to_f32.restype = ctypes.c_float
         _r = r
     return _r
 

@@ -2,6 +2,7 @@
 declares; its Hash64, posting writer, filter grammar and filter-program compiler agree with the
 golden vectors and the oracle; the index directory round-trips through the reference's posting-file
 format. No GPU is touched (tables are built host-only, device = -1)."""
+import json
 import os
 import re
 import struct
@@ -242,3 +243,78 @@ def test_accumulator_form_equals_postfix_program():
         want = oracle.eval_postfix(prog, opn, [words[int(r)] for r in rows], 16)
         got = _run_accumulator(ops, [words[int(r)] for r in slot_rows])
         assert want is not None and (got == want).all(), e
+
+
+def _ref_half(x):
+    """The reference's own Float32ToFloat16 (trans_number.cpp:38-83) of every float in x."""
+    r = oracle.ref()
+    return np.array([r.ref_f32_to_f16(float(v)) for v in np.ravel(x)], np.uint16).reshape(np.shape(x))
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="needs the reference's CPU build (oracle/_ref)")
+def test_reference_index_directory_roundtrip(tmp_path):
+    # write the reference's own index layout (fr_builder's output: meta, id mapping, FP16 Zn vector
+    # blocks, posting files) and read it back the way its DataTable::LoadData does
+    mix, vec, bits, table = _small_table(seed=7, n=3000, tags=96, p=1024)
+    vec = vec.copy()
+    # edge values of the FP16 conversion: halfway cases, values that flush to zero, overflow
+    vec[0, :8] = [1.0 + 2.0 ** -11, 1.0 + 3 * 2.0 ** -11, 2.0 ** -15, -2.0 ** -25, 65504.0, 65520.0, -70000.0, 0.0]
+    table = hss.DataTable.build(vec, bits, 96, device=-1, doc_num_per_segment=1024)
+    zn = 16
+    table.save_reference(tmp_path, zn)
+    segs, dim, n = table.info["segment_num"], vec.shape[1], vec.shape[0]
+    meta = json.loads((tmp_path / "poissonengine_1.meta").read_text())
+    assert meta == {"config": {"docNumPerSegment": 1024, "splitDocNumZn": zn},
+                    "schema": {"posting": ["content"], "vector": ["content"]},
+                    "statistics": {"docNum": n, "segmentNum": segs}}
+    want_half = _ref_half(vec)
+    groups = (dim + 15) // 16
+    for s in range(segs):
+        d0, seg_docs = s * 1024, min(1024, n - s * 1024)
+        idm = (tmp_path / "id" / f"poissonengine_1_{s}.idm").read_bytes()
+        assert idm[:9] == bytes([1, 0, 0, 0, 0, 0, 1, 0]) + b"0"
+        assert (np.frombuffer(idm[9:], np.uint64) == np.arange(d0, d0 + seg_docs)).all()
+        raw = (tmp_path / "content" / f"poissonengine_1_{s}_content.vector").read_bytes()
+        assert raw[:8] == bytes([1, 0, 0, 0, 0, 0, 2, 0]) and struct.unpack_from("<H", raw, 8)[0] == dim
+        body = np.frombuffer(raw[10:], np.uint16)
+        assert body.size == -(-seg_docs // zn) * zn * groups * 16  # the last segment padded to whole blocks
+        # doc l, dims 16j..16j+15 sit at (l // zn) * zn * groups * 16 + (zn * j + l % zn) * 16
+        # (vector_builder.cpp:52-56)
+        for l in (0, 1, zn - 1, zn, seg_docs - 1):
+            for j in range(groups):
+                at = (l // zn) * zn * groups * 16 + (zn * j + l % zn) * 16
+                assert (body[at:at + 16] == want_half[d0 + l, 16 * j:16 * j + 16]).all(), (s, l, j)
+    loaded = hss.DataTable.load_reference(tmp_path, device=-1)
+    assert loaded.info["doc_num"] == n and loaded.info["segment_num"] == segs and loaded.info["dim"] == dim
+    for t in range(0, 96, 3):
+        tok = hss.hash64(str(t))
+        for s in range(segs):
+            assert loaded.posting(tok, s) == table.posting(tok, s)
+    for e in data.make_filters(mix, 20, n_tags=(1, 4), seed=13):
+        a, b = table.compile_filter(e), loaded.compile_filter(e)
+        assert (a[0] == b[0]).all() and (a[1] == b[1]).all()
+    # the loaded rows are the FP16 values, widened exactly
+    loaded.save(tmp_path / "own")
+    got = np.fromfile(tmp_path / "own" / "vectors.f32", np.float32).reshape(n, dim)
+    r = oracle.ref()
+    want = np.array([r.ref_f16_to_f32(int(h)) for h in want_half.ravel()], np.float32).reshape(n, dim)
+    assert (got.view(np.uint32) == want.view(np.uint32)).all() or \
+        np.array_equal(np.isnan(got), np.isnan(want)) and (got[~np.isnan(got)] == want[~np.isnan(want)]).all()
+    assert loaded.load_times["vector_bytes"] == n * dim * 4
+
+
+def test_reference_index_directory_rejections(tmp_path):
+    mix, vec, bits, table = _small_table(seed=8, n=600, tags=16, p=256)
+    table.save_reference(tmp_path, 16)
+    meta = tmp_path / "poissonengine_1.meta"
+    text = meta.read_text()
+    meta.write_text(text.replace('"docNumPerSegment":256', '"docNumPerSegment":200'))
+    with pytest.raises(hss.HssError):
+        hss.DataTable.load_reference(tmp_path, device=-1)  # not a multiple of 128
+    meta.write_text(text)
+    idm = tmp_path / "id" / "poissonengine_1_0.idm"
+    raw = bytearray(idm.read_bytes())
+    raw[8:9] = b"1"  # string doc ids
+    idm.write_bytes(bytes(raw))
+    with pytest.raises(hss.HssError):
+        hss.DataTable.load_reference(tmp_path, device=-1)
