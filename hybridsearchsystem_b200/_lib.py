@@ -103,6 +103,10 @@ SIGNATURES = [
      [vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(c_u8p), c_u32p]),
     ("hss_table_device_ptrs", ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)]),
     ("hss_searcher_create", ctypes.c_int, [vp, ctypes.POINTER(SearcherConfig), ctypes.POINTER(vp)]),
+    ("hss_searcher_workspace_bytes", ctypes.c_size_t, [vp, ctypes.POINTER(SearcherConfig)]),
+    ("hss_table_prepare", ctypes.c_int, [vp, ctypes.POINTER(SearcherConfig)]),
+    ("hss_searcher_create_in", ctypes.c_int,
+     [vp, ctypes.POINTER(SearcherConfig), vp, ctypes.c_size_t, ctypes.POINTER(vp)]),
     ("hss_searcher_free", None, [vp]),
     ("hss_searcher_add_query", ctypes.c_int, [vp, ctypes.c_char_p, vp, ctypes.c_uint32, ctypes.c_uint32]),
     ("hss_searcher_batch_search", ctypes.c_int, [vp, vp, vp, vp, ctypes.c_uint32]),
@@ -114,6 +118,7 @@ SIGNATURES = [
     ("hss_searcher_last_status", ctypes.c_int, [vp, vp, ctypes.c_uint32]),
     ("hss_searcher_last_candidates", ctypes.c_int,
      [vp, ctypes.c_uint32, vp, vp, ctypes.c_uint32, c_u32p, c_f32p, c_f32p]),
+    ("hss_searcher_set_pipeline_test", ctypes.c_int, [vp, ctypes.c_uint32, ctypes.c_uint64]),
     ("hss_searcher_set_timing", ctypes.c_int, [vp, ctypes.c_int32]),
     ("hss_searcher_last_times", ctypes.c_int, [vp, vp, c_u32p, c_u32p]),
     ("hss_hash64", ctypes.c_uint64, [ctypes.c_char_p, ctypes.c_uint32]),

@@ -175,16 +175,36 @@ class Filters:
 
 class FullRecallSearcher:
     def __init__(self, table, max_batch=256, candidate_cap=1 << 18, sample_docs=32768, max_retries=4, method=0,
-                 decode_in_place=False):
+                 decode_in_place=False, workspace=None):
+        """workspace: (device pointer, bytes) of a caller-owned arena of at least workspace_bytes(...)
+        bytes (hss_searcher_create_in); None lets the searcher allocate its own."""
         lib = _lib.load()
         self.table = table
         self.dim = table.info["dim"]
         cfg = _lib.SearcherConfig(max_batch, candidate_cap, sample_docs, max_retries, method, int(decode_in_place))
         h = ctypes.c_void_p()
-        check(lib.hss_searcher_create(table._h, ctypes.byref(cfg), ctypes.byref(h)))
+        if workspace is None:
+            check(lib.hss_searcher_create(table._h, ctypes.byref(cfg), ctypes.byref(h)))
+        else:
+            check(lib.hss_searcher_create_in(table._h, ctypes.byref(cfg), ctypes.c_void_p(workspace[0]),
+                                             workspace[1], ctypes.byref(h)))
         self._h = h
         self.max_batch = max_batch
         self._pending = 0
+
+    @staticmethod
+    def workspace_bytes(table, max_batch=256, candidate_cap=1 << 18, sample_docs=32768, max_retries=4, method=0,
+                        decode_in_place=False):
+        """Device bytes of one searcher's arena for this table and configuration."""
+        cfg = _lib.SearcherConfig(max_batch, candidate_cap, sample_docs, max_retries, method, int(decode_in_place))
+        return _lib.load().hss_searcher_workspace_bytes(table._h, ctypes.byref(cfg))
+
+    @staticmethod
+    def prepare_table(table, max_batch=256, candidate_cap=1 << 18, sample_docs=32768, max_retries=4, method=0,
+                      decode_in_place=False):
+        """Builds the table's resident data a searcher of this configuration reads (hss_table_prepare)."""
+        cfg = _lib.SearcherConfig(max_batch, candidate_cap, sample_docs, max_retries, method, int(decode_in_place))
+        check(_lib.load().hss_table_prepare(table._h, ctypes.byref(cfg)))
 
     def close(self):
         if self._h:
@@ -275,6 +295,11 @@ class FullRecallSearcher:
         c = np.zeros(max(n, 1), np.uint32)
         check(_lib.load().hss_searcher_last_estimate_counts(self._h, _np_ptr(c), n))
         return c[:n]
+
+    def set_pipeline_test(self, hold_load, wait_budget_cycles=0):
+        """The next batch's first single-SM tensor-core pass withholds its hold_load-th corpus load
+        (hss_searcher_set_pipeline_test): its bounded wait runs out and the batch reports the error."""
+        check(_lib.load().hss_searcher_set_pipeline_test(self._h, hold_load, wait_budget_cycles))
 
     def set_timing(self, on=True):
         check(_lib.load().hss_searcher_set_timing(self._h, int(on)))

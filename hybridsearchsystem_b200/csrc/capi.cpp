@@ -351,18 +351,64 @@ int hss_table_device_ptrs(const hss_table* table, const float** vectors, const u
 // ---------------------------------------------------------------------------------------------
 // searcher
 
-int hss_searcher_create(hss_table* table, const hss_searcher_config* cfg, hss_searcher** out) {
-    if (!table || !out) return SetError(HSS_ERR_INVALID, "hss_searcher_create: null argument");
-    hss::SearcherConfig c;
+namespace {
+bool ToSearcherConfig(const hss_searcher_config* cfg, hss::SearcherConfig& c) {
     if (cfg) {
         if (cfg->maxBatch) c.maxBatch = cfg->maxBatch;
         if (cfg->candidateCap) c.candidateCap = cfg->candidateCap;
         if (cfg->sampleDocs) c.sampleDocs = cfg->sampleDocs;
         c.maxRetries = cfg->maxRetries;
-        if (cfg->method < 0 || cfg->method > 3) return SetError(HSS_ERR_INVALID, "unknown scoring method");
+        if (cfg->method < 0 || cfg->method > 3) return false;
         c.method = static_cast<hss::ScoreMethod>(cfg->method);
         c.densePostings = cfg->decodeInPlace == 0;
     }
+    return true;
+}
+}  // namespace
+
+size_t hss_searcher_workspace_bytes(const hss_table* table, const hss_searcher_config* cfg) {
+    hss::SearcherConfig c;
+    if (!table || !ToSearcherConfig(cfg, c)) return 0;
+    return hss::FullRecallSearcher::WorkspaceBytes(*table->t, c);
+}
+
+int hss_table_prepare(hss_table* table, const hss_searcher_config* cfg) {
+    hss::SearcherConfig c;
+    if (!table || !ToSearcherConfig(cfg, c)) return SetError(HSS_ERR_INVALID, "hss_table_prepare: bad arguments");
+    if (table->t->GetDeviceId() < 0) return SetError(HSS_ERR_INVALID, "hss_table_prepare: host-only table");
+    if (cudaSetDevice(table->t->GetDeviceId()) != cudaSuccess) return SetError(HSS_ERR_CUDA, "cudaSetDevice");
+    std::string err;
+    if (c.densePostings) {
+        size_t freeB = 0, totalB = 0;
+        if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) return SetError(HSS_ERR_CUDA, "cudaMemGetInfo");
+        if (!table->t->EnableDensePostings(static_cast<uint64_t>(freeB) / 5 * 2, &err)) return SetError(HSS_ERR_CUDA, err);
+    }
+    if (c.method != hss::ScoreMethod::SIMT_FP32 && !table->t->EnableFormat(static_cast<int>(c.method) - 1, &err))
+        return SetError(HSS_ERR_INVALID, err);
+    return HSS_OK;
+}
+
+int hss_searcher_create_in(hss_table* table, const hss_searcher_config* cfg, void* dWorkspace, size_t workspaceBytes,
+                           hss_searcher** out) {
+    if (!table || !out || !dWorkspace) return SetError(HSS_ERR_INVALID, "hss_searcher_create_in: null argument");
+    hss::SearcherConfig c;
+    if (!ToSearcherConfig(cfg, c)) return SetError(HSS_ERR_INVALID, "unknown scoring method");
+    auto* s = new hss_searcher;
+    s->t = table->t;
+    s->s = std::make_unique<hss::FullRecallSearcher>(table->t->GetDeviceId(), table->t, c, dWorkspace, workspaceBytes);
+    if (!s->s->Ok()) {
+        const std::string e = s->s->Error();
+        delete s;
+        return SetError(HSS_ERR_INVALID, e);
+    }
+    *out = s;
+    return HSS_OK;
+}
+
+int hss_searcher_create(hss_table* table, const hss_searcher_config* cfg, hss_searcher** out) {
+    if (!table || !out) return SetError(HSS_ERR_INVALID, "hss_searcher_create: null argument");
+    hss::SearcherConfig c;
+    if (!ToSearcherConfig(cfg, c)) return SetError(HSS_ERR_INVALID, "unknown scoring method");
     auto* s = new hss_searcher;
     s->t = table->t;
     s->s = std::make_unique<hss::FullRecallSearcher>(table->t->GetDeviceId(), table->t, c);
@@ -469,6 +515,13 @@ int hss_searcher_last_candidates(hss_searcher* s, uint32_t query, float* scores,
         return SetError(HSS_ERR_INVALID, "hss_searcher_last_candidates: null argument");
     const int rc = s->s->LastCandidates(query, scores, locations, cap, count, theta, eps);
     if (rc < 0) return SetError(rc == -1 ? HSS_ERR_INVALID : HSS_ERR_CUDA, "hss_searcher_last_candidates");
+    return HSS_OK;
+}
+
+int hss_searcher_set_pipeline_test(hss_searcher* s, uint32_t holdLoad, uint64_t waitBudgetCycles) {
+    if (!s) return SetError(HSS_ERR_INVALID, "null searcher");
+    if (waitBudgetCycles > (1ull << 40)) return SetError(HSS_ERR_LIMIT, "wait budget too large");
+    s->s->SetPipelineTest(holdLoad, static_cast<long long>(waitBudgetCycles));
     return HSS_OK;
 }
 

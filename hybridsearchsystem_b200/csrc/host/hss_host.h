@@ -416,8 +416,16 @@ class ThresholdModel {
 
 class FullRecallSearcher {
    public:
-    FullRecallSearcher(int32_t deviceId, std::shared_ptr<DataTable> dataTable, const SearcherConfig& cfg = {});
+    // dArena: a caller-owned device arena of at least WorkspaceBytes(table, cfg) bytes (256-byte
+    // aligned, on the table's device) that holds every device buffer of the searcher and is never
+    // freed by it; null: the searcher allocates that arena itself (one cudaMalloc).
+    FullRecallSearcher(int32_t deviceId, std::shared_ptr<DataTable> dataTable, const SearcherConfig& cfg = {},
+                       void* dArena = nullptr, size_t arenaBytes = 0);
     ~FullRecallSearcher();
+    // Device bytes of a searcher's arena for this table and configuration: the filter bitmaps,
+    // candidate lists, select workspace, doc sample, staging, results and model features (the
+    // reference's named pools hold the same kinds of blocks, gm_memory_manager.cpp:9-47).
+    static size_t WorkspaceBytes(const DataTable& table, const SearcherConfig& cfg);
     FullRecallSearcher(const FullRecallSearcher&) = delete;
     FullRecallSearcher& operator=(const FullRecallSearcher&) = delete;
 
@@ -469,6 +477,13 @@ class FullRecallSearcher {
     // without a model). Reads the device; call before the next batch.
     int LastEstimateCounts(uint32_t n, uint32_t* counts);
 
+    // Pipeline test: the next batch's first single-SM tensor-core pass stops issuing corpus loads
+    // before its holdLoad-th, with waitBudget clock cycles (0: the default) for its waits; the pass
+    // then aborts through its bounded-wait path and the batch reports the error.
+    void SetPipelineTest(uint32_t holdLoad, long long waitBudget) {
+        m_testHold = holdLoad;
+        m_testBudget = waitBudget;
+    }
     const StageTimes& LastTimes() const { return m_times; }
     void SetTiming(bool on) { m_timing = on; }
     const SearcherConfig& Config() const { return m_cfg; }
@@ -476,7 +491,14 @@ class FullRecallSearcher {
     const std::vector<int32_t>& LastStatus() const { return m_lastStatus; }
 
    private:
-    bool Allocate();
+    struct ArenaLayout {
+        size_t bits, candScore, candLoc, work, sampScore, sampLoc, stage, queries, outScore, outId, outCount, stats,
+            features, predictions, staged, qScale, error, total;
+        size_t stageBytes;
+        uint32_t sampCap;
+    };
+    static ArenaLayout Layout(const DataTable& table, const SearcherConfig& cfg);
+    bool Allocate(void* dArena, size_t arenaBytes);
     int StageAndFilter(uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks, uint64_t* dBits,
                        uint64_t bitsStride, uint32_t* maxKOut, cudaStream_t stream);
 
@@ -491,7 +513,9 @@ class FullRecallSearcher {
     std::vector<float> m_queryVectors;
     std::vector<uint32_t> m_topKs;
 
-    // device workspace (allocated once)
+    // device workspace: one arena (the caller's, or owned), carved by Layout()
+    uint8_t* m_dArena = nullptr;
+    bool m_arenaOwned = false;
     uint64_t* m_dBits = nullptr;
     float* m_dCandScore = nullptr;
     uint32_t* m_dCandLoc = nullptr;
@@ -532,6 +556,8 @@ class FullRecallSearcher {
     float* m_featuresOut = nullptr;  // Features(): stop after writing the feature rows here
     std::vector<float> m_lastTheta1, m_lastThetaA;
     uint32_t m_lastEstSegs = 0;  // list segments of the last estimation pass (0: none ran)
+    uint32_t m_testHold = 0;
+    long long m_testBudget = 0;
 };
 
 // ---------------------------------------------------------------------------------------------

@@ -101,28 +101,81 @@ StageLayout MakeLayout(uint32_t B) {
 }
 }  // namespace
 
+namespace {
+// The clamps every searcher applies to its configuration.
+SearcherConfig Normalised(SearcherConfig c) {
+    if (c.candidateCap < static_cast<uint32_t>(kMaxTopK)) c.candidateCap = kMaxTopK;
+    if (c.maxBatch == 0) c.maxBatch = 1;
+    // the tensor-core pass stages at most 2 x 128 query rows per launch
+    if (c.method != ScoreMethod::SIMT_FP32 && c.maxBatch > 256) c.maxBatch = 256;
+    if (c.maxBatch > kMaxSimtBatch) c.maxBatch = kMaxSimtBatch;
+    return c;
+}
+
+// Entries of the doc-sample buffer per query: room for the sample a K of up to 1024 asks for (see
+// SearchDevice) plus the rounding of its tiles to segments; a larger K's sample overflows it, which
+// only weakens its threshold (the stored part is still a subset).
+uint32_t SampleCap(const DataTable& T, const SearcherConfig& c) {
+    const uint64_t forK = (4ull * 1024 * T.GetDocNum() + c.candidateCap - 1) / c.candidateCap;
+    return static_cast<uint32_t>(
+        std::min<uint64_t>(std::max<uint64_t>({forK, c.sampleDocs, static_cast<uint64_t>(kMaxTopK)}), 1u << 19) +
+        128ull * kMaxCandSegs);
+}
+}  // namespace
+
+// Byte offsets of every device buffer of a searcher inside its arena (256-byte aligned).
+FullRecallSearcher::ArenaLayout FullRecallSearcher::Layout(const DataTable& T, const SearcherConfig& cfgIn) {
+    const SearcherConfig c = Normalised(cfgIn);
+    ArenaLayout A{};
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        const size_t r = at;
+        at = AlignUp(at + bytes, 256);
+        return r;
+    };
+    const uint64_t B = c.maxBatch, C = c.candidateCap, dim = T.GetDimension();
+    A.sampCap = SampleCap(T, c);
+    A.bits = take(B * T.GetBitmapWords() * 8);
+    A.candScore = take(B * C * 4);
+    A.candLoc = take(B * C * 4);
+    A.work = take(B * C * 8);
+    A.sampScore = take(B * A.sampCap * 4ull);
+    A.sampLoc = take(B * A.sampCap * 4ull);
+    A.stageBytes = MakeLayout(c.maxBatch).total;
+    A.stage = take(A.stageBytes);
+    A.queries = take(B * dim * 4);
+    A.outScore = take(B * kMaxTopK * 4ull);
+    A.outId = take(B * kMaxTopK * 8ull);
+    A.outCount = take(B * 4);
+    A.stats = take(B * static_cast<uint64_t>(kSampleStats) * sizeof(float));
+    A.features = take(B * (dim + T.PostingRows() + kFeatureTail) * sizeof(float));
+    A.predictions = take(B * sizeof(float));
+    if (c.method != ScoreMethod::SIMT_FP32) {
+        A.staged = take(256ull * dim * 4);
+        A.qScale = take(256 * sizeof(float));
+        A.error = take(sizeof(int32_t));
+    }
+    A.total = at;
+    return A;
+}
+
+size_t FullRecallSearcher::WorkspaceBytes(const DataTable& T, const SearcherConfig& cfg) {
+    return Layout(T, cfg).total;
+}
+
 FullRecallSearcher::FullRecallSearcher(int32_t deviceId, std::shared_ptr<DataTable> dataTable,
-                                       const SearcherConfig& cfg)
-    : m_deviceId(deviceId), m_table(std::move(dataTable)), m_cfg(cfg) {
+                                       const SearcherConfig& cfg, void* dArena, size_t arenaBytes)
+    : m_deviceId(deviceId), m_table(std::move(dataTable)), m_cfg(Normalised(cfg)) {
     if (!m_table) {
         m_err = "null DataTable";
         return;
     }
-    if (m_cfg.candidateCap < static_cast<uint32_t>(kMaxTopK)) m_cfg.candidateCap = kMaxTopK;
-    if (m_cfg.maxBatch == 0) m_cfg.maxBatch = 1;
-    // the tensor-core pass stages at most 2 x 128 query rows per launch
-    if (m_cfg.method != ScoreMethod::SIMT_FP32 && m_cfg.maxBatch > 256) m_cfg.maxBatch = 256;
-    if (m_cfg.maxBatch > kMaxSimtBatch) m_cfg.maxBatch = kMaxSimtBatch;
-    m_ok = Allocate();
+    m_ok = Allocate(dArena, arenaBytes);
 }
 
 FullRecallSearcher::~FullRecallSearcher() {
     cudaSetDevice(m_deviceId);
-    void* dptrs[] = {m_dBits,    m_dCandScore, m_dCandLoc, m_dWork,     m_dSampScore, m_dSampLoc, m_dStage,
-                     m_dQueries, m_dOutScore,  m_dOutId,   m_dOutCount, m_dStaged,    m_dQScale,  m_dError,
-                     m_dX,       m_dYp,        m_dStats};
-    for (void* p : dptrs)
-        if (p) cudaFree(p);
+    if (m_arenaOwned && m_dArena) cudaFree(m_dArena);
     void* hptrs[] = {m_hStage, m_hOutScore, m_hOutId, m_hOutCount, m_hThetaA};
     for (void* p : hptrs)
         if (p) cudaFreeHost(p);
@@ -130,7 +183,7 @@ FullRecallSearcher::~FullRecallSearcher() {
         if (e) cudaEventDestroy(e);
 }
 
-bool FullRecallSearcher::Allocate() {
+bool FullRecallSearcher::Allocate(void* dArena, size_t arenaBytes) {
     auto ck = [&](cudaError_t e, const char* what) {
         if (e == cudaSuccess) return true;
         m_err = std::string(what) + ": " + cudaGetErrorString(e);
@@ -140,40 +193,8 @@ bool FullRecallSearcher::Allocate() {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m_deviceId) == cudaSuccess && sms > 0)
         m_numSms = sms;
-    const uint64_t B = m_cfg.maxBatch, C = m_cfg.candidateCap;
-    const uint64_t words = m_table->GetBitmapWords();
-    // Sample buffer: room for the sample a K of up to 1024 asks for (see SearchDevice) plus the
-    // rounding of its tiles to segments; a larger K's sample overflows it, which only weakens its
-    // threshold (the stored part is still a subset).
-    const uint64_t forK = (4ull * 1024 * m_table->GetDocNum() + C - 1) / C;
-    m_sampCap = static_cast<uint32_t>(
-        std::min<uint64_t>(std::max<uint64_t>({forK, m_cfg.sampleDocs, static_cast<uint64_t>(kMaxTopK)}), 1u << 19) +
-        128ull * kMaxCandSegs);
-    const uint32_t dim = m_table->GetDimension();
-    const StageLayout L = MakeLayout(static_cast<uint32_t>(B));
-    m_stageBytes = L.total;
-    if (!ck(cudaMalloc(&m_dBits, B * words * 8), "cudaMalloc bitmaps")) return false;
-    if (!ck(cudaMalloc(&m_dCandScore, B * C * 4), "cudaMalloc candidates")) return false;
-    if (!ck(cudaMalloc(&m_dCandLoc, B * C * 4), "cudaMalloc candidates")) return false;
-    if (!ck(cudaMalloc(&m_dWork, B * C * 8), "cudaMalloc select workspace")) return false;
-    if (!ck(cudaMalloc(&m_dSampScore, B * m_sampCap * 4ull), "cudaMalloc sample")) return false;
-    if (!ck(cudaMalloc(&m_dSampLoc, B * m_sampCap * 4ull), "cudaMalloc sample")) return false;
-    if (!ck(cudaMalloc(&m_dStage, m_stageBytes), "cudaMalloc staging")) return false;
-    if (!ck(cudaMallocHost(&m_hStage, m_stageBytes), "cudaMallocHost staging")) return false;
-    std::memset(m_hStage, 0, m_stageBytes);
-    float* negInf = reinterpret_cast<float*>(m_hStage + L.negInf);
-    for (uint64_t i = 0; i < B; ++i) negInf[i] = -INFINITY;
-    if (!ck(cudaMalloc(&m_dQueries, B * dim * 4ull), "cudaMalloc queries")) return false;
-    if (!ck(cudaMalloc(&m_dOutScore, B * kMaxTopK * 4ull), "cudaMalloc results")) return false;
-    if (!ck(cudaMalloc(&m_dOutId, B * kMaxTopK * 8ull), "cudaMalloc results")) return false;
-    if (!ck(cudaMalloc(&m_dOutCount, B * 4ull), "cudaMalloc results")) return false;
-    if (!ck(cudaMallocHost(&m_hOutScore, B * kMaxTopK * 4ull), "cudaMallocHost results")) return false;
-    if (!ck(cudaMallocHost(&m_hOutId, B * kMaxTopK * 8ull), "cudaMallocHost results")) return false;
-    if (!ck(cudaMallocHost(&m_hOutCount, B * 4ull), "cudaMallocHost results")) return false;
-    if (!ck(cudaMalloc(&m_dStats, B * static_cast<uint64_t>(kSampleStats) * sizeof(float)), "cudaMalloc sample statistics")) return false;
-    if (!ck(cudaMallocHost(&m_hThetaA, B * sizeof(float)), "cudaMallocHost thresholds")) return false;
-    for (auto& e : m_ev)
-        if (!ck(cudaEventCreate(&e), "cudaEventCreate")) return false;
+    // Index-side residency first (it belongs to the table and is shared by its searchers): the
+    // dense posting matrix and the copy of the rows the tensor-core pass reads.
     if (m_cfg.densePostings) {
         // every posting decoded once into a dense bitmap when that takes at most 40% of free memory
         size_t freeB = 0, totalB = 0;
@@ -184,10 +205,65 @@ bool FullRecallSearcher::Allocate() {
         m_tcFormat = static_cast<int>(m_cfg.method) - 1;
         if (!m_table->EnableFormat(m_tcFormat, &m_err)) return false;
         const uint32_t elem = m_tcFormat == kTcTF32 ? 4 : (m_tcFormat == kTcBF16 ? 2 : 1);
-        m_tcKblocks = dim * elem / 128;
-        if (!ck(cudaMalloc(&m_dStaged, 256ull * dim * 4), "cudaMalloc staged queries")) return false;
-        if (!ck(cudaMalloc(&m_dQScale, 256 * sizeof(float)), "cudaMalloc query scales")) return false;
-        if (!ck(cudaMalloc(&m_dError, sizeof(int32_t)), "cudaMalloc error word")) return false;
+        m_tcKblocks = m_table->GetDimension() * elem / 128;
+    }
+    // The searcher's own device buffers: one arena, the caller's or allocated here.
+    const ArenaLayout A = Layout(*m_table, m_cfg);
+    if (dArena) {
+        cudaPointerAttributes at{};
+        if (arenaBytes < A.total || (reinterpret_cast<uintptr_t>(dArena) & 255u)) {
+            m_err = "workspace smaller than hss_searcher_workspace_bytes() or not 256-byte aligned";
+            return false;
+        }
+        if (cudaPointerGetAttributes(&at, dArena) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+            at.device != m_deviceId) {
+            cudaGetLastError();
+            m_err = "workspace is not device memory of the table's device";
+            return false;
+        }
+        m_dArena = static_cast<uint8_t*>(dArena);
+        m_arenaOwned = false;
+    } else {
+        void* p = nullptr;
+        if (!ck(cudaMalloc(&p, A.total), "cudaMalloc searcher workspace")) return false;
+        m_dArena = static_cast<uint8_t*>(p);
+        m_arenaOwned = true;
+    }
+    uint8_t* W = m_dArena;
+    m_sampCap = A.sampCap;
+    m_stageBytes = A.stageBytes;
+    m_dBits = reinterpret_cast<uint64_t*>(W + A.bits);
+    m_dCandScore = reinterpret_cast<float*>(W + A.candScore);
+    m_dCandLoc = reinterpret_cast<uint32_t*>(W + A.candLoc);
+    m_dWork = reinterpret_cast<unsigned long long*>(W + A.work);
+    m_dSampScore = reinterpret_cast<float*>(W + A.sampScore);
+    m_dSampLoc = reinterpret_cast<uint32_t*>(W + A.sampLoc);
+    m_dStage = W + A.stage;
+    m_dQueries = reinterpret_cast<float*>(W + A.queries);
+    m_dOutScore = reinterpret_cast<float*>(W + A.outScore);
+    m_dOutId = reinterpret_cast<int64_t*>(W + A.outId);
+    m_dOutCount = reinterpret_cast<uint32_t*>(W + A.outCount);
+    m_dStats = reinterpret_cast<float*>(W + A.stats);
+    m_dX = reinterpret_cast<float*>(W + A.features);
+    m_dYp = reinterpret_cast<float*>(W + A.predictions);
+
+    const uint64_t B = m_cfg.maxBatch;
+    if (!ck(cudaMallocHost(&m_hStage, m_stageBytes), "cudaMallocHost staging")) return false;
+    std::memset(m_hStage, 0, m_stageBytes);
+    const StageLayout L = MakeLayout(static_cast<uint32_t>(B));
+    float* negInf = reinterpret_cast<float*>(m_hStage + L.negInf);
+    for (uint64_t i = 0; i < B; ++i) negInf[i] = -INFINITY;
+    if (!ck(cudaMallocHost(&m_hOutScore, B * kMaxTopK * 4ull), "cudaMallocHost results")) return false;
+    if (!ck(cudaMallocHost(&m_hOutId, B * kMaxTopK * 8ull), "cudaMallocHost results")) return false;
+    if (!ck(cudaMallocHost(&m_hOutCount, B * 4ull), "cudaMallocHost results")) return false;
+    if (!ck(cudaMallocHost(&m_hThetaA, B * sizeof(float)), "cudaMallocHost thresholds")) return false;
+    for (auto& e : m_ev)
+        if (!ck(cudaEventCreate(&e), "cudaEventCreate")) return false;
+    if (m_tcFormat >= 0) {
+        const uint32_t dim = m_table->GetDimension();
+        m_dStaged = W + A.staged;
+        m_dQScale = reinterpret_cast<float*>(W + A.qScale);
+        m_dError = reinterpret_cast<int32_t*>(W + A.error);
         if (!ck(cudaMemset(m_dError, 0, sizeof(int32_t)), "cudaMemset error word")) return false;
         if (!make_tc_map(&m_docMap, m_tcFormat, m_table->DeviceRows(m_tcFormat), m_table->GetTileNum() * 128, dim) ||
             !make_tc_map(&m_qryMap, m_tcFormat, m_dStaged, 256, dim)) {
@@ -413,14 +489,6 @@ int FullRecallSearcher::SetThresholdModel(std::shared_ptr<ThresholdModel> model,
         m_err = "threshold model does not fit this searcher (feature width or device)";
         return -1;
     }
-    if (model && !m_dX) {
-        if (cudaSetDevice(m_deviceId) != cudaSuccess ||
-            cudaMalloc(&m_dX, static_cast<size_t>(m_cfg.maxBatch) * FeatureDim() * sizeof(float)) != cudaSuccess ||
-            cudaMalloc(&m_dYp, static_cast<size_t>(m_cfg.maxBatch) * sizeof(float)) != cudaSuccess) {
-            m_err = "cudaMalloc model features";
-            return -2;
-        }
-    }
     m_model = std::move(model);
     m_margin = margin;
     return 0;
@@ -620,6 +688,11 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         C.tile_skip = skip;
         C.tiles128 = tiles;
         C.error = m_dError;
+        if (m_testHold && tc_tile_docs(rows, m_tcKblocks) == 128u) {  // the single-SM kernel only
+            C.hold_load = m_testHold;
+            C.wait_budget = m_testBudget;
+            m_testHold = 0;
+        }
         ck(launch_tc_cand(C, m_docMap, m_qryMap, m_numSms, stream));
     };
 

@@ -200,6 +200,11 @@ struct TcCandLaunch {
     uint32_t tile_skip;
     uint64_t tiles128;         // 128-doc tiles of the corpus (rows of the tensor map / 128)
     int32_t* error;            // device error bits (bounded waits that expired)
+    // Pipeline test knobs (single-SM kernel): wait_budget > 0 replaces the clock budget of the waits
+    // that can abort the pass; hold_load > 0 makes the producer stop before issuing its
+    // (hold_load)-th corpus k-block load, so the MMA issuer's wait for it runs out.
+    long long wait_budget;
+    uint32_t hold_load;
 };
 
 // Whether a tensor-core pass over rows of `kblocks` 128-byte k-blocks streams the queries' k-blocks

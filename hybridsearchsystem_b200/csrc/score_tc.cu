@@ -78,11 +78,12 @@ __device__ inline bool mbar_wait_drain(unsigned long long* bar, uint32_t parity)
 
 // Bounded wait for the phase of `parity`; false (and the CTA marked aborted) when the budget runs out
 // or another role already aborted.
-__device__ inline bool mbar_wait(unsigned long long* bar, uint32_t parity, TcShared& S, int32_t* err, int code) {
+__device__ inline bool mbar_wait(unsigned long long* bar, uint32_t parity, TcShared& S, int32_t* err, int code,
+                                 long long budget = kWaitBudget) {
     const long long t0 = clock64();
     while (!mbar_try(bar, parity)) {
         if (S.abort) return false;
-        if (clock64() - t0 > kWaitBudget) {
+        if (clock64() - t0 > budget) {
             S.abort = 1;
             if (err) atomicOr(err, code);
             return false;
@@ -426,6 +427,7 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
     fence_after();
     const uint32_t tmem = S.tmem_base;
     const uint64_t ntiles = L.tile_count;
+    const long long budget = L.wait_budget > 0 ? L.wait_budget : kWaitBudget;
 
     if (warp == 0) {
         if (lane == 0) {
@@ -436,12 +438,17 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
                     tma_load_2d(qsm + (static_cast<size_t>(h) * kb_n + kb) * kStageBytes, &qry_map,
                                 static_cast<int>(kb * (128 / Fmt<F>::elem)), h * kRows, &S.qbar);
             uint32_t n = 0;
+            bool held = false;
             TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, blockIdx.x, gridDim.x);
-            for (uint64_t it = blockIdx.x; it < ntiles && !S.abort; it += gridDim.x, walk.advance()) {
+            for (uint64_t it = blockIdx.x; it < ntiles && !S.abort && !held; it += gridDim.x, walk.advance()) {
                 const int y = static_cast<int>(walk.tile() * kRows);
                 for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
-                    if (!mbar_wait(&S.empty[s], ph ^ 1u, S, L.error, 1)) break;
+                    if (L.hold_load && n + 1 >= L.hold_load) {  // pipeline test: stop issuing here
+                        held = true;
+                        break;
+                    }
+                    if (!mbar_wait(&S.empty[s], ph ^ 1u, S, L.error, 1, budget)) break;
                     mbar_expect_tx(&S.full[s], kStageBytes);
                     tma_load_2d(ring + static_cast<size_t>(s) * kStageBytes, &doc_map,
                                 static_cast<int>(kb * (128 / Fmt<F>::elem)), y, &S.full[s]);
@@ -452,15 +459,15 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
     } else if (warp == 1) {
         if (lane == 0) {
             uint32_t n = 0, iter = 0;
-            if (!mbar_wait(&S.qbar, 0, S, L.error, 2)) iter = 0xffffffffu;  // nothing to issue
+            if (!mbar_wait(&S.qbar, 0, S, L.error, 2, budget)) iter = 0xffffffffu;  // nothing to issue
             for (uint64_t it = blockIdx.x; iter != 0xffffffffu && it < ntiles && !S.abort; it += gridDim.x, ++iter) {
                 const uint32_t buf = iter & 1u;
-                if (!mbar_wait(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4)) break;
+                if (!mbar_wait(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4, budget)) break;
                 fence_after();
                 bool ok = true;
                 for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
-                    if (!mbar_wait(&S.full[s], ph, S, L.error, 8)) {
+                    if (!mbar_wait(&S.full[s], ph, S, L.error, 8, budget)) {
                         ok = false;
                         break;
                     }
@@ -530,7 +537,7 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
             for (int c = 0; c < 2; ++c) live[c] = __any_sync(0xffffffffu, m[c] != 0u);
             // every lane waits; the warp leaves together if any lane gave up (the warp collectives
             // below need all 32 lanes)
-            const bool ready = mbar_wait(&S.acc_full[buf], (iter >> 1) & 1u, S, L.error, 16);
+            const bool ready = mbar_wait(&S.acc_full[buf], (iter >> 1) & 1u, S, L.error, 16, budget);
             if (!__all_sync(0xffffffffu, ready)) break;
             fence_after();
             const uint32_t tbase = tmem + ((sub * 32u) << 16) + (buf * H + half) * 128u + colh * 64u;

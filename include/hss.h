@@ -207,6 +207,26 @@ typedef struct hss_searcher_config {
 
 /* cfg may be NULL for the defaults. The searcher allocates its whole device arena here. */
 int hss_searcher_create(hss_table* table, const hss_searcher_config* cfg, hss_searcher** out);
+
+/* Caller-owned workspace (the reference's ownership model: the host owns every device block, the
+ * library is given sizes; GmMemoryPool / GmMemoryManager, gm_memory_pool.h:40-181,
+ * gm_memory_manager.cpp:9-47, named pools of full_recall_result.h:9-20).
+ * hss_searcher_workspace_bytes: device bytes of one searcher's arena for this table and config --
+ * filter bitmaps, candidate lists, select workspace, doc sample, per-batch staging, results and
+ * model features; 0 for bad arguments. It grows with maxBatch x candidateCap.
+ * hss_table_prepare: builds the table's resident data a searcher of this config reads (the dense
+ * posting matrix unless decodeInPlace; the BF16 / E4M3 copy of the rows for methods 2 / 3), which
+ * belongs to the table and is shared by all its searchers; call it at load time so that searcher
+ * creation allocates no device memory.
+ * hss_searcher_create_in: hss_searcher_create on a caller-owned device arena of at least
+ * hss_searcher_workspace_bytes bytes, 256-byte aligned, on the table's device. The searcher keeps
+ * every device buffer there, never frees it, and allocates only its pinned host staging (and, if
+ * hss_table_prepare was not called, the table's resident data). The arena must outlive the searcher
+ * and may not be shared with another searcher that runs at the same time. */
+size_t hss_searcher_workspace_bytes(const hss_table* table, const hss_searcher_config* cfg);
+int hss_table_prepare(hss_table* table, const hss_searcher_config* cfg);
+int hss_searcher_create_in(hss_table* table, const hss_searcher_config* cfg, void* dWorkspace, size_t workspaceBytes,
+                           hss_searcher** out);
 void hss_searcher_free(hss_searcher* s);
 
 /* FullRecallSearcher::AddQuery (full_recall_searcher.cpp:93-105): the filter is given as text in the
@@ -245,6 +265,13 @@ int hss_searcher_last_candidates(hss_searcher* s, uint32_t query, float* scores,
 /* Stage times of the last batch in ms (filter, sample, candidates, select, total; needs
  * hss_searcher_set_timing(s, 1)), candidate re-runs and kernel launches. */
 int hss_searcher_set_timing(hss_searcher* s, int32_t on);
+/* Test of the tensor-core pass's bounded waits (no counterpart in the reference, whose kernels
+ * have no error channel). The next batch's first single-SM tensor-core candidate pass (<= 128
+ * queries) stops issuing corpus loads before its holdLoad-th, so its MMA issuer's wait for that load
+ * runs out after waitBudgetCycles clock cycles (0: the default, about 2 s). The pass records an
+ * error bit, drains its copies and MMAs, frees its tensor memory and returns; the batch returns
+ * HSS_ERR_CUDA ("timed out waiting on its pipeline"), and the searcher stays usable. */
+int hss_searcher_set_pipeline_test(hss_searcher* s, uint32_t holdLoad, uint64_t waitBudgetCycles);
 int hss_searcher_last_times(const hss_searcher* s, float* ms5, uint32_t* retries, uint32_t* launches);
 
 /* ---- learned threshold predictor ----

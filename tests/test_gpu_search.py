@@ -170,3 +170,36 @@ def test_bad_filter_is_reported_not_run(torch_cuda):
     assert ei.value.code == _lib.HSS_ERR_PARSE
     with pytest.raises(hss.HssError):
         s.add_query("1", np.zeros(8, np.float32), 10)  # wrong dimension
+
+
+@pytest.mark.parametrize("method", [0, 2], ids=["simt", "bf16"])
+def test_searcher_in_caller_owned_workspace(torch_cuda, method):
+    # the reference's ownership model: the caller sizes and owns the device arena; after the table's
+    # resident data is prepared, creating the searcher allocates no device memory
+    torch = torch_cuda
+    mix = data.Mixture(128, 64, (1e-3, 0.5), seed=31)
+    vec, bits, _ = mix.corpus(20000, seed=32)
+    table = hss.DataTable.build(vec, bits, 64, device=0, doc_num_per_segment=8192)
+    nq = 48
+    cfg = dict(max_batch=64, candidate_cap=1 << 16, method=method)
+    nbytes = hss.FullRecallSearcher.workspace_bytes(table, **cfg)
+    assert nbytes > 64 * (1 << 16) * 16
+    hss.FullRecallSearcher.prepare_table(table, **cfg)
+    arena = torch.empty(nbytes + 256, dtype=torch.uint8, device="cuda:0")
+    base = (arena.data_ptr() + 255) // 256 * 256
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    s = hss.FullRecallSearcher(table, workspace=(base, nbytes), **cfg)
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free0 - free1 < (4 << 20), (free0, free1)  # no device arena of its own
+    q = mix.queries(nq, seed=33)
+    exprs = data.make_filters(mix, nq, n_tags=(1, 4), seed=34)
+    for a, e in zip(q, exprs):
+        s.add_query(e, a, 100)
+    res = s.batch_search()
+    _check(res, oracle.topk(q, exprs, [100] * nq, vec, bits, threads=8), nq)
+    s.close()
+    with pytest.raises(hss.HssError):
+        hss.FullRecallSearcher(table, workspace=(base, nbytes - 4096), **cfg)  # too small
+    with pytest.raises(hss.HssError):
+        hss.FullRecallSearcher(table, workspace=(base + 64, nbytes), **cfg)  # misaligned

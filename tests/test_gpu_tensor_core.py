@@ -126,3 +126,30 @@ def test_long_vectors_are_exact(torch_cuda, method, nq):
         assert int(counts[i]) == c, (method, i)
         assert (ids[i][:c] == wi[i][:c]).all(), (method, i)
         assert (scores[i][:c].view(np.uint32) == ws[i][:c].view(np.uint32)).all(), (method, i)
+
+
+def test_pipeline_wait_runs_out_and_the_searcher_recovers(torch_cuda):
+    # The single-SM pass's producer stops before its 3rd corpus load, so the MMA issuer's bounded wait
+    # (about 1 ms of clock here) runs out: the pass records its error bit, drains, frees its tensor
+    # memory and returns; the batch reports the error and the same searcher's next batch is exact.
+    # Nothing faults: the wait ends by its own budget.
+    mix, vec, bits = _corpus()
+    table = hss.DataTable.build(vec, bits, 64, device=0, doc_num_per_segment=8192)
+    nq = 40
+    q = mix.queries(nq, seed=71)
+    exprs = data.make_filters(mix, nq, n_tags=(1, 3), seed=72)
+    s = hss.FullRecallSearcher(table, max_batch=64, method=METHODS["bf16"])
+    s.set_pipeline_test(3, 2_000_000)
+    for a, e in zip(q, exprs):
+        s.add_query(e, a, 50)
+    with pytest.raises(hss.HssError) as err:
+        s.batch_search()
+    assert err.value.code == hss._lib.HSS_ERR_CUDA and "timed out" in str(err.value)
+    for a, e in zip(q, exprs):
+        s.add_query(e, a, 50)
+    scores, ids, counts = s.batch_search()
+    ws, wi, wc = oracle.topk(q, exprs, 50, vec, bits, threads=8)
+    for i in range(nq):
+        c = int(wc[i])
+        assert int(counts[i]) == c
+        assert (ids[i][:c] == wi[i][:c]).all() and (scores[i][:c].view(np.uint32) == ws[i][:c].view(np.uint32)).all()

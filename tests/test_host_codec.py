@@ -318,3 +318,15 @@ def test_reference_index_directory_rejections(tmp_path):
     idm.write_bytes(bytes(raw))
     with pytest.raises(hss.HssError):
         hss.DataTable.load_reference(tmp_path, device=-1)
+
+
+def test_searcher_workspace_bytes_follow_the_configuration():
+    _, _, _, table = _small_table(seed=11, n=4000, tags=32, p=1024)
+    ws = hss.FullRecallSearcher.workspace_bytes
+    small = ws(table, max_batch=16, candidate_cap=1 << 14)
+    assert small > 16 * (1 << 14) * 16  # candidate lists (score + location) and the select workspace
+    assert ws(table, max_batch=32, candidate_cap=1 << 14) > small
+    assert ws(table, max_batch=16, candidate_cap=1 << 15) > small
+    # the tensor-core methods add the staged query tile; the candidate cap never drops below 4096
+    assert ws(table, max_batch=16, candidate_cap=1 << 14, method=2) > small
+    assert ws(table, max_batch=16, candidate_cap=1) == ws(table, max_batch=16, candidate_cap=4096)
