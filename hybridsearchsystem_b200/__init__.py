@@ -6,10 +6,10 @@ FullRecallSearcher / QueryNode interface.
 from . import data
 from ._lib import HssError, load
 from .api import (DataTable, Filters, FullRecallSearcher, Server, ThresholdModel, aggregator, aggregator_noalloc, aggregator_workspace_size,
-                  bitmap_text_filter, device_count, hash64, posting_bitlist_to_set, posting_serialize, topk,
+                  bitmap_text_filter, device_count, hash64, merge_shards, posting_bitlist_to_set, posting_serialize, topk,
                   vector_score)
 
 __all__ = ["DataTable", "Filters", "FullRecallSearcher", "HssError", "Server", "ThresholdModel", "aggregator", "aggregator_noalloc",
            "aggregator_workspace_size",
-           "bitmap_text_filter", "data", "device_count", "hash64", "load", "posting_bitlist_to_set",
+           "bitmap_text_filter", "data", "device_count", "hash64", "load", "merge_shards", "posting_bitlist_to_set",
            "posting_serialize", "topk", "vector_score"]

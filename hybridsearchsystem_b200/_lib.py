@@ -86,6 +86,9 @@ SIGNATURES = [
      [vp, vp, vp, vp, vp, vp, ctypes.c_uint32, vp, ctypes.c_size_t, vp]),
     ("hss_aggregator_launch_noalloc", ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_uint32, vp]),
     ("hss_topk_launch", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32, vp, vp, vp, vp]),
+    ("hss_merge_shards_launch", ctypes.c_int,
+     [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp, ctypes.c_uint32,
+      vp]),
     ("hss_table_build", ctypes.c_int,
      [ctypes.c_int32, vp, vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
       ctypes.POINTER(IndexConfig), ctypes.POINTER(vp)]),

@@ -471,6 +471,16 @@ def topk(d_scores, d_locs, d_count, k, d_out_scores, d_out_locs, d_out_count, st
     check(_lib.load().hss_topk_launch(d_scores, d_locs, d_count, k, d_out_scores, d_out_locs, d_out_count, stream))
 
 
+def merge_shards(d_scores, d_ids, d_counts, nq, in_stride, k, d_out_scores, d_out_ids, d_out_counts, out_stride,
+                 stream=0):
+    """hss_merge_shards_launch: per-shard sorted results (lists of device pointers) merged into the
+    global top-k on the device."""
+    n = len(d_scores)
+    arr = lambda xs: (ctypes.c_void_p * n)(*xs)
+    check(_lib.load().hss_merge_shards_launch(arr(d_scores), arr(d_ids), arr(d_counts), n, nq, in_stride, k,
+                                              d_out_scores, d_out_ids, d_out_counts, out_stride, stream))
+
+
 def hash64(token):
     b = token.encode() if isinstance(token, str) else bytes(token)
     return _lib.load().hss_hash64(b, len(b))

@@ -225,6 +225,32 @@ int hss_topk_launch(const float* scores, const uint32_t* locations, const uint32
     return FromCuda(hss::launch_topk_op(scores, locations, count, topK, outScores, outLocations, outCount, S(stream)));
 }
 
+int hss_merge_shards_launch(const float* const* shardScores, const int64_t* const* shardIds,
+                            const uint32_t* const* shardCounts, uint32_t shards, uint32_t nq, uint32_t inStride,
+                            uint32_t topK, float* outScores, int64_t* outIds, uint32_t* outCounts, uint32_t outStride,
+                            hss_stream_t stream) {
+    if (!shardScores || !shardIds || !shardCounts || !outScores || !outIds || !outCounts || shards == 0)
+        return SetError(HSS_ERR_INVALID, "hss_merge_shards_launch: null argument");
+    if (shards > hss::kMaxShards || topK > static_cast<uint32_t>(hss::kMaxTopK))
+        return SetError(HSS_ERR_LIMIT, "shards beyond HSS_MAX_SHARDS or topK beyond HSS_MAX_TOPK");
+    if (topK > outStride) return SetError(HSS_ERR_INVALID, "topK larger than the output stride");
+    hss::ShardMergeLaunch L{};
+    for (uint32_t s = 0; s < shards; ++s) {
+        L.scores[s] = shardScores[s];
+        L.ids[s] = shardIds[s];
+        L.counts[s] = shardCounts[s];
+    }
+    L.shards = shards;
+    L.nq = nq;
+    L.in_stride = inStride;
+    L.topk = topK;
+    L.out_score = outScores;
+    L.out_id = outIds;
+    L.out_count = outCounts;
+    L.out_stride = outStride;
+    return FromCuda(hss::launch_merge_shards(L, S(stream)));
+}
+
 // ---------------------------------------------------------------------------------------------
 // index
 

@@ -294,6 +294,20 @@ cudaError_t launch_features(const FeatureLaunch& L, cudaStream_t stream);
 cudaError_t launch_predict_theta(const float* y, const float* theta, uint32_t nq, float scale, float shift,
                                  float margin, float* theta_a, cudaStream_t stream);
 
+// Cross-shard merge of sorted per-shard top-K lists (select.cu).
+constexpr uint32_t kMaxShards = 64;
+struct ShardMergeLaunch {
+    const float* scores[kMaxShards];    // shard s: [nq][in_stride], score descending
+    const int64_t* ids[kMaxShards];     // shard s: [nq][in_stride]
+    const uint32_t* counts[kMaxShards]; // shard s: [nq]
+    uint32_t shards, nq, in_stride, topk;
+    float* out_score;                   // [nq][out_stride]
+    int64_t* out_id;
+    uint32_t* out_count;                // [nq]
+    uint32_t out_stride;
+};
+cudaError_t launch_merge_shards(const ShardMergeLaunch& L, cudaStream_t stream);
+
 cudaError_t launch_topk_op(const float* scores, const uint32_t* locs, const uint32_t* count, uint32_t k,
                            float* out_scores, uint32_t* out_locs, uint32_t* out_count, cudaStream_t stream);
 

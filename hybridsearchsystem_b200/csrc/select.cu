@@ -835,4 +835,73 @@ cudaError_t launch_topk_op(const float* scores, const uint32_t* locs, const uint
     return cudaGetLastError();
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Cross-shard merge (the reference's k-way merge of per-shard results, run_context.cpp:86-118 and
+// 237-270): the shards' sorted lists are merged by score descending, equal scores taking the lower
+// shard first (within a shard, list order). Every entry finds its output position directly: its
+// index in its own list plus, for every other shard, how many of that shard's entries precede it
+// (a binary search on the score), so one thread places one entry and no thread waits on another.
+namespace {
+// Entries of a list sorted by score descending that come before score x: those with score > x, or
+// with score >= x when `ties_first` (a lower shard).
+__device__ inline uint32_t preceding(const float* sc, uint32_t n, float x, bool ties_first) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const float v = sc[mid];
+        if (ties_first ? (v >= x) : (v > x))
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) merge_shards_kernel(const __grid_constant__ ShardMergeLaunch L) {
+    const uint32_t q = blockIdx.x;
+    __shared__ uint32_t s_n[kMaxShards], s_off[kMaxShards + 1];
+    if (threadIdx.x == 0) {
+        uint32_t total = 0;
+        for (uint32_t s = 0; s < L.shards; ++s) {
+            uint32_t c = L.counts[s][q];
+            c = min(c, min(L.in_stride, L.topk));
+            s_n[s] = c;
+            s_off[s] = total;
+            total += c;
+        }
+        s_off[L.shards] = total;
+        L.out_count[q] = min(total, L.topk);
+    }
+    __syncthreads();
+    const uint32_t total = s_off[L.shards];
+    for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
+        uint32_t s = 0;
+        while (e >= s_off[s + 1]) ++s;
+        const uint32_t i = e - s_off[s];
+        const uint64_t row = static_cast<uint64_t>(q) * L.in_stride;
+        const float x = L.scores[s][row + i];
+        uint32_t pos = i;
+        for (uint32_t t = 0; t < L.shards && pos < L.topk; ++t)
+            if (t != s) pos += preceding(L.scores[t] + row, s_n[t], x, t < s);
+        if (pos < L.topk) {
+            const uint64_t o = static_cast<uint64_t>(q) * L.out_stride + pos;
+            L.out_score[o] = x;
+            L.out_id[o] = L.ids[s][row + i];
+        }
+    }
+}
+}  // namespace
+
+cudaError_t launch_merge_shards(const ShardMergeLaunch& L, cudaStream_t stream) {
+    if (L.nq == 0) return cudaSuccess;
+    if (L.shards == 0 || L.shards > kMaxShards || L.topk > static_cast<uint32_t>(kMaxTopK) || L.topk > L.out_stride ||
+        !L.out_score || !L.out_id || !L.out_count)
+        return cudaErrorInvalidValue;
+    for (uint32_t s = 0; s < L.shards; ++s)
+        if (!L.scores[s] || !L.ids[s] || !L.counts[s]) return cudaErrorInvalidValue;
+    merge_shards_kernel<<<L.nq, 256, 0, stream>>>(L);
+    return cudaGetLastError();
+}
+
 }  // namespace hss

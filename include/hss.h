@@ -132,6 +132,20 @@ int hss_aggregator_launch_noalloc(const uint8_t* filterResult, const float* docS
 int hss_topk_launch(const float* scores, const uint32_t* locations, const uint32_t* count, uint32_t topK,
                     float* outScores, uint32_t* outLocations, uint32_t* outCount, hss_stream_t stream);
 
+/* Replaces the reference's cross-shard merge of per-shard results (RunContext::FoldShardIntoAcc and
+ * the k-way merge, src/harness/run/run_context.cpp:86-118,237-270): shard s's results for query q are
+ * shardScores[s][q * inStride + i], shardIds[s][...] (i < shardCounts[s][q], score descending, as the
+ * searcher returns them); the merged top min(topK, sum of counts) go to outScores / outIds
+ * [q * outStride + j] and outCounts[q], by score descending, equal scores to the lower shard first
+ * (then list order). With shards holding ascending doc ranges this is the ground truth's (score
+ * descending, doc id ascending) order. The pointer arrays are host arrays of device pointers on the
+ * current device (gather other GPUs' results there first). shards <= HSS_MAX_SHARDS. */
+#define HSS_MAX_SHARDS 64
+int hss_merge_shards_launch(const float* const* shardScores, const int64_t* const* shardIds,
+                            const uint32_t* const* shardCounts, uint32_t shards, uint32_t nq, uint32_t inStride,
+                            uint32_t topK, float* outScores, int64_t* outIds, uint32_t* outCounts, uint32_t outStride,
+                            hss_stream_t stream);
+
 /* ---- index (DataTable, src/engine/index/data_table.h:10-92) ---- */
 typedef struct hss_table hss_table;
 

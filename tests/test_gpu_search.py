@@ -203,3 +203,39 @@ def test_searcher_in_caller_owned_workspace(torch_cuda, method):
         hss.FullRecallSearcher(table, workspace=(base, nbytes - 4096), **cfg)  # too small
     with pytest.raises(hss.HssError):
         hss.FullRecallSearcher(table, workspace=(base + 64, nbytes), **cfg)  # misaligned
+
+
+def test_cross_shard_merge_equals_the_unsharded_search(torch_cuda):
+    # three shards holding ascending doc ranges (global ids via doc offsets), each searched alone,
+    # their top-K lists merged on the device: the result is the whole corpus's ground truth
+    torch = torch_cuda
+    mix = data.Mixture(128, 64, (1e-3, 0.5), n_clusters=32, seed=41)
+    vec, bits, _ = mix.corpus(30000, seed=42)
+    vec[7000] = vec[12000] = vec[25000]  # equal scores across shards: the lower shard (lower id) first
+    bounds = [0, 9000, 21000, 30000]
+    nq, K = 40, 100
+    q = mix.queries(nq, seed=43)
+    exprs = data.make_filters(mix, nq, n_tags=(1, 3), seed=44)
+    exprs[1] = ""
+    d_q = torch.tensor(q, device="cuda:0")
+    outs = []
+    for s in range(3):
+        a, b = bounds[s], bounds[s + 1]
+        table = hss.DataTable.build(vec[a:b], bits[a:b], 64, device=0, doc_num_per_segment=4096, doc_offset=a)
+        srch = hss.FullRecallSearcher(table, max_batch=nq, method=2 if s == 1 else 0)
+        f = srch.compile_filters(exprs)
+        sc = torch.zeros((nq, K), dtype=torch.float32, device="cuda:0")
+        ids = torch.zeros((nq, K), dtype=torch.int64, device="cuda:0")
+        cnt = torch.zeros(nq, dtype=torch.int32, device="cuda:0")
+        assert srch.search_device(d_q.data_ptr(), nq, f, [K] * nq, sc.data_ptr(), ids.data_ptr(), cnt.data_ptr(),
+                                  K) == 0
+        torch.cuda.synchronize()
+        outs.append((sc, ids, cnt, table, srch, f))
+    m_sc = torch.zeros((nq, K), dtype=torch.float32, device="cuda:0")
+    m_id = torch.zeros((nq, K), dtype=torch.int64, device="cuda:0")
+    m_n = torch.zeros(nq, dtype=torch.int32, device="cuda:0")
+    hss.merge_shards([o[0].data_ptr() for o in outs], [o[1].data_ptr() for o in outs], [o[2].data_ptr() for o in outs],
+                     nq, K, K, m_sc.data_ptr(), m_id.data_ptr(), m_n.data_ptr(), K)
+    torch.cuda.synchronize()
+    want = oracle.topk(q, exprs, [K] * nq, vec, bits, threads=8)
+    _check((m_sc.cpu().numpy(), m_id.cpu().numpy(), m_n.cpu().numpy()), want, nq)
