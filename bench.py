@@ -398,26 +398,43 @@ def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=12
         tk = np.random.default_rng(22).choice([10, 100, 1000], args.train_queries).astype(np.uint32)
         model, margin, report = fit_threshold_model(searcher, tq, te, tk, hidden=256, steps=2000, seed=3)
         searcher.set_threshold_model(model, margin)
-    searcher.set_timing(True)
+    # A second searcher of the same form: batch i runs on searcher i % 2, so while the host finishes
+    # one batch (its statuses, rare re-runs) the next is already queued on the stream.
+    twin = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[method],
+                                  sample_docs=args.sample_docs)
+    if learned:
+        twin.set_threshold_model(model, margin)
+    searchers = (searcher, twin)
+    for srch in searchers:
+        srch.set_timing(True)
     nb = max(1, len(queries) // B)
     filters = [searcher.compile_filters(exprs[i * B:(i + 1) * B]) for i in range(nb)]
     topks = _topks(args, B, nb, kmix)
     d_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1), device=dev)
-    o_sc = torch.zeros((B, kmax), dtype=torch.float32, device=dev)
-    o_id = torch.zeros((B, kmax), dtype=torch.int64, device=dev)
-    o_n = torch.zeros(B, dtype=torch.int32, device=dev)
+    o_sc = torch.zeros((2, B, kmax), dtype=torch.float32, device=dev)
+    o_id = torch.zeros((2, B, kmax), dtype=torch.int64, device=dev)
+    o_n = torch.zeros((2, B), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
 
-    def step(i):
+    def enqueue(i, d_queries=None):
         j = (rank * 7919 + i) % nb
-        rc = searcher.search_device(d_q[j].data_ptr(), B, filters[j], topks[j], o_sc.data_ptr(), o_id.data_ptr(),
-                                    o_n.data_ptr(), kmax, sh)
-        assert rc == 0, searcher.last_status(B)
-        return searcher.last_times()
+        p = i % 2
+        searchers[p].search_device_async(d_q[j].data_ptr() if d_queries is None else d_queries, B, filters[j],
+                                         topks[j], o_sc[p].data_ptr(), o_id[p].data_ptr(), o_n[p].data_ptr(), kmax, sh)
+
+    def finish(i):
+        srch = searchers[i % 2]
+        rc = srch.finish()
+        assert rc == 0, srch.last_status(B)
+        return srch.last_times()
 
     for i in range(args.warmup):
-        step(i)
+        enqueue(i)
+        if i > 0:
+            finish(i - 1)
+    if args.warmup:
+        finish(args.warmup - 1)
     torch.cuda.synchronize()
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev) if flush_l2 else None
     pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -430,16 +447,26 @@ def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=12
         barrier()
         torch.cuda.synchronize()
         ev0.record(stream)
-        for i in range(args.steps):
-            if flush_l2:
-                flush.fill_(float(i))
-                pairs[i][0].record(stream)
-            t = step(args.warmup + i)
-            if flush_l2:
-                pairs[i][1].record(stream)
+
+        def done(t):
+            nonlocal launches
             cand_ms.append(t["candidates_ms"])
             stage_ms.append([t["filter_ms"], t["sample_ms"], t["candidates_ms"], t["select_ms"], t["total_ms"]])
             launches += t["launches"]
+
+        for i in range(args.steps):
+            if flush_l2:  # timed one step at a time, L2 written over between steps (no overlap)
+                flush.fill_(float(i))
+                pairs[i][0].record(stream)
+                enqueue(args.warmup + i)
+                done(finish(args.warmup + i))
+                pairs[i][1].record(stream)
+                continue
+            enqueue(args.warmup + i)
+            if i > 0:
+                done(finish(args.warmup + i - 1))
+        if not flush_l2:
+            done(finish(args.warmup + args.steps - 1))
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -449,24 +476,41 @@ def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=12
     value = whole_job_qps(world, args.steps, B, t_max)
 
     # end-to-end leg through the C-ABI: pinned host queries in, results out, every step. Each step
-    # is one batch through hss_filters_compile + hss_searcher_search_device with its host->device
-    # query copy and device->host result copy, on one searcher and stream. A second host thread
-    # compiles the next batch's filters (host-only work, table read-only) while this batch is on the
-    # GPU; the ctypes calls release the interpreter lock.
+    # is one batch through hss_filters_compile + hss_searcher_search_device_async / hss_searcher_finish
+    # with its host->device query copy and device->host result copy, the two searchers alternating on
+    # one stream. A second host thread compiles the next batch's filters (host-only work, table
+    # read-only) while this batch is on the GPU; the ctypes calls release the interpreter lock.
     from concurrent.futures import ThreadPoolExecutor
     h_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1)).pin_memory()
-    h_sc = torch.zeros((B, kmax), dtype=torch.float32).pin_memory()
-    h_id = torch.zeros((B, kmax), dtype=torch.int64).pin_memory()
-    h_n = torch.zeros(B, dtype=torch.int32).pin_memory()
-    d_stage = torch.zeros((B, dim), dtype=torch.float32, device=dev)
+    h_sc = torch.zeros((2, B, kmax), dtype=torch.float32).pin_memory()
+    h_id = torch.zeros((2, B, kmax), dtype=torch.int64).pin_memory()
+    h_n = torch.zeros((2, B), dtype=torch.int32).pin_memory()
+    d_stage = torch.zeros((2, B, dim), dtype=torch.float32, device=dev)
+    out_ev = [torch.cuda.Event(), torch.cuda.Event()]
 
     def batch_of(i):
         return (rank * 7919 + args.warmup + i) % nb
 
     def e2e_run(steps, pool, ev=None):
+        # per step: the next batch's filters compiled on a second host thread, its queries copied in
+        # from pinned memory, the batch enqueued; then the previous batch finished and its results
+        # copied out to pinned memory (read once its copy event has passed)
         fut = pool.submit(lambda: searcher.compile_filters(exprs[batch_of(0) * B:(batch_of(0) + 1) * B]))
+        pending = []
+
+        def retire(i, f):
+            p = i % 2
+            rc = searchers[p].finish()
+            assert rc == 0
+            h_sc[p].copy_(o_sc[p], non_blocking=True)
+            h_id[p].copy_(o_id[p], non_blocking=True)
+            h_n[p].copy_(o_n[p], non_blocking=True)
+            out_ev[p].record(stream)
+            f.close()
+
         for i in range(steps):
             j = batch_of(i)
+            p = i % 2
             f = fut.result()
             if i + 1 < steps:
                 jn = batch_of(i + 1)
@@ -474,17 +518,21 @@ def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=12
             if ev is not None:
                 flush.fill_(float(i))
                 ev[i][0].record(stream)
-            d_stage.copy_(h_q[j], non_blocking=True)
-            rc = searcher.search_device(d_stage.data_ptr(), B, f, topks[j], o_sc.data_ptr(), o_id.data_ptr(),
-                                        o_n.data_ptr(), kmax, sh)
-            assert rc == 0
-            h_sc.copy_(o_sc, non_blocking=True)
-            h_id.copy_(o_id, non_blocking=True)
-            h_n.copy_(o_n, non_blocking=True)
-            if ev is not None:
+            out_ev[p].synchronize()  # this slot's previous results have reached the host
+            d_stage[p].copy_(h_q[j], non_blocking=True)
+            searchers[p].search_device_async(d_stage[p].data_ptr(), B, f, topks[j], o_sc[p].data_ptr(),
+                                             o_id[p].data_ptr(), o_n[p].data_ptr(), kmax, sh)
+            if ev is not None:  # one step at a time
+                retire(i, f)
                 ev[i][1].record(stream)
-            stream.synchronize()
-            f.close()
+                stream.synchronize()
+                continue
+            if pending:
+                retire(*pending.pop())
+            pending.append((i, f))
+        if pending:
+            retire(*pending.pop())
+        stream.synchronize()
 
     with ThreadPoolExecutor(1) as pool:
         e2e_run(2, pool)  # warm-up of the compile thread
@@ -537,7 +585,10 @@ def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=12
            "form": form_name(method, learned) + (", K from {10, 100, 1000} per query" if kmix else ""),
            "l2": "flushed between steps (256 MB write outside the step's events)" if flush_l2 else
                  "inputs larger than L2",
-           "method": method, "learned": learned, "searcher": searcher, "dev": dev}
+           "method": method, "learned": learned, "searcher": searcher, "dev": dev,
+           "pipelined": "two searchers of the form alternate batches on one stream (enqueue batch i, then "
+                        "finish batch i - 1)"}
+    twin.close()
     for f in filters:
         f.close()
     if report:
@@ -872,8 +923,9 @@ def run_ours(args):
            "config": config_of(args, world),
            "e2e": {"value": chosen["e2e"], "unit": "QPS", "h2d_bytes_per_step": B * 128 * 4,
                    "d2h_bytes_per_step": B * K * (4 + 8) + B * 4,
-                   "path": "hss_filters_compile (next batch, compile thread) + hss_searcher_search_device "
-                           "per batch, pinned host queries in and results out"},
+                   "path": "hss_filters_compile (next batch, compile thread) + hss_searcher_search_device_async / "
+                           "hss_searcher_finish per batch (two searchers alternating on one stream), pinned host "
+                           "queries in and results out"},
            "roofline": chosen["roofline"], "clocks": chosen["clocks"], "gpu_launches": chosen["launches"],
            "stages_ms": chosen["stages_ms"], "forms": {k: summary(v, args.steps) for k, v in forms.items()}}
     if "plain_fp32" in forms:

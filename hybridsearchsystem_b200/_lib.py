@@ -117,6 +117,9 @@ SIGNATURES = [
     ("hss_filters_free", None, [vp]),
     ("hss_searcher_search_device", ctypes.c_int,
      [vp, vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.c_uint32, vp]),
+    ("hss_searcher_search_device_async", ctypes.c_int,
+     [vp, vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.c_uint32, vp]),
+    ("hss_searcher_finish", ctypes.c_int, [vp]),
     ("hss_searcher_filter_device", ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, ctypes.c_uint64, vp, vp]),
     ("hss_searcher_last_status", ctypes.c_int, [vp, vp, ctypes.c_uint32]),
     ("hss_searcher_last_candidates", ctypes.c_int,

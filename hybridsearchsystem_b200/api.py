@@ -247,6 +247,19 @@ class FullRecallSearcher:
             check(rc)
         return rc
 
+    def search_device_async(self, d_queries, nq, filters, topks, d_scores, d_ids, d_counts, out_stride, stream=0):
+        """Enqueues a device-resident batch and returns at once; finish() completes it."""
+        t = np.ascontiguousarray(topks, dtype=np.uint32)
+        check(_lib.load().hss_searcher_search_device_async(self._h, d_queries, nq, filters._h, _np_ptr(t), d_scores,
+                                                           d_ids, d_counts, out_stride, stream))
+
+    def finish(self):
+        """Waits for the enqueued batch (re-running overflowed queries). Returns HSS_OK or HSS_ERR_QUERY."""
+        rc = _lib.load().hss_searcher_finish(self._h)
+        if rc != _lib.HSS_ERR_QUERY:
+            check(rc)
+        return rc
+
     def filter_device(self, filters, nq, d_bits, stride_words, d_pass=None, stream=0):
         """Filter stage alone: per-query doc bitmaps into d_bits. Returns the status code."""
         rc = _lib.load().hss_searcher_filter_device(self._h, filters._h, nq, d_bits, stride_words, d_pass, stream)

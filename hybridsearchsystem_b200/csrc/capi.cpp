@@ -516,6 +516,28 @@ int hss_searcher_search_device(hss_searcher* s, const float* dQueries, uint32_t 
     return HSS_OK;
 }
 
+int hss_searcher_search_device_async(hss_searcher* s, const float* dQueries, uint32_t nq, const hss_filters* filters,
+                                     const uint32_t* topks, float* dOutScores, int64_t* dOutIds, uint32_t* dOutCounts,
+                                     uint32_t outStride, hss_stream_t stream) {
+    if (!s || !filters || !topks || (nq && (!dQueries || !dOutScores || !dOutIds || !dOutCounts)))
+        return SetError(HSS_ERR_INVALID, "hss_searcher_search_device_async: null argument");
+    if (filters->exprs.size() < nq) return SetError(HSS_ERR_INVALID, "fewer filters than queries");
+    std::vector<const hss::FilterExpr*> ptrs(nq);
+    for (uint32_t i = 0; i < nq; ++i) ptrs[i] = &filters->exprs[i];
+    const int rc = s->s->SearchEnqueue(dQueries, nq, ptrs.data(), topks, dOutScores, dOutIds, dOutCounts, outStride,
+                                       S(stream));
+    if (rc < 0) return SetError(rc == -1 ? HSS_ERR_INVALID : HSS_ERR_CUDA, s->s->Error());
+    return HSS_OK;
+}
+
+int hss_searcher_finish(hss_searcher* s) {
+    if (!s) return SetError(HSS_ERR_INVALID, "hss_searcher_finish: null searcher");
+    const int rc = s->s->SearchFinish();
+    if (rc < 0) return SetError(HSS_ERR_CUDA, s->s->Error());
+    if (rc > 0) return SetError(HSS_ERR_QUERY, "some queries failed (see hss_searcher_last_status)");
+    return HSS_OK;
+}
+
 int hss_searcher_filter_device(hss_searcher* s, const hss_filters* filters, uint32_t nq, uint64_t* dOutBits,
                                uint64_t outStrideWords, uint32_t* dPassCounts, hss_stream_t stream) {
     if (!s || !filters || (nq && !dOutBits)) return SetError(HSS_ERR_INVALID, "hss_searcher_filter_device: null argument");

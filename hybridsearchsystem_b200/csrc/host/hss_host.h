@@ -13,6 +13,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include "../hss_kernels.h"
+
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -441,10 +443,22 @@ class FullRecallSearcher {
                      bool isMultiShard);
 
     // Device-resident batch: queries [nq][dim] and results live in device memory; the filters were
-    // compiled by PrepareExpr. Synchronises `stream` once (to read the overflow status).
+    // compiled by PrepareExpr. Synchronises `stream` once (to read the overflow status). Returns the
+    // number of failed queries, or a negative status.
     int SearchDevice(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks,
                      float* dOutScores, int64_t* dOutIds, uint32_t* dOutCounts, uint32_t outStride,
                      cudaStream_t stream);
+    // SearchDevice in two halves, so that a caller can keep the GPU busy while it waits: the first
+    // enqueues the whole batch on `stream` (its host work -- filter compilation into the staging
+    // buffer, launch planning -- done) and returns without waiting; the second waits for the batch's
+    // statuses, runs any candidate-overflow re-runs (enqueued on the same stream, then waited for) and
+    // returns what SearchDevice returns. The queries and outputs must stay valid until it returns; the
+    // searcher takes no other batch in between (two searchers alternate to overlap batches).
+    int SearchEnqueue(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks,
+                      float* dOutScores, int64_t* dOutIds, uint32_t* dOutCounts, uint32_t outStride,
+                      cudaStream_t stream);
+    int SearchFinish();
+    bool Pending() const { return m_b.pending; }
 
     // Filter stage alone (FullRecallSearcher::OneFilter, full_recall_searcher.cpp:233-262): the
     // per-query doc bitmaps [nq][outStrideWords] and pass counts; synchronises `stream` once.
@@ -499,6 +513,32 @@ class FullRecallSearcher {
     };
     static ArenaLayout Layout(const DataTable& table, const SearcherConfig& cfg);
     bool Allocate(void* dArena, size_t arenaBytes);
+    // The batch between SearchEnqueue and SearchFinish.
+    struct Batch {
+        const float* dQueries = nullptr;
+        uint32_t nq = 0;
+        cudaStream_t stream = nullptr;
+        SelectLaunch se{};
+        uint32_t launches = 0;
+        uint64_t want = 0;  // doc-sample size of the batch
+        bool pending = false, learned = false;
+        cudaError_t ce = cudaSuccess;
+    };
+    void Ck(cudaError_t e) {
+        if (m_b.ce == cudaSuccess && e != cudaSuccess) m_b.ce = e;
+    }
+    // Launch planning of the candidate passes (see SearchEnqueue).
+    bool UseSimt(bool simt) const { return m_tcFormat < 0 || simt; }
+    uint32_t UnitOf(uint32_t rows, bool simt) const;
+    uint64_t TilesOf(uint32_t unit) const;
+    uint32_t CtasOf(uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) const;
+    uint32_t SegsOf(uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) const;
+    uint32_t SegCapOf(uint32_t rows, uint64_t countTiles, uint32_t cap, uint32_t segs, bool simt) const;
+    void Stage(const uint32_t* dList, uint32_t rows);
+    void Cand(const float* theta, float* score, uint32_t* loc, uint32_t* count, uint32_t cap, uint32_t segBase,
+              uint32_t segCap, uint64_t begin, uint64_t step, uint32_t skip, uint64_t countTiles, const uint32_t* dList,
+              uint32_t rows, bool simt);
+    uint64_t Sample(const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly = false, float* stats = nullptr);
     int StageAndFilter(uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks, uint64_t* dBits,
                        uint64_t bitsStride, uint32_t* maxKOut, cudaStream_t stream);
 
@@ -542,6 +582,8 @@ class FullRecallSearcher {
     float* m_dQScale = nullptr;
     int32_t* m_dError = nullptr;
     cudaEvent_t m_ev[6] = {};
+    cudaEvent_t m_evStatus = nullptr;  // the batch's statuses are on the host
+    Batch m_b;
     bool m_timing = false;
     StageTimes m_times;
     std::vector<int32_t> m_lastStatus;

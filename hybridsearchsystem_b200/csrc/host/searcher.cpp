@@ -62,7 +62,8 @@ double TcAccumulationBound(int format, uint32_t d) {
 
 // Offsets of the packed per-batch staging buffer.
 struct StageLayout {
-    size_t progOff, opndOff, microOff, rowList, topk, epsMain, epsSamp, negInf, theta, qlist, counters, passCount,
+    size_t progOff, opndOff, microOff, rowList, topk, epsMain, epsSamp, negInf, theta, qlist, errWord, counters,
+        passCount,
         candCount, sampCount, status, prog, opnd, micro, total;
 };
 
@@ -87,6 +88,7 @@ StageLayout MakeLayout(uint32_t B) {
     L.negInf = take(B * 4ull);
     L.theta = take(B * 4ull);
     L.qlist = take(B * 4ull);
+    L.errWord = take(4);  // host copy of the tensor-core pass's error bits
     L.counters = at;  // zeroed per batch: passCount and status
     L.passCount = take(B * 4ull);
     L.status = take(B * 4ull);
@@ -181,6 +183,7 @@ FullRecallSearcher::~FullRecallSearcher() {
         if (p) cudaFreeHost(p);
     for (auto& e : m_ev)
         if (e) cudaEventDestroy(e);
+    if (m_evStatus) cudaEventDestroy(m_evStatus);
 }
 
 bool FullRecallSearcher::Allocate(void* dArena, size_t arenaBytes) {
@@ -538,10 +541,177 @@ int FullRecallSearcher::Features(const float* dQueries, uint32_t nq, const Filte
     return rc;
 }
 
+uint32_t FullRecallSearcher::UnitOf(uint32_t rows, bool simt) const {
+    return UseSimt(simt) ? 128u : tc_tile_docs(rows, m_tcKblocks);
+}
+
+uint64_t FullRecallSearcher::TilesOf(uint32_t unit) const { return (m_table->GetDocNum() + unit - 1) / unit; }
+
+uint32_t FullRecallSearcher::CtasOf(uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) const {
+    return UseSimt(simt) ? cand_simt_segments(countTiles, m_numSms, cap)
+                         : tc_cand_ctas(rows, m_tcKblocks, countTiles, m_numSms, cap);
+}
+
+uint32_t FullRecallSearcher::SegsOf(uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) const {
+    const uint32_t g = CtasOf(rows, countTiles, cap, simt);
+    return UseSimt(simt) ? g : 2 * g;  // a tensor-core CTA fills two segments
+}
+
+// Entries per segment: the docs one segment can see at most, within the list's share.
+uint32_t FullRecallSearcher::SegCapOf(uint32_t rows, uint64_t countTiles, uint32_t cap, uint32_t segs,
+                                      bool simt) const {
+    const uint32_t g = CtasOf(rows, countTiles, cap, simt);
+    // SIMT: a CTA's tiles; single SM: half of a CTA's tiles' docs; pair: a quarter of a pair's
+    const uint64_t groups = UseSimt(simt) ? g : (UnitOf(rows, simt) == 256 ? g / 2 : g);
+    const uint64_t perTile = UseSimt(simt) ? 128ull : 64ull;
+    const uint64_t perSeg = (countTiles + groups - 1) / groups * perTile;
+    return static_cast<uint32_t>(std::min<uint64_t>(perSeg, cap / segs));
+}
+
+// Error bounds (and, for the tensor-core pass, the staged queries in its format) of queries dList
+// (or 0..rows-1).
+void FullRecallSearcher::Stage(const uint32_t* dList, uint32_t rows) {
+    const DataTable& T = *m_table;
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    auto* dEpsMain = reinterpret_cast<float*>(m_dStage + SL.epsMain);
+    auto* dEpsSamp = reinterpret_cast<float*>(m_dStage + SL.epsSamp);
+    const uint32_t dim = T.GetDimension();
+    if (m_tcFormat < 0) {
+        const double rel = SimtRelBound(dim);
+        Ck(launch_query_eps(m_b.dQueries, dList, rows, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, m_b.stream));
+        return;
+    }
+    StageQueriesLaunch Q{};
+    Q.qry = m_b.dQueries;
+    Q.qlist = dList;
+    Q.nq_rows = rows;
+    Q.rows_alloc = 256;
+    Q.dim = dim;
+    Q.format = m_tcFormat;
+    Q.staged = m_dStaged;
+    Q.q_scale = m_dQScale;
+    Q.eps_main = dEpsMain;
+    Q.eps_sample = dEpsSamp;
+    Q.doc_norm_max = T.NormMax(m_tcFormat);
+    Q.doc_err_max = T.ErrMax(m_tcFormat);
+    Q.acc_rel = TcAccumulationBound(m_tcFormat, dim);
+    Ck(launch_stage_queries(Q, m_b.stream));
+}
+
+// A candidate pass: tiles begin + i * step (or, with skip >= 2, all tiles that are not multiples of
+// skip), i < countTiles, for `rows` queries (dList or 0..rows-1), writing the list segments
+// [segBase, segBase + its segments) of segCap entries each. Tiles hold UnitOf() docs: 128 for the
+// SIMT pass and the single-SM tensor-core pass, 256 for the SM-pair pass.
+void FullRecallSearcher::Cand(const float* theta, float* score, uint32_t* loc, uint32_t* count, uint32_t cap,
+                              uint32_t segBase, uint32_t segCap, uint64_t begin, uint64_t step, uint32_t skip,
+                              uint64_t countTiles, const uint32_t* dList, uint32_t rows, bool simt) {
+    const DataTable& T = *m_table;
+    const uint32_t g = CtasOf(rows, countTiles, cap, simt);
+    if (UseSimt(simt)) {
+        CandLaunch C{};
+        C.vec = T.DeviceVectors();
+        C.qry = m_b.dQueries;
+        C.bits = m_dBits;
+        C.bits_stride = T.GetBitmapWords();
+        C.theta = theta;
+        C.qlist = dList;
+        C.nq_list = rows;
+        C.cand_score = score;
+        C.cand_loc = loc;
+        C.cand_count = count;
+        C.cap = cap;
+        C.segs = g;
+        C.seg_cap = segCap;
+        C.seg_base = segBase;
+        C.dim = T.GetDimension();
+        C.tile_begin = begin;
+        C.tile_step = step;
+        C.tile_count = countTiles;
+        C.tile_skip = skip;
+        Ck(launch_cand_simt(C, m_numSms, m_b.stream));
+        return;
+    }
+    TcCandLaunch C{};
+    C.format = m_tcFormat;
+    C.kblocks = m_tcKblocks;
+    C.doc_scale = T.DeviceDocScale();
+    C.tile_scale = T.DeviceTileScale();
+    C.q_scale = m_dQScale;
+    C.bits = m_dBits;
+    C.bits_stride = T.GetBitmapWords();
+    C.theta = theta;
+    C.qlist = dList;
+    C.nq_rows = rows;
+    C.cand_score = score;
+    C.cand_loc = loc;
+    C.cand_count = count;
+    C.cap = cap;
+    C.ctas = g;
+    C.seg_cap = segCap;
+    C.seg_base = segBase;
+    C.tile_begin = begin;
+    C.tile_step = step;
+    C.tile_count = countTiles;
+    C.tile_skip = skip;
+    C.tiles128 = T.GetTileNum();
+    C.error = m_dError;
+    if (m_testHold && tc_tile_docs(rows, m_tcKblocks) == 128u) {  // the single-SM kernel only
+        C.hold_load = m_testHold;
+        C.wait_budget = m_testBudget;
+        m_testHold = 0;
+    }
+    Ck(launch_tc_cand(C, m_docMap, m_qryMap, m_numSms, m_b.stream));
+}
+
+// The doc sample: evenly spaced tiles, every filtered doc kept; its K-th best bounds the threshold.
+// Returns the sample's tile count.
+uint64_t FullRecallSearcher::Sample(const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly, float* stats) {
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    uint8_t* D = m_dStage;
+    const uint32_t unit = UnitOf(rows, simt);
+    const uint64_t tilesU = TilesOf(unit);
+    const uint64_t sampTiles = std::min<uint64_t>(tilesU, std::max<uint64_t>(1, (m_b.want + unit - 1) / unit));
+    const uint64_t step = std::max<uint64_t>(1, tilesU / sampTiles);
+    const uint64_t count = std::min<uint64_t>(sampTiles, (tilesU + step - 1) / step);
+    const uint32_t segs = SegsOf(rows, count, m_sampCap, simt);
+    const uint32_t segCap = SegCapOf(rows, count, m_sampCap, segs, simt);
+    auto* dSampCount = reinterpret_cast<uint32_t*>(D + SL.sampCount);
+    Cand(reinterpret_cast<const float*>(D + SL.negInf), m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, segCap, 0,
+         step, 0, count, dList, rows, simt);
+    SampleThresholdLaunch ST{};
+    ST.score = m_dSampScore;
+    ST.count = dSampCount;
+    ST.cap = m_sampCap;
+    ST.segs = segs;
+    ST.seg_cap = segCap;
+    ST.raise_only = raiseOnly ? 1 : 0;
+    ST.topk = reinterpret_cast<const uint32_t*>(D + SL.topk);
+    ST.eps_sample = reinterpret_cast<const float*>(D + SL.epsSamp);
+    ST.eps_main = reinterpret_cast<const float*>(D + SL.epsMain);
+    ST.theta = reinterpret_cast<float*>(D + SL.theta);
+    ST.qlist = dList;
+    ST.nq_list = rows;
+    ST.stats = stats;
+    Ck(launch_sample_threshold(ST, m_b.stream));
+    return count;
+}
+
 int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs,
                                      const uint32_t* topks, float* dOutScores, int64_t* dOutIds,
                                      uint32_t* dOutCounts, uint32_t outStride, cudaStream_t stream) {
+    const int rc = SearchEnqueue(dQueries, nq, exprs, topks, dOutScores, dOutIds, dOutCounts, outStride, stream);
+    if (rc != 0 || !m_b.pending) return rc;
+    return SearchFinish();
+}
+
+int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs,
+                                      const uint32_t* topks, float* dOutScores, int64_t* dOutIds,
+                                      uint32_t* dOutCounts, uint32_t outStride, cudaStream_t stream) {
     if (!m_ok) return -1;
+    if (m_b.pending) {
+        m_err = "the searcher's previous batch was not finished";
+        return -1;
+    }
     m_times = StageTimes{};
     m_lastStatus.assign(nq, 0);
     if (nq == 0) return 0;
@@ -560,214 +730,72 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
     const StageLayout SL = MakeLayout(m_cfg.maxBatch);
     uint8_t* H = m_hStage;
     uint8_t* D = m_dStage;
-    cudaError_t ce = cudaSuccess;
-    auto ck = [&](cudaError_t e) {
-        if (ce == cudaSuccess && e != cudaSuccess) ce = e;
-    };
+    m_b = Batch{};
+    m_b.dQueries = dQueries;
+    m_b.nq = nq;
+    m_b.stream = stream;
     auto* dTopk = reinterpret_cast<uint32_t*>(D + SL.topk);
     auto* dEpsMain = reinterpret_cast<float*>(D + SL.epsMain);
-    auto* dEpsSamp = reinterpret_cast<float*>(D + SL.epsSamp);
-    auto* dNegInf = reinterpret_cast<float*>(D + SL.negInf);
     auto* dTheta = reinterpret_cast<float*>(D + SL.theta);
-    auto* dQlist = reinterpret_cast<uint32_t*>(D + SL.qlist);
     auto* dCandCount = reinterpret_cast<uint32_t*>(D + SL.candCount);
     auto* dSampCount = reinterpret_cast<uint32_t*>(D + SL.sampCount);
     auto* dStatus = reinterpret_cast<int32_t*>(D + SL.status);
 
     const DataTable& T = *m_table;
     const uint64_t words = T.GetBitmapWords();
-    const uint64_t tiles = T.GetTileNum();
-    const uint32_t dim = T.GetDimension();
-    uint32_t launches = 0;
-    if (m_timing) ck(cudaEventRecord(m_ev[0], stream));
+    if (m_timing) Ck(cudaEventRecord(m_ev[0], stream));
     uint32_t maxK = 0;
-    if (StageAndFilter(nq, exprs, topks, m_dBits, words, &maxK, stream) != 0) ck(cudaErrorUnknown);
-    ++launches;
-
-    const bool tc = m_tcFormat >= 0;
-    // Error bounds (and, for the tensor-core pass, the staged queries in its format).
-    auto stage = [&](const uint32_t* dList, uint32_t rows) {
-        if (!tc) {
-            const double rel = SimtRelBound(dim);
-            ck(launch_query_eps(dQueries, dList, rows, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
-            return;
-        }
-        StageQueriesLaunch Q{};
-        Q.qry = dQueries;
-        Q.qlist = dList;
-        Q.nq_rows = rows;
-        Q.rows_alloc = 256;
-        Q.dim = dim;
-        Q.format = m_tcFormat;
-        Q.staged = m_dStaged;
-        Q.q_scale = m_dQScale;
-        Q.eps_main = dEpsMain;
-        Q.eps_sample = dEpsSamp;
-        Q.doc_norm_max = T.NormMax(m_tcFormat);
-        Q.doc_err_max = T.ErrMax(m_tcFormat);
-        Q.acc_rel = TcAccumulationBound(m_tcFormat, dim);
-        ck(launch_stage_queries(Q, stream));
-    };
-    stage(nullptr, nq);
-    ++launches;
-    if (m_timing) ck(cudaEventRecord(m_ev[1], stream));
-
-    // Candidate passes. A pass covers tiles begin + i * step (or, with skip >= 2, all tiles that are not
-    // multiples of skip), i < countTiles, for `rows` queries (dList or 0..rows-1), and writes the list
-    // segments [segBase, segBase + its segments) of segCap entries each. Tiles hold unitOf() docs:
-    // 128 for the SIMT pass and the single-SM tensor-core pass, 256 for the SM-pair pass.
-    auto useSimt = [&](bool simt) { return !tc || simt; };
-    auto unitOf = [&](uint32_t rows, bool simt) { return useSimt(simt) ? 128u : tc_tile_docs(rows, m_tcKblocks); };
-    auto tilesOf = [&](uint32_t unit) { return (T.GetDocNum() + unit - 1) / unit; };
-    auto ctasOf = [&](uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) {
-        return useSimt(simt) ? cand_simt_segments(countTiles, m_numSms, cap)
-                             : tc_cand_ctas(rows, m_tcKblocks, countTiles, m_numSms, cap);
-    };
-    auto segsOf = [&](uint32_t rows, uint64_t countTiles, uint32_t cap, bool simt) {
-        const uint32_t g = ctasOf(rows, countTiles, cap, simt);
-        return useSimt(simt) ? g : 2 * g;  // a tensor-core CTA fills two segments
-    };
-    // entries per segment: the docs one segment can see at most, within the list's share
-    auto segCapOf = [&](uint32_t rows, uint64_t countTiles, uint32_t cap, uint32_t segs, bool simt) {
-        const uint32_t g = ctasOf(rows, countTiles, cap, simt);
-        // SIMT: a CTA's tiles; single SM: half of a CTA's tiles' docs; pair: a quarter of a pair's
-        const uint64_t groups = useSimt(simt) ? g : (unitOf(rows, simt) == 256 ? g / 2 : g);
-        const uint64_t perTile = useSimt(simt) ? 128ull : 64ull;
-        const uint64_t perSeg = (countTiles + groups - 1) / groups * perTile;
-        return static_cast<uint32_t>(std::min<uint64_t>(perSeg, cap / segs));
-    };
-    auto cand = [&](const float* theta, float* score, uint32_t* loc, uint32_t* count, uint32_t cap, uint32_t segBase,
-                    uint32_t segCap, uint64_t begin, uint64_t step, uint32_t skip, uint64_t countTiles,
-                    const uint32_t* dList, uint32_t rows, bool simt) {
-        const uint32_t g = ctasOf(rows, countTiles, cap, simt);
-        if (useSimt(simt)) {
-            CandLaunch C{};
-            C.vec = T.DeviceVectors();
-            C.qry = dQueries;
-            C.bits = m_dBits;
-            C.bits_stride = words;
-            C.theta = theta;
-            C.qlist = dList;
-            C.nq_list = rows;
-            C.cand_score = score;
-            C.cand_loc = loc;
-            C.cand_count = count;
-            C.cap = cap;
-            C.segs = g;
-            C.seg_cap = segCap;
-            C.seg_base = segBase;
-            C.dim = dim;
-            C.tile_begin = begin;
-            C.tile_step = step;
-            C.tile_count = countTiles;
-            C.tile_skip = skip;
-            ck(launch_cand_simt(C, m_numSms, stream));
-            return;
-        }
-        TcCandLaunch C{};
-        C.format = m_tcFormat;
-        C.kblocks = m_tcKblocks;
-        C.doc_scale = T.DeviceDocScale();
-        C.tile_scale = T.DeviceTileScale();
-        C.q_scale = m_dQScale;
-        C.bits = m_dBits;
-        C.bits_stride = words;
-        C.theta = theta;
-        C.qlist = dList;
-        C.nq_rows = rows;
-        C.cand_score = score;
-        C.cand_loc = loc;
-        C.cand_count = count;
-        C.cap = cap;
-        C.ctas = g;
-        C.seg_cap = segCap;
-        C.seg_base = segBase;
-        C.tile_begin = begin;
-        C.tile_step = step;
-        C.tile_count = countTiles;
-        C.tile_skip = skip;
-        C.tiles128 = tiles;
-        C.error = m_dError;
-        if (m_testHold && tc_tile_docs(rows, m_tcKblocks) == 128u) {  // the single-SM kernel only
-            C.hold_load = m_testHold;
-            C.wait_budget = m_testBudget;
-            m_testHold = 0;
-        }
-        ck(launch_tc_cand(C, m_docMap, m_qryMap, m_numSms, stream));
-    };
+    if (StageAndFilter(nq, exprs, topks, m_dBits, words, &maxK, stream) != 0) Ck(cudaErrorUnknown);
+    ++m_b.launches;
+    Stage(nullptr, nq);
+    ++m_b.launches;
+    if (m_timing) Ck(cudaEventRecord(m_ev[1], stream));
 
     // 1. doc sample: evenly spaced tiles, every filtered doc kept; its K-th best bounds the threshold
-    const uint64_t want = std::max<uint64_t>(m_cfg.sampleDocs,
-                                             (4ull * std::max<uint32_t>(maxK, 1u) * T.GetDocNum() +
-                                              m_cfg.candidateCap - 1) / m_cfg.candidateCap);
-    auto sample = [&](const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly = false,
-                      float* stats = nullptr) {
-        const uint32_t unit = unitOf(rows, simt);
-        const uint64_t tilesU = tilesOf(unit);
-        const uint64_t sampTiles = std::min<uint64_t>(tilesU, std::max<uint64_t>(1, (want + unit - 1) / unit));
-        const uint64_t step = std::max<uint64_t>(1, tilesU / sampTiles);
-        const uint64_t count = std::min<uint64_t>(sampTiles, (tilesU + step - 1) / step);
-        const uint32_t segs = segsOf(rows, count, m_sampCap, simt);
-        const uint32_t segCap = segCapOf(rows, count, m_sampCap, segs, simt);
-        cand(dNegInf, m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, segCap, 0, step, 0, count, dList, rows,
-             simt);
-        SampleThresholdLaunch ST{};
-        ST.score = m_dSampScore;
-        ST.count = dSampCount;
-        ST.cap = m_sampCap;
-        ST.segs = segs;
-        ST.seg_cap = segCap;
-        ST.raise_only = raiseOnly ? 1 : 0;
-        ST.topk = dTopk;
-        ST.eps_sample = dEpsSamp;
-        ST.eps_main = dEpsMain;
-        ST.theta = dTheta;
-        ST.qlist = dList;
-        ST.nq_list = rows;
-        ST.stats = stats;
-        ck(launch_sample_threshold(ST, stream));
-        return count;
-    };
+    m_b.want = std::max<uint64_t>(m_cfg.sampleDocs,
+                                  (4ull * std::max<uint32_t>(maxK, 1u) * T.GetDocNum() + m_cfg.candidateCap - 1) /
+                                      m_cfg.candidateCap);
     const bool learned = static_cast<bool>(m_model);
+    m_b.learned = learned;
     const bool wantStats = learned || m_featuresOut != nullptr;
     m_lastEstSegs = 0;
-    const uint64_t sampCount = sample(nullptr, nq, false, false, wantStats ? m_dStats : nullptr);
-    launches += 2;
+    const uint64_t sampCount = Sample(nullptr, nq, false, false, wantStats ? m_dStats : nullptr);
+    m_b.launches += 2;
     // the sample's proven thresholds (theta_1), read after the batch's first synchronisation
-    ck(cudaMemcpyAsync(H + SL.theta, dTheta, nq * 4ull, cudaMemcpyDeviceToHost, stream));
+    Ck(cudaMemcpyAsync(H + SL.theta, dTheta, nq * 4ull, cudaMemcpyDeviceToHost, stream));
     if (m_featuresOut) {
-        ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
+        Ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
                           m_featuresOut, stream));
-        ck(cudaStreamSynchronize(stream));
-        if (ce != cudaSuccess) {
-            m_err = cudaGetErrorString(ce);
+        Ck(cudaStreamSynchronize(stream));
+        if (m_b.ce != cudaSuccess) {
+            m_err = cudaGetErrorString(m_b.ce);
             return -2;
         }
         return 0;
     }
     if (learned) {
         // the model's predicted K-th score minus the margin, never below theta_1
-        ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
+        Ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
                           m_dX, stream));
-        if (m_model->Forward(m_dX, nq, m_dYp, stream) != 0) ck(cudaErrorUnknown);
-        ck(launch_predict_theta(m_dYp, dTheta, nq, m_model->scale, m_model->shift, m_margin, m_dYp, stream));
-        ck(cudaMemcpyAsync(m_hThetaA, m_dYp, nq * 4ull, cudaMemcpyDeviceToHost, stream));
-        launches += 5;
+        if (m_model->Forward(m_dX, nq, m_dYp, stream) != 0) Ck(cudaErrorUnknown);
+        Ck(launch_predict_theta(m_dYp, dTheta, nq, m_model->scale, m_model->shift, m_margin, m_dYp, stream));
+        Ck(cudaMemcpyAsync(m_hThetaA, m_dYp, nq * 4ull, cudaMemcpyDeviceToHost, stream));
+        m_b.launches += 5;
     }
-    if (m_timing) ck(cudaEventRecord(m_ev[2], stream));
+    if (m_timing) Ck(cudaEventRecord(m_ev[2], stream));
 
     // 2. the full pass, progressively: first every split-th tile (about sqrt(sample / corpus) of it)
     // with the sample's threshold; the K-th best of that part then raises each query's threshold
     // (every doc of the top K scores at least K-th best - 2 eps) for the remaining tiles. Both parts'
     // candidates form one segmented list.
     const uint32_t C = m_cfg.candidateCap;
-    const uint64_t tilesM = tilesOf(unitOf(nq, false));
+    const uint64_t tilesM = TilesOf(UnitOf(nq, false));
     uint32_t split = static_cast<uint32_t>(std::sqrt(static_cast<double>(tilesM) / static_cast<double>(sampCount)));
     split = std::min<uint32_t>(split, 64);
-    SelectLaunch SE{};
+    SelectLaunch& SE = m_b.se;
     SE.vec = T.DeviceVectors();
     SE.qry = dQueries;
-    SE.dim = dim;
+    SE.dim = T.GetDimension();
     SE.cand_score = m_dCandScore;
     SE.cand_loc = m_dCandLoc;
     SE.cand_count = dCandCount;
@@ -791,10 +819,10 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         // whose candidates alone feed the select step. A prediction that kept fewer than K docs
         // leaves theta_1 in place; no prediction can make the results inexact or force a re-run.
         const uint64_t countA = (tilesM + kLearnedSplit - 1) / kLearnedSplit;
-        const uint32_t segsA = segsOf(nq, countA, m_sampCap, false);
-        const uint32_t capA = segCapOf(nq, countA, m_sampCap, segsA, false);
+        const uint32_t segsA = SegsOf(nq, countA, m_sampCap, false);
+        const uint32_t capA = SegCapOf(nq, countA, m_sampCap, segsA, false);
         m_lastEstSegs = segsA;
-        cand(m_dYp, m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, capA, 0, kLearnedSplit, 0, countA, nullptr, nq,
+        Cand(m_dYp, m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, capA, 0, kLearnedSplit, 0, countA, nullptr, nq,
              false);
         SampleThresholdLaunch RT{};
         RT.score = m_dSampScore;
@@ -809,18 +837,18 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         RT.theta = dTheta;
         RT.qlist = nullptr;
         RT.nq_list = nq;
-        ck(launch_sample_threshold(RT, stream));
-        const uint32_t segs = segsOf(nq, tilesM, C, false);
+        Ck(launch_sample_threshold(RT, stream));
+        const uint32_t segs = SegsOf(nq, tilesM, C, false);
         SE.segs = segs;
-        SE.seg_cap = segCapOf(nq, tilesM, C, segs, false);
-        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tilesM, nullptr, nq, false);
-        launches += 3;
+        SE.seg_cap = SegCapOf(nq, tilesM, C, segs, false);
+        Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tilesM, nullptr, nq, false);
+        m_b.launches += 3;
     } else if (split >= 2) {
         const uint64_t countA = (tilesM + split - 1) / split, countB = tilesM - countA;
-        const uint32_t segsA = segsOf(nq, countA, C, false), segsB = segsOf(nq, countB, C, false);
-        const uint32_t segCap = std::min(segCapOf(nq, countA, C, segsA + segsB, false),
-                                         segCapOf(nq, countB, C, segsA + segsB, false));
-        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, split, 0, countA, nullptr, nq, false);
+        const uint32_t segsA = SegsOf(nq, countA, C, false), segsB = SegsOf(nq, countB, C, false);
+        const uint32_t segCap = std::min(SegCapOf(nq, countA, C, segsA + segsB, false),
+                                         SegCapOf(nq, countB, C, segsA + segsB, false));
+        Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, split, 0, countA, nullptr, nq, false);
         SampleThresholdLaunch RT{};
         RT.score = m_dCandScore;
         RT.count = dCandCount;
@@ -834,43 +862,76 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         RT.theta = dTheta;
         RT.qlist = nullptr;
         RT.nq_list = nq;
-        ck(launch_sample_threshold(RT, stream));
-        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, segsA, segCap, 0, 1, split, countB, nullptr, nq, false);
-        launches += 3;
+        Ck(launch_sample_threshold(RT, stream));
+        Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, segsA, segCap, 0, 1, split, countB, nullptr, nq, false);
+        m_b.launches += 3;
         SE.segs = segsA + segsB;
         SE.seg_cap = segCap;
     } else {
-        const uint32_t segs = segsOf(nq, tilesM, C, false);
+        const uint32_t segs = SegsOf(nq, tilesM, C, false);
         SE.segs = segs;
-        SE.seg_cap = segCapOf(nq, tilesM, C, segs, false);
-        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tilesM, nullptr, nq, false);
-        ++launches;
+        SE.seg_cap = SegCapOf(nq, tilesM, C, segs, false);
+        Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tilesM, nullptr, nq, false);
+        ++m_b.launches;
     }
     m_lastSegs.assign(nq, {SE.segs, SE.seg_cap});
-    if (m_timing) ck(cudaEventRecord(m_ev[3], stream));
+    if (m_timing) Ck(cudaEventRecord(m_ev[3], stream));
 
     // 3. exact rescoring and the top K
-    ck(launch_select_topk(SE, stream));
-    ++launches;
-    if (m_timing) ck(cudaEventRecord(m_ev[4], stream));
+    Ck(launch_select_topk(SE, stream));
+    ++m_b.launches;
+    if (m_timing) Ck(cudaEventRecord(m_ev[4], stream));
+    // the statuses that decide re-runs (and the tensor-core pass's error bits), on the host when
+    // m_evStatus completes
+    Ck(cudaMemcpyAsync(H + SL.status, dStatus, nq * 4ull, cudaMemcpyDeviceToHost, stream));
+    if (m_tcFormat >= 0) Ck(cudaMemcpyAsync(H + SL.errWord, m_dError, 4, cudaMemcpyDeviceToHost, stream));
+    if (!m_evStatus) Ck(cudaEventCreateWithFlags(&m_evStatus, cudaEventDisableTiming));
+    Ck(cudaEventRecord(m_evStatus, stream));
+    if (m_b.ce != cudaSuccess) {
+        m_err = cudaGetErrorString(m_b.ce);
+        return -2;
+    }
+    m_b.pending = true;
+    return 0;
+}
 
+int FullRecallSearcher::SearchFinish() {
+    if (!m_b.pending) return 0;
+    m_b.pending = false;
+    if (cudaSetDevice(m_deviceId) != cudaSuccess) return -2;
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    uint8_t* H = m_hStage;
+    uint8_t* D = m_dStage;
+    const uint32_t nq = m_b.nq;
+    cudaStream_t stream = m_b.stream;
+    auto* dQlist = reinterpret_cast<uint32_t*>(D + SL.qlist);
+    auto* dStatus = reinterpret_cast<int32_t*>(D + SL.status);
+    auto* dTheta = reinterpret_cast<float*>(D + SL.theta);
+    auto* dCandCount = reinterpret_cast<uint32_t*>(D + SL.candCount);
     auto* hStatus = reinterpret_cast<int32_t*>(H + SL.status);
     auto* hQlist = reinterpret_cast<uint32_t*>(H + SL.qlist);
+    const bool tc = m_tcFormat >= 0;
+    const uint32_t C = m_cfg.candidateCap;
+    SelectLaunch& SE = m_b.se;
     uint32_t retries = 0;
     bool firstSync = true;
     for (;;) {
-        ck(cudaMemcpyAsync(hStatus, dStatus, nq * 4ull, cudaMemcpyDeviceToHost, stream));
-        ck(cudaStreamSynchronize(stream));
-        if (firstSync && ce == cudaSuccess) {
+        if (firstSync) {
+            Ck(cudaEventSynchronize(m_evStatus));
+        } else {
+            Ck(cudaMemcpyAsync(hStatus, dStatus, nq * 4ull, cudaMemcpyDeviceToHost, stream));
+            Ck(cudaStreamSynchronize(stream));
+        }
+        if (firstSync && m_b.ce == cudaSuccess) {
             const float* h1 = reinterpret_cast<const float*>(H + SL.theta);
             m_lastTheta1.assign(h1, h1 + nq);
-            if (learned)
+            if (m_b.learned)
                 m_lastThetaA.assign(m_hThetaA, m_hThetaA + nq);
             else
                 m_lastThetaA.assign(nq, -INFINITY);
-            firstSync = false;
         }
-        if (ce != cudaSuccess) break;
+        firstSync = false;
+        if (m_b.ce != cudaSuccess) break;
         uint32_t nre = 0;
         for (uint32_t q = 0; q < nq; ++q) {
             m_lastStatus[q] |= hStatus[q] & ~kStatusOverflow;
@@ -882,8 +943,8 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
             break;
         }
         ++retries;
-        ck(cudaMemcpyAsync(dQlist, hQlist, nre * 4ull, cudaMemcpyHostToDevice, stream));
-        ck(cudaMemsetAsync(dStatus, 0, nq * 4ull, stream));
+        Ck(cudaMemcpyAsync(dQlist, hQlist, nre * 4ull, cudaMemcpyHostToDevice, stream));
+        Ck(cudaMemsetAsync(dStatus, 0, nq * 4ull, stream));
         // A tensor-core re-run helps when the first threshold was loose. When the docs inside the
         // 2 eps band around the K-th score alone overflow the list, only a tighter bound helps: from the
         // second re-run on, the queries go through the FP32 SIMT pass (bound ~2 gamma_d |q||v|). Their
@@ -892,38 +953,49 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         if (simt) {
             // the plain path for these queries: SIMT bounds (for the re-run queries only, so every other
             // query keeps the bound its own pass used), a SIMT doc sample for a fresh threshold
-            const double rel = SimtRelBound(dim);
-            ck(launch_query_eps(dQueries, dQlist, nre, dim, T.GetMaxNorm(), rel, rel, dEpsMain, dEpsSamp, stream));
-            (void)sample(dQlist, nre, true);
-            launches += 3;
+            const DataTable& T = *m_table;
+            const double rel = SimtRelBound(T.GetDimension());
+            Ck(launch_query_eps(m_b.dQueries, dQlist, nre, T.GetDimension(), T.GetMaxNorm(), rel, rel,
+                                reinterpret_cast<float*>(D + SL.epsMain), reinterpret_cast<float*>(D + SL.epsSamp),
+                                stream));
+            (void)Sample(dQlist, nre, true);
+            m_b.launches += 3;
         } else if (tc) {
-            stage(dQlist, nre);  // the staged rows become the re-run queries (their bounds unchanged)
-            ++launches;
+            Stage(dQlist, nre);  // the staged rows become the re-run queries (their bounds unchanged)
+            ++m_b.launches;
         }
         // one pass over every tile with the raised threshold
-        const uint64_t tilesR = tilesOf(unitOf(nre, simt));
-        const uint32_t segs = segsOf(nre, tilesR, C, simt);
-        const uint32_t segCap = segCapOf(nre, tilesR, C, segs, simt);
-        cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, 1, 0, tilesR, dQlist, nre, simt);
+        const uint64_t tilesR = TilesOf(UnitOf(nre, simt));
+        const uint32_t segs = SegsOf(nre, tilesR, C, simt);
+        const uint32_t segCap = SegCapOf(nre, tilesR, C, segs, simt);
+        Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, 1, 0, tilesR, dQlist, nre, simt);
         for (uint32_t i = 0; i < nre; ++i) m_lastSegs[hQlist[i]] = {segs, segCap};
         SE.segs = segs;
         SE.seg_cap = segCap;
         SE.qlist = dQlist;
         SE.nq_list = nre;
-        ck(launch_select_topk(SE, stream));
-        launches += 2;
+        Ck(launch_select_topk(SE, stream));
+        m_b.launches += 2;
     }
-    if (tc && ce == cudaSuccess) {
-        int32_t herr = 0;
-        ck(cudaMemcpy(&herr, m_dError, sizeof(herr), cudaMemcpyDeviceToHost));
-        if (herr != 0) {
+    if (tc && m_b.ce == cudaSuccess) {
+        // the copy made with the statuses covers the first attempt; re-runs need a fresh one (stream
+        // ordered: no device-wide synchronisation, so another searcher's batch queued behind this one
+        // keeps running)
+        auto* hErr = reinterpret_cast<int32_t*>(H + SL.errWord);
+        if (retries > 0) {
+            Ck(cudaMemcpyAsync(hErr, m_dError, 4, cudaMemcpyDeviceToHost, stream));
+            Ck(cudaStreamSynchronize(stream));
+        }
+        const int32_t herr = *hErr;
+        if (m_b.ce == cudaSuccess && herr != 0) {
             m_err = "tensor-core candidate pass timed out waiting on its pipeline (error bits " +
                     std::to_string(herr) + ")";
-            cudaMemset(m_dError, 0, sizeof(int32_t));
+            cudaMemsetAsync(m_dError, 0, sizeof(int32_t), stream);
+            cudaStreamSynchronize(stream);
             return -2;
         }
     }
-    if (m_timing && ce == cudaSuccess) {
+    if (m_timing && m_b.ce == cudaSuccess) {
         cudaEventSynchronize(m_ev[4]);
         cudaEventElapsedTime(&m_times.filter, m_ev[0], m_ev[1]);
         cudaEventElapsedTime(&m_times.sample, m_ev[1], m_ev[2]);
@@ -932,9 +1004,9 @@ int FullRecallSearcher::SearchDevice(const float* dQueries, uint32_t nq, const F
         cudaEventElapsedTime(&m_times.total, m_ev[0], m_ev[4]);
     }
     m_times.retries = retries;
-    m_times.launches = launches;
-    if (ce != cudaSuccess) {
-        m_err = cudaGetErrorString(ce);
+    m_times.launches = m_b.launches;
+    if (m_b.ce != cudaSuccess) {
+        m_err = cudaGetErrorString(m_b.ce);
         return -2;
     }
     int bad = 0;

@@ -262,6 +262,19 @@ int hss_searcher_search_device(hss_searcher* s, const float* dQueries, uint32_t 
                                const uint32_t* topks, float* dOutScores, int64_t* dOutIds, uint32_t* dOutCounts,
                                uint32_t outStride, hss_stream_t stream);
 
+/* hss_searcher_search_device in two halves, so that the caller keeps the GPU busy while it waits.
+ * The first enqueues the whole batch on `stream` (the filter programs are compiled into the
+ * searcher's staging on the calling thread) and returns without waiting; the filters may be freed
+ * after it returns, the queries and outputs must stay valid until the second returns. The second
+ * waits for the batch's statuses, runs any candidate-overflow re-runs on the same stream and returns
+ * what hss_searcher_search_device returns. A searcher takes no other batch in between: two
+ * searchers of one table alternate (batch i on one while the host finishes batch i - 1 of the
+ * other), so the GPU never idles between batches while the host waits. */
+int hss_searcher_search_device_async(hss_searcher* s, const float* dQueries, uint32_t nq, const hss_filters* filters,
+                                     const uint32_t* topks, float* dOutScores, int64_t* dOutIds, uint32_t* dOutCounts,
+                                     uint32_t outStride, hss_stream_t stream);
+int hss_searcher_finish(hss_searcher* s);
+
 /* The filter stage alone (FullRecallSearcher::OneFilter, full_recall_searcher.cpp:233-262): row q of
  * dOutBits (outStrideWords u64 per row, >= segmentNum * docNumPerSegment / 64) gets query q's doc
  * bitmap (bit b of word w = doc 64w+b, docs past docNum cleared) and dPassCounts[q] (may be NULL) its

@@ -239,3 +239,45 @@ def test_cross_shard_merge_equals_the_unsharded_search(torch_cuda):
     torch.cuda.synchronize()
     want = oracle.topk(q, exprs, [K] * nq, vec, bits, threads=8)
     _check((m_sc.cpu().numpy(), m_id.cpu().numpy(), m_n.cpu().numpy()), want, nq)
+
+
+@pytest.mark.parametrize("method", [0, 2], ids=["simt", "bf16"])
+def test_two_searchers_alternate_batches_on_one_stream(torch_cuda, method):
+    # batch i is enqueued on searcher i % 2 before batch i - 1 is finished: every batch must still equal
+    # the ground truth, including batches whose candidate lists overflow and re-run in the finish half
+    torch = torch_cuda
+    mix = data.Mixture(128, 32, (0.05, 0.9), n_clusters=16, seed=51)
+    vec, bits, _ = mix.corpus(30000, seed=52)
+    table = hss.DataTable.build(vec, bits, 32, device=0, doc_num_per_segment=8192)
+    nq, nb = 32, 6
+    kk = [50, 50, 2000, 50, 2000, 50]  # K = 2000 with a small candidate cap forces re-runs
+    srch = [hss.FullRecallSearcher(table, max_batch=nq, candidate_cap=8192, sample_docs=4096, method=method)
+            for _ in range(2)]
+    q = mix.queries(nq * nb, seed=53)
+    exprs = data.make_filters(mix, nq * nb, n_tags=(1, 2), seed=54)
+    d_q = torch.tensor(q, device="cuda:0")
+    sc = torch.zeros((nb, nq, 2000), dtype=torch.float32, device="cuda:0")
+    ids = torch.zeros((nb, nq, 2000), dtype=torch.int64, device="cuda:0")
+    cnt = torch.zeros((nb, nq), dtype=torch.int32, device="cuda:0")
+    filt = [srch[0].compile_filters(exprs[b * nq:(b + 1) * nq]) for b in range(nb)]
+    sh = torch.cuda.current_stream().cuda_stream
+    retries = 0
+    for b in range(nb):
+        srch[b % 2].search_device_async(d_q[b * nq].data_ptr(), nq, filt[b], [kk[b]] * nq, sc[b].data_ptr(),
+                                        ids[b].data_ptr(), cnt[b].data_ptr(), 2000, sh)
+        if b > 0:
+            assert srch[(b - 1) % 2].finish() == 0
+            retries += srch[(b - 1) % 2].last_times()["retries"]
+    assert srch[(nb - 1) % 2].finish() == 0
+    torch.cuda.synchronize()
+    for b in range(nb):
+        qb, eb = q[b * nq:(b + 1) * nq], exprs[b * nq:(b + 1) * nq]
+        want = oracle.topk(qb, eb, [kk[b]] * nq, vec, bits, threads=8)
+        _check((sc[b].cpu().numpy(), ids[b].cpu().numpy(), cnt[b].cpu().numpy()), want, nq)
+    # a searcher refuses a second batch before the first is finished
+    srch[0].search_device_async(d_q.data_ptr(), nq, filt[0], [50] * nq, sc[0].data_ptr(), ids[0].data_ptr(),
+                                cnt[0].data_ptr(), 2000, sh)
+    with pytest.raises(hss.HssError):
+        srch[0].search_device_async(d_q.data_ptr(), nq, filt[0], [50] * nq, sc[0].data_ptr(), ids[0].data_ptr(),
+                                    cnt[0].data_ptr(), 2000, sh)
+    assert srch[0].finish() == 0
