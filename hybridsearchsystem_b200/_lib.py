@@ -132,8 +132,6 @@ SIGNATURES = [
      [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, vp, ctypes.c_uint64]),
     ("hss_filter_compile", ctypes.c_int,
      [vp, ctypes.c_char_p, vp, ctypes.c_uint32, c_u32p, vp, ctypes.c_uint32, c_u32p, c_u32p, c_i32p]),
-    ("hss_filter_compile_accumulator", ctypes.c_int,
-     [vp, ctypes.c_char_p, vp, ctypes.c_uint32, c_u32p, vp, ctypes.c_uint32, c_u32p, c_i32p]),
     ("hss_searcher_feature_dim", ctypes.c_uint32, [vp]),
     ("hss_searcher_features", ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, vp, vp, vp]),
     ("hss_searcher_set_threshold_model", ctypes.c_int, [vp, vp, ctypes.c_float]),

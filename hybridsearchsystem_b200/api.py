@@ -137,18 +137,6 @@ class DataTable:
                                              ctypes.byref(empty)))
         return prog[:pl.value].copy(), rows[:rl.value].copy(), opn.value, bool(empty.value)
 
-    def compile_filter_accumulator(self, expr):
-        """(accumulator ops, posting row of each slot, empty_tree) the range filter runs for one filter
-        text (include/hss.h, hss_filter_compile_accumulator)."""
-        ops = np.zeros(_lib.HSS_MAX_PROGRAM + _lib.HSS_MAX_OPERANDS, np.uint32)
-        rows = np.zeros(_lib.HSS_MAX_OPERANDS, np.uint32)
-        ol, rl = ctypes.c_uint32(), ctypes.c_uint32()
-        empty = ctypes.c_int32()
-        check(_lib.load().hss_filter_compile_accumulator(self._h, expr.encode(), _np_ptr(ops), ops.size,
-                                                         ctypes.byref(ol), _np_ptr(rows), rows.size, ctypes.byref(rl),
-                                                         ctypes.byref(empty)))
-        return ops[:ol.value].copy(), rows[:rl.value].copy(), bool(empty.value)
-
 
 class Filters:
     """A batch's filter texts compiled once (TextFilter::PrepareExpr)."""

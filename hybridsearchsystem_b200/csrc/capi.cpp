@@ -803,38 +803,4 @@ int hss_filter_compile(const hss_table* table, const char* filterExpr, uint32_t*
     return HSS_OK;
 }
 
-int hss_filter_compile_accumulator(const hss_table* table, const char* filterExpr, uint32_t* ops, uint32_t opCap,
-                                   uint32_t* opLen, uint32_t* slotRows, uint32_t slotCap, uint32_t* slotLen,
-                                   int32_t* emptyTree) {
-    if (!table || !opLen || !slotLen) return SetError(HSS_ERR_INVALID, "null argument");
-    bool ok = true;
-    auto ast = hss::ParseFilter(filterExpr ? filterExpr : "", ok);
-    if (!ok) return SetError(HSS_ERR_PARSE, "filter does not parse");
-    auto tree = hss::BuildQueryNode(ast.get(), table->t->GetConfig().postingField);
-    hss::FilterExpr e;
-    std::string err;
-    if (!hss::PrepareExpr(tree.get(), *table->t, e, &err)) return SetError(HSS_ERR_PROGRAM, err);
-    if (emptyTree) *emptyTree = e.emptyTree ? 1 : 0;
-    // slots in first-use order over the operand list, as the searcher assigns them within a batch
-    std::vector<uint32_t> rows, slots(e.postingRows.size());
-    for (size_t j = 0; j < e.postingRows.size(); ++j) {
-        const uint32_t r = std::min(e.postingRows[j], table->t->PostingRows() - 1);
-        const auto it = std::find(rows.begin(), rows.end(), r);
-        slots[j] = static_cast<uint32_t>(it - rows.begin());
-        if (it == rows.end()) rows.push_back(r);
-    }
-    std::vector<uint32_t> code;
-    bool fits = true;
-    if (!e.emptyTree && !hss::CompileMicro(e.postExpr.data(), static_cast<uint32_t>(e.postExpr.size()), slots.data(),
-                                           static_cast<uint32_t>(slots.size()), code, &fits))
-        return SetError(HSS_ERR_PROGRAM, "malformed filter program");
-    if (!fits) return SetError(HSS_ERR_LIMIT, "filter program deeper than the range filter's register stack");
-    *opLen = static_cast<uint32_t>(code.size());
-    *slotLen = static_cast<uint32_t>(rows.size());
-    if (*opLen > opCap || *slotLen > slotCap) return SetError(HSS_ERR_LIMIT, "output buffers too small");
-    if (ops) std::copy(code.begin(), code.end(), ops);
-    if (slotRows) std::copy(rows.begin(), rows.end(), slotRows);
-    return HSS_OK;
-}
-
 }  // extern "C"

@@ -689,133 +689,6 @@ __global__ void __launch_bounds__(kWideT, kWideCtasPerSm) filter_dense_wide_kern
     if (t == 0 && L.status && !empty && !ok) atomicOr(L.status + q, kStatusBadProgram);
 }
 
-// ---------------------------------------------------------------------------------------------
-// Range filter. A persistent CTA per SM walks ranges of kRangeT-aligned word columns. For each range
-// it copies the range's words of every row the batch reads into shared memory (16-byte cp.async,
-// double buffered: the next range's copy overlaps this range's evaluation), then evaluates the
-// batch's programs there: a warp takes one (query, 32-word chunk) item at a time, one word per lane,
-// so the program is uniform across the warp. The programs are the host-compiled accumulator form
-// (MicroOp): no stack in memory, every operand a shared-memory load. Operand rows cross DRAM once
-// per batch, coalesced; each bitmap row is written in 256-byte runs.
-constexpr int kRangeT = 512;
-constexpr size_t kRangeSmem = 225 * 1024;  // dynamic shared memory of one CTA
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, uint32_t src_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
-                     static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
-                 "l"(gmem), "r"(src_bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// One word of an accumulator program: row slot i's word is rows[i * W] (rows points at this lane's
-// word of slot 0). Slots are clamped into [0, nrows); pops below the register stack read zero.
-__device__ __forceinline__ uint64_t eval_micro(const uint32_t* __restrict__ mp, uint32_t len,
-                                               const uint64_t* rows, uint32_t W, uint32_t nrows) {
-    uint64_t acc = 0, s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    for (uint32_t i = 0; i < len; ++i) {
-        const uint32_t m = __ldg(mp + i);
-        const uint32_t code = m & 15u;
-        uint64_t x = 0;
-        if (code <= kMicroOr && nrows) {
-            uint32_t slot = m >> kMicroSlotShift;
-            slot = slot < nrows ? slot : nrows - 1;
-            x = rows[static_cast<size_t>(slot) * W];
-        }
-        if (m & kMicroNeg) x = ~x;
-        switch (code) {
-            case kMicroPush:
-            case kMicroZero:
-                s3 = s2;
-                s2 = s1;
-                s1 = s0;
-                s0 = acc;
-                acc = code == kMicroZero ? 0ull : x;
-                break;
-            case kMicroAnd: acc &= x; break;
-            case kMicroOr: acc |= x; break;
-            case kMicroAndPop:
-            case kMicroOrPop:
-                acc = code == kMicroAndPop ? (acc & s0) : (acc | s0);
-                s0 = s1;
-                s1 = s2;
-                s2 = s3;
-                s3 = 0;
-                break;
-            case kMicroNot: acc = ~acc; break;
-            default: break;
-        }
-    }
-    return acc;
-}
-
-__global__ void __launch_bounds__(kRangeT, 1) filter_range_kernel(RangeFilterLaunch L, uint32_t W) {
-    extern __shared__ __align__(16) uint64_t rbuf[];  // [2][nrows][W], then [nq] counts
-    const uint32_t nrows = L.nrows;
-    const size_t buf_words = static_cast<size_t>(nrows) * W;
-    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(rbuf + 2 * buf_words);
-    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
-    constexpr uint32_t nwarps = kRangeT / 32;
-    const uint64_t nranges = (L.row_words + W - 1) / W;
-    for (uint32_t q = t; q < L.nq; q += kRangeT) s_cnt[q] = 0;
-
-    // copy range r's words of every listed row into buffer b (words past the row read as zero)
-    auto issue = [&](uint64_t r, uint32_t b) {
-        const uint32_t per_row = W / 2;  // 16-byte chunks
-        const uint32_t chunks = nrows * per_row;
-        uint64_t* dst0 = rbuf + b * buf_words;
-        for (uint32_t c = t; c < chunks; c += kRangeT) {
-            const uint32_t slot = c / per_row, k = c - slot * per_row;
-            const uint64_t gw = r * W + 2ull * k;
-            uint32_t row = L.row_list[slot];
-            row = row < L.rows ? row : L.rows - 1;
-            const bool in = gw < L.row_words;  // row_words is even: both words of the chunk are in
-            const uint64_t* src = in ? L.dense + static_cast<uint64_t>(row) * L.row_words + gw : L.dense;
-            cp_async16(dst0 + static_cast<size_t>(slot) * W + 2 * k, src, in ? 16u : 0u);
-        }
-        cp_async_commit();
-    };
-
-    uint32_t b = 0;
-    if (blockIdx.x < nranges) issue(blockIdx.x, 0);
-    const uint32_t chunks = W / 32;
-    const uint32_t items = L.nq * chunks;
-    for (uint64_t r = blockIdx.x; r < nranges; r += gridDim.x, b ^= 1u) {
-        if (r + gridDim.x < nranges)
-            issue(r + gridDim.x, b ^ 1u);
-        else
-            cp_async_commit();  // an empty group keeps the group count uniform
-        cp_async_wait<1>();     // this range's copy (all but the newest group) has landed
-        __syncthreads();
-        const uint64_t* rows = rbuf + b * buf_words;
-        for (uint32_t item = warp; item < items; item += nwarps) {
-            const uint32_t q = item / chunks, c = item - q * chunks;
-            const uint32_t wl = c * 32u + lane;
-            const uint64_t gw = r * W + wl;
-            const uint32_t m0 = __ldg(L.micro_off + q), m1 = __ldg(L.micro_off + q + 1);
-            uint64_t v = m1 == m0 ? ~0ull : eval_micro(L.micro + m0, m1 - m0, rows + wl, W, nrows);
-            uint32_t cnt = 0;
-            if (gw < L.row_words) {
-                if ((gw + 1) * 64 > L.doc_num) v &= tail_mask(gw, L.doc_num);
-                L.out[static_cast<uint64_t>(q) * L.out_stride + gw] = v;
-                cnt = __popcll(v);
-            }
-            cnt = warp_sum(cnt);
-            if (lane == 0 && cnt) atomicAdd(s_cnt + q, cnt);
-        }
-        __syncthreads();  // buffer b is refilled two ranges on
-    }
-    cp_async_wait<0>();
-    __syncthreads();
-    if (L.pass_count)
-        for (uint32_t q = t; q < L.nq; q += kRangeT)
-            if (s_cnt[q]) atomicAdd(L.pass_count + q, s_cnt[q]);
-}
-
 // One CTA per posting: expand `src[i]` (any layout) into the dense bitset `dst[i]` of
 // byte_size bytes (the PostingBitListToSet operator, bitlist_to_set.h:6-155).
 __global__ void __launch_bounds__(256) posting_expand_kernel(const uint64_t* src, const uint64_t* dst, uint32_t count,
@@ -935,27 +808,6 @@ cudaError_t launch_filter_dense(const DenseFilterLaunch& L, cudaStream_t stream)
     if (4 * kDenseT * per_word <= 48 * 1024 && L.seg_words >= 2 * kDenseT) return launch_filter_dense_wpt<4>(L, stream);
     if (2 * kDenseT * per_word <= 48 * 1024) return launch_filter_dense_wpt<2>(L, stream);
     return launch_filter_dense_wpt<1>(L, stream);
-}
-
-cudaError_t launch_filter_range(const RangeFilterLaunch& L, cudaStream_t stream) {
-    if (L.nq == 0 || L.row_words == 0) return cudaSuccess;
-    if (L.rows == 0 || L.nrows > kRangeMaxRows || (L.row_words & 1u) || (reinterpret_cast<uintptr_t>(L.dense) & 15u) ||
-        (L.nrows && !L.row_list) || !L.micro_off || !L.out)
-        return cudaErrorInvalidValue;
-    // words per range: as many as two buffers of every listed row hold, 32 to 1024
-    const size_t counts = static_cast<size_t>(L.nq) * sizeof(uint32_t);
-    if (counts + 2 * 32 * 8 * static_cast<size_t>(L.nrows) > kRangeSmem) return cudaErrorInvalidValue;
-    uint64_t W = L.nrows ? (kRangeSmem - counts) / (16ull * L.nrows) : 1024;
-    W = W > 1024 ? 1024 : W & ~31ull;
-    const size_t smem = 2 * static_cast<size_t>(L.nrows) * W * 8 + counts;
-    const uint64_t nranges = (L.row_words + W - 1) / W;
-    const uint32_t sms = L.sm_count ? L.sm_count : 148;
-    const uint32_t grid = static_cast<uint32_t>(nranges < sms ? nranges : sms);
-    cudaError_t e = cudaFuncSetAttribute(filter_range_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kRangeSmem));
-    if (e != cudaSuccess) return e;
-    filter_range_kernel<<<grid, kRangeT, smem, stream>>>(L, static_cast<uint32_t>(W));
-    return cudaGetLastError();
 }
 
 cudaError_t launch_posting_expand(const uint64_t* src, const uint64_t* dst, uint32_t count, uint32_t byte_size,

@@ -83,12 +83,6 @@ struct FilterExpr {
     bool emptyTree = false;  // match all
 };
 
-// The range filter's accumulator form (MicroOp) of a postfix program whose operand j reads row slot
-// slots[j]; false for a malformed program (the stack-machine kernels' rules), *fits false when the
-// program needs more stack than the range filter's registers hold (query_node.cpp).
-bool CompileMicro(const uint32_t* prog, uint32_t plen, const uint32_t* slots, uint32_t nop, std::vector<uint32_t>& out,
-                  bool* fits);
-
 class QueryNode {
    public:
     virtual ~QueryNode() = default;
@@ -587,7 +581,6 @@ class FullRecallSearcher {
     bool m_timing = false;
     StageTimes m_times;
     std::vector<int32_t> m_lastStatus;
-    std::vector<uint32_t> m_slotOfRow;  // range filter: shared-memory slot of each posting row in a batch
     std::vector<std::pair<uint32_t, uint32_t>> m_lastSegs;  // per query: (segments, entries per segment)
     std::shared_ptr<ThresholdModel> m_model;
     float m_margin = 0.0f;

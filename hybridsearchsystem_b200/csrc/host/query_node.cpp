@@ -7,9 +7,6 @@
 //   CONJUNCTION:  [0, parts, n_1 .. n_parts]: AND over parts of the OR of each part's postings.
 // Postings are consumed in the order they are appended, so operand i of the program is
 // FilterExpr::postingRows[i].
-#include <algorithm>
-
-#include "../hss_device.cuh"
 #include "hss_host.h"
 
 namespace hss {
@@ -235,76 +232,5 @@ bool PrepareExpr(const QueryNode* tree, const DataTable& table, FilterExpr& out,
     }
     return true;
 }
-
-// Compiles a postfix program of the reference's form ([AND|OR|NOT, postingNum, stackNum],
-// [CONJUNCTION, parts, n_1..n_parts]; the kernels' interpretation and checks) into the range
-// filter's accumulator form (MicroOp), operand j addressed by its row slot slots[j]. AND and OR are
-// associative and commutative on bits, so the popped entries and the operand rows may be combined
-// in any order. False for a malformed program; *fits is false when it needs more than the register
-// stack holds (the caller then uses the stack-machine kernel).
-bool CompileMicro(const uint32_t* prog, uint32_t plen, const uint32_t* slots, uint32_t nop, std::vector<uint32_t>& out,
-                  bool* fits) {
-    uint32_t sp = 0, next = 0, pc = 0, deepest = 0;
-    auto emit = [&](uint32_t code, uint32_t slot, bool neg) {
-        out.push_back(code | (neg ? kMicroNeg : 0u) | (slot << kMicroSlotShift));
-    };
-    auto grow = [&]() { deepest = std::max(deepest, ++sp); };
-    while (pc < plen) {
-        const uint32_t op = prog[pc];
-        if (op == AND || op == OR || op == NOT) {
-            if (pc + 2 >= plen) return false;
-            const uint32_t pn = prog[pc + 1], sn = prog[pc + 2];
-            pc += 3;
-            const bool ok = op == NOT ? ((pn == 1 && sn == 0) || (pn == 0 && sn == 1)) : (pn != 0 || sn != 0);
-            if (!ok || pn > nop - next || sn > sp) return false;
-            if (op == NOT) {
-                if (pn) {
-                    emit(kMicroPush, slots[next], true);
-                    grow();
-                } else {
-                    emit(kMicroNot, 0, false);
-                }
-            } else {
-                const uint32_t rowOp = op == AND ? kMicroAnd : kMicroOr;
-                const uint32_t popOp = op == AND ? kMicroAndPop : kMicroOrPop;
-                uint32_t j = 0;
-                if (sn == 0) {
-                    emit(kMicroPush, slots[next], false);  // the accumulator holds the first popped entry
-                    grow();
-                    j = 1;
-                } else {
-                    for (uint32_t k = 1; k < sn; ++k) emit(popOp, 0, false);
-                    sp -= sn - 1;
-                }
-                for (; j < pn; ++j) emit(rowOp, slots[next + j], false);
-            }
-            next += pn;
-        } else if (op == CONJUNCTION) {
-            if (pc + 1 >= plen) return false;
-            const uint32_t parts = prog[pc + 1];
-            if (parts == 0 || parts > plen - pc - 2) return false;
-            for (uint32_t p = 0; p < parts; ++p) {
-                const uint32_t pn = prog[pc + 2 + p];
-                if (pn == 0 || pn > nop - next) return false;
-                emit(kMicroPush, slots[next], false);
-                grow();
-                for (uint32_t j = 1; j < pn; ++j) emit(kMicroOr, slots[next + j], false);
-                if (p > 0) {
-                    emit(kMicroAndPop, 0, false);
-                    --sp;
-                }
-                next += pn;
-            }
-            pc += 2 + parts;
-        } else {
-            return false;
-        }
-        if (sp > static_cast<uint32_t>(kMaxStack)) return false;  // the stack machine's limit
-    }
-    if (sp != 1 || next != nop) return false;
-    *fits = deepest <= static_cast<uint32_t>(kMicroStack) + 1;  // the accumulator plus the register stack
-    return true;
-}
-
 
 }  // namespace hss

@@ -62,13 +62,9 @@ double TcAccumulationBound(int format, uint32_t d) {
 
 // Offsets of the packed per-batch staging buffer.
 struct StageLayout {
-    size_t progOff, opndOff, microOff, rowList, topk, epsMain, epsSamp, negInf, theta, qlist, errWord, counters,
-        passCount,
-        candCount, sampCount, status, prog, opnd, micro, total;
+    size_t progOff, opndOff, topk, epsMain, epsSamp, negInf, theta, qlist, errWord, counters, passCount,
+        candCount, sampCount, status, prog, opnd, total;
 };
-
-// u32 words of one query's accumulator program at most: one op per operand plus one per program word.
-constexpr uint32_t kMaxMicro = kMaxProgram + kMaxOperands;
 
 StageLayout MakeLayout(uint32_t B) {
     StageLayout L{};
@@ -80,8 +76,6 @@ StageLayout MakeLayout(uint32_t B) {
     };
     L.progOff = take((B + 1) * 4ull);
     L.opndOff = take((B + 1) * 4ull);
-    L.microOff = take((B + 1) * 4ull);
-    L.rowList = take(kRangeMaxRows * 4ull);
     L.topk = take(B * 4ull);
     L.epsMain = take(B * 4ull);
     L.epsSamp = take(B * 4ull);
@@ -94,7 +88,6 @@ StageLayout MakeLayout(uint32_t B) {
     L.status = take(B * 4ull);
     L.prog = take(static_cast<size_t>(B) * kMaxProgram * 4ull);
     L.opnd = take(static_cast<size_t>(B) * kMaxOperands * 4ull);
-    L.micro = take(static_cast<size_t>(B) * kMaxMicro * 4ull);
     // per-segment candidate counts: every producing CTA writes its own, no clearing
     L.candCount = take(static_cast<size_t>(B) * kMaxCandSegs * 4ull);
     L.sampCount = take(static_cast<size_t>(B) * kMaxCandSegs * 4ull);
@@ -332,52 +325,7 @@ int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exp
         if (topk[q] > static_cast<uint32_t>(kMaxTopK)) m_lastStatus[q] |= kStatusTopKTooLarge;
     *maxKOut = maxK;
 
-    // The range filter when every program compiles into the accumulator form and the batch's
-    // distinct rows fit its shared-memory table; else the stack-machine kernel.
     const DataTable& T = *m_table;
-    const bool dense = m_cfg.densePostings && T.DeviceDensePostings() != nullptr;
-    uint32_t nrows = 0, nm = 0;
-    bool range = dense;
-    if (dense) {
-        auto* microOff = reinterpret_cast<uint32_t*>(H + SL.microOff);
-        auto* rowList = reinterpret_cast<uint32_t*>(H + SL.rowList);
-        auto* micro = reinterpret_cast<uint32_t*>(H + SL.micro);
-        m_slotOfRow.assign(T.PostingRows(), 0xffffffffu);
-        std::vector<uint32_t> slots, code;
-        for (uint32_t q = 0; q < nq && range; ++q) {
-            microOff[q] = nm;
-            const uint32_t o0 = opndOff[q], o1 = opndOff[q + 1];
-            const uint32_t pl = progOff[q + 1] - progOff[q];
-            if (pl == 0) continue;  // match all
-            slots.resize(o1 - o0);
-            for (uint32_t j = o0; j < o1 && range; ++j) {
-                const uint32_t r = std::min(opnd[j], T.PostingRows() - 1);
-                if (m_slotOfRow[r] == 0xffffffffu) {
-                    if (nrows == kRangeMaxRows) {
-                        range = false;
-                        break;
-                    }
-                    m_slotOfRow[r] = nrows;
-                    rowList[nrows++] = r;
-                }
-                slots[j - o0] = m_slotOfRow[r];
-            }
-            if (!range) break;
-            code.clear();
-            bool fits = true;
-            if (!CompileMicro(prog + progOff[q], pl, slots.data(), o1 - o0, code, &fits)) {
-                m_lastStatus[q] |= kStatusBadProgram;  // as the stack machine reports it: match nothing
-                code.assign(1, kMicroZero);
-            } else if (!fits) {
-                range = false;
-                break;
-            }
-            std::memcpy(micro + nm, code.data(), code.size() * 4);
-            nm += static_cast<uint32_t>(code.size());
-        }
-        if (range) microOff[nq] = nm;
-    }
-
     cudaError_t ce = cudaSuccess;
     auto ck = [&](cudaError_t e) {
         if (ce == cudaSuccess && e != cudaSuccess) ce = e;
@@ -388,27 +336,7 @@ int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exp
     ck(cudaMemcpyAsync(D + SL.opnd, H + SL.opnd, no * 4ull, cudaMemcpyHostToDevice, stream));
     ck(cudaMemsetAsync(D + SL.counters, 0, SL.prog - SL.counters, stream));
 
-    if (dense) {
-        if (range) {
-            // (the offsets and the row list went with the bulk copy above)
-            if (nm) ck(cudaMemcpyAsync(D + SL.micro, H + SL.micro, nm * 4ull, cudaMemcpyHostToDevice, stream));
-            RangeFilterLaunch R{};
-            R.micro = reinterpret_cast<const uint32_t*>(D + SL.micro);
-            R.micro_off = reinterpret_cast<const uint32_t*>(D + SL.microOff);
-            R.row_list = reinterpret_cast<const uint32_t*>(D + SL.rowList);
-            R.nrows = nrows;
-            R.dense = T.DeviceDensePostings();
-            R.rows = T.PostingRows();
-            R.row_words = T.GetBitmapWords();
-            R.out = dBits;
-            R.out_stride = bitsStride;
-            R.pass_count = reinterpret_cast<uint32_t*>(D + SL.passCount);
-            R.nq = nq;
-            R.doc_num = T.GetDocNum();
-            R.sm_count = m_numSms;
-            ck(launch_filter_range(R, stream));
-            return ce == cudaSuccess ? 0 : static_cast<int>(ce);
-        }
+    if (m_cfg.densePostings && T.DeviceDensePostings()) {
         DenseFilterLaunch F{};
         F.prog = reinterpret_cast<const uint32_t*>(D + SL.prog);
         F.prog_off = reinterpret_cast<const uint32_t*>(D + SL.progOff);

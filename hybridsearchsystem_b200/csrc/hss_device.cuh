@@ -18,24 +18,6 @@ constexpr int kDocTile = 128;        // docs per scoring tile
 // Filter operator codes (the reference's FilterOpType, query_node.h:17-22).
 enum DeviceFilterOp : uint32_t { kOpConjunction = 0, kOpAnd = 1, kOpOr = 2, kOpNot = 3 };
 
-// Accumulator form of a filter program, compiled on the host from the postfix program for the
-// range filter (filter.cu, filter_range_kernel). One u32 per op: code in bits 0-3, kMicroNeg
-// (complement the row word first), the operand's shared-memory row slot in bits 16-31. The
-// accumulator holds the newest value; kMicroPush moves it onto a register stack of kMicroStack
-// entries, the *Pop ops combine the accumulator with the entry they pop.
-enum MicroOp : uint32_t {
-    kMicroPush = 0,    // push acc; acc = row
-    kMicroAnd = 1,     // acc &= row
-    kMicroOr = 2,      // acc |= row
-    kMicroAndPop = 3,  // acc &= pop
-    kMicroOrPop = 4,   // acc |= pop
-    kMicroNot = 5,     // acc = ~acc
-    kMicroZero = 6,    // push acc; acc = 0 (a program that matches nothing)
-};
-constexpr uint32_t kMicroNeg = 0x10u;
-constexpr uint32_t kMicroSlotShift = 16;
-constexpr int kMicroStack = 4;
-
 // Posting layouts (the reference's PostingLayout, posting_layout.h:8).
 enum Layout : uint32_t {
     kDenseBitmap = 0,

@@ -61,28 +61,6 @@ struct DenseFilterLaunch {
 };
 cudaError_t launch_filter_dense(const DenseFilterLaunch& L, cudaStream_t stream);
 
-// Batched filter over the dense posting matrix by word ranges (filter.cu): a CTA copies one range of
-// words of every row the batch reads (row_list) into shared memory, then evaluates every query's
-// accumulator program (MicroOp, operands addressed by row slot) over that range. Every operand word
-// comes from DRAM once per batch and each bitmap word is written once.
-struct RangeFilterLaunch {
-    const uint32_t* micro;      // concatenated accumulator programs
-    const uint32_t* micro_off;  // [nq + 1]; an empty program matches all
-    const uint32_t* row_list;   // [nrows] dense-matrix row of each shared-memory slot
-    uint32_t nrows;
-    const uint64_t* dense;      // [rows][row_words], 16-byte aligned
-    uint32_t rows;
-    uint64_t row_words;         // words of a dense row = words of a bitmap row (even)
-    uint64_t* out;              // [nq][out_stride]
-    uint64_t out_stride;
-    uint32_t* pass_count;       // [nq] docs passing, accumulated (zeroed by the caller), or null
-    uint32_t nq;
-    uint64_t doc_num;
-    uint32_t sm_count;          // SMs of the device (0: 148)
-};
-// Largest shared-memory row count the range filter takes (the caller uses filter_dense beyond it).
-constexpr uint32_t kRangeMaxRows = 768;
-cudaError_t launch_filter_range(const RangeFilterLaunch& L, cudaStream_t stream);
 
 // Candidate lists are segmented so that no producer needs a global atomic: query q's region
 // [q * cap, (q + 1) * cap) is cut into segments of seg_cap entries; segment g (at g * seg_cap) is

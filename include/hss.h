@@ -407,17 +407,6 @@ int hss_filter_compile(const hss_table* table, const char* filterExpr, uint32_t*
                        uint32_t* progLen, uint32_t* rows, uint32_t rowCap, uint32_t* rowLen, uint32_t* opNum,
                        int32_t* emptyTree);
 
-/* Inspection of the accumulator form the searcher's range filter runs for one filter text: ops
- * (one u32 each: bits 0-3 the op -- 0 push row, 1 AND row, 2 OR row, 3 AND pop, 4 OR pop, 5 NOT,
- * 6 push zero; bit 4 complements the row; bits 16-31 the row slot) and, per slot, the posting row it
- * reads. An accumulator holds the newest value; "push" moves it onto a stack. No counterpart in the
- * reference, which interprets the postfix program with a stack in global memory
- * (kernel_bitmap_text_filter.cpp:52-119); this form is the same program compiled for registers.
- * HSS_ERR_LIMIT when the program needs a deeper stack (the searcher then runs the postfix form). */
-int hss_filter_compile_accumulator(const hss_table* table, const char* filterExpr, uint32_t* ops, uint32_t opCap,
-                                   uint32_t* opLen, uint32_t* slotRows, uint32_t slotCap, uint32_t* slotLen,
-                                   int32_t* emptyTree);
-
 /* Last error message of this thread ("" when none). */
 const char* hss_last_error(void);
 /* Number of visible CUDA devices (0 without a GPU). */

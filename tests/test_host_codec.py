@@ -194,57 +194,6 @@ def test_index_config_is_validated():
         hss.DataTable.build(np.zeros((10, 6), np.float32), bits, 8, device=-1, doc_num_per_segment=128)  # dim % 4
 
 
-def _run_accumulator(ops, slot_words):
-    """Reference interpretation of the range filter's accumulator ops (include/hss.h,
-    hss_filter_compile_accumulator) over per-slot word arrays."""
-    n = slot_words[0].size if slot_words else 1
-    full = np.full(n, np.uint64(0xFFFFFFFFFFFFFFFF), np.uint64)
-    acc, stack = np.zeros(n, np.uint64), []
-    for m in ops.tolist():
-        code, neg, slot = m & 15, (m >> 4) & 1, m >> 16
-        x = slot_words[slot] if code <= 2 else None
-        if x is not None and neg:
-            x = x ^ full
-        if code in (0, 6):
-            stack.append(acc)
-            acc = np.zeros(n, np.uint64) if code == 6 else x.copy()
-        elif code == 1:
-            acc = acc & x
-        elif code == 2:
-            acc = acc | x
-        elif code in (3, 4):
-            top = stack.pop()
-            acc = (acc & top) if code == 3 else (acc | top)
-        elif code == 5:
-            acc = acc ^ full
-        else:
-            raise AssertionError(f"unknown op {m:#x}")
-    assert len(stack) <= 4, "deeper than the range filter's register stack"
-    return acc
-
-
-def test_accumulator_form_equals_postfix_program():
-    # the form the range filter evaluates in registers must equal the postfix program (the oracle's
-    # stack machine) on random operand words, for every filter shape the searcher sees
-    mix, vec, bits, table = _small_table(seed=5, tags=64)
-    rng = np.random.default_rng(9)
-    exprs = data.make_filters(mix, 300, n_tags=(1, 6), seed=10) + \
-        ["1 AND (2 OR 3) AND NOT (4 AND (5 OR NOT 6))", "NOT 7", "(1 OR 2) AND (3 OR 4) AND (5 OR 6)",
-         "NOT (1 AND 2) OR NOT (3 OR 4)", "9999", "NOT 9999 AND 3"]
-    for e in exprs:
-        prog, rows, opn, empty = table.compile_filter(e)
-        ops, slot_rows, empty2 = table.compile_filter_accumulator(e)
-        assert empty == empty2
-        if empty:
-            assert ops.size == 0
-            continue
-        words = {int(r): rng.integers(0, 2 ** 63, 16, dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, 16, dtype=np.uint64)
-                 for r in set(rows.tolist())}
-        want = oracle.eval_postfix(prog, opn, [words[int(r)] for r in rows], 16)
-        got = _run_accumulator(ops, [words[int(r)] for r in slot_rows])
-        assert want is not None and (got == want).all(), e
-
-
 def _ref_half(x):
     """The reference's own Float32ToFloat16 (trans_number.cpp:38-83) of every float in x."""
     r = oracle.ref()
