@@ -159,7 +159,8 @@ constexpr int kMaxTcStages = 12;
 struct TcCandLaunch {
     int format;                // TcFormat of both the corpus copy and the staged queries
     uint32_t kblocks;          // dim * element bytes / 128
-    uint32_t stages;           // k-block stages in the TMA ring (set by launch_tc_cand)
+    uint32_t stages;           // stages in the TMA ring (set by launch_tc_cand)
+    uint32_t group;            // corpus k-blocks per ring stage (set by launch_tc_cand; 1 or 2)
     const float* doc_scale;    // E4M3: per-doc dequantisation scale
     const float2* tile_scale;  // E4M3: per 128-doc tile (min, max) of doc_scale
     const float* q_scale;      // E4M3: per staged query row
@@ -180,7 +181,7 @@ struct TcCandLaunch {
     int32_t* error;            // device error bits (bounded waits that expired)
     // Pipeline test knobs (single-SM kernel): wait_budget > 0 replaces the clock budget of the waits
     // that can abort the pass; hold_load > 0 makes the producer stop before issuing its
-    // (hold_load)-th corpus k-block load, so the MMA issuer's wait for it runs out.
+    // (hold_load)-th corpus stage, so the MMA issuer's wait for it runs out.
     long long wait_budget;
     uint32_t hold_load;
 };
@@ -195,8 +196,12 @@ uint32_t tc_tile_docs(uint32_t rows, uint32_t kblocks);
 // CTAs of a tensor-core pass over tile_count such tiles into lists of `cap` entries; it writes two
 // list segments per CTA.
 uint32_t tc_cand_ctas(uint32_t rows, uint32_t kblocks, uint64_t tile_count, int num_sms, uint32_t cap);
-size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages);
-size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages);
+// Corpus k-blocks per ring stage of a pass over `kblocks` k-blocks (single SM or SM pair): two when
+// they divide the row and three such stages still fit beside the resident queries, else one. A
+// stage is one TMA barrier: the fewer stages per tile, the fewer waits in the MMA issuer's loop.
+uint32_t tc_group(uint32_t kblocks, bool pair);
+size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages, uint32_t group);
+size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages, uint32_t group);
 cudaError_t launch_tc_cand(const TcCandLaunch& L, const CUtensorMap& doc_map, const CUtensorMap& qry_map, int sms,
                            cudaStream_t stream);
 // 2D tensor map over [rows][dim] elements of `format`, 128-byte swizzle, box {128 bytes, 128 rows}.

@@ -80,6 +80,7 @@ __device__ inline bool mbar_wait_drain(unsigned long long* bar, uint32_t parity)
 // or another role already aborted.
 __device__ inline bool mbar_wait(unsigned long long* bar, uint32_t parity, TcShared& S, int32_t* err, int code,
                                  long long budget = kWaitBudget) {
+    if (mbar_try(bar, parity)) return true;  // no clock read when the phase is already complete
     const long long t0 = clock64();
     while (!mbar_try(bar, parity)) {
         if (S.abort) return false;
@@ -395,9 +396,12 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
     // 1024-byte aligned operand region: queries [H][kb][16 KB], then the stage ring
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t kb_n = L.kblocks;
+    const uint32_t G = L.group;                           // k-blocks per stage
+    const uint32_t sg_n = kb_n / G;                       // stages per tile
+    const size_t stage_bytes = static_cast<size_t>(G) * kStageBytes;
     unsigned char* qsm = base;
     unsigned char* ring = base + static_cast<size_t>(H) * kb_n * kStageBytes;
-    TcShared& S = *reinterpret_cast<TcShared*>(ring + static_cast<size_t>(L.stages) * kStageBytes);
+    TcShared& S = *reinterpret_cast<TcShared*>(ring + static_cast<size_t>(L.stages) * stage_bytes);
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t stages = L.stages;
@@ -442,16 +446,17 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
             TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, blockIdx.x, gridDim.x);
             for (uint64_t it = blockIdx.x; it < ntiles && !S.abort && !held; it += gridDim.x, walk.advance()) {
                 const int y = static_cast<int>(walk.tile() * kRows);
-                for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                for (uint32_t g = 0; g < sg_n; ++g, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
                     if (L.hold_load && n + 1 >= L.hold_load) {  // pipeline test: stop issuing here
                         held = true;
                         break;
                     }
                     if (!mbar_wait(&S.empty[s], ph ^ 1u, S, L.error, 1, budget)) break;
-                    mbar_expect_tx(&S.full[s], kStageBytes);
-                    tma_load_2d(ring + static_cast<size_t>(s) * kStageBytes, &doc_map,
-                                static_cast<int>(kb * (128 / Fmt<F>::elem)), y, &S.full[s]);
+                    mbar_expect_tx(&S.full[s], static_cast<uint32_t>(stage_bytes));
+                    for (uint32_t j = 0; j < G; ++j)
+                        tma_load_2d(ring + s * stage_bytes + j * kStageBytes, &doc_map,
+                                    static_cast<int>((g * G + j) * (128 / Fmt<F>::elem)), y, &S.full[s]);
                 }
             }
             S.n_issued = n;
@@ -465,21 +470,24 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
                 if (!mbar_wait(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4, budget)) break;
                 fence_after();
                 bool ok = true;
-                for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                for (uint32_t g = 0; g < sg_n; ++g, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
                     if (!mbar_wait(&S.full[s], ph, S, L.error, 8, budget)) {
                         ok = false;
                         break;
                     }
                     fence_after();
-                    const uint64_t bdesc = smem_desc(smem_u32(ring + static_cast<size_t>(s) * kStageBytes));
+                    for (uint32_t j = 0; j < G; ++j) {
+                        const uint32_t kb = g * G + j;
+                        const uint64_t bdesc = smem_desc(smem_u32(ring + s * stage_bytes + j * kStageBytes));
 #pragma unroll
-                    for (uint32_t ks = 0; ks < 4; ++ks) {  // 32 bytes of K per instruction
+                        for (uint32_t ks = 0; ks < 4; ++ks) {  // 32 bytes of K per instruction
 #pragma unroll
-                        for (int h = 0; h < H; ++h) {
-                            const uint64_t adesc =
-                                smem_desc(smem_u32(qsm + (static_cast<size_t>(h) * kb_n + kb) * kStageBytes));
-                            mma<F>(tmem + (buf * H + h) * 128u, adesc + ks * 2u, bdesc + ks * 2u, (kb | ks) != 0);
+                            for (int h = 0; h < H; ++h) {
+                                const uint64_t adesc =
+                                    smem_desc(smem_u32(qsm + (static_cast<size_t>(h) * kb_n + kb) * kStageBytes));
+                                mma<F>(tmem + (buf * H + h) * 128u, adesc + ks * 2u, bdesc + ks * 2u, (kb | ks) != 0);
+                            }
                         }
                     }
                     mma_commit(&S.empty[s]);  // frees the stage once these MMAs have read it
@@ -588,17 +596,19 @@ __global__ void __launch_bounds__(64 + 256 * H, 1) tc_cand_kernel(const __grid_c
 // memory bandwidth before the tensor pipe.
 //
 // Each CTA's TMA loads complete on its own barriers; warp 1 of the odd CTA forwards each completed
-// stage (and the queries) to the even CTA with a remote arrive, so each CTA can always drain its own
-// copies. The even CTA's warp 1 issues the MMAs and commits them to both CTAs' barriers. Epilogue
-// warps of both CTAs return an accumulator buffer with a remote arrive on the even CTA's acc_empty.
+// stage (and the queries) to the even CTA with a remote arrive on the even CTA's barrier of the same
+// stage, which therefore takes two arrivals (its own producer's and the forwarded one): the MMA
+// issuer waits on one barrier per stage, and each CTA can always drain its own copies. The even
+// CTA's warp 1 issues the MMAs and commits them to both CTAs' barriers. Epilogue warps of both CTAs
+// return an accumulator buffer with a remote arrive on the even CTA's acc_empty. (Every wait in the
+// issuer's loop costs MMA issue slots: the issuing thread does not overlap a barrier wait with the
+// MMAs it has queued, so one wait per stage and stages of two k-blocks keep their number low.)
 struct PairShared {
-    unsigned long long full[kMaxTcStages];   // this CTA's stage loaded (TMA)
+    unsigned long long full[kMaxTcStages];   // stage loaded (TMA; even CTA: also the odd CTA's, forwarded)
     unsigned long long empty[kMaxTcStages];  // stage free (pair MMA commit, both CTAs)
-    unsigned long long pfull[kMaxTcStages];  // even CTA: the odd CTA's stage loaded (forwarded)
     unsigned long long acc_full[2];          // accumulator buffer ready (pair MMA commit, both CTAs)
     unsigned long long acc_empty[2];         // even CTA: buffer drained by the epilogue warps of both CTAs
-    unsigned long long qbar;                 // this CTA's queries loaded
-    unsigned long long pqbar;                // even CTA: the odd CTA's queries loaded (forwarded)
+    unsigned long long qbar;                 // queries loaded (even CTA: also the odd CTA's, forwarded)
     unsigned long long drain;
     uint32_t tmem_base;
     uint32_t n_issued, n_consumed;  // stage loads issued by TMA / waited for by the MMA issuer or forwarder
@@ -611,6 +621,8 @@ constexpr int kPairThreads = 64 + 32 * kPairEpiWarps;
 template <int F>
 __device__ inline bool pair_wait(unsigned long long* bar, uint32_t parity, PairShared& S, int32_t* err, int code,
                                  bool cluster_scope) {
+    // no clock read when the phase is already complete
+    if (cluster_scope ? mbar_try_cluster(bar, parity) : mbar_try(bar, parity)) return true;
     const long long t0 = clock64();
     while (!(cluster_scope ? mbar_try_cluster(bar, parity) : mbar_try(bar, parity))) {
         if (S.abort) return false;
@@ -632,7 +644,10 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t kb_n = L.kblocks;
-    constexpr size_t kStage = SQ ? 2 * kStageBytes : kStageBytes;  // bytes of one ring stage
+    const uint32_t G = SQ ? 1u : L.group;  // corpus k-blocks per stage
+    const uint32_t sg_n = kb_n / G;        // stages per tile
+    // bytes of one ring stage: G doc k-blocks, or (streamed queries) a query k-block and a doc k-block
+    const size_t kStage = SQ ? 2 * kStageBytes : static_cast<size_t>(G) * kStageBytes;
     unsigned char* qsm = base;
     unsigned char* ring = base + (SQ ? 0 : static_cast<size_t>(kb_n) * kStageBytes);
     PairShared& S = *reinterpret_cast<PairShared*>(ring + static_cast<size_t>(L.stages) * kStage);
@@ -644,16 +659,14 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < stages; ++s) {
-            mbar_init(&S.full[s], 1);
+            mbar_init(&S.full[s], rank == 0 ? 2 : 1);  // even CTA: own load + the odd CTA's, forwarded
             mbar_init(&S.empty[s], 1);
-            mbar_init(&S.pfull[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&S.acc_full[b], 1);
             mbar_init(&S.acc_empty[b], 2 * kPairEpiWarps);
         }
-        mbar_init(&S.qbar, 1);
-        mbar_init(&S.pqbar, 1);
+        mbar_init(&S.qbar, (rank == 0 && !SQ) ? 2 : 1);
         mbar_init(&S.drain, 1);
         S.abort = 0;
         S.n_issued = 0;
@@ -683,16 +696,21 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
             TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, pair, npairs);
             for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs, walk.advance()) {
                 const int y = static_cast<int>(walk.tile() * 2 * kRows + rank * kRows);
-                for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                for (uint32_t g = 0; g < sg_n; ++g, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
                     if (!pair_wait<F>(&S.empty[s], ph ^ 1u, S, L.error, 1, false)) break;
                     unsigned char* st = ring + static_cast<size_t>(s) * kStage;
                     mbar_expect_tx(&S.full[s], static_cast<uint32_t>(kStage));
-                    if (SQ)
-                        tma_load_2d(st, &qry_map, static_cast<int>(kb * (128 / Fmt<F>::elem)),
+                    if (SQ) {
+                        tma_load_2d(st, &qry_map, static_cast<int>(g * (128 / Fmt<F>::elem)),
                                     static_cast<int>(rank * kRows), &S.full[s]);
-                    tma_load_2d(st + (SQ ? kStageBytes : 0), &doc_map, static_cast<int>(kb * (128 / Fmt<F>::elem)), y,
-                                &S.full[s]);
+                        tma_load_2d(st + kStageBytes, &doc_map, static_cast<int>(g * (128 / Fmt<F>::elem)), y,
+                                    &S.full[s]);
+                    } else {
+                        for (uint32_t j = 0; j < G; ++j)
+                            tma_load_2d(st + j * kStageBytes, &doc_map,
+                                        static_cast<int>((g * G + j) * (128 / Fmt<F>::elem)), y, &S.full[s]);
+                    }
                 }
             }
             S.n_issued = n;
@@ -702,16 +720,16 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
             // forwarder: the even CTA's MMAs read this CTA's queries and stages; tell it when they land
             uint32_t n = 0;
             if (SQ || pair_wait<F>(&S.qbar, 0, S, L.error, 2, false)) {
-                if (!SQ) mbar_arrive_cluster(peer_addr(&S.pqbar, 0));
+                if (!SQ) mbar_arrive_cluster(peer_addr(&S.qbar, 0));
                 for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs) {
                     bool ok = true;
-                    for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                    for (uint32_t g = 0; g < sg_n; ++g, ++n) {
                         const uint32_t s = n % stages, ph = (n / stages) & 1u;
                         if (!pair_wait<F>(&S.full[s], ph, S, L.error, 8, false)) {
                             ok = false;
                             break;
                         }
-                        mbar_arrive_cluster(peer_addr(&S.pfull[s], 0));
+                        mbar_arrive_cluster(peer_addr(&S.full[s], 0));
                     }
                     if (!ok) break;
                 }
@@ -722,27 +740,33 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
             constexpr uint32_t idesc =
                 (1u << 4) | (Fmt<F>::ab << 7) | (Fmt<F>::ab << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
             uint32_t n = 0, iter = 0;
-            bool ok = SQ || (pair_wait<F>(&S.qbar, 0, S, L.error, 2, false) && pair_wait<F>(&S.pqbar, 0, S, L.error, 2, true));
+            // the even CTA's query barrier completes with both CTAs' query tiles (one forwarded); a
+            // one-time wait, acquired at cluster scope
+            bool ok = SQ || pair_wait<F>(&S.qbar, 0, S, L.error, 2, true);
             for (uint64_t it = pair; ok && it < ntiles && !S.abort; it += npairs, ++iter) {
                 const uint32_t buf = iter & 1u;
                 // CTA-scope waits on the barriers the odd CTA arrives on remotely (as its arrives are
                 // CTA-scope): a cluster-scope acquire on every stage cost the TF32 pass about 4 %
                 if (!pair_wait<F>(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4, false)) break;
                 fence_after();
-                for (uint32_t kb = 0; kb < kb_n; ++kb, ++n) {
+                for (uint32_t g = 0; g < sg_n; ++g, ++n) {
                     const uint32_t s = n % stages, ph = (n / stages) & 1u;
-                    if (!pair_wait<F>(&S.full[s], ph, S, L.error, 8, false) ||
-                        !pair_wait<F>(&S.pfull[s], ph, S, L.error, 8, false)) {
+                    // both CTAs' halves of the stage: this CTA's load and the odd CTA's, forwarded
+                    if (!pair_wait<F>(&S.full[s], ph, S, L.error, 8, false)) {
                         ok = false;
                         break;
                     }
                     fence_after();
                     unsigned char* st = ring + static_cast<size_t>(s) * kStage;
-                    const uint64_t adesc = smem_desc(smem_u32(SQ ? st : qsm + static_cast<size_t>(kb) * kStageBytes));
-                    const uint64_t bdesc = smem_desc(smem_u32(st + (SQ ? kStageBytes : 0)));
+                    for (uint32_t j = 0; j < G; ++j) {
+                        const uint32_t kb = g * G + j;
+                        const uint64_t adesc =
+                            smem_desc(smem_u32(SQ ? st : qsm + static_cast<size_t>(kb) * kStageBytes));
+                        const uint64_t bdesc = smem_desc(smem_u32(st + (SQ ? kStageBytes : j * kStageBytes)));
 #pragma unroll
-                    for (uint32_t ks = 0; ks < 4; ++ks)  // 32 bytes of K per instruction
-                        mma_pair<F>(tmem + buf * 256u, adesc + ks * 2u, bdesc + ks * 2u, idesc, (kb | ks) != 0);
+                        for (uint32_t ks = 0; ks < 4; ++ks)  // 32 bytes of K per instruction
+                            mma_pair<F>(tmem + buf * 256u, adesc + ks * 2u, bdesc + ks * 2u, idesc, (kb | ks) != 0);
+                    }
                     mma_commit_pair(&S.empty[s]);  // frees the stage in both CTAs once read
                 }
                 if (!ok) break;
@@ -847,7 +871,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
 template <int F, bool SQ>
 cudaError_t launch_tc2_typed(const TcCandLaunch& L, const CUtensorMap& dmap, const CUtensorMap& qmap,
                              cudaStream_t stream) {
-    const size_t smem = tc_pair_smem_bytes(L.kblocks, L.stages);
+    const size_t smem = tc_pair_smem_bytes(L.kblocks, L.stages, L.group);
     cudaError_t e = cudaFuncSetAttribute(tc2_cand_kernel<F, SQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -869,7 +893,7 @@ cudaError_t launch_tc2_typed(const TcCandLaunch& L, const CUtensorMap& dmap, con
 template <int F>
 cudaError_t launch_tc1_typed(const TcCandLaunch& L, const CUtensorMap& dmap, const CUtensorMap& qmap,
                              cudaStream_t stream) {
-    const size_t smem = tc_smem_bytes(1, L.kblocks, L.stages);
+    const size_t smem = tc_smem_bytes(1, L.kblocks, L.stages, L.group);
     cudaError_t e = cudaFuncSetAttribute(tc_cand_kernel<F, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -903,16 +927,22 @@ uint32_t tc_cand_ctas(uint32_t rows, uint32_t kblocks, uint64_t tile_count, int 
     return static_cast<uint32_t>(g * unit);
 }
 
-size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages) {
-    return 1024 + static_cast<size_t>(halves) * kblocks * kStageBytes + static_cast<size_t>(stages) * kStageBytes +
-           sizeof(TcShared);
+size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages, uint32_t group) {
+    return 1024 + static_cast<size_t>(halves) * kblocks * kStageBytes +
+           static_cast<size_t>(stages) * group * kStageBytes + sizeof(TcShared);
 }
 
-size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages) {
+size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages, uint32_t group) {
     if (tc_stream_queries(kblocks))  // no resident queries; a stage holds a query and a doc k-block
         return 1024 + static_cast<size_t>(stages) * 2 * kStageBytes + sizeof(PairShared);
-    return 1024 + static_cast<size_t>(kblocks) * kStageBytes + static_cast<size_t>(stages) * kStageBytes +
+    return 1024 + static_cast<size_t>(kblocks) * kStageBytes + static_cast<size_t>(stages) * group * kStageBytes +
            sizeof(PairShared);
+}
+
+uint32_t tc_group(uint32_t kblocks, bool pair) {
+    if (kblocks % 2 != 0 || (pair && tc_stream_queries(kblocks))) return 1;
+    const size_t fixed = pair ? tc_pair_smem_bytes(kblocks, 0, 2) : tc_smem_bytes(1, kblocks, 0, 2);
+    return fixed + 3 * 2 * static_cast<size_t>(kStageBytes) <= kSmemBudget ? 2u : 1u;
 }
 
 cudaError_t launch_tc_cand(const TcCandLaunch& Lin, const CUtensorMap& doc_map, const CUtensorMap& qry_map, int sms,
@@ -925,9 +955,10 @@ cudaError_t launch_tc_cand(const TcCandLaunch& Lin, const CUtensorMap& doc_map, 
     const bool sq = tc_stream_queries(L.kblocks);
     const bool pair = tc_tile_docs(L.nq_rows, L.kblocks) == 256u;
     // as many stages as shared memory holds next to the resident queries (or, streamed, as many
-    // query + doc stage pairs as it holds)
-    const size_t stage = sq ? 2 * kStageBytes : kStageBytes;
-    const size_t fixed = pair ? tc_pair_smem_bytes(L.kblocks, 0) : tc_smem_bytes(1, L.kblocks, 0);
+    // query + doc stage pairs as it holds); a stage holds `group` doc k-blocks
+    L.group = tc_group(L.kblocks, pair);
+    const size_t stage = sq ? 2 * kStageBytes : static_cast<size_t>(L.group) * kStageBytes;
+    const size_t fixed = pair ? tc_pair_smem_bytes(L.kblocks, 0, L.group) : tc_smem_bytes(1, L.kblocks, 0, L.group);
     if (fixed + 2 * stage > kSmemBudget) return cudaErrorInvalidValue;
     const size_t st = (kSmemBudget - fixed) / stage;
     L.stages = static_cast<uint32_t>(st < static_cast<size_t>(kMaxTcStages) ? st : kMaxTcStages);
