@@ -129,17 +129,18 @@ def test_long_vectors_are_exact(torch_cuda, method, nq):
 
 
 def test_pipeline_wait_runs_out_and_the_searcher_recovers(torch_cuda):
-    # The single-SM pass's producer stops before its 3rd corpus load, so the MMA issuer's bounded wait
-    # (about 1 ms of clock here) runs out: the pass records its error bit, drains, frees its tensor
-    # memory and returns; the batch reports the error and the same searcher's next batch is exact.
-    # Nothing faults: the wait ends by its own budget.
+    # The single-SM pass's producer stops before its first corpus stage, so every CTA's MMA issuer
+    # waits for a stage that never comes until its bounded wait (about 1 ms of clock here) runs out:
+    # the pass records its error bit, drains, frees its tensor memory and returns; the batch reports
+    # the error and the same searcher's next batch is exact. Nothing faults: each wait ends by its own
+    # budget.
     mix, vec, bits = _corpus()
     table = hss.DataTable.build(vec, bits, 64, device=0, doc_num_per_segment=8192)
     nq = 40
     q = mix.queries(nq, seed=71)
     exprs = data.make_filters(mix, nq, n_tags=(1, 3), seed=72)
     s = hss.FullRecallSearcher(table, max_batch=64, method=METHODS["bf16"])
-    s.set_pipeline_test(3, 2_000_000)
+    s.set_pipeline_test(1, 2_000_000)
     for a, e in zip(q, exprs):
         s.add_query(e, a, 50)
     with pytest.raises(hss.HssError) as err:
