@@ -69,7 +69,12 @@ def parse_args(argv=None):
                     help="the chosen form's candidate pass: simt (FP32 FFMA), tf32 (tensor cores over the FP32 "
                          "rows), bf16, e4m3")
     ap.add_argument("--learned", action="store_true", help="the chosen form uses the learned threshold")
-    ap.add_argument("--train-queries", type=int, default=32768, help="training queries of the learned threshold")
+    ap.add_argument("--train-queries", type=int, default=200_000, help="training queries of the learned threshold")
+    ap.add_argument("--val-queries", type=int, default=10_000,
+                    help="held-out queries of the learned threshold (early stop and margin)")
+    ap.add_argument("--train-steps", type=int, default=4000, help="Adam steps (batches of 512) of the model")
+    ap.add_argument("--margin-quantile", type=float, default=1.0,
+                    help="quantile of the held-out (prediction - label) residuals taken as the margin")
     ap.add_argument("--no-learned-form", dest="learned_form", action="store_false",
                     help="skip measuring the chosen format with the learned threshold beside it")
     ap.add_argument("--no-plain", dest="plain", action="store_false",
@@ -365,15 +370,42 @@ def _peaks():
         return {}
 
 
-def _topks(args, B, nb, kmix):
-    """Per-batch K arrays: the headline K, or K drawn from {10, 100, 1000} per query."""
-    if not kmix:
+def _topks(args, B, nb, kmode):
+    """Per-batch K arrays: the headline K (kmode None), K drawn from {10, 100, 1000} per query
+    ("mix"), or one K for every query (an int)."""
+    if kmode is None:
         return [np.full(B, args.topk, np.uint32) for _ in range(nb)]
+    if kmode != "mix":
+        return [np.full(B, int(kmode), np.uint32) for _ in range(nb)]
     rng = np.random.default_rng(99)
     return [rng.choice(np.array(PARITY_KS, np.uint32), B) for _ in range(nb)]
 
 
-def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=128, flush_l2=False):
+def _kmode_note(kmode):
+    if kmode is None:
+        return ""
+    return ", K from {10, 100, 1000} per query" if kmode == "mix" else f", K = {int(kmode)} for every query"
+
+
+def trained_model(args, ctx, searcher, method):
+    """The learned threshold model of a form's method, trained once per run on its own queries (seeded
+    apart from the measured ones, the same selectivity range, K drawn from {10, 100, 1000}), labels
+    from the exact path, with args.val_queries of them held out."""
+    from hybridsearchsystem_b200.threshold import fit_threshold_model
+    models = ctx.setdefault("models", {})
+    if method not in models:
+        n = args.train_queries + args.val_queries
+        tq = ctx["mix"].queries(n, seed=20)
+        te = data_filters(ctx["mix"], n, 21, pool_factor=4)  # a smaller pool keeps 210k draws to seconds
+        tk = np.random.default_rng(22).choice([10, 100, 1000], n).astype(np.uint32)
+        t0 = time.perf_counter()
+        models[method] = fit_threshold_model(searcher, tq, te, tk, hidden=256, steps=args.train_steps, seed=3,
+                                             n_val=args.val_queries, quantile=args.margin_quantile)
+        models[method][2]["train_seconds"] = round(time.perf_counter() - t0, 1)
+    return models[method]
+
+
+def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=128, flush_l2=False):
     """One form of the path (candidate-pass method, with or without the learned threshold) over the
     context's workload: device-resident QPS (CUDA events, max over ranks), end-to-end QPS through the
     C-ABI, stage times and the candidate stage's roofline. With flush_l2 (a corpus that fits in L2),
@@ -382,21 +414,16 @@ def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=12
     import torch
 
     import hybridsearchsystem_b200 as hss
-    from hybridsearchsystem_b200.threshold import fit_threshold_model
     rank, world, dev, table = ctx["rank"], ctx["world"], ctx["dev"], ctx["table"]
     queries, exprs, barrier = ctx["queries"], ctx["exprs"], ctx["barrier"]
     docs = docs or args.docs
     B = args.batch
-    kmax = max(PARITY_KS) if kmix else args.topk
+    kmax = args.topk if kmode is None else max(PARITY_KS)
     searcher = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[method],
                                       sample_docs=args.sample_docs)
     report = None
     if learned:
-        # trained on its own queries (seeded apart from the measured ones), labels from the exact path
-        tq = ctx["mix"].queries(args.train_queries, seed=20)
-        te = data_filters(ctx["mix"], args.train_queries, 21)
-        tk = np.random.default_rng(22).choice([10, 100, 1000], args.train_queries).astype(np.uint32)
-        model, margin, report = fit_threshold_model(searcher, tq, te, tk, hidden=256, steps=2000, seed=3)
+        model, margin, report = trained_model(args, ctx, searcher, method)
         searcher.set_threshold_model(model, margin)
     # A second searcher of the same form: batch i runs on searcher i % 2, so while the host finishes
     # one batch (its statuses, rare re-runs) the next is already queued on the stream.
@@ -409,7 +436,7 @@ def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=12
         srch.set_timing(True)
     nb = max(1, len(queries) // B)
     filters = [searcher.compile_filters(exprs[i * B:(i + 1) * B]) for i in range(nb)]
-    topks = _topks(args, B, nb, kmix)
+    topks = _topks(args, B, nb, kmode)
     d_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1), device=dev)
     o_sc = torch.zeros((2, B, kmax), dtype=torch.float32, device=dev)
     o_id = torch.zeros((2, B, kmax), dtype=torch.int64, device=dev)
@@ -582,7 +609,7 @@ def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=12
            "launches": launches,
            "stages_ms": dict(zip(["filter", "sample", "candidates", "select", "total"],
                                  [round(float(x), 4) for x in np.mean(np.array(stage_ms), axis=0)])),
-           "form": form_name(method, learned) + (", K from {10, 100, 1000} per query" if kmix else ""),
+           "form": form_name(method, learned) + _kmode_note(kmode),
            "l2": "flushed between steps (256 MB write outside the step's events)" if flush_l2 else
                  "inputs larger than L2",
            "method": method, "learned": learned, "searcher": searcher, "dev": dev,
@@ -594,26 +621,36 @@ def measure_form(args, ctx, method, learned=False, kmix=False, docs=None, dim=12
     if report:
         out["model"], out["margin"] = model, margin
         out["learned_report"] = {k: (round(v, 5) if isinstance(v, float) else v) for k, v in report.items()}
-        # what the model does on this workload: its estimation pass against the same pass at the doc
-        # sample's proven threshold (margin 1e9 turns the prediction into -inf), over the measured batches
-        at_sample, at_model, kk = [], [], []
-        for j in range(min(nb, 8)):
+        # what the model does on this workload, over measured batches: the docs each query's candidate
+        # passes kept (what the select step reads) without the model and with it, and the queries
+        # whose predicted threshold was too high (re-run at a proven threshold)
+        plain, with_model, miss, kk = [], [], [], []
+        for j in range(min(nb, 16)):
             f = searcher.compile_filters(exprs[j * B:(j + 1) * B])
-            for m, sink in ((1e9, at_sample), (margin, at_model)):
-                searcher.set_threshold_model(model, m)
+            for m in (None, model):
+                searcher.set_threshold_model(m, margin)
                 rc = searcher.search_device(d_q[j].data_ptr(), B, f, topks[j], o_sc.data_ptr(), o_id.data_ptr(),
                                             o_n.data_ptr(), kmax, sh)
                 assert rc == 0
-                sink.append(searcher.last_estimate_counts(B).astype(np.int64))
+                (with_model if m else plain).append(searcher.last_candidate_counts(B).astype(np.int64))
+            miss.append(searcher.last_threshold_misses(B))
             f.close()
             kk.append(topks[j].astype(np.int64))
-        at_sample, at_model, kk = np.concatenate(at_sample), np.concatenate(at_model), np.concatenate(kk)
+        plain, with_model, miss, kk = (np.concatenate(plain), np.concatenate(with_model), np.stack(miss),
+                                       np.concatenate(kk))
         searcher.set_threshold_model(model, margin)
+        by_k = {}
+        for k in sorted(set(kk.tolist())):
+            sel = kk == k
+            by_k[f"K{k}"] = {"candidates_without_model": int(plain[sel].sum()),
+                             "candidates_with_model": int(with_model[sel].sum()),
+                             "miss_rate": round(float(miss.reshape(-1)[sel].mean()), 5)}
         out["learned_report"].update({
-            "estimation_pass_docs_at_sample_threshold": int(at_sample.sum()),
-            "estimation_pass_docs_at_model_threshold": int(at_model.sum()),
-            "pruned_fraction": round(1.0 - at_model.sum() / max(1, at_sample.sum()), 4),
-            "miss_rate": round(float(np.mean(at_model < kk)), 4), "queries": int(len(kk))})
+            "candidates_without_model": int(plain.sum()), "candidates_with_model": int(with_model.sum()),
+            "pruned_fraction": round(1.0 - with_model.sum() / max(1, plain.sum()), 4),
+            "miss_rate": round(float(miss.mean()), 5),
+            "batches_with_a_miss": round(float(miss.any(axis=1).mean()), 4), "queries": int(len(kk)),
+            "by_k": by_k})
     return out
 
 
@@ -669,9 +706,10 @@ def fp64_error(vec, queries, scores, ids, counts):
             "median_rel": float(np.median(er))}
 
 
-def data_filters(mix, n, seed):
+def data_filters(mix, n, seed, pool_factor=24):
     from hybridsearchsystem_b200 import data
-    return data.make_filters(mix, n, n_tags=(1, 6), seed=seed, selectivity_range=(1e-4, 1.0))
+    return data.make_filters(mix, n, n_tags=(1, 6), seed=seed, selectivity_range=(1e-4, 1.0),
+                             pool_factor=pool_factor)
 
 
 def measure_serving(args, ctx, method, rates, model=None, margin=0.0):
@@ -868,14 +906,14 @@ def run_ours(args):
 
     forms = {}
 
-    def run_form(key, method, learned=False, batch=None, kmix=False):
+    def run_form(key, method, learned=False, batch=None, kmode=None):
         import copy
         a = args
         if batch and batch != args.batch:
             a = copy.copy(args)
             a.batch = batch
-        f = measure_form(a, ctx, method, learned=learned, kmix=kmix)
-        if truth is not None and not kmix:
+        f = measure_form(a, ctx, method, learned=learned, kmode=kmode)
+        if truth is not None and kmode is None:
             f["parity"], last = parity_of_form(f["searcher"], dev, a.batch, pq, pe, truth)
             if key == "chosen":
                 f["fp64"] = fp64_error(vec, pq, *last)
@@ -901,9 +939,15 @@ def run_ours(args):
         if args.plain:
             run_form("plain_fp32_batch64", "tf32", batch=64)
     if args.kmix:
-        run_form("chosen_kmix", args.method, kmix=True)
+        run_form("chosen_kmix", args.method, kmode="mix")
+        if args.learned_form and not args.learned:
+            run_form("chosen_learned_kmix", args.method, learned=True, kmode="mix")
         if args.plain:
-            run_form("plain_fp32_kmix", "tf32", kmix=True)
+            run_form("plain_fp32_kmix", "tf32", kmode="mix")
+        # the K = 1000 slice, where the doc sample's threshold is loosest
+        run_form("chosen_k1000", args.method, kmode=1000)
+        if args.learned_form and not args.learned:
+            run_form("chosen_learned_k1000", args.method, learned=True, kmode=1000)
     serving = None
     if solo and args.serve:
         rates = [float(r) for r in args.serve_rates.split(",")]

@@ -136,7 +136,8 @@ SIGNATURES = [
     ("hss_searcher_features", ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, vp, vp, vp]),
     ("hss_searcher_set_threshold_model", ctypes.c_int, [vp, vp, ctypes.c_float]),
     ("hss_searcher_last_thresholds", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32]),
-    ("hss_searcher_last_estimate_counts", ctypes.c_int, [vp, vp, ctypes.c_uint32]),
+    ("hss_searcher_last_candidate_counts", ctypes.c_int, [vp, vp, ctypes.c_uint32]),
+    ("hss_searcher_last_threshold_misses", ctypes.c_int, [vp, vp, ctypes.c_uint32]),
     ("hss_model_create", ctypes.c_int, [ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
                                         ctypes.POINTER(vp)]),
     ("hss_model_free", None, [vp]),
@@ -144,6 +145,7 @@ SIGNATURES = [
     ("hss_model_get_params", ctypes.c_int, [vp, vp]),
     ("hss_model_set_params", ctypes.c_int, [vp, vp]),
     ("hss_model_set_output_scale", ctypes.c_int, [vp, ctypes.c_float, ctypes.c_float]),
+    ("hss_model_set_quantile", ctypes.c_int, [vp, ctypes.c_float]),
     ("hss_model_forward", ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, vp]),
     ("hss_model_train_step", ctypes.c_int, [vp, vp, vp, ctypes.c_uint32, ctypes.c_float,
                                             ctypes.POINTER(ctypes.c_float), vp]),

@@ -285,17 +285,24 @@ class FullRecallSearcher:
         self._model = model  # kept alive while the searcher uses it
 
     def last_thresholds(self, n):
-        """(doc sample's proven thresholds, the model's estimation-pass thresholds) of the last batch."""
+        """(doc sample's proven thresholds, the thresholds the model set) of the last batch."""
         t1 = np.zeros(max(n, 1), np.float32)
         ta = np.zeros(max(n, 1), np.float32)
         check(_lib.load().hss_searcher_last_thresholds(self._h, _np_ptr(t1), _np_ptr(ta), n))
         return t1[:n], ta[:n]
 
-    def last_estimate_counts(self, n):
-        """Docs each query's threshold-estimation pass kept in the last batch (0 without a model)."""
+    def last_candidate_counts(self, n):
+        """Docs that cleared each query's threshold in its last candidate pass of the last batch."""
         c = np.zeros(max(n, 1), np.uint32)
-        check(_lib.load().hss_searcher_last_estimate_counts(self._h, _np_ptr(c), n))
+        check(_lib.load().hss_searcher_last_candidate_counts(self._h, _np_ptr(c), n))
         return c[:n]
+
+    def last_threshold_misses(self, n):
+        """Per query of the last batch: True where the model's threshold was too high and the query was
+        re-run at a proven threshold."""
+        m = np.zeros(max(n, 1), np.uint8)
+        check(_lib.load().hss_searcher_last_threshold_misses(self._h, _np_ptr(m), n))
+        return m[:n].astype(bool)
 
     def set_pipeline_test(self, hold_load, wait_budget_cycles=0):
         """The next batch's first single-SM tensor-core pass withholds its hold_load-th corpus load
@@ -421,6 +428,10 @@ class ThresholdModel:
     def set_output_scale(self, scale, shift):
         self.scale, self.shift = float(scale), float(shift)
         check(_lib.load().hss_model_set_output_scale(self._h, self.scale, self.shift))
+
+    def set_quantile(self, tau):
+        """Training loss: 0 the mean squared error; tau in (0, 1) the pinball loss of the tau-quantile."""
+        check(_lib.load().hss_model_set_quantile(self._h, float(tau)))
 
     def forward(self, d_x, batch, d_y, stream=0):
         check(_lib.load().hss_model_forward(self._h, d_x, batch, d_y, stream))

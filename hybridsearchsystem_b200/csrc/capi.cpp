@@ -633,11 +633,18 @@ int hss_searcher_last_thresholds(const hss_searcher* s, float* sampleTheta, floa
     return HSS_OK;
 }
 
-int hss_searcher_last_estimate_counts(hss_searcher* s, uint32_t* counts, uint32_t n) {
-    if (!s || (n && !counts)) return SetError(HSS_ERR_INVALID, "hss_searcher_last_estimate_counts: bad arguments");
-    const int rc = s->s->LastEstimateCounts(n, counts);
-    if (rc == -1) return SetError(HSS_ERR_INVALID, "hss_searcher_last_estimate_counts: n beyond maxBatch");
-    if (rc != 0) return SetError(HSS_ERR_CUDA, "hss_searcher_last_estimate_counts");
+int hss_searcher_last_candidate_counts(hss_searcher* s, uint32_t* counts, uint32_t n) {
+    if (!s || (n && !counts)) return SetError(HSS_ERR_INVALID, "hss_searcher_last_candidate_counts: bad arguments");
+    const int rc = s->s->LastCandidateCounts(n, counts);
+    if (rc == -1) return SetError(HSS_ERR_INVALID, "hss_searcher_last_candidate_counts: n beyond maxBatch");
+    if (rc != 0) return SetError(HSS_ERR_CUDA, "hss_searcher_last_candidate_counts");
+    return HSS_OK;
+}
+
+int hss_searcher_last_threshold_misses(const hss_searcher* s, uint8_t* miss, uint32_t n) {
+    if (!s || (n && !miss)) return SetError(HSS_ERR_INVALID, "hss_searcher_last_threshold_misses: bad arguments");
+    const auto& m = s->s->LastThresholdMisses();
+    for (uint32_t i = 0; i < n; ++i) miss[i] = i < m.size() ? m[i] : 0;
     return HSS_OK;
 }
 
@@ -667,6 +674,12 @@ int hss_model_set_output_scale(hss_model* m, float scale, float shift) {
     if (!m) return SetError(HSS_ERR_INVALID, "hss_model_set_output_scale: null model");
     m->m->scale = scale;
     m->m->shift = shift;
+    return HSS_OK;
+}
+
+int hss_model_set_quantile(hss_model* m, float tau) {
+    if (!m) return SetError(HSS_ERR_INVALID, "hss_model_set_quantile: null model");
+    if (m->m->SetQuantile(tau) != 0) return SetError(HSS_ERR_INVALID, m->m->Error());
     return HSS_OK;
 }
 

@@ -375,11 +375,15 @@ class ThresholdModel {
     uint32_t Hidden() const { return m_h; }
     size_t ParamCount() const { return m_np; }
 
-    // y[B] (standardised) of device features dX [B][din].
+    // y[B] (standardised) of device features dX [B][din], in one launch.
     int Forward(const float* dX, uint32_t B, float* dY, cudaStream_t s);
-    // One Adam step on mean((y - t)^2) over a batch of device features / standardised targets.
+    // The training loss: 0 (the default) the mean squared error, tau in (0, 1) the pinball loss of the
+    // tau-quantile (the network then predicts a conditional tau-quantile of the target).
+    int SetQuantile(float tau);
+    float Quantile() const { return m_tau; }
+    // One Adam step on the loss over a batch of device features / standardised targets.
     int TrainStep(const float* dX, const float* dT, uint32_t B, float lr, float* hLoss, cudaStream_t s);
-    // The gradient of mean((y - t)^2) at the current parameters, into a host vector of ParamCount().
+    // The gradient of the loss at the current parameters, into a host vector of ParamCount().
     int Gradients(const float* dX, const float* dT, uint32_t B, float* hGrad, float* hLoss, cudaStream_t s);
     int GetParams(float* h) const;
     int SetParams(const float* h);
@@ -400,6 +404,7 @@ class ThresholdModel {
 
     int32_t m_deviceId;
     uint32_t m_din, m_h;
+    float m_tau = 0.0f;
     size_t m_np = 0;
     bool m_ok = false;
     std::string m_err;
@@ -464,26 +469,29 @@ class FullRecallSearcher {
     int LastCandidates(uint32_t q, float* scores, uint32_t* locs, uint32_t cap, uint32_t* count, float* theta,
                        float* eps);
 
-    // Learned threshold: with a model set, the two-part pass becomes: pass A over every
-    // kLearnedSplit-th tile at max(theta_1, prediction - margin), theta_1 being the doc sample's
-    // proven threshold. Its candidates only estimate theta_2 = max(theta_1, K-th best of pass A -
-    // 2 eps), which is proven because pass A's K-th best exists. A full pass B at theta_2 gives the
-    // candidates of the select step. A bad prediction costs candidates, never exactness, and never
-    // forces a re-run. nullptr switches the model off.
+    // Learned threshold: with a model set, the doc sample stays at sampleDocs whatever K (it feeds the
+    // model's features and gives the proven threshold theta_1), and the passes run at
+    // max(theta_1, prediction - margin - eps). That threshold is not proven: the select step checks,
+    // per query, that the K-th best exact score clears it by eps; a query that fails (a "miss") is
+    // re-run at a proven threshold. A bad prediction costs candidates or a re-run, never exactness.
+    // nullptr switches the model off.
     int SetThresholdModel(std::shared_ptr<ThresholdModel> model, float margin);
     // Width of a query's feature row: dim + posting rows + 12.
     uint32_t FeatureDim() const;
     // Feature rows [nq][FeatureDim()] of a batch (runs the filter stage and the doc sample).
     int Features(const float* dQueries, uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks,
                  float* dX, cudaStream_t stream);
-    // Per query of the last batch: the doc sample's proven threshold theta_1, and the threshold pass A
-    // used (-inf without a model).
+    // Per query of the last batch: the doc sample's proven threshold theta_1, and the threshold the
+    // model set (-inf without a model).
     const std::vector<float>& LastSampleThreshold() const { return m_lastTheta1; }
     const std::vector<float>& LastModelThreshold() const { return m_lastThetaA; }
-    static constexpr uint32_t kLearnedSplit = 4;
-    // Per query of the last batch with a model: the docs its threshold-estimation pass kept (0
-    // without a model). Reads the device; call before the next batch.
-    int LastEstimateCounts(uint32_t n, uint32_t* counts);
+    // Per query of the last batch: 1 when the model's threshold failed the check and the query was
+    // re-run at a proven one.
+    const std::vector<uint8_t>& LastThresholdMisses() const { return m_lastMiss; }
+    // Per query of the last batch: the docs that cleared the threshold of its last candidate pass
+    // (those the select step read, plus any beyond the list's capacity). Reads the device; call before
+    // the next batch.
+    int LastCandidateCounts(uint32_t n, uint32_t* counts);
 
     // Pipeline test: the next batch's first single-SM tensor-core pass stops issuing corpus loads
     // before its holdLoad-th, with waitBudget clock cycles (0: the default) for its waits; the pass
@@ -514,7 +522,8 @@ class FullRecallSearcher {
         cudaStream_t stream = nullptr;
         SelectLaunch se{};
         uint32_t launches = 0;
-        uint64_t want = 0;  // doc-sample size of the batch
+        uint64_t want = 0;        // doc-sample size of the batch
+        uint64_t wantRerun = 0;   // doc-sample size of a SIMT re-run (grows with K, model or not)
         bool pending = false, learned = false;
         cudaError_t ce = cudaSuccess;
     };
@@ -590,7 +599,7 @@ class FullRecallSearcher {
     float* m_hThetaA = nullptr;      // pinned copy of pass A's thresholds
     float* m_featuresOut = nullptr;  // Features(): stop after writing the feature rows here
     std::vector<float> m_lastTheta1, m_lastThetaA;
-    uint32_t m_lastEstSegs = 0;  // list segments of the last estimation pass (0: none ran)
+    std::vector<uint8_t> m_lastMiss;
     uint32_t m_testHold = 0;
     long long m_testBudget = 0;
 };

@@ -62,7 +62,7 @@ double TcAccumulationBound(int format, uint32_t d) {
 
 // Offsets of the packed per-batch staging buffer.
 struct StageLayout {
-    size_t progOff, opndOff, topk, epsMain, epsSamp, negInf, theta, qlist, errWord, counters, passCount,
+    size_t progOff, opndOff, topk, epsMain, epsSamp, negInf, theta, thetaPr, qlist, errWord, counters, passCount,
         candCount, sampCount, status, prog, opnd, total;
 };
 
@@ -81,6 +81,7 @@ StageLayout MakeLayout(uint32_t B) {
     L.epsSamp = take(B * 4ull);
     L.negInf = take(B * 4ull);
     L.theta = take(B * 4ull);
+    L.thetaPr = take(B * 4ull);  // proven thresholds beside predicted ones (learned threshold)
     L.qlist = take(B * 4ull);
     L.errWord = take(4);  // host copy of the tensor-core pass's error bits
     L.counters = at;  // zeroed per batch: passCount and status
@@ -447,16 +448,17 @@ static cudaError_t LaunchFeatures(const DataTable& T, const uint8_t* D, size_t o
     return launch_features(F, stream);
 }
 
-int FullRecallSearcher::LastEstimateCounts(uint32_t n, uint32_t* counts) {
+int FullRecallSearcher::LastCandidateCounts(uint32_t n, uint32_t* counts) {
     if (!m_ok || n > m_cfg.maxBatch) return -1;
     std::fill(counts, counts + n, 0u);
-    if (m_lastEstSegs == 0 || n == 0) return 0;
+    if (n == 0 || m_lastSegs.empty()) return 0;
     if (cudaSetDevice(m_deviceId) != cudaSuccess) return -2;
     const StageLayout SL = MakeLayout(m_cfg.maxBatch);
     std::vector<uint32_t> c(static_cast<size_t>(n) * kMaxCandSegs);
-    if (cudaMemcpy(c.data(), m_dStage + SL.sampCount, c.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
-    for (uint32_t q = 0; q < n; ++q)
-        for (uint32_t g = 0; g < m_lastEstSegs; ++g) counts[q] += c[static_cast<size_t>(q) * kMaxCandSegs + g];
+    if (cudaMemcpy(c.data(), m_dStage + SL.candCount, c.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+    const uint32_t m = std::min<uint32_t>(n, static_cast<uint32_t>(m_lastSegs.size()));
+    for (uint32_t q = 0; q < m; ++q)
+        for (uint32_t g = 0; g < m_lastSegs[q].first; ++g) counts[q] += c[static_cast<size_t>(q) * kMaxCandSegs + g];
     return 0;
 }
 
@@ -642,6 +644,7 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
     }
     m_times = StageTimes{};
     m_lastStatus.assign(nq, 0);
+    m_lastMiss.assign(nq, 0);
     if (nq == 0) return 0;
     if (nq > m_cfg.maxBatch) {
         m_err = "batch larger than the searcher's maxBatch";
@@ -666,7 +669,6 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
     auto* dEpsMain = reinterpret_cast<float*>(D + SL.epsMain);
     auto* dTheta = reinterpret_cast<float*>(D + SL.theta);
     auto* dCandCount = reinterpret_cast<uint32_t*>(D + SL.candCount);
-    auto* dSampCount = reinterpret_cast<uint32_t*>(D + SL.sampCount);
     auto* dStatus = reinterpret_cast<int32_t*>(D + SL.status);
 
     const DataTable& T = *m_table;
@@ -679,14 +681,17 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
     ++m_b.launches;
     if (m_timing) Ck(cudaEventRecord(m_ev[1], stream));
 
-    // 1. doc sample: evenly spaced tiles, every filtered doc kept; its K-th best bounds the threshold
-    m_b.want = std::max<uint64_t>(m_cfg.sampleDocs,
-                                  (4ull * std::max<uint32_t>(maxK, 1u) * T.GetDocNum() + m_cfg.candidateCap - 1) /
-                                      m_cfg.candidateCap);
+    // 1. doc sample: evenly spaced tiles, every filtered doc kept; its K-th best bounds the threshold.
+    // Without a model it grows with K so that its threshold keeps the full pass within the list
+    // capacity; with one, the prediction sets the threshold and the sample only feeds the features
+    // (which are made from the same sample size, with or without a model set).
     const bool learned = static_cast<bool>(m_model);
+    m_b.wantRerun = std::max<uint64_t>(
+        m_cfg.sampleDocs,
+        (4ull * std::max<uint32_t>(maxK, 1u) * T.GetDocNum() + m_cfg.candidateCap - 1) / m_cfg.candidateCap);
+    m_b.want = learned || m_featuresOut != nullptr ? m_cfg.sampleDocs : m_b.wantRerun;
     m_b.learned = learned;
     const bool wantStats = learned || m_featuresOut != nullptr;
-    m_lastEstSegs = 0;
     const uint64_t sampCount = Sample(nullptr, nq, false, false, wantStats ? m_dStats : nullptr);
     m_b.launches += 2;
     // the sample's proven thresholds (theta_1), read after the batch's first synchronisation
@@ -701,12 +706,15 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
         }
         return 0;
     }
+    auto* dThetaPr = reinterpret_cast<float*>(D + SL.thetaPr);
     if (learned) {
-        // the model's predicted K-th score minus the margin, never below theta_1
+        // the model's predicted K-th score minus the margin and the error bound, never below theta_1;
+        // theta_1 stays in dThetaPr for the select step's check
         Ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
                           m_dX, stream));
         if (m_model->Forward(m_dX, nq, m_dYp, stream) != 0) Ck(cudaErrorUnknown);
-        Ck(launch_predict_theta(m_dYp, dTheta, nq, m_model->scale, m_model->shift, m_margin, m_dYp, stream));
+        Ck(launch_predict_theta(m_dYp, dEpsMain, reinterpret_cast<const uint32_t*>(D + SL.passCount), dTopk, nq,
+                                m_model->scale, m_model->shift, m_margin, dTheta, dThetaPr, m_dYp, stream));
         Ck(cudaMemcpyAsync(m_hThetaA, m_dYp, nq * 4ull, cudaMemcpyDeviceToHost, stream));
         m_b.launches += 5;
     }
@@ -740,38 +748,11 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
     SE.status = dStatus;
     SE.qlist = nullptr;
     SE.nq_list = nq;
-    if (learned) {
-        // Pass A, every kLearnedSplit-th tile at the predicted thresholds, only estimates: its
-        // candidates go to the sample buffer. Its K-th best is a proven bound whenever it kept K docs
-        // (they exist), so theta_2 = max(theta_1, K-th best - 2 eps) is safe for the full pass B,
-        // whose candidates alone feed the select step. A prediction that kept fewer than K docs
-        // leaves theta_1 in place; no prediction can make the results inexact or force a re-run.
-        const uint64_t countA = (tilesM + kLearnedSplit - 1) / kLearnedSplit;
-        const uint32_t segsA = SegsOf(nq, countA, m_sampCap, false);
-        const uint32_t capA = SegCapOf(nq, countA, m_sampCap, segsA, false);
-        m_lastEstSegs = segsA;
-        Cand(m_dYp, m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, capA, 0, kLearnedSplit, 0, countA, nullptr, nq,
-             false);
-        SampleThresholdLaunch RT{};
-        RT.score = m_dSampScore;
-        RT.count = dSampCount;
-        RT.cap = m_sampCap;
-        RT.segs = segsA;
-        RT.seg_cap = capA;
-        RT.raise_only = 1;
-        RT.topk = dTopk;
-        RT.eps_sample = dEpsMain;  // t - 2 eps_main
-        RT.eps_main = dEpsMain;
-        RT.theta = dTheta;
-        RT.qlist = nullptr;
-        RT.nq_list = nq;
-        Ck(launch_sample_threshold(RT, stream));
-        const uint32_t segs = SegsOf(nq, tilesM, C, false);
-        SE.segs = segs;
-        SE.seg_cap = SegCapOf(nq, tilesM, C, segs, false);
-        Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tilesM, nullptr, nq, false);
-        m_b.launches += 3;
-    } else if (split >= 2) {
+    // With a model, theta is the prediction: the passes below run at it (raised like a proven one
+    // when pass A's K-th best allows), and the select step checks every query whose theta stayed
+    // above its proven threshold; a query that fails is re-run at a proven threshold.
+    SE.theta_proven = learned ? dThetaPr : nullptr;
+    if (split >= 2) {
         const uint64_t countA = (tilesM + split - 1) / split, countB = tilesM - countA;
         const uint32_t segsA = SegsOf(nq, countA, C, false), segsB = SegsOf(nq, countB, C, false);
         const uint32_t segCap = std::min(SegCapOf(nq, countA, C, segsA + segsB, false),
@@ -788,6 +769,7 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
         RT.eps_sample = dEpsMain;  // t - 2 eps_main
         RT.eps_main = dEpsMain;
         RT.theta = dTheta;
+        RT.theta_also = learned ? dThetaPr : nullptr;
         RT.qlist = nullptr;
         RT.nq_list = nq;
         Ck(launch_sample_threshold(RT, stream));
@@ -862,7 +844,8 @@ int FullRecallSearcher::SearchFinish() {
         if (m_b.ce != cudaSuccess) break;
         uint32_t nre = 0;
         for (uint32_t q = 0; q < nq; ++q) {
-            m_lastStatus[q] |= hStatus[q] & ~kStatusOverflow;
+            m_lastStatus[q] |= hStatus[q] & ~(kStatusOverflow | kStatusThresholdMiss);
+            if (hStatus[q] & kStatusThresholdMiss) m_lastMiss[q] = 1;
             if (hStatus[q] & kStatusOverflow) hQlist[nre++] = q;
         }
         if (nre == 0) break;
@@ -886,6 +869,7 @@ int FullRecallSearcher::SearchFinish() {
             Ck(launch_query_eps(m_b.dQueries, dQlist, nre, T.GetDimension(), T.GetMaxNorm(), rel, rel,
                                 reinterpret_cast<float*>(D + SL.epsMain), reinterpret_cast<float*>(D + SL.epsSamp),
                                 stream));
+            m_b.want = m_b.wantRerun;
             (void)Sample(dQlist, nre, true);
             m_b.launches += 3;
         } else if (tc) {

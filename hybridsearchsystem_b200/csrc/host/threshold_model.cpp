@@ -100,10 +100,11 @@ cudaError_t ThresholdModel::ForwardInto(const float* dX, uint32_t B, cudaStream_
     return e;
 }
 
-// Gradients of mean((y - t)^2) after ForwardInto, into m_dG (same layout as the parameters).
+// Gradients of the loss (mean squared error, or the pinball loss of the tau-quantile) after
+// ForwardInto, into m_dG (same layout as the parameters).
 cudaError_t ThresholdModel::Backward(const float* dX, const float* dT, uint32_t B, cudaStream_t s) {
     const int H = static_cast<int>(m_h), D = static_cast<int>(m_din), n = static_cast<int>(B);
-    cudaError_t e = launch_mse_grad(m_dY, dT, n, m_dDy, m_dSq, s);
+    cudaError_t e = launch_loss_grad(m_dY, dT, n, m_tau, m_dDy, m_dSq, s);
     // output layer: dw3 = A2^T dy, db3 = sum dy, dA2 = dy w3^T
     if (e == cudaSuccess)
         e = launch_gemm(true, false, m_dA2, m_dDy, m_dG + OffW3(), H, 1, n, H, 1, 1, nullptr, 0, nullptr, false, s);
@@ -147,9 +148,9 @@ int ThresholdModel::Finish(cudaError_t e, float* hLoss, uint32_t B, cudaStream_t
 int ThresholdModel::Forward(const float* dX, uint32_t B, float* dY, cudaStream_t s) {
     if (!m_ok) return -1;
     if (B == 0) return 0;
-    if (cudaSetDevice(m_deviceId) != cudaSuccess || !Reserve(B)) return -1;
-    cudaError_t e = ForwardInto(dX, B, s);
-    if (e == cudaSuccess && dY != m_dY) e = cudaMemcpyAsync(dY, m_dY, B * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    if (cudaSetDevice(m_deviceId) != cudaSuccess) return -1;
+    cudaError_t e = launch_mlp_forward(dX, static_cast<int>(B), static_cast<int>(m_din), static_cast<int>(m_h), m_dP,
+                                       dY, s);
     if (e != cudaSuccess) {
         m_err = cudaGetErrorString(e);
         return -2;
@@ -175,6 +176,15 @@ int ThresholdModel::TrainStep(const float* dX, const float* dT, uint32_t B, floa
     if (e == cudaSuccess)
         e = launch_adam(m_dP, m_dG, m_dM, m_dV, static_cast<int64_t>(m_np), lr, 0.9f, 0.999f, 1e-8f, ++m_step, s);
     return Finish(e, hLoss, B, s);
+}
+
+int ThresholdModel::SetQuantile(float tau) {
+    if (!(tau >= 0.0f && tau < 1.0f)) {
+        m_err = "quantile outside [0, 1)";
+        return -1;
+    }
+    m_tau = tau;
+    return 0;
 }
 
 int ThresholdModel::GetParams(float* h) const {

@@ -33,6 +33,9 @@ enum DeviceStatus : int32_t {
     kStatusBadPosting = 2,
     kStatusOverflow = 4,
     kStatusTopKTooLarge = 8,
+    // internal: the query's threshold was a prediction above its proven one and failed the select
+    // step's check (the host re-runs it at a proven threshold; never reported as an error)
+    kStatusThresholdMiss = 16,
 };
 
 // Order-preserving map float -> u32 (larger float -> larger key). -0.0 is folded onto +0.0 so the two

@@ -124,6 +124,7 @@ struct SampleThresholdLaunch {
     const float* eps_sample;   // [nq] error bound of the sample pass
     const float* eps_main;     // [nq] error bound of the main pass
     float* theta;              // [nq] out
+    float* theta_also;         // [nq] or null: raised with theta (raise_only launches)
     const uint32_t* qlist;
     uint32_t nq_list;
     float* stats;              // [nq][kSampleStats] or null (layout at kSampleStats)
@@ -142,6 +143,10 @@ struct SelectLaunch {
     const uint32_t* topk;
     const float* eps_main;
     float* theta;              // raised on overflow
+    // [nq] proven thresholds, or null when every theta is proven. A query whose theta is above its
+    // proven one (a predicted threshold) has its result checked; when the check fails both are set to
+    // a proven threshold and the query is flagged for a re-run.
+    float* theta_proven;
     const int64_t* gdocid;     // location -> global doc id, or null (identity)
     float* out_score;          // [nq][out_stride]
     int64_t* out_id;
@@ -256,7 +261,12 @@ cudaError_t launch_gemm(bool ta, bool tb, const float* A, const float* B, float*
                         cudaStream_t stream);
 cudaError_t launch_gelu_backward(float* dA, const float* Z, int64_t n, cudaStream_t stream);
 cudaError_t launch_colsum(const float* G, int M, int N, int ld, float* out, cudaStream_t stream);
-cudaError_t launch_mse_grad(const float* y, const float* t, int B, float* dy, float* sq, cudaStream_t stream);
+// dL/dy and the per-row loss terms: squared error (tau = 0) or the pinball loss of the tau-quantile.
+cudaError_t launch_loss_grad(const float* y, const float* t, int B, float tau, float* dy, float* term,
+                             cudaStream_t stream);
+// The whole inference forward pass of the MLP (parameters P in ThresholdModel's layout) in one launch;
+// bit-identical to the three-GEMM pass. H <= 1024, 4 (D + 2H) floats of shared memory <= 48 KB.
+cudaError_t launch_mlp_forward(const float* X, int B, int D, int H, const float* P, float* y, cudaStream_t stream);
 cudaError_t launch_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2,
                         float eps, int step, cudaStream_t stream);
 struct FeatureLaunch {
@@ -272,10 +282,13 @@ struct FeatureLaunch {
     uint64_t doc_num;
 };
 cudaError_t launch_features(const FeatureLaunch& L, cudaStream_t stream);
-// theta_a[q] = max(theta[q], y[q] * scale + shift - margin): the predicted threshold, never below the
-// proven one. theta_a may alias y.
-cudaError_t launch_predict_theta(const float* y, const float* theta, uint32_t nq, float scale, float shift,
-                                 float margin, float* theta_a, cudaStream_t stream);
+// The learned threshold of each query: theta_proven[q] = theta[q] (the proven one), then
+// theta[q] = max(theta[q], y[q] * scale + shift - margin - eps[q]) where the filter passes more than
+// kLearnedMinPass * topk[q] docs; theta_model[q] gets the new theta (it may alias y).
+constexpr uint32_t kLearnedMinPass = 4;
+cudaError_t launch_predict_theta(const float* y, const float* eps, const uint32_t* pass_count, const uint32_t* topk,
+                                 uint32_t nq, float scale, float shift, float margin, float* theta,
+                                 float* theta_proven, float* theta_model, cudaStream_t stream);
 
 // Cross-shard merge of sorted per-shard top-K lists (select.cu).
 constexpr uint32_t kMaxShards = 64;

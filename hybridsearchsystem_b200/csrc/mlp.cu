@@ -7,6 +7,8 @@
 //   adam      one Adam step over the flat parameter vector
 // FP32 throughout. The GEMMs are small (batch x ~400 x 256): a shared-memory tiled SIMT GEMM with a
 // fused bias + activation epilogue is enough; they are nowhere near the search's critical path.
+#include <algorithm>
+
 #include "hss_device.cuh"
 #include "hss_kernels.h"
 
@@ -103,14 +105,77 @@ __global__ void colsum_kernel(const float* __restrict__ G, int M, int N, int ld,
     out[n] = s;
 }
 
-// dy = 2 (y - t) / B for the mean squared error; sq[i] = (y - t)^2.
-__global__ void mse_grad_kernel(const float* __restrict__ y, const float* __restrict__ t, int B, float* __restrict__ dy,
-                                float* __restrict__ sq) {
+// The loss's gradient dL/dy and each row's loss term. tau = 0: mean squared error, dy = 2 (y - t) / B,
+// term (y - t)^2. tau in (0, 1): the pinball loss of the tau-quantile, term tau (t - y) when t >= y and
+// (1 - tau) (y - t) otherwise, dy = (y > t ? 1 - tau : -tau) / B (the network then predicts a
+// conditional tau-quantile of the target).
+__global__ void loss_grad_kernel(const float* __restrict__ y, const float* __restrict__ t, int B, float tau,
+                                 float* __restrict__ dy, float* __restrict__ term) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B) return;
     const float d = y[i] - t[i];
-    dy[i] = 2.0f * d / static_cast<float>(B);
-    if (sq) sq[i] = d * d;
+    if (tau <= 0.0f) {
+        dy[i] = 2.0f * d / static_cast<float>(B);
+        if (term) term[i] = d * d;
+    } else {
+        dy[i] = (d > 0.0f ? 1.0f - tau : -tau) / static_cast<float>(B);
+        if (term) term[i] = d > 0.0f ? (1.0f - tau) * d : -tau * d;
+    }
+}
+
+// Inference forward pass fused into one launch: a CTA takes kFwdRows feature rows, thread j computes
+// hidden unit j of both layers for all of them, and thread r < kFwdRows the output of row r. Every sum
+// runs over k in ascending order with fmaf, the bias added after, as gemm_kernel does: the outputs equal
+// the three-GEMM forward pass (ForwardInto) bit for bit.
+constexpr int kFwdRows = 4;
+
+__global__ void mlp_forward_kernel(const float* __restrict__ X, int B, int D, int H, const float* __restrict__ P,
+                                   float* __restrict__ y) {
+    extern __shared__ float fsm[];
+    float* xs = fsm;                  // [kFwdRows][D]
+    float* a1 = xs + kFwdRows * D;    // [kFwdRows][H]
+    float* a2 = a1 + kFwdRows * H;    // [kFwdRows][H]
+    const int r0 = blockIdx.x * kFwdRows;
+    const int rows = min(kFwdRows, B - r0);
+    for (int i = threadIdx.x; i < kFwdRows * D; i += blockDim.x) {
+        const int r = i / D;
+        xs[i] = r < rows ? X[static_cast<int64_t>(r0 + r) * D + i % D] : 0.0f;
+    }
+    __syncthreads();
+    const float* W1 = P;
+    const float* b1 = W1 + static_cast<int64_t>(D) * H;
+    const float* W2 = b1 + H;
+    const float* b2 = W2 + static_cast<int64_t>(H) * H;
+    const float* w3 = b2 + H;
+    const float* b3 = w3 + H;
+    const int j = threadIdx.x;
+    if (j < H) {
+        float acc[kFwdRows] = {};
+        for (int k = 0; k < D; ++k) {
+            const float w = W1[static_cast<int64_t>(k) * H + j];
+#pragma unroll
+            for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(xs[r * D + k], w, acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < kFwdRows; ++r) a1[r * H + j] = gelu(acc[r] + b1[j]);
+    }
+    __syncthreads();
+    if (j < H) {
+        float acc[kFwdRows] = {};
+        for (int k = 0; k < H; ++k) {
+            const float w = W2[static_cast<int64_t>(k) * H + j];
+#pragma unroll
+            for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(a1[r * H + k], w, acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < kFwdRows; ++r) a2[r * H + j] = gelu(acc[r] + b2[j]);
+    }
+    __syncthreads();
+    if (j < rows) {
+        float acc = 0.0f;
+        for (int k = 0; k < H; ++k) acc = fmaf(a2[j * H + k], w3[k], acc);
+        y[r0 + j] = acc + b3[0];
+    }
 }
 
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
@@ -158,13 +223,25 @@ __global__ void features_kernel(FeatureLaunch L) {
     }
 }
 
-// theta_a[q] = max(proven threshold, predicted K-th score (y * scale + shift) minus the margin). fmaxf
-// drops a NaN prediction. theta_a may alias y (each thread reads, then writes, its own element).
-__global__ void predict_theta_kernel(const float* y, const float* __restrict__ theta, uint32_t nq, float scale,
-                                     float shift, float margin, float* theta_a) {
+// theta[q] = max(proven threshold, predicted K-th score (y * scale + shift) minus the margin and the
+// query's error bound), the proven one kept in theta_proven. A doc of the true top K then clears
+// theta whenever the prediction minus the margin is at most the true K-th score. A query whose filter
+// passes at most kLearnedMinPass * K docs keeps its proven threshold: its candidates are few whatever
+// the threshold, and its K-th score is the hardest to predict. fmaxf drops a NaN prediction.
+// theta_model may alias y (each thread reads, then writes, its own element).
+__global__ void predict_theta_kernel(const float* y, const float* __restrict__ eps,
+                                     const uint32_t* __restrict__ pass_count, const uint32_t* __restrict__ topk,
+                                     uint32_t nq, float scale, float shift, float margin, float* theta,
+                                     float* theta_proven, float* theta_model) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
-    theta_a[q] = fmaxf(theta[q], __fsub_rd(fmaf(y[q], scale, shift), margin));
+    const float t1 = theta[q];
+    const float t = static_cast<uint64_t>(pass_count[q]) <= static_cast<uint64_t>(kLearnedMinPass) * topk[q]
+                        ? t1
+                        : fmaxf(t1, __fsub_rd(__fsub_rd(fmaf(y[q], scale, shift), margin), eps[q]));
+    theta_proven[q] = t1;
+    theta[q] = t;
+    theta_model[q] = t;
 }
 
 }  // namespace
@@ -199,9 +276,20 @@ cudaError_t launch_colsum(const float* G, int M, int N, int ld, float* out, cuda
     return cudaGetLastError();
 }
 
-cudaError_t launch_mse_grad(const float* y, const float* t, int B, float* dy, float* sq, cudaStream_t stream) {
+cudaError_t launch_loss_grad(const float* y, const float* t, int B, float tau, float* dy, float* term,
+                             cudaStream_t stream) {
     if (B <= 0) return cudaSuccess;
-    mse_grad_kernel<<<(B + 255) / 256, 256, 0, stream>>>(y, t, B, dy, sq);
+    if (!(tau >= 0.0f && tau < 1.0f)) return cudaErrorInvalidValue;
+    loss_grad_kernel<<<(B + 255) / 256, 256, 0, stream>>>(y, t, B, tau, dy, term);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_forward(const float* X, int B, int D, int H, const float* P, float* y, cudaStream_t stream) {
+    if (B <= 0) return cudaSuccess;
+    const int threads = ((std::max(H, kFwdRows) + 31) / 32) * 32;
+    const size_t smem = static_cast<size_t>(kFwdRows) * (D + 2 * H) * sizeof(float);
+    if (threads > 1024 || smem > 48 * 1024) return cudaErrorInvalidValue;
+    mlp_forward_kernel<<<(B + kFwdRows - 1) / kFwdRows, threads, smem, stream>>>(X, B, D, H, P, y);
     return cudaGetLastError();
 }
 
@@ -221,10 +309,12 @@ cudaError_t launch_features(const FeatureLaunch& L, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_predict_theta(const float* y, const float* theta, uint32_t nq, float scale, float shift,
-                                 float margin, float* theta_a, cudaStream_t stream) {
+cudaError_t launch_predict_theta(const float* y, const float* eps, const uint32_t* pass_count, const uint32_t* topk,
+                                 uint32_t nq, float scale, float shift, float margin, float* theta,
+                                 float* theta_proven, float* theta_model, cudaStream_t stream) {
     if (nq == 0) return cudaSuccess;
-    predict_theta_kernel<<<(nq + 127) / 128, 128, 0, stream>>>(y, theta, nq, scale, shift, margin, theta_a);
+    predict_theta_kernel<<<(nq + 127) / 128, 128, 0, stream>>>(y, eps, pass_count, topk, nq, scale, shift, margin,
+                                                               theta, theta_proven, theta_model);
     return cudaGetLastError();
 }
 

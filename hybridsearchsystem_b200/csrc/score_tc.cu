@@ -615,6 +615,9 @@ struct PairShared {
     volatile int abort;
 };
 
+// shared-memory bytes the barriers take ahead of the 1024-byte aligned query tile
+constexpr size_t kPairSharedBytes = (sizeof(PairShared) + 1023) & ~static_cast<size_t>(1023);
+
 constexpr int kPairEpiWarps = 16;  // 4 column groups x 4 TMEM lane quarters
 constexpr int kPairThreads = 64 + 32 * kPairEpiWarps;
 
@@ -648,9 +651,11 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
     const uint32_t sg_n = kb_n / G;        // stages per tile
     // bytes of one ring stage: G doc k-blocks, or (streamed queries) a query k-block and a doc k-block
     const size_t kStage = SQ ? 2 * kStageBytes : static_cast<size_t>(G) * kStageBytes;
-    unsigned char* qsm = base;
-    unsigned char* ring = base + (SQ ? 0 : static_cast<size_t>(kb_n) * kStageBytes);
-    PairShared& S = *reinterpret_cast<PairShared*>(ring + static_cast<size_t>(L.stages) * kStage);
+    // barriers first (a fixed offset, so the epilogue keeps no pointer to them in registers), then
+    // the resident query tile and the ring, both 1024-byte aligned for the 128-byte swizzle
+    PairShared& S = *reinterpret_cast<PairShared*>(base);
+    unsigned char* qsm = base + kPairSharedBytes;
+    unsigned char* ring = qsm + (SQ ? 0 : static_cast<size_t>(kb_n) * kStageBytes);
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t stages = L.stages;
@@ -692,12 +697,11 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
                     tma_load_2d(qsm + static_cast<size_t>(kb) * kStageBytes, &qry_map,
                                 static_cast<int>(kb * (128 / Fmt<F>::elem)), static_cast<int>(rank * kRows), &S.qbar);
             }
-            uint32_t n = 0;
+            uint32_t n = 0, s = 0, ph = 0;  // stages issued; ring slot and phase of the next
             TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, pair, npairs);
             for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs, walk.advance()) {
                 const int y = static_cast<int>(walk.tile() * 2 * kRows + rank * kRows);
-                for (uint32_t g = 0; g < sg_n; ++g, ++n) {
-                    const uint32_t s = n % stages, ph = (n / stages) & 1u;
+                for (uint32_t g = 0; g < sg_n; ++g, ++n, s = s + 1 == stages ? 0 : s + 1, ph ^= s == 0 ? 1u : 0u) {
                     if (!pair_wait<F>(&S.empty[s], ph ^ 1u, S, L.error, 1, false)) break;
                     unsigned char* st = ring + static_cast<size_t>(s) * kStage;
                     mbar_expect_tx(&S.full[s], static_cast<uint32_t>(kStage));
@@ -718,13 +722,12 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
     } else if (warp == 1) {
         if (lane == 0 && rank == 1) {
             // forwarder: the even CTA's MMAs read this CTA's queries and stages; tell it when they land
-            uint32_t n = 0;
+            uint32_t n = 0, s = 0, ph = 0;
             if (SQ || pair_wait<F>(&S.qbar, 0, S, L.error, 2, false)) {
                 if (!SQ) mbar_arrive_cluster(peer_addr(&S.qbar, 0));
                 for (uint64_t it = pair; it < ntiles && !S.abort; it += npairs) {
                     bool ok = true;
-                    for (uint32_t g = 0; g < sg_n; ++g, ++n) {
-                        const uint32_t s = n % stages, ph = (n / stages) & 1u;
+                    for (uint32_t g = 0; g < sg_n; ++g, ++n, s = s + 1 == stages ? 0 : s + 1, ph ^= s == 0 ? 1u : 0u) {
                         if (!pair_wait<F>(&S.full[s], ph, S, L.error, 8, false)) {
                             ok = false;
                             break;
@@ -739,7 +742,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
             // MMA issuer of the pair
             constexpr uint32_t idesc =
                 (1u << 4) | (Fmt<F>::ab << 7) | (Fmt<F>::ab << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
-            uint32_t n = 0, iter = 0;
+            uint32_t n = 0, iter = 0, s = 0, ph = 0;
             // the even CTA's query barrier completes with both CTAs' query tiles (one forwarded); a
             // one-time wait, acquired at cluster scope
             bool ok = SQ || pair_wait<F>(&S.qbar, 0, S, L.error, 2, true);
@@ -749,8 +752,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
                 // CTA-scope): a cluster-scope acquire on every stage cost the TF32 pass about 4 %
                 if (!pair_wait<F>(&S.acc_empty[buf], ((iter >> 1) & 1u) ^ 1u, S, L.error, 4, false)) break;
                 fence_after();
-                for (uint32_t g = 0; g < sg_n; ++g, ++n) {
-                    const uint32_t s = n % stages, ph = (n / stages) & 1u;
+                for (uint32_t g = 0; g < sg_n; ++g, ++n, s = s + 1 == stages ? 0 : s + 1, ph ^= s == 0 ? 1u : 0u) {
                     // both CTAs' halves of the stage: this CTA's load and the odd CTA's, forwarded
                     if (!pair_wait<F>(&S.full[s], ph, S, L.error, 8, false)) {
                         ok = false;
@@ -906,7 +908,7 @@ constexpr size_t kSmemBudget = 232448;  // dynamic shared memory of one CTA
 }  // namespace
 
 bool tc_stream_queries(uint32_t kblocks) {
-    return 1024 + (static_cast<size_t>(kblocks) + 4) * kStageBytes + sizeof(PairShared) > kSmemBudget;
+    return 1024 + kPairSharedBytes + (static_cast<size_t>(kblocks) + 4) * kStageBytes > kSmemBudget;
 }
 
 uint32_t tc_tile_docs(uint32_t rows, uint32_t kblocks) {
@@ -934,9 +936,9 @@ size_t tc_smem_bytes(int halves, uint32_t kblocks, uint32_t stages, uint32_t gro
 
 size_t tc_pair_smem_bytes(uint32_t kblocks, uint32_t stages, uint32_t group) {
     if (tc_stream_queries(kblocks))  // no resident queries; a stage holds a query and a doc k-block
-        return 1024 + static_cast<size_t>(stages) * 2 * kStageBytes + sizeof(PairShared);
-    return 1024 + static_cast<size_t>(kblocks) * kStageBytes + static_cast<size_t>(stages) * group * kStageBytes +
-           sizeof(PairShared);
+        return 1024 + kPairSharedBytes + static_cast<size_t>(stages) * 2 * kStageBytes;
+    return 1024 + kPairSharedBytes + static_cast<size_t>(kblocks) * kStageBytes +
+           static_cast<size_t>(stages) * group * kStageBytes;
 }
 
 uint32_t tc_group(uint32_t kblocks, bool pair) {

@@ -492,6 +492,7 @@ __global__ void __launch_bounds__(kST) sample_threshold_kernel(SampleThresholdLa
         const float t = __fsub_rd(__fsub_rd(key_float(kk), L.eps_sample[qi]), L.eps_main[qi]);
         theta = L.raise_only ? fmaxf(theta, t) : t;
         if (L.stats && threadIdx.x == 0) L.stats[static_cast<uint64_t>(qi) * kSampleStats + kSampleRanks] = key_float(kk);
+        if (L.theta_also && L.raise_only && threadIdx.x == 0) L.theta_also[qi] = fmaxf(L.theta_also[qi], t);
     }
     __syncthreads();  // every thread has read the old theta
     if (threadIdx.x == 0) L.theta[qi] = theta;
@@ -530,22 +531,43 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
             if (ok) fn(float_key(v));
         });
     };
+    // A threshold above the proven one (a prediction) has to be checked: the list holds every doc
+    // with s~ >= theta, so a doc left out scores s < theta + eps, and the K best candidates are the
+    // K best docs when their K-th exact score s_K >= theta + eps. A query that fails goes back to a
+    // proven threshold: the larger of its proven one and s_K - eps (every true top-K doc scores at
+    // least s_K, the candidates' K-th best, hence s~ >= s_K - eps).
+    const float theta_q = L.theta[qi];
+    const bool unproven = L.theta_proven != nullptr && theta_q > L.theta_proven[qi];
+    auto threshold_miss = [&](float raised) {
+        if (tid == 0) {
+            const float t = fmaxf(L.theta_proven[qi], raised);
+            L.theta[qi] = t;
+            L.theta_proven[qi] = t;
+            L.out_count[qi] = 0;
+            atomicOr(L.status + qi, kStatusOverflow | kStatusThresholdMiss);
+        }
+    };
     if (overflow) {
         // The stored candidates are a subset of the qualifying docs, so their K-th best still bounds
         // the true K-th best from below: raise the threshold and let the host re-run this query.
-        float theta = L.theta[qi];
+        float theta = unproven ? L.theta_proven[qi] : theta_q;
         if (n >= k && k > 0) {
             const uint32_t kk = kth_lower_bound_u32_visit(visit_scores, k, S);
             theta = fmaxf(theta, __fsub_rd(key_float(kk), 2.0f * eps));
         }
         if (tid == 0) {
             L.theta[qi] = theta;
+            if (L.theta_proven) L.theta_proven[qi] = theta;
             L.out_count[qi] = 0;
             atomicOr(L.status + qi, kStatusOverflow);
         }
         return;
     }
     if (n == 0 || k == 0) {
+        if (unproven && k > 0) {
+            threshold_miss(-INFINITY);
+            return;
+        }
         if (tid == 0) L.out_count[qi] = 0;
         return;
     }
@@ -609,6 +631,13 @@ __global__ void __launch_bounds__(kST) select_topk_kernel(SelectLaunch L) {
     const uint32_t nf = S.counter;
     __syncthreads();
     top_keys([&](uint32_t i) { return static_cast<uint64_t>(ws[i]); }, nf, kq, S);
+    if (unproven) {
+        const float lo = kq == k ? __fsub_rd(result_key_score(S.sortbuf[kq - 1]), eps) : -INFINITY;
+        if (!(lo >= theta_q)) {
+            threshold_miss(lo);
+            return;
+        }
+    }
     const uint64_t orow = static_cast<uint64_t>(qi) * L.out_stride;
     for (uint32_t i = tid; i < kq; i += blockDim.x) {
         const uint64_t key = S.sortbuf[i];

@@ -212,14 +212,49 @@ def make_filters(mix, nq, n_tags=(1, 4), seed=3, selectivity_range=None, pool_fa
     pool = [draw() for _ in range(nq * pool_factor)]
     logsel = np.array([math.log(max(1e-12, mix.selectivity(a))) for a in pool])
     targets = rng.uniform(lo, hi, nq)
-    used = np.zeros(len(pool), bool)
+    return [ast_text(pool[j]) for j in _nearest_unused(logsel, targets)]
+
+
+def _nearest_unused(values, targets):
+    """For each target in turn, the index of the unused value nearest to it (lowest index among equally
+    near ones), which is then used: the greedy match, in O((n + m) log n) with a sorted order and
+    skip pointers over used positions."""
+    n = len(values)
+    order = np.lexsort((np.arange(n), values))  # by value, then index
+    sv = values[order]
+    # start of each run of equal values in sorted order (its lowest index comes first)
+    run_start = np.zeros(n, np.int64)
+    for i in range(1, n):
+        run_start[i] = run_start[i - 1] if sv[i] == sv[i - 1] else i
+    right = list(range(n + 1))  # right[i]: first unused position >= i (n: none)
+    left = list(range(-1, n))   # left[i + 1]: last unused position <= i (-1: none)
+
+    def find(ptr, i, off):
+        root = i
+        while ptr[root + off] != root:
+            root = ptr[root + off]
+        while ptr[i + off] != root:  # path compression
+            ptr[i + off], i = root, ptr[i + off]
+        return root
+
     out = []
     for t in targets:
-        d = np.abs(logsel - t)
-        d[used] = np.inf
-        j = int(np.argmin(d))
-        used[j] = True
-        out.append(ast_text(pool[j]))
+        pos = int(np.searchsorted(sv, t))
+        best = None
+        r = find(right, pos, 0) if pos < n else n
+        if r < n:
+            best = (abs(sv[r] - t), order[r], r)
+        lpos = find(left, pos - 1, 1) if pos > 0 else -1
+        if lpos >= 0:
+            # the lowest unused index among the values equal to the left neighbour
+            l = find(right, int(run_start[lpos]), 0)
+            c = (abs(sv[l] - t), order[l], l)
+            if best is None or (c[0], c[1]) < (best[0], best[1]):
+                best = c
+        _, j, p = best
+        right[p] = p + 1
+        left[p + 1] = p - 1
+        out.append(int(j))
     return out
 
 

@@ -1,34 +1,39 @@
 """Training of the learned threshold predictor on the GPU.
 
-With a model set, a searcher's threshold-estimation pass scores every LEARNED_SPLIT-th tile (a
-quarter of the corpus) at max(doc sample's proven threshold, prediction - margin). That pass must keep
-at least K docs for its K-th best to raise the proven threshold of the full pass, and its K-th best
-is about the corpus's (LEARNED_SPLIT * K)-th best score. So the label of a query is its exact score
-at rank LEARNED_SPLIT * K, from the searcher's own exact path (no model set, top LEARNED_SPLIT * K).
-A query whose filter lets through fewer docs has no label and is left out.
+With a model set, a searcher's candidate passes prune at max(doc sample's proven threshold,
+prediction - margin - error bound), and its select step checks each such query: the K-th best exact
+score must clear that threshold by the error bound, else the query is re-run at a proven threshold
+(a miss). So the label of a query is its exact K-th best score, from the searcher's own exact path
+(no model set). The searcher predicts only for queries whose filter passes more than
+MIN_PASS_FACTOR * K docs (the others have few candidates whatever the threshold); the queries trained
+and calibrated on are those whose filter passes at least that many.
 
-The network regresses the standardised label with the library's own forward / backward / Adam
-kernels (ThresholdModel.train_step), keeping the parameters with the lowest held-out error. The margin is a quantile of (prediction - label) over a held-out
-split: a query predicted above its label by more than the margin keeps fewer than K docs in the
-estimation pass and falls back to the sample's threshold (more candidates, never a wrong result).
+The network predicts the standardised label with the library's own forward / backward / Adam kernels
+(ThresholdModel.train_step). With tau > 0 it is trained on the pinball loss of the tau-quantile, so it
+predicts a low conditional quantile of the K-th score: low where the features say little (a wide
+margin for that query alone), close where they pin it down. It keeps the parameters with the lowest
+held-out loss. The margin is a quantile of (prediction - label) over the held-out queries: a query
+predicted above its label by more than the margin is a miss, so that quantile sets the miss rate
+(quantile 1.0: the largest held-out residual).
 """
 import numpy as np
 
 from .api import ThresholdModel
 
-LEARNED_SPLIT = 4  # FullRecallSearcher::kLearnedSplit
+MIN_PASS_FACTOR = 4  # kLearnedMinPass of the searcher's prediction step
 
 
-def label_and_features(searcher, queries, exprs, topks, batch=None, rank_factor=LEARNED_SPLIT):
+def label_and_features(searcher, queries, exprs, topks, batch=None, min_pass_factor=MIN_PASS_FACTOR):
     """(X [n][din] device tensor, labels [n] float32 numpy): the feature rows and each query's exact
-    score at rank rank_factor * K (NaN where fewer docs pass its filter)."""
+    K-th best score (NaN where its filter passes fewer than min(min_pass_factor * K, HSS_MAX_TOPK)
+    docs)."""
     import torch
     from ._lib import HSS_MAX_TOPK
     dev = torch.device("cuda", searcher.table.device)
     B = batch or searcher.max_batch
     din = searcher.feature_dim()
     topks = np.asarray(topks, dtype=np.uint32)
-    ranks = np.minimum(topks.astype(np.int64) * rank_factor, HSS_MAX_TOPK).astype(np.uint32)
+    ranks = np.minimum(topks.astype(np.int64) * max(1, min_pass_factor), HSS_MAX_TOPK).astype(np.uint32)
     R = int(ranks.max())
     n = len(queries)
     X = torch.zeros((n, din), dtype=torch.float32, device=dev)
@@ -49,23 +54,24 @@ def label_and_features(searcher, queries, exprs, topks, batch=None, rank_factor=
         s_h = sc[:nb].cpu().numpy()
         c_h = cnt[:nb].cpu().numpy()
         for i in range(nb):
-            r = int(rk[i])
-            if r > 0 and c_h[i] >= r:
-                labels[b0 + i] = s_h[i, r - 1]
+            k = int(topks[b0 + i])
+            if k > 0 and c_h[i] >= int(rk[i]):
+                labels[b0 + i] = s_h[i, k - 1]
         f.close()
     return X, labels
 
 
 def fit_threshold_model(searcher, queries, exprs, topks, hidden=256, steps=2000, batch=512, lr=2e-3, seed=0,
-                        val_fraction=0.15, quantile=0.95, slack=0.0):
-    """Trains a ThresholdModel for `searcher` (which must have no model set) on the given queries.
-    Returns (model, margin, report)."""
+                        val_fraction=0.15, quantile=0.999, slack=0.0, n_val=None, tau=0.02):
+    """Trains a ThresholdModel for `searcher` (which must have no model set) on the given queries,
+    holding out n_val of them (or val_fraction) for the early stop and the margin; tau is the quantile
+    the network is trained to predict (0: the mean, by squared error). Returns (model, margin, report)."""
     import torch
     X, labels = label_and_features(searcher, queries, exprs, topks)
     keep = np.nonzero(np.isfinite(labels))[0]
     rng = np.random.default_rng(seed)
     rng.shuffle(keep)
-    nval = max(1, int(len(keep) * val_fraction))
+    nval = max(1, min(len(keep) - 1, n_val) if n_val else int(len(keep) * val_fraction))
     val, tr = keep[:nval], keep[nval:]
     mu, sd = float(labels[tr].mean()), float(labels[tr].std() + 1e-6)
     dev = X.device
@@ -73,6 +79,11 @@ def fit_threshold_model(searcher, queries, exprs, topks, hidden=256, steps=2000,
     din = X.shape[1]
     model = ThresholdModel(din, hidden, device=dev.index or 0, seed=seed)
     model.set_output_scale(sd, mu)
+    model.set_quantile(tau)
+
+    def held_out_loss(res):  # the training loss over residuals (prediction - label), in score units
+        return float(np.mean(res * res)) if tau <= 0 else float(np.mean(np.where(res > 0, (1 - tau) * res, -tau * res)))
+
     stream = torch.cuda.current_stream(dev).cuda_stream
     tr_t = torch.from_numpy(tr.astype(np.int64)).to(dev)
     xb = torch.zeros((batch, din), dtype=torch.float32, device=dev)
@@ -85,7 +96,7 @@ def fit_threshold_model(searcher, queries, exprs, topks, hidden=256, steps=2000,
         model.forward(xs.data_ptr(), len(idx), y.data_ptr(), stream)
         return y.cpu().numpy() * sd + mu
 
-    # minibatch Adam with cosine decay; the parameters kept are those with the lowest held-out error
+    # minibatch Adam with cosine decay; the parameters kept are those with the lowest held-out loss
     # (checked every `check_every` steps), which stops the network from memorising the training queries
     losses = []
     batch = min(batch, len(tr))
@@ -108,7 +119,7 @@ def fit_threshold_model(searcher, queries, exprs, topks, hidden=256, steps=2000,
             n_ep += 1
             step += 1
             if step % check_every == 0 or step == steps:
-                err = float(np.mean((predict(val) - labels[val]) ** 2))
+                err = held_out_loss(predict(val) - labels[val])
                 if err < best[0]:
                     best = (err, model.get_params(), step)
         losses.append(ep_loss / max(1, n_ep))
@@ -122,5 +133,7 @@ def fit_threshold_model(searcher, queries, exprs, topks, hidden=256, steps=2000,
               "val_abs_err_median": float(np.median(np.abs(res_val))),
               "val_rmse": float(np.sqrt(np.mean(res_val ** 2))), "train_rmse": float(np.sqrt(np.mean(res_tr ** 2))),
               "margin": margin, "val_overshoot_rate_at_margin": float(np.mean(res_val > margin)),
+              "val_residual_quantiles": {str(q): float(np.quantile(res_val, q)) for q in (0.5, 0.9, 0.99, 0.999, 1.0)},
+              "tau": tau, "labelled_fraction": float(len(keep) / max(1, len(labels))),
               "steps": steps, "best_step": best[2]}
     return model, margin, report

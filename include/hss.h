@@ -303,12 +303,13 @@ int hss_searcher_last_times(const hss_searcher* s, float* ms5, uint32_t* retries
 
 /* ---- learned threshold predictor ----
  * An MLP (feature row -> hidden -> hidden -> 1, GELU) that predicts a query's K-th filtered score,
- * trained and run on the GPU by this library's own kernels. With a model set, a searcher runs a
- * threshold-estimation pass over every 4th tile at max(doc sample's proven threshold, prediction -
- * margin), raises each query's threshold to that pass's K-th best minus the error bound (proven), and
- * takes the select step's candidates from one full pass at that threshold. A bad prediction costs
- * candidates, never exactness. No counterpart in the reference (whose only threshold is its TOPK
- * pivot pre-select). */
+ * trained and run on the GPU by this library's own kernels. With a model set, a searcher's candidate
+ * passes prune at max(doc sample's proven threshold, prediction - margin - error bound) inside the
+ * scoring epilogue, and its doc sample stays at sample_docs for every K. The select step checks each
+ * query whose threshold came from the prediction: its K-th best exact score must clear that
+ * threshold by the error bound, else the query is re-run at a proven threshold. A bad prediction
+ * costs candidates or a re-run, never exactness. No counterpart in the reference (whose only
+ * threshold is its TOPK pivot pre-select). */
 typedef struct hss_model hss_model;
 
 /* dim + posting rows + 12: the feature row width a model for this searcher must take. */
@@ -320,16 +321,21 @@ uint32_t hss_searcher_feature_dim(const hss_searcher* s);
  * Runs the filter stage and the doc sample; synchronises `stream`. */
 int hss_searcher_features(hss_searcher* s, const float* dQueries, uint32_t nq, const hss_filters* filters,
                           const uint32_t* topks, float* dX, hss_stream_t stream);
-/* model NULL switches the learned threshold off. margin is subtracted from the prediction. */
+/* model NULL switches the learned threshold off. margin (score units) is subtracted from the
+ * prediction. */
 int hss_searcher_set_threshold_model(hss_searcher* s, hss_model* model, float margin);
-/* Per query of the last batch: the doc sample's proven threshold and the threshold the model set for
- * the estimation pass (-inf without a model); host arrays of n floats, either may be NULL. */
+/* Per query of the last batch: the doc sample's proven threshold and the threshold the model set
+ * (-inf without a model); host arrays of n floats, either may be NULL. */
 int hss_searcher_last_thresholds(const hss_searcher* s, float* sampleTheta, float* modelTheta, uint32_t n);
 
-/* Per query of the last batch run with a model: the docs its threshold-estimation pass kept (0 when no
- * model was set). A count below K means the prediction was too high for that query (its sample
- * threshold stood). Call before the next batch. */
-int hss_searcher_last_estimate_counts(hss_searcher* s, uint32_t* counts, uint32_t n);
+/* Per query of the last batch: the docs that cleared the threshold of its last candidate pass (the
+ * list the select step read, counting any beyond the list's capacity). Call before the next batch. */
+int hss_searcher_last_candidate_counts(hss_searcher* s, uint32_t* counts, uint32_t n);
+
+/* Per query of the last batch: 1 when the model's threshold was too high for it (its K-th best exact
+ * score did not clear the threshold by the error bound) and the query was re-run at a proven
+ * threshold, else 0. Its results are exact either way. */
+int hss_searcher_last_threshold_misses(const hss_searcher* s, uint8_t* miss, uint32_t n);
 
 int hss_model_create(int32_t deviceId, uint32_t din, uint32_t hidden, uint64_t seed, hss_model** out);
 void hss_model_free(hss_model* m);
@@ -339,13 +345,17 @@ int hss_model_get_params(const hss_model* m, float* params);
 int hss_model_set_params(hss_model* m, const float* params);
 /* The model predicts standardised scores: score = output * scale + shift. */
 int hss_model_set_output_scale(hss_model* m, float scale, float shift);
-/* Outputs dY [B] (standardised) of device features dX [B][din]. */
+/* Outputs dY [B] (standardised) of device features dX [B][din], in one launch (hidden <= 1024). */
 int hss_model_forward(hss_model* m, const float* dX, uint32_t B, float* dY, hss_stream_t stream);
-/* One Adam step (b1 0.9, b2 0.999, eps 1e-8) on mean((y - t)^2) over device dX [B][din] and dT [B]
+/* The training loss: tau = 0 (the default) the mean squared error, mean((y - t)^2); tau in (0, 1) the
+ * pinball loss of the tau-quantile, mean(tau (t - y) where t >= y, (1 - tau) (y - t) elsewhere), so
+ * the network predicts a conditional tau-quantile of the target. */
+int hss_model_set_quantile(hss_model* m, float tau);
+/* One Adam step (b1 0.9, b2 0.999, eps 1e-8) on the loss over device dX [B][din] and dT [B]
  * (standardised targets); *loss (may be NULL) = the batch loss before the step. Synchronises. */
 int hss_model_train_step(hss_model* m, const float* dX, const float* dT, uint32_t B, float lr, float* loss,
                          hss_stream_t stream);
-/* The gradient of mean((y - t)^2) at the current parameters into a host array of param_count floats
+/* The gradient of the loss at the current parameters into a host array of param_count floats
  * (parameter order); *loss (may be NULL) = the loss. Synchronises `stream`. */
 int hss_model_gradients(hss_model* m, const float* dX, const float* dT, uint32_t B, float* grad, float* loss,
                         hss_stream_t stream);

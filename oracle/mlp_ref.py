@@ -4,7 +4,9 @@ TEST INFRASTRUCTURE ONLY: imported by tests/ as the checker of the GPU forward p
 nothing in the product calls it. Float64 throughout.
 
 Network: y = w3 . gelu(W2^T gelu(W1^T x + b1) + b2) + b3 with the exact (erf) GELU, parameters in one
-flat vector W1 [din][H], b1 [H], W2 [H][H], b2 [H], w3 [H], b3 [1]; loss = mean((y - t)^2).
+flat vector W1 [din][H], b1 [H], W2 [H][H], b2 [H], w3 [H], b3 [1]; loss = mean((y - t)^2), or with
+tau in (0, 1) the pinball loss of the tau-quantile, mean(tau (t - y) where t >= y, (1 - tau) (y - t)
+elsewhere).
 """
 import math
 
@@ -47,14 +49,19 @@ def forward(p, X, din, h):
     return A2 @ w3 + b3, (X, Z1, A1, Z2, A2)
 
 
-def loss_and_grad(p, X, t, din, h):
-    """(mean squared error, its gradient as a flat vector in parameter order)."""
+def loss_and_grad(p, X, t, din, h, tau=0.0):
+    """(loss, its gradient as a flat vector in parameter order): the mean squared error for tau = 0,
+    else the pinball loss of the tau-quantile."""
     W1, b1, W2, b2, w3, b3 = unpack(p, din, h)
     y, (X, Z1, A1, Z2, A2) = forward(p, X, din, h)
     t = np.asarray(t, np.float64)
     d = y - t
-    loss = float(np.mean(d * d))
-    dy = 2.0 * d / len(t)
+    if tau <= 0.0:
+        loss = float(np.mean(d * d))
+        dy = 2.0 * d / len(t)
+    else:
+        loss = float(np.mean(np.where(d > 0, (1.0 - tau) * d, -tau * d)))
+        dy = np.where(d > 0, 1.0 - tau, -tau) / len(t)
     gw3 = A2.T @ dy
     gb3 = dy.sum()
     dZ2 = np.outer(dy, w3) * gelu_grad(Z2)

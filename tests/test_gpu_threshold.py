@@ -4,10 +4,10 @@
    FP32 tolerance: relative 2e-4 of the gradient's scale, written below.
 2. Training with the library's own kernels lowers the loss.
 3. A searcher using a trained model returns the oracle's results bit for bit; so do models whose
-   thresholds are far too high (the estimation pass keeps nothing and the sample's threshold stands)
-   and far too low.
-4. What the model gains: on held-out queries its threshold-estimation pass keeps far fewer docs than
-   the same pass at the doc sample's threshold, and few queries' predictions were too high.
+   thresholds are far too high (every query with more than K passing docs misses the select step's
+   check and is re-run at its proven threshold) and far too low.
+4. What the model gains: on held-out K = 1000 queries its candidate passes keep far fewer docs than
+   the same searcher without it, and few queries' predictions were too high.
 """
 import numpy as np
 import pytest
@@ -23,11 +23,13 @@ pytestmark = pytest.mark.gpu
 GRAD_RTOL = 2e-4  # relative to the largest gradient magnitude (FP32 GEMMs, sums of up to 64 terms)
 
 
-def test_mlp_forward_and_gradients_match_cpu(torch_cuda):
+@pytest.mark.parametrize("tau", [0.0, 0.05], ids=["mse", "pinball"])
+def test_mlp_forward_and_gradients_match_cpu(torch_cuda, tau):
     torch = torch_cuda
     rng = np.random.default_rng(71)
     din, h, B = 37, 48, 53
     m = hss.ThresholdModel(din, h, device=0, seed=3)
+    m.set_quantile(tau)
     p = m.get_params().astype(np.float64)
     X = rng.standard_normal((B, din)).astype(np.float32)
     t = rng.standard_normal(B).astype(np.float32)
@@ -39,10 +41,29 @@ def test_mlp_forward_and_gradients_match_cpu(torch_cuda):
     y_ref, _ = mlp_ref.forward(p, X, din, h)
     assert np.allclose(dY.cpu().numpy(), y_ref, rtol=1e-4, atol=1e-4 * np.abs(y_ref).max())
     g, loss = m.gradients(dX.data_ptr(), dT.data_ptr(), B)
-    loss_ref, g_ref = mlp_ref.loss_and_grad(p, X, t, din, h)
+    loss_ref, g_ref = mlp_ref.loss_and_grad(p, X, t, din, h, tau)
     assert abs(loss - loss_ref) <= 1e-4 * max(1.0, loss_ref)
     scale = np.abs(g_ref).max()
     assert np.abs(g - g_ref).max() <= GRAD_RTOL * scale, np.abs(g - g_ref).max() / scale
+
+
+def test_fused_forward_equals_the_training_forward(torch_cuda):
+    # the one-launch inference pass sums in the GEMMs' order, so its outputs match the training pass's
+    # (whose loss against a zero target is the mean squared output) to rounding of the loss sum
+    torch = torch_cuda
+    rng = np.random.default_rng(73)
+    for din, h, B in ((37, 48, 53), (396, 256, 256), (844, 256, 7)):
+        m = hss.ThresholdModel(din, h, device=0, seed=5)
+        X = torch.tensor(rng.standard_normal((B, din)).astype(np.float32), device="cuda")
+        dY = torch.zeros(B, dtype=torch.float32, device="cuda")
+        m.forward(X.data_ptr(), B, dY.data_ptr())
+        zero = torch.zeros(B, dtype=torch.float32, device="cuda")
+        _, loss = m.gradients(X.data_ptr(), zero.data_ptr(), B)
+        torch.cuda.synchronize()
+        y = dY.cpu().numpy().astype(np.float64)
+        assert abs(loss - float(np.mean(y * y))) <= 1e-6 * max(1.0, loss), (din, h, B)
+        y_ref, _ = mlp_ref.forward(m.get_params().astype(np.float64), X.cpu().numpy(), din, h)
+        assert np.allclose(y, y_ref, rtol=1e-4, atol=1e-4 * np.abs(y_ref).max()), (din, h, B)
 
 
 def test_training_steps_lower_the_loss(torch_cuda):
@@ -79,6 +100,15 @@ def _search(s, q, exprs, topks):
     for a, e, k in zip(q, exprs, topks):
         s.add_query(e, a, int(k))
     return s.batch_search()
+
+
+def _predicted(q, exprs, topks, vec, bits):
+    """The queries the searcher predicts a threshold for: those whose filter passes more than
+    MIN_PASS_FACTOR * K docs (counted by the oracle)."""
+    from hybridsearchsystem_b200.threshold import MIN_PASS_FACTOR
+    limit = np.asarray(topks, np.int64) * MIN_PASS_FACTOR
+    _, _, c = oracle.topk(q, exprs, int(limit.max()) + 1, vec, bits, threads=8)
+    return np.asarray(c, np.int64) > limit
 
 
 def _check_exact(res, want, nq):
@@ -131,31 +161,39 @@ def test_learned_threshold_search_is_exact(torch_cuda, method):
     assert report["loss_last_epoch"] < report["loss_first_epoch"]
     qv, ev, kv = _queries(mix, 200, 95)
     want = oracle.topk(qv, ev, kv, vec, bits, threads=8)
+    gated = _predicted(qv, ev, kv, vec, bits)
     for m in (margin, -1.0, 1.5):  # calibrated, far too high a threshold, far too low
         s.set_threshold_model(model, m)
         _check_exact(_search(s, qv, ev, kv), want, len(qv))
         assert (s.last_status(len(qv)) == 0).all()
+        miss = s.last_threshold_misses(len(qv))
+        assert not miss[~gated].any()  # their proven thresholds stand
+        if m == -1.0:  # far too high: the queries the prediction applies to miss
+            assert miss[gated].mean() > 0.9, miss.mean()
+        if m == 1.5:
+            assert not miss.any()
 
 
-def test_learned_threshold_prunes_the_estimation_pass(torch_cuda):
-    # 400k docs against a 4096-doc sample: the sample's proven threshold is loose, so the estimation
-    # pass at that threshold keeps many docs; the model's threshold should keep far fewer, with few
-    # queries whose prediction was too high (kept fewer than K, so the sample's threshold stood)
+def test_learned_threshold_prunes_the_candidates(torch_cuda):
+    # 400k docs, K = 1000: without a model the doc sample grows with K and the two-part pass keeps the
+    # docs above the sample's (then pass A's) proven threshold; with the model the passes prune at the
+    # predicted K-th score less the margin, so far fewer docs reach the select step, and few
+    # predictions were too high (re-runs)
     mix, vec, bits, table = _world(seed=83, n=400000)
     s = hss.FullRecallSearcher(table, max_batch=256, method=2, sample_docs=4096)
     qt, et, kt = _queries(mix, 8192, 96)
     model, margin, report = fit_threshold_model(s, qt, et, kt, hidden=128, steps=3000, seed=2)
-    qv, ev, kv = _queries(mix, 256, 99, k=100)
-    s.set_threshold_model(model, 1e9)  # a threshold of -inf: the estimation pass at the sample's threshold
+    qv, ev, kv = _queries(mix, 256, 99, k=1000)
+    want = oracle.topk(qv, ev, kv, vec, bits, threads=8)
     _search(s, qv, ev, kv)
-    at_sample = s.last_estimate_counts(len(qv)).astype(np.int64)
+    without = s.last_candidate_counts(len(qv)).astype(np.int64)
     s.set_threshold_model(model, margin)
-    _search(s, qv, ev, kv)
-    learned = s.last_estimate_counts(len(qv)).astype(np.int64)
-    assert (learned <= at_sample).all()  # the model can only raise the threshold
-    miss = np.mean(learned < kv)
-    pruned = 1.0 - learned.sum() / max(1, at_sample.sum())
-    print("learned threshold: estimation-pass docs", at_sample.sum(), "->", learned.sum(), "pruned", pruned,
-          "miss rate", miss, report)
-    assert pruned > 0.3, (pruned, miss, report)
-    assert miss < 0.15, (pruned, miss, report)
+    _check_exact(_search(s, qv, ev, kv), want, len(qv))
+    learned = s.last_candidate_counts(len(qv)).astype(np.int64)
+    miss = s.last_threshold_misses(len(qv))
+    many = _predicted(qv, ev, kv, vec, bits)  # the queries the prediction applies to
+    pruned = 1.0 - learned[many & ~miss].sum() / max(1, without[many & ~miss].sum())
+    print("learned threshold: candidates", without[many].sum(), "->", learned[many].sum(), "pruned", pruned,
+          "miss rate", miss[many].mean(), report)
+    assert pruned > 0.3, (pruned, miss.mean(), report)
+    assert miss[many].mean() < 0.15, (pruned, miss.mean(), report)
