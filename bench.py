@@ -93,6 +93,7 @@ def parse_args(argv=None):
     ap.add_argument("--serve-rates", default="1000,10000,50000,100000,150000,200000",
                     help="offered Poisson rates (QPS) of the serving sweep")
     ap.add_argument("--serve-wait-us", type=int, default=300)
+    ap.add_argument("--serve-slots", type=int, default=3, help="serving-loop slots (concurrent batches)")
     return ap.parse_args(argv)
 
 
@@ -717,10 +718,11 @@ def measure_serving(args, ctx, method, rates, model=None, margin=0.0):
     Poisson arrival rates. Requests mix the workload's filters (selectivity log-uniform in
     [1e-4, 1]) with per-request K log-uniform in [1, 1000]."""
     import hybridsearchsystem_b200 as hss
-    srv = hss.Server(ctx["table"], slots=2, max_batch=args.batch, max_wait_us=args.serve_wait_us,
+    srv = hss.Server(ctx["table"], slots=args.serve_slots, max_batch=args.batch, max_wait_us=args.serve_wait_us,
                      method=METHODS[method], candidate_cap=args.cand_cap)
     if model is not None:
         srv.set_threshold_model(model, margin)
+    srv_slots = srv.stats()["slots"]  # admitted within the device-memory budget
     q, ex = ctx["queries"], ctx["exprs"]
     kk = np.exp(np.random.default_rng(77).uniform(0.0, np.log(1000.0), len(q))).astype(np.uint32) + 1
     kk = np.minimum(kk, 1000)
@@ -734,7 +736,7 @@ def measure_serving(args, ctx, method, rates, model=None, margin=0.0):
         out.append({"offered_qps": round(offered), "completed_qps": round(n / wall), "p50_ms": round(st["p50_ms"], 3),
                     "p99_ms": round(st["p99_ms"], 3), "mean_batch": round(st["mean_batch"], 1)})
     srv.close()
-    return {"form": form_name(method, model is not None), "slots": 2,
+    return {"form": form_name(method, model is not None), "slots": srv_slots,
             "max_wait_us": args.serve_wait_us, "topk": "log-uniform in [1, 1000] per request", "rates": out}
 
 

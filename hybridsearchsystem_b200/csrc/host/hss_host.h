@@ -493,6 +493,8 @@ class FullRecallSearcher {
     // the next batch.
     int LastCandidateCounts(uint32_t n, uint32_t* counts);
 
+    static constexpr uint32_t kRerunSplit = 16;  // a tensor-core re-run's first part: every 16th tile
+
     // Pipeline test: the next batch's first single-SM tensor-core pass stops issuing corpus loads
     // before its holdLoad-th, with waitBudget clock cycles (0: the default) for its waits; the pass
     // then aborts through its bounded-wait path and the batch reports the error.

@@ -713,8 +713,9 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
         Ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
                           m_dX, stream));
         if (m_model->Forward(m_dX, nq, m_dYp, stream) != 0) Ck(cudaErrorUnknown);
-        Ck(launch_predict_theta(m_dYp, dEpsMain, reinterpret_cast<const uint32_t*>(D + SL.passCount), dTopk, nq,
-                                m_model->scale, m_model->shift, m_margin, dTheta, dThetaPr, m_dYp, stream));
+        Ck(launch_predict_theta(m_dYp, dEpsMain, reinterpret_cast<const uint32_t*>(D + SL.passCount), dTopk,
+                                m_dStats, nq, m_model->scale, m_model->shift, m_margin, dTheta, dThetaPr, m_dYp,
+                                stream));
         Ck(cudaMemcpyAsync(m_hThetaA, m_dYp, nq * 4ull, cudaMemcpyDeviceToHost, stream));
         m_b.launches += 5;
     }
@@ -876,11 +877,43 @@ int FullRecallSearcher::SearchFinish() {
             Stage(dQlist, nre);  // the staged rows become the re-run queries (their bounds unchanged)
             ++m_b.launches;
         }
-        // one pass over every tile with the raised threshold
+        // one pass over every tile with the raised threshold; on the tensor-core path in two parts, as
+        // in the first attempt: every kRerunSplit-th tile first, whose K-th best raises the threshold
+        // for the rest (a query re-run because its predicted threshold kept fewer than K docs comes
+        // back with only its doc sample's threshold, which may be far too low for one full pass)
         const uint64_t tilesR = TilesOf(UnitOf(nre, simt));
-        const uint32_t segs = SegsOf(nre, tilesR, C, simt);
-        const uint32_t segCap = SegCapOf(nre, tilesR, C, segs, simt);
-        Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, 1, 0, tilesR, dQlist, nre, simt);
+        uint32_t segs, segCap;
+        if (!simt && tilesR >= 2ull * kRerunSplit) {
+            const uint64_t countA = (tilesR + kRerunSplit - 1) / kRerunSplit, countB = tilesR - countA;
+            const uint32_t segsA = SegsOf(nre, countA, C, false), segsB = SegsOf(nre, countB, C, false);
+            segCap = std::min(SegCapOf(nre, countA, C, segsA + segsB, false),
+                              SegCapOf(nre, countB, C, segsA + segsB, false));
+            segs = segsA + segsB;
+            Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, kRerunSplit, 0, countA, dQlist, nre,
+                 false);
+            SampleThresholdLaunch RT{};
+            RT.score = m_dCandScore;
+            RT.count = dCandCount;
+            RT.cap = C;
+            RT.segs = segsA;
+            RT.seg_cap = segCap;
+            RT.raise_only = 1;
+            RT.topk = reinterpret_cast<const uint32_t*>(D + SL.topk);
+            RT.eps_sample = reinterpret_cast<const float*>(D + SL.epsMain);  // t - 2 eps_main
+            RT.eps_main = reinterpret_cast<const float*>(D + SL.epsMain);
+            RT.theta = dTheta;
+            RT.theta_also = SE.theta_proven;
+            RT.qlist = dQlist;
+            RT.nq_list = nre;
+            Ck(launch_sample_threshold(RT, stream));
+            Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, segsA, segCap, 0, 1, kRerunSplit, countB, dQlist,
+                 nre, false);
+            m_b.launches += 2;
+        } else {
+            segs = SegsOf(nre, tilesR, C, simt);
+            segCap = SegCapOf(nre, tilesR, C, segs, simt);
+            Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, segCap, 0, 1, 0, tilesR, dQlist, nre, simt);
+        }
         for (uint32_t i = 0; i < nre; ++i) m_lastSegs[hQlist[i]] = {segs, segCap};
         SE.segs = segs;
         SE.seg_cap = segCap;

@@ -284,11 +284,13 @@ struct FeatureLaunch {
 cudaError_t launch_features(const FeatureLaunch& L, cudaStream_t stream);
 // The learned threshold of each query: theta_proven[q] = theta[q] (the proven one), then
 // theta[q] = max(theta[q], y[q] * scale + shift - margin - eps[q]) where the filter passes more than
-// kLearnedMinPass * topk[q] docs; theta_model[q] gets the new theta (it may alias y).
+// kLearnedMinPass * topk[q] docs and the doc sample (stats [nq][kSampleStats]) held at least
+// kLearnedMinSample of them; theta_model[q] gets the new theta (it may alias y).
 constexpr uint32_t kLearnedMinPass = 4;
+constexpr float kLearnedMinSample = 64.0f;  // every sample rank feature (1, 2, 4, ..., 64) present
 cudaError_t launch_predict_theta(const float* y, const float* eps, const uint32_t* pass_count, const uint32_t* topk,
-                                 uint32_t nq, float scale, float shift, float margin, float* theta,
-                                 float* theta_proven, float* theta_model, cudaStream_t stream);
+                                 const float* stats, uint32_t nq, float scale, float shift, float margin,
+                                 float* theta, float* theta_proven, float* theta_model, cudaStream_t stream);
 
 // Cross-shard merge of sorted per-shard top-K lists (select.cu).
 constexpr uint32_t kMaxShards = 64;

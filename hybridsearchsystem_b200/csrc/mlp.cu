@@ -128,6 +128,7 @@ __global__ void loss_grad_kernel(const float* __restrict__ y, const float* __res
 // runs over k in ascending order with fmaf, the bias added after, as gemm_kernel does: the outputs equal
 // the three-GEMM forward pass (ForwardInto) bit for bit.
 constexpr int kFwdRows = 4;
+constexpr int kFwdUnroll = 16;
 
 __global__ void mlp_forward_kernel(const float* __restrict__ X, int B, int D, int H, const float* __restrict__ P,
                                    float* __restrict__ y) {
@@ -149,24 +150,35 @@ __global__ void mlp_forward_kernel(const float* __restrict__ X, int B, int D, in
     const float* w3 = b2 + H;
     const float* b3 = w3 + H;
     const int j = threadIdx.x;
+    // acc[r] += in[r][k] * W[k][j] for k ascending; the weights of kFwdUnroll k's are loaded before
+    // they are used, so that many loads are in flight (the loop is otherwise bound by load latency)
+    auto layer = [&](const float* __restrict__ W, const float* in, int K, float (&acc)[kFwdRows]) {
+        int k = 0;
+        for (; k + kFwdUnroll <= K; k += kFwdUnroll) {
+            float w[kFwdUnroll];
+#pragma unroll
+            for (int u = 0; u < kFwdUnroll; ++u) w[u] = __ldg(W + static_cast<int64_t>(k + u) * H + j);
+#pragma unroll
+            for (int u = 0; u < kFwdUnroll; ++u)
+#pragma unroll
+                for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(in[r * K + k + u], w[u], acc[r]);
+        }
+        for (; k < K; ++k) {
+            const float w = __ldg(W + static_cast<int64_t>(k) * H + j);
+#pragma unroll
+            for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(in[r * K + k], w, acc[r]);
+        }
+    };
     if (j < H) {
         float acc[kFwdRows] = {};
-        for (int k = 0; k < D; ++k) {
-            const float w = W1[static_cast<int64_t>(k) * H + j];
-#pragma unroll
-            for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(xs[r * D + k], w, acc[r]);
-        }
+        layer(W1, xs, D, acc);
 #pragma unroll
         for (int r = 0; r < kFwdRows; ++r) a1[r * H + j] = gelu(acc[r] + b1[j]);
     }
     __syncthreads();
     if (j < H) {
         float acc[kFwdRows] = {};
-        for (int k = 0; k < H; ++k) {
-            const float w = W2[static_cast<int64_t>(k) * H + j];
-#pragma unroll
-            for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(a1[r * H + k], w, acc[r]);
-        }
+        layer(W2, a1, H, acc);
 #pragma unroll
         for (int r = 0; r < kFwdRows; ++r) a2[r * H + j] = gelu(acc[r] + b2[j]);
     }
@@ -227,18 +239,20 @@ __global__ void features_kernel(FeatureLaunch L) {
 // query's error bound), the proven one kept in theta_proven. A doc of the true top K then clears
 // theta whenever the prediction minus the margin is at most the true K-th score. A query whose filter
 // passes at most kLearnedMinPass * K docs keeps its proven threshold: its candidates are few whatever
-// the threshold, and its K-th score is the hardest to predict. fmaxf drops a NaN prediction.
+// the threshold, and its K-th score is the hardest to predict. So does a query whose doc sample held
+// fewer than kLearnedMinSample filtered docs (its sample rank features are missing). fmaxf drops a
+// NaN prediction.
 // theta_model may alias y (each thread reads, then writes, its own element).
 __global__ void predict_theta_kernel(const float* y, const float* __restrict__ eps,
                                      const uint32_t* __restrict__ pass_count, const uint32_t* __restrict__ topk,
-                                     uint32_t nq, float scale, float shift, float margin, float* theta,
-                                     float* theta_proven, float* theta_model) {
+                                     const float* __restrict__ stats, uint32_t nq, float scale, float shift,
+                                     float margin, float* theta, float* theta_proven, float* theta_model) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
     const float t1 = theta[q];
-    const float t = static_cast<uint64_t>(pass_count[q]) <= static_cast<uint64_t>(kLearnedMinPass) * topk[q]
-                        ? t1
-                        : fmaxf(t1, __fsub_rd(__fsub_rd(fmaf(y[q], scale, shift), margin), eps[q]));
+    const bool use = static_cast<uint64_t>(pass_count[q]) > static_cast<uint64_t>(kLearnedMinPass) * topk[q] &&
+                     stats[static_cast<uint64_t>(q) * kSampleStats + kSampleRanks + 1] >= kLearnedMinSample;
+    const float t = use ? fmaxf(t1, __fsub_rd(__fsub_rd(fmaf(y[q], scale, shift), margin), eps[q])) : t1;
     theta_proven[q] = t1;
     theta[q] = t;
     theta_model[q] = t;
@@ -310,11 +324,11 @@ cudaError_t launch_features(const FeatureLaunch& L, cudaStream_t stream) {
 }
 
 cudaError_t launch_predict_theta(const float* y, const float* eps, const uint32_t* pass_count, const uint32_t* topk,
-                                 uint32_t nq, float scale, float shift, float margin, float* theta,
-                                 float* theta_proven, float* theta_model, cudaStream_t stream) {
+                                 const float* stats, uint32_t nq, float scale, float shift, float margin,
+                                 float* theta, float* theta_proven, float* theta_model, cudaStream_t stream) {
     if (nq == 0) return cudaSuccess;
-    predict_theta_kernel<<<(nq + 127) / 128, 128, 0, stream>>>(y, eps, pass_count, topk, nq, scale, shift, margin,
-                                                               theta, theta_proven, theta_model);
+    predict_theta_kernel<<<(nq + 127) / 128, 128, 0, stream>>>(y, eps, pass_count, topk, stats, nq, scale, shift,
+                                                               margin, theta, theta_proven, theta_model);
     return cudaGetLastError();
 }
 

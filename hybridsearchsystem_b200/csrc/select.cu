@@ -429,26 +429,29 @@ __global__ void __launch_bounds__(kST) sample_threshold_kernel(SampleThresholdLa
     const uint32_t n = load_segments(S, L.count + static_cast<uint64_t>(qi) * kMaxCandSegs, L.segs, L.seg_cap, &lost);
     float theta = L.raise_only ? L.theta[qi] : -INFINITY;
     if (L.stats) {
-        // the sample's best scores at ranks 1, 2, 4, ..., 64: the key at rank r = min(64, n), then the
-        // (fewer than r) keys above it, each placed by counting the keys that precede it
+        // the sample's best scores at ranks 1, 2, 4, ..., 64: a lower bound of the key at rank
+        // r = min(64, n) (its 24-bit prefix, two walks of the list), then the (fewer than r) keys above
+        // that prefix's bucket, each placed by counting the keys that precede it; a rank inside the
+        // bucket gets the bound (at most 2^-15 relative below the score)
         float* st = L.stats + static_cast<uint64_t>(qi) * kSampleStats;
         const float* sc = L.score + static_cast<uint64_t>(qi) * L.cap;
         const uint32_t r = min(n, 64u);
         uint32_t key_r = 0;
         if (r > 0)
-            key_r = kth_largest_u32_visit(
+            key_r = kth_lower_bound_u32_visit(
                 [&](auto fn) {
                     for_each_segment_entry(S, L.segs, L.seg_cap, sc, [&](uint32_t, bool ok, float v) {
                         if (ok) fn(float_key(v));
                     });
                 },
                 r, S);
+        const uint32_t bucket_top = key_r | 0xFFu;
         if (threadIdx.x == 0) S.counter = 0;
         __syncthreads();
         if (r > 0)
             for_each_segment_entry(S, L.segs, L.seg_cap, sc, [&](uint32_t, bool ok, float v) {
                 const uint32_t key = ok ? float_key(v) : 0u;
-                if (ok && key > key_r) {
+                if (ok && key > bucket_top) {
                     const uint32_t slot = atomicAdd(&S.counter, 1u);
                     if (slot < 64u) S.sortbuf[slot] = key;
                 }

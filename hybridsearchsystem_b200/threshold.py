@@ -5,8 +5,9 @@ prediction - margin - error bound), and its select step checks each such query: 
 score must clear that threshold by the error bound, else the query is re-run at a proven threshold
 (a miss). So the label of a query is its exact K-th best score, from the searcher's own exact path
 (no model set). The searcher predicts only for queries whose filter passes more than
-MIN_PASS_FACTOR * K docs (the others have few candidates whatever the threshold); the queries trained
-and calibrated on are those whose filter passes at least that many.
+MIN_PASS_FACTOR * K docs (the others have few candidates whatever the threshold) and whose doc sample
+held at least 64 of them (every sample rank feature present); the queries trained and calibrated on
+are those.
 
 The network predicts the standardised label with the library's own forward / backward / Adam kernels
 (ThresholdModel.train_step). With tau > 0 it is trained on the pinball loss of the tau-quantile, so it
@@ -26,7 +27,7 @@ MIN_PASS_FACTOR = 4  # kLearnedMinPass of the searcher's prediction step
 def label_and_features(searcher, queries, exprs, topks, batch=None, min_pass_factor=MIN_PASS_FACTOR):
     """(X [n][din] device tensor, labels [n] float32 numpy): the feature rows and each query's exact
     K-th best score (NaN where its filter passes fewer than min(min_pass_factor * K, HSS_MAX_TOPK)
-    docs)."""
+    docs, or where its doc sample held fewer than 64 of them)."""
     import torch
     from ._lib import HSS_MAX_TOPK
     dev = torch.device("cuda", searcher.table.device)
@@ -53,9 +54,11 @@ def label_and_features(searcher, queries, exprs, topks, batch=None, min_pass_fac
         assert rc == 0, searcher.last_status(nb)
         s_h = sc[:nb].cpu().numpy()
         c_h = cnt[:nb].cpu().numpy()
+        # the sample's rank-64 feature (-2 when its sample held fewer than 64 filtered docs)
+        full = X[b0:b0 + nb, din - 3].cpu().numpy() != -2.0
         for i in range(nb):
             k = int(topks[b0 + i])
-            if k > 0 and c_h[i] >= int(rk[i]):
+            if k > 0 and c_h[i] >= int(rk[i]) and full[i]:
                 labels[b0 + i] = s_h[i, k - 1]
         f.close()
     return X, labels

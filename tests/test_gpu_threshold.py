@@ -102,13 +102,23 @@ def _search(s, q, exprs, topks):
     return s.batch_search()
 
 
-def _predicted(q, exprs, topks, vec, bits):
-    """The queries the searcher predicts a threshold for: those whose filter passes more than
-    MIN_PASS_FACTOR * K docs (counted by the oracle)."""
+def _predicted(s, q, exprs, topks, vec, bits):
+    """The queries searcher s predicts a threshold for: those whose filter passes more than
+    MIN_PASS_FACTOR * K docs (counted by the oracle) and whose doc sample held at least 64 of them
+    (the sample's rank-64 feature is present)."""
+    import torch
     from hybridsearchsystem_b200.threshold import MIN_PASS_FACTOR
     limit = np.asarray(topks, np.int64) * MIN_PASS_FACTOR
     _, _, c = oracle.topk(q, exprs, int(limit.max()) + 1, vec, bits, threads=8)
-    return np.asarray(c, np.int64) > limit
+    din = s.feature_dim()
+    X = torch.zeros((len(q), din), dtype=torch.float32, device="cuda")
+    dq = torch.tensor(np.ascontiguousarray(q, np.float32), device="cuda")
+    f = s.compile_filters(list(exprs))
+    s.features(dq.data_ptr(), len(q), f, np.asarray(topks, np.uint32), X.data_ptr(),
+               torch.cuda.current_stream().cuda_stream)
+    f.close()
+    full = X[:, din - 3].cpu().numpy() != -2.0
+    return (np.asarray(c, np.int64) > limit) & full
 
 
 def _check_exact(res, want, nq):
@@ -161,7 +171,7 @@ def test_learned_threshold_search_is_exact(torch_cuda, method):
     assert report["loss_last_epoch"] < report["loss_first_epoch"]
     qv, ev, kv = _queries(mix, 200, 95)
     want = oracle.topk(qv, ev, kv, vec, bits, threads=8)
-    gated = _predicted(qv, ev, kv, vec, bits)
+    gated = _predicted(s, qv, ev, kv, vec, bits)
     for m in (margin, -1.0, 1.5):  # calibrated, far too high a threshold, far too low
         s.set_threshold_model(model, m)
         _check_exact(_search(s, qv, ev, kv), want, len(qv))
@@ -182,7 +192,8 @@ def test_learned_threshold_prunes_the_candidates(torch_cuda):
     mix, vec, bits, table = _world(seed=83, n=400000)
     s = hss.FullRecallSearcher(table, max_batch=256, method=2, sample_docs=4096)
     qt, et, kt = _queries(mix, 8192, 96)
-    model, margin, report = fit_threshold_model(s, qt, et, kt, hidden=128, steps=3000, seed=2)
+    # the margin at the 0.99 quantile of the held-out residuals: about 1 % misses, each re-run exactly
+    model, margin, report = fit_threshold_model(s, qt, et, kt, hidden=128, steps=3000, seed=2, quantile=0.99)
     qv, ev, kv = _queries(mix, 256, 99, k=1000)
     want = oracle.topk(qv, ev, kv, vec, bits, threads=8)
     _search(s, qv, ev, kv)
@@ -191,7 +202,7 @@ def test_learned_threshold_prunes_the_candidates(torch_cuda):
     _check_exact(_search(s, qv, ev, kv), want, len(qv))
     learned = s.last_candidate_counts(len(qv)).astype(np.int64)
     miss = s.last_threshold_misses(len(qv))
-    many = _predicted(qv, ev, kv, vec, bits)  # the queries the prediction applies to
+    many = _predicted(s, qv, ev, kv, vec, bits)  # the queries the prediction applies to
     pruned = 1.0 - learned[many & ~miss].sum() / max(1, without[many & ~miss].sum())
     print("learned threshold: candidates", without[many].sum(), "->", learned[many].sum(), "pruned", pruned,
           "miss rate", miss[many].mean(), report)
