@@ -128,7 +128,7 @@ __global__ void loss_grad_kernel(const float* __restrict__ y, const float* __res
 // runs over k in ascending order with fmaf, the bias added after, as gemm_kernel does: the outputs equal
 // the three-GEMM forward pass (ForwardInto) bit for bit.
 constexpr int kFwdRows = 4;
-constexpr int kFwdUnroll = 16;
+constexpr int kFwdUnroll = 64;  // weight loads in flight per thread
 
 __global__ void mlp_forward_kernel(const float* __restrict__ X, int B, int D, int H, const float* __restrict__ P,
                                    float* __restrict__ y) {
@@ -152,21 +152,19 @@ __global__ void mlp_forward_kernel(const float* __restrict__ X, int B, int D, in
     const int j = threadIdx.x;
     // acc[r] += in[r][k] * W[k][j] for k ascending; the weights of kFwdUnroll k's are loaded before
     // they are used, so that many loads are in flight (the loop is otherwise bound by load latency)
+    // (the last block is partial: its loads and sums stop at K, a uniform condition)
     auto layer = [&](const float* __restrict__ W, const float* in, int K, float (&acc)[kFwdRows]) {
-        int k = 0;
-        for (; k + kFwdUnroll <= K; k += kFwdUnroll) {
+        for (int k = 0; k < K; k += kFwdUnroll) {
             float w[kFwdUnroll];
 #pragma unroll
-            for (int u = 0; u < kFwdUnroll; ++u) w[u] = __ldg(W + static_cast<int64_t>(k + u) * H + j);
+            for (int u = 0; u < kFwdUnroll; ++u) w[u] = k + u < K ? __ldg(W + static_cast<int64_t>(k + u) * H + j) : 0.0f;
 #pragma unroll
-            for (int u = 0; u < kFwdUnroll; ++u)
+            for (int u = 0; u < kFwdUnroll; ++u) {
+                if (k + u < K) {
 #pragma unroll
-                for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(in[r * K + k + u], w[u], acc[r]);
-        }
-        for (; k < K; ++k) {
-            const float w = __ldg(W + static_cast<int64_t>(k) * H + j);
-#pragma unroll
-            for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(in[r * K + k], w, acc[r]);
+                    for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(in[r * K + k + u], w[u], acc[r]);
+                }
+            }
         }
     };
     if (j < H) {

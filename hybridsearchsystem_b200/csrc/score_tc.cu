@@ -618,12 +618,7 @@ struct PairShared {
 // shared-memory bytes the barriers take ahead of the 1024-byte aligned query tile
 constexpr size_t kPairSharedBytes = (sizeof(PairShared) + 1023) & ~static_cast<size_t>(1023);
 
-// Epilogue warps: 4 TMEM lane quarters x 2 column groups of 128 docs. (With 16 warps of 64 columns,
-// 18 warps share the SM's four 16,384-register files, five on two of them, so a thread gets at most
-// 96 registers and the epilogue spilled; with 8 warps each thread reads its columns one 64-doc block
-// at a time in 124-127 registers, and the per-tile overhead of the wait, the filter words and the loop
-// is paid once per 128 columns.)
-constexpr int kPairEpiWarps = 8;
+constexpr int kPairEpiWarps = 16;  // 4 column groups x 4 TMEM lane quarters
 constexpr int kPairThreads = 64 + 32 * kPairEpiWarps;
 
 template <int F>
@@ -785,12 +780,8 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
         }
     } else {
         // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (query rows) and doc columns
-        // [kEpiCols g, kEpiCols (g + 1)) of the 256, g = (w - 2) / 4. A thread owns one query row and
-        // that column group for the whole launch; the candidates of each 64-doc block of the group go
-        // to the block's own list segment (four per pair and query), so no atomics.
-        constexpr uint32_t kEpiCols = 256u / (kPairEpiWarps / 4);  // columns per thread
-        constexpr uint32_t kBlk = kEpiCols / 64u;                   // 64-doc blocks (filter words) per thread
-        constexpr uint32_t kChunks = 2 * kBlk;                      // 32-doc chunks per thread
+        // [64 g, 64 g + 64) of the 256, g = (w - 2) / 4. A thread owns one query row and one 64-doc
+        // column group for the whole launch: candidates go to its own list segment, no atomics.
         const uint32_t g = (warp - 2) / 4;
         const uint32_t sub = warp & 3u;
         const uint32_t row = rank * 128u + sub * 32u + lane;
@@ -799,90 +790,68 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
         const float theta = valid ? L.theta[qi] : INFINITY;
         const float qs = (F == kTcE4M3 && valid) ? L.q_scale[row] : 1.0f;
         const uint64_t* brow = L.bits + static_cast<uint64_t>(qi) * L.bits_stride;
-        const uint32_t seg0 = L.seg_base + 4u * pair + g * kBlk;  // segment of the thread's first block
-        const uint64_t rowbase = static_cast<uint64_t>(qi) * L.cap;
+        const uint32_t segment = L.seg_base + 4u * pair + g;
+        const uint64_t seg = static_cast<uint64_t>(qi) * L.cap + static_cast<uint64_t>(segment) * L.seg_cap;
+        float* out_score = L.cand_score + seg;
+        uint32_t* out_loc = L.cand_loc + seg;
         const uint32_t seg_cap = L.seg_cap;
         const uint32_t acc_empty_addr0 = peer_addr(&S.acc_empty[0], 0);
         const uint32_t acc_empty_addr1 = peer_addr(&S.acc_empty[1], 0);
-        uint32_t ncand[kBlk];
-#pragma unroll
-        for (uint32_t b = 0; b < kBlk; ++b) ncand[b] = 0;
+        uint32_t ncand = 0;
         uint32_t iter = 0;
-        // filter word of block b of this thread's columns in a tile (past the bitmap: none pass)
-        auto word_of = [&](uint64_t tile, uint32_t b) -> uint64_t {
-            const uint64_t w = tile * 4 + g * kBlk + b;
+        // filter word of this thread's 64 docs of a tile (past the bitmap: none pass)
+        auto word_of = [&](uint64_t tile) -> uint64_t {
+            const uint64_t w = tile * 4 + g;
             return (valid && w < L.bits_stride) ? brow[w] : 0ull;
         };
-        // 32-bit tile counters (the launcher checks tile_walk_fits)
+        // 32-bit tile counters (the launcher checks tile_walk_fits): registers are tight at 576 threads
         TileWalk walk(L.tile_begin, L.tile_step, L.tile_skip, pair, npairs);
         const uint32_t nt = static_cast<uint32_t>(ntiles);
         uint32_t tile_next = static_cast<uint32_t>(walk.tile());
-        uint64_t fw_next[kBlk];
-#pragma unroll
-        for (uint32_t b = 0; b < kBlk; ++b) fw_next[b] = pair < nt ? word_of(tile_next, b) : 0ull;
+        uint64_t fw_next = pair < nt ? word_of(tile_next) : 0ull;
         for (uint32_t it = pair; it < nt; it += npairs, ++iter) {
             const uint32_t buf = iter & 1u;
             const uint64_t tile = tile_next;
-            uint32_t m[kChunks];
-#pragma unroll
-            for (uint32_t b = 0; b < kBlk; ++b) {
-                m[2 * b] = static_cast<uint32_t>(fw_next[b]);
-                m[2 * b + 1] = static_cast<uint32_t>(fw_next[b] >> 32);
-            }
+            const uint64_t fw = fw_next;
             walk.advance();
             tile_next = static_cast<uint32_t>(walk.tile());
-            if (it + npairs < nt) {
-#pragma unroll
-                for (uint32_t b = 0; b < kBlk; ++b) fw_next[b] = word_of(tile_next, b);
-            }
+            if (it + npairs < nt) fw_next = word_of(tile_next);
             float t = theta;
             if (F == kTcE4M3) {
-                uint64_t ts = tile * 2 + (g * kEpiCols) / 128u;  // 128-doc tile holding this thread's docs
+                uint64_t ts = tile * 2 + g / 2;  // 128-doc tile holding this thread's docs
                 ts = ts < L.tiles128 ? ts : L.tiles128 - 1;
                 t = e4m3_tile_threshold(theta, qs, L.tile_scale[ts]);
             }
-            bool live[kChunks];
+            const uint32_t m[2] = {static_cast<uint32_t>(fw), static_cast<uint32_t>(fw >> 32)};
+            bool live[2];
 #pragma unroll
-            for (uint32_t c = 0; c < kChunks; ++c) live[c] = __any_sync(0xffffffffu, m[c] != 0u);
+            for (int c = 0; c < 2; ++c) live[c] = __any_sync(0xffffffffu, m[c] != 0u);
             const bool ready = pair_wait<F>(&S.acc_full[buf], (iter >> 1) & 1u, S, L.error, 16, false);
             if (!__all_sync(0xffffffffu, ready)) break;
             fence_after();
-            const uint32_t tbase = tmem + ((sub * 32u) << 16) + buf * 256u + g * kEpiCols;
-            // one 64-doc block at a time (two chunks in registers); the buffer goes back to the MMA
-            // issuer once the last block's columns are loaded
+            const uint32_t tbase = tmem + ((sub * 32u) << 16) + buf * 256u + g * 64u;
+            uint32_t v[2][32];
 #pragma unroll
-            for (uint32_t b = 0; b < kBlk; ++b) {
-                uint32_t v[2][32];
+            for (int c = 0; c < 2; ++c)
+                if (live[c]) tmem_ld32(tbase + c * 32u, v[c]);
+            tmem_wait_ld();
 #pragma unroll
-                for (uint32_t h = 0; h < 2; ++h)
-                    if (live[2 * b + h]) tmem_ld32(tbase + (2 * b + h) * 32u, v[h]);
-                tmem_wait_ld();
+            for (int c = 0; c < 2; ++c) reg_fence(v[c]);
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(buf ? acc_empty_addr1 : acc_empty_addr0);
 #pragma unroll
-                for (uint32_t h = 0; h < 2; ++h) reg_fence(v[h]);
-                if (b + 1 == kBlk) {
-                    fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive_cluster(buf ? acc_empty_addr1 : acc_empty_addr0);
-                }
-                const uint64_t seg = rowbase + static_cast<uint64_t>(seg0 + b) * seg_cap;
-#pragma unroll
-                for (uint32_t h = 0; h < 2; ++h) {
-                    const uint32_t c = 2 * b + h;
-                    const uint64_t doc0 = tile * 256u + g * kEpiCols + c * 32u;
-                    if constexpr (F == kTcE4M3) {
-                        emit_chunk<F>(live[c], m[c], v[h], t, theta, qs, L.doc_scale, doc0, L.cand_score + seg,
-                                      L.cand_loc + seg, seg_cap, ncand[b]);
-                    } else if (live[c]) {
-                        emit_lane(m[c], v[h], t, doc0, L.cand_score + seg, L.cand_loc + seg, seg_cap, ncand[b]);
-                    }
+            for (int c = 0; c < 2; ++c) {
+                const uint64_t doc0 = tile * 256u + g * 64u + c * 32u;
+                if constexpr (F == kTcE4M3) {
+                    emit_chunk<F>(live[c], m[c], v[c], t, theta, qs, L.doc_scale, doc0, out_score, out_loc, seg_cap,
+                                  ncand);
+                } else if (live[c]) {
+                    emit_lane(m[c], v[c], t, doc0, out_score, out_loc, seg_cap, ncand);
                 }
             }
         }
-        if (valid) {
-#pragma unroll
-            for (uint32_t b = 0; b < kBlk; ++b)
-                L.cand_count[static_cast<uint64_t>(qi) * kMaxCandSegs + seg0 + b] = ncand[b];
-        }
+        if (valid) L.cand_count[static_cast<uint64_t>(qi) * kMaxCandSegs + segment] = ncand;
     }
     __syncthreads();
     if (threadIdx.x == 0 && S.n_consumed < S.n_issued) {

@@ -70,6 +70,7 @@ def fit_threshold_model(searcher, queries, exprs, topks, hidden=256, steps=2000,
     holding out n_val of them (or val_fraction) for the early stop and the margin; tau is the quantile
     the network is trained to predict (0: the mean, by squared error). Returns (model, margin, report)."""
     import torch
+    topks = np.asarray(topks, np.uint32)
     X, labels = label_and_features(searcher, queries, exprs, topks)
     keep = np.nonzero(np.isfinite(labels))[0]
     rng = np.random.default_rng(seed)
@@ -137,6 +138,9 @@ def fit_threshold_model(searcher, queries, exprs, topks, hidden=256, steps=2000,
               "val_rmse": float(np.sqrt(np.mean(res_val ** 2))), "train_rmse": float(np.sqrt(np.mean(res_tr ** 2))),
               "margin": margin, "val_overshoot_rate_at_margin": float(np.mean(res_val > margin)),
               "val_residual_quantiles": {str(q): float(np.quantile(res_val, q)) for q in (0.5, 0.9, 0.99, 0.999, 1.0)},
+              "val_residual_quantiles_by_k": {
+                  f"K{int(k)}": {str(q): float(np.quantile(res_val[topks[val] == k], q)) for q in (0.99, 0.999, 1.0)}
+                  for k in np.unique(topks[val])},
               "tau": tau, "labelled_fraction": float(len(keep) / max(1, len(labels))),
               "steps": steps, "best_step": best[2]}
     return model, margin, report
