@@ -585,6 +585,7 @@ void FullRecallSearcher::Cand(const float* theta, float* score, uint32_t* loc, u
     C.tile_skip = skip;
     C.tiles128 = T.GetTileNum();
     C.error = m_dError;
+    C.emit_all = theta == reinterpret_cast<const float*>(m_dStage + MakeLayout(m_cfg.maxBatch).negInf) ? 1 : 0;
     if (m_testHold && tc_tile_docs(rows, m_tcKblocks) == 128u) {  // the single-SM kernel only
         C.hold_load = m_testHold;
         C.wait_budget = m_testBudget;

@@ -166,6 +166,7 @@ struct TcCandLaunch {
     uint32_t kblocks;          // dim * element bytes / 128
     uint32_t stages;           // stages in the TMA ring (set by launch_tc_cand)
     uint32_t group;            // corpus k-blocks per ring stage (set by launch_tc_cand; 1 or 2)
+    int emit_all;              // every row's threshold is -inf (the doc sample): most docs are kept
     const float* doc_scale;    // E4M3: per-doc dequantisation scale
     const float2* tile_scale;  // E4M3: per 128-doc tile (min, max) of doc_scale
     const float* q_scale;      // E4M3: per staged query row

@@ -640,7 +640,7 @@ __device__ inline bool pair_wait(unsigned long long* bar, uint32_t parity, PairS
 
 // SQ (streamed queries, long vectors): no resident query tile; each stage holds the query k-block
 // (16 KB, from the L2-resident staged queries) followed by the doc k-block, loaded together.
-template <int F, bool SQ>
+template <int F, bool SQ, bool WIDE>
 __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_constant__ CUtensorMap doc_map,
                                                                   const __grid_constant__ CUtensorMap qry_map,
                                                                   TcCandLaunch L) {
@@ -830,24 +830,51 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
             if (!__all_sync(0xffffffffu, ready)) break;
             fence_after();
             const uint32_t tbase = tmem + ((sub * 32u) << 16) + buf * 256u + g * 64u;
-            uint32_t v[2][32];
+            if constexpr (WIDE) {
+                // a pass that keeps most docs (the doc sample): both chunks in registers, the buffer
+                // back to the issuer before the long emission (spills a little at 96 registers)
+                uint32_t v[2][32];
 #pragma unroll
-            for (int c = 0; c < 2; ++c)
-                if (live[c]) tmem_ld32(tbase + c * 32u, v[c]);
-            tmem_wait_ld();
+                for (int c = 0; c < 2; ++c)
+                    if (live[c]) tmem_ld32(tbase + c * 32u, v[c]);
+                tmem_wait_ld();
 #pragma unroll
-            for (int c = 0; c < 2; ++c) reg_fence(v[c]);
-            fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive_cluster(buf ? acc_empty_addr1 : acc_empty_addr0);
+                for (int c = 0; c < 2; ++c) reg_fence(v[c]);
+                fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_cluster(buf ? acc_empty_addr1 : acc_empty_addr0);
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const uint64_t doc0 = tile * 256u + g * 64u + c * 32u;
-                if constexpr (F == kTcE4M3) {
-                    emit_chunk<F>(live[c], m[c], v[c], t, theta, qs, L.doc_scale, doc0, out_score, out_loc, seg_cap,
-                                  ncand);
-                } else if (live[c]) {
-                    emit_lane(m[c], v[c], t, doc0, out_score, out_loc, seg_cap, ncand);
+                for (int c = 0; c < 2; ++c) {
+                    const uint64_t doc0 = tile * 256u + g * 64u + c * 32u;
+                    if constexpr (F == kTcE4M3) {
+                        emit_chunk<F>(live[c], m[c], v[c], t, theta, qs, L.doc_scale, doc0, out_score, out_loc,
+                                      seg_cap, ncand);
+                    } else if (live[c]) {
+                        emit_lane(m[c], v[c], t, doc0, out_score, out_loc, seg_cap, ncand);
+                    }
+                }
+            } else {
+                // one 32-doc chunk in registers at a time (79 registers, where both chunks at once
+                // spilled at the 96-register ceiling); the buffer goes back to the issuer once the
+                // second is loaded
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    uint32_t v[32];
+                    if (live[c]) tmem_ld32(tbase + c * 32u, v);
+                    tmem_wait_ld();
+                    reg_fence(v);
+                    if (c == 1) {
+                        fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive_cluster(buf ? acc_empty_addr1 : acc_empty_addr0);
+                    }
+                    const uint64_t doc0 = tile * 256u + g * 64u + c * 32u;
+                    if constexpr (F == kTcE4M3) {
+                        emit_chunk<F>(live[c], m[c], v, t, theta, qs, L.doc_scale, doc0, out_score, out_loc, seg_cap,
+                                      ncand);
+                    } else if (live[c]) {
+                        emit_lane(m[c], v, t, doc0, out_score, out_loc, seg_cap, ncand);
+                    }
                 }
             }
         }
@@ -874,8 +901,8 @@ template <int F, bool SQ>
 cudaError_t launch_tc2_typed(const TcCandLaunch& L, const CUtensorMap& dmap, const CUtensorMap& qmap,
                              cudaStream_t stream) {
     const size_t smem = tc_pair_smem_bytes(L.kblocks, L.stages, L.group);
-    cudaError_t e = cudaFuncSetAttribute(tc2_cand_kernel<F, SQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    auto kernel = L.emit_all ? tc2_cand_kernel<F, SQ, true> : tc2_cand_kernel<F, SQ, false>;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(L.ctas, 1, 1);
@@ -889,7 +916,7 @@ cudaError_t launch_tc2_typed(const TcCandLaunch& L, const CUtensorMap& dmap, con
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, tc2_cand_kernel<F, SQ>, dmap, qmap, L);
+    return cudaLaunchKernelEx(&cfg, kernel, dmap, qmap, L);
 }
 
 template <int F>
