@@ -16,6 +16,8 @@ namespace hss {
 namespace {
 
 constexpr int kTile = kFilterTileWords;  // == blockDim.x
+// the operand slots' shared memory at most: one 256-word tile of kMaxOperands operands
+constexpr size_t kFilterSmemCeiling = static_cast<size_t>(kFilterTileWords) * kMaxOperands * sizeof(uint64_t);
 
 // Operand descriptor for one (operand, segment) pair, resolved once per CTA.
 struct OperandInfo {
@@ -456,9 +458,11 @@ cudaError_t launch_filter_dense_wpt(const DenseFilterLaunch& L, cudaStream_t str
     const uint64_t gy = static_cast<uint64_t>(L.seg_num) * tiles;
     if (gy > 65535u) return cudaErrorInvalidValue;
     const size_t smem = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * TW * sizeof(uint64_t);
-    // opt in always: static plus dynamic shared memory may pass 48 KB even when the dynamic part does not
+    // opt in always (static plus dynamic shared memory may pass 48 KB even when the dynamic part does
+    // not), to the one ceiling every caller sets: searchers on other threads launch it concurrently
+    if (smem > kFilterSmemCeiling) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(filter_dense_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+                                         static_cast<int>(kFilterSmemCeiling));
     if (e != cudaSuccess) return e;
     filter_dense_kernel<WPT><<<dim3(L.nq, static_cast<uint32_t>(gy)), kDenseT, smem, stream>>>(L);
     return cudaGetLastError();
@@ -751,9 +755,11 @@ cudaError_t launch_filter_wpt(const FilterLaunch& L, cudaStream_t stream) {
     const uint64_t gy = static_cast<uint64_t>(L.seg_num) * tiles;
     if (gy > 65535u) return cudaErrorInvalidValue;
     const size_t smem = static_cast<size_t>(L.max_opnd > 0 ? L.max_opnd : 1) * TW * sizeof(uint64_t);
-    // opt in always: static plus dynamic shared memory may pass 48 KB even when the dynamic part does not
+    // opt in always (static plus dynamic shared memory may pass 48 KB even when the dynamic part does
+    // not), to the one ceiling every caller sets: searchers on other threads launch it concurrently
+    if (smem > kFilterSmemCeiling) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(filter_batch_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+                                         static_cast<int>(kFilterSmemCeiling));
     if (e != cudaSuccess) return e;
     dim3 grid(L.nq, static_cast<uint32_t>(gy));
     filter_batch_kernel<WPT><<<grid, kTile, smem, stream>>>(L);

@@ -182,8 +182,11 @@ cudaError_t launch_exact_score(const float* qry, const float* docs, float* out, 
     if (m == 0 || n == 0) return cudaSuccess;
     const size_t smem = static_cast<size_t>(kExactQ) * dim * sizeof(float);
     if (smem > 48 * 1024) {
+        // one ceiling for every caller (concurrent callers with other dimensions launch it too)
+        constexpr size_t kCeiling = 200 * 1024;
+        if (smem > kCeiling) return cudaErrorInvalidValue;
         cudaError_t e = cudaFuncSetAttribute(exact_score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem));
+                                             static_cast<int>(kCeiling));
         if (e != cudaSuccess) return e;
     }
     dim3 grid((n + kExactDocs - 1) / kExactDocs, (m + kExactQ - 1) / kExactQ);

@@ -897,12 +897,16 @@ __global__ void __launch_bounds__(kPairThreads, 1) tc2_cand_kernel(const __grid_
     }
 }
 
+constexpr size_t kTcSmemCeiling = 232448;  // dynamic shared memory of one CTA (the launchers check smem <= it)
+
 template <int F, bool SQ>
 cudaError_t launch_tc2_typed(const TcCandLaunch& L, const CUtensorMap& dmap, const CUtensorMap& qmap,
                              cudaStream_t stream) {
     const size_t smem = tc_pair_smem_bytes(L.kblocks, L.stages, L.group);
     auto kernel = L.emit_all ? tc2_cand_kernel<F, SQ, true> : tc2_cand_kernel<F, SQ, false>;
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    // the ceiling, not this launch's size: searchers of other tables launch it concurrently
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kTcSmemCeiling));
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(L.ctas, 1, 1);
@@ -924,7 +928,7 @@ cudaError_t launch_tc1_typed(const TcCandLaunch& L, const CUtensorMap& dmap, con
                              cudaStream_t stream) {
     const size_t smem = tc_smem_bytes(1, L.kblocks, L.stages, L.group);
     cudaError_t e = cudaFuncSetAttribute(tc_cand_kernel<F, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+                                         static_cast<int>(kTcSmemCeiling));
     if (e != cudaSuccess) return e;
     tc_cand_kernel<F, 1><<<L.ctas, 64 + 256, smem, stream>>>(dmap, qmap, L);
     return cudaGetLastError();

@@ -787,10 +787,15 @@ __global__ void query_eps_kernel(const float* __restrict__ qry, const uint32_t* 
     }
 }
 
+// Opts a kernel into more than 48 KB of dynamic shared memory, always to the same ceiling: searchers
+// on other threads launch the same kernel concurrently with their own sizes, and a per-call value
+// could drop below another caller's launch.
 template <class K>
 cudaError_t set_smem(K kernel, size_t bytes) {
+    constexpr size_t kCeiling = 200 * 1024;
     if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (bytes > kCeiling) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kCeiling));
 }
 
 }  // namespace
