@@ -750,6 +750,9 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
     SE.status = dStatus;
     SE.qlist = nullptr;
     SE.nq_list = nq;
+    // a batch with a large K keeps long candidate lists (K = 1000: about 13k per query at 10M, past
+    // the default shared-memory buffer): select K from {10, 100, 1000} 0.302 -> 0.199 ms
+    SE.fast_large = maxK > 256 ? 1 : 0;
     // With a model, theta is the prediction: the passes below run at it (raised like a proven one
     // when pass A's K-th best allows), and the select step checks every query whose theta stayed
     // above its proven threshold; a query that fails is re-run at a proven threshold.

@@ -155,6 +155,7 @@ struct SelectLaunch {
     int32_t* status;
     const uint32_t* qlist;
     uint32_t nq_list;
+    int fast_large;            // hold up to 32,768 candidate scores in shared memory (else 12,288)
 };
 
 // Tensor-core candidate pass (score_tc.cu).
