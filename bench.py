@@ -445,11 +445,22 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
 
+    # Two ways to drive the two searchers: on one stream (a batch's stages run alone, so their event
+    # times are the stage times and the candidate stage's roofline), or each on its own stream, so
+    # that one batch's latency-bound stages (filter, sample threshold, select) overlap the other's
+    # candidate pass: the throughput a caller gets from two searchers (the headline value).
+    own_streams = [torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)]
+    mode = {"split": False}
+
+    def stream_of(p):
+        return own_streams[p] if mode["split"] else stream
+
     def enqueue(i, d_queries=None):
         j = (rank * 7919 + i) % nb
         p = i % 2
         searchers[p].search_device_async(d_q[j].data_ptr() if d_queries is None else d_queries, B, filters[j],
-                                         topks[j], o_sc[p].data_ptr(), o_id[p].data_ptr(), o_n[p].data_ptr(), kmax, sh)
+                                         topks[j], o_sc[p].data_ptr(), o_id[p].data_ptr(), o_n[p].data_ptr(), kmax,
+                                         stream_of(p).cuda_stream)
 
     def finish(i):
         srch = searchers[i % 2]
@@ -467,47 +478,64 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev) if flush_l2 else None
     pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
              for _ in range(args.steps)] if flush_l2 else None
-    # device-resident leg
+    # device-resident legs
     gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
-    cand_ms, launches, stage_ms = [], 0, []
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(gpu_uuid) as clk:
-        barrier()
-        torch.cuda.synchronize()
-        ev0.record(stream)
 
-        def done(t):
-            nonlocal launches
-            cand_ms.append(t["candidates_ms"])
-            stage_ms.append([t["filter_ms"], t["sample_ms"], t["candidates_ms"], t["select_ms"], t["total_ms"]])
-            launches += t["launches"]
+    def device_leg(split):
+        """Times args.steps batches (events on the launching stream; with split, the default stream
+        waits for both searchers' streams before the end event). Returns (ms, per-batch stage times,
+        candidate stage times, launches, clocks)."""
+        mode["split"] = split
+        cand_ms, launches, stage_ms = [], 0, []
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(gpu_uuid) as clk:
+            barrier()
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            for t2 in own_streams:
+                t2.wait_stream(stream)
 
-        for i in range(args.steps):
-            if flush_l2:  # timed one step at a time, L2 written over between steps (no overlap)
-                flush.fill_(float(i))
-                pairs[i][0].record(stream)
+            def done(t):
+                nonlocal launches
+                cand_ms.append(t["candidates_ms"])
+                stage_ms.append([t["filter_ms"], t["sample_ms"], t["candidates_ms"], t["select_ms"], t["total_ms"]])
+                launches += t["launches"]
+
+            for i in range(args.steps):
+                if flush_l2:  # timed one step at a time, L2 written over between steps (no overlap)
+                    flush.fill_(float(i))
+                    pairs[i][0].record(stream)
+                    enqueue(args.warmup + i)
+                    done(finish(args.warmup + i))
+                    pairs[i][1].record(stream)
+                    continue
                 enqueue(args.warmup + i)
-                done(finish(args.warmup + i))
-                pairs[i][1].record(stream)
-                continue
-            enqueue(args.warmup + i)
-            if i > 0:
-                done(finish(args.warmup + i - 1))
-        if not flush_l2:
-            done(finish(args.warmup + args.steps - 1))
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-    clocks = clk.summary()
-    own_ms = sum(a.elapsed_time(b) for a, b in pairs) if flush_l2 else ev0.elapsed_time(ev1)
+                if i > 0:
+                    done(finish(args.warmup + i - 1))
+            if not flush_l2:
+                done(finish(args.warmup + args.steps - 1))
+            for t2 in own_streams:
+                stream.wait_stream(t2)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+        own = sum(a.elapsed_time(b) for a, b in pairs) if flush_l2 else ev0.elapsed_time(ev1)
+        mode["split"] = False
+        return own, stage_ms, cand_ms, launches, clk.summary()
+
+    # stage times and the roofline from the one-stream leg; the value from the two-stream leg (the
+    # one-stream leg's when each step is timed alone)
+    _, stage_ms, cand_ms, _, _ = device_leg(False)
+    own_ms, _, _, launches, clocks = device_leg(False) if flush_l2 else device_leg(True)
     t_max = max_over_ranks(own_ms, dev)
     value = whole_job_qps(world, args.steps, B, t_max)
 
     # end-to-end leg through the C-ABI: pinned host queries in, results out, every step. Each step
     # is one batch through hss_filters_compile + hss_searcher_search_device_async / hss_searcher_finish
-    # with its host->device query copy and device->host result copy, the two searchers alternating on
-    # one stream. A second host thread compiles the next batch's filters (host-only work, table
-    # read-only) while this batch is on the GPU; the ctypes calls release the interpreter lock.
+    # with its host->device query copy and device->host result copy, the two searchers alternating,
+    # each on its own stream (one shared stream when each step is timed alone). A second host thread
+    # compiles the next batch's filters (host-only work, table read-only) while this batch is on the
+    # GPU; the ctypes calls release the interpreter lock.
     from concurrent.futures import ThreadPoolExecutor
     h_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1)).pin_memory()
     h_sc = torch.zeros((2, B, kmax), dtype=torch.float32).pin_memory()
@@ -537,7 +565,7 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
             rc = searchers[p].finish()
             assert rc == 0
             if searchers[p].last_times()["retries"]:
-                done_ev[p].record(stream)  # the re-runs ran behind later work on the compute stream
+                done_ev[p].record(ss[p])  # the re-runs ran behind later work on that stream
             copy_stream.wait_event(done_ev[p])
             with torch.cuda.stream(copy_stream):
                 h_sc[p].copy_(o_sc[p], non_blocking=True)
@@ -557,10 +585,11 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
                 flush.fill_(float(i))
                 ev[i][0].record(stream)
             out_ev[p].synchronize()  # this slot's previous results have reached the host
-            d_stage[p].copy_(h_q[j], non_blocking=True)
+            with torch.cuda.stream(ss[p]):
+                d_stage[p].copy_(h_q[j], non_blocking=True)
             searchers[p].search_device_async(d_stage[p].data_ptr(), B, f, topks[j], o_sc[p].data_ptr(),
-                                             o_id[p].data_ptr(), o_n[p].data_ptr(), kmax, sh)
-            done_ev[p].record(stream)  # the batch's work as enqueued (re-runs, if any, come later)
+                                             o_id[p].data_ptr(), o_n[p].data_ptr(), kmax, ss[p].cuda_stream)
+            done_ev[p].record(ss[p])  # the batch's work as enqueued (re-runs, if any, come later)
             if ev is not None:  # one step at a time
                 retire(i, f)
                 stream.wait_event(out_ev[p])
@@ -576,12 +605,17 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
             stream.wait_event(e)
         stream.synchronize()
 
+    # each searcher on its own stream, or (each step timed alone) both on the default stream
+    ss = [stream, stream] if flush_l2 else own_streams
+
     with ThreadPoolExecutor(1) as pool:
         e2e_run(2, pool)  # warm-up of the compile thread
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         torch.cuda.synchronize()
         e0.record(stream)
+        for t2 in own_streams:
+            t2.wait_stream(stream)
         e2e_run(args.steps, pool, pairs)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -628,8 +662,11 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
            "l2": "flushed between steps (256 MB write outside the step's events)" if flush_l2 else
                  "inputs larger than L2",
            "method": method, "learned": learned, "searcher": searcher, "dev": dev,
-           "pipelined": "two searchers of the form alternate batches on one stream (enqueue batch i, then "
-                        "finish batch i - 1)"}
+           "pipelined": "two searchers of the form alternate batches (enqueue batch i, then finish batch "
+                        "i - 1), each on its own stream so that one batch's filter, sample and select overlap "
+                        "the other's candidate pass (value, e2e); stages_ms and the roofline come from a "
+                        "run of the same batches with both searchers on one stream, where stages do not "
+                        "overlap"}
     twin.close()
     for f in filters:
         f.close()
@@ -984,8 +1021,8 @@ def run_ours(args):
            "e2e": {"value": chosen["e2e"], "unit": "QPS", "h2d_bytes_per_step": B * 128 * 4,
                    "d2h_bytes_per_step": B * K * (4 + 8) + B * 4,
                    "path": "hss_filters_compile (next batch, compile thread) + hss_searcher_search_device_async / "
-                           "hss_searcher_finish per batch (two searchers alternating on one stream), pinned host "
-                           "queries in, results out on a copy stream"},
+                           "hss_searcher_finish per batch (two searchers alternating, each on its own stream), "
+                           "pinned host queries in, results out on a copy stream"},
            "roofline": chosen["roofline"], "clocks": chosen["clocks"], "gpu_launches": chosen["launches"],
            "stages_ms": chosen["stages_ms"], "forms": {k: summary(v, args.steps) for k, v in forms.items()}}
     if "plain_fp32" in forms:
