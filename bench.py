@@ -94,6 +94,8 @@ def parse_args(argv=None):
                     help="offered Poisson rates (QPS) of the serving sweep")
     ap.add_argument("--serve-wait-us", type=int, default=300)
     ap.add_argument("--serve-slots", type=int, default=3, help="serving-loop slots (concurrent batches)")
+    ap.add_argument("--searchers", type=int, default=4,
+                    help="searchers per form taking batches in turn, each on its own stream (at least 2)")
     return ap.parse_args(argv)
 
 
@@ -426,22 +428,24 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
     if learned:
         model, margin, report = trained_model(args, ctx, searcher, method)
         searcher.set_threshold_model(model, margin)
-    # A second searcher of the same form: batch i runs on searcher i % 2, so while the host finishes
-    # one batch (its statuses, rare re-runs) the next is already queued on the stream.
-    twin = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[method],
-                                  sample_docs=args.sample_docs)
+    # args.searchers searchers of the same form: batch i runs on searcher i % D, so while the host
+    # finishes one batch (its statuses, rare re-runs) the next ones are already queued.
+    D = max(2, args.searchers)
+    others = [hss.FullRecallSearcher(table, max_batch=B, candidate_cap=args.cand_cap, method=METHODS[method],
+                                     sample_docs=args.sample_docs) for _ in range(D - 1)]
     if learned:
-        twin.set_threshold_model(model, margin)
-    searchers = (searcher, twin)
+        for o in others:
+            o.set_threshold_model(model, margin)
+    searchers = (searcher, *others)
     for srch in searchers:
         srch.set_timing(True)
     nb = max(1, len(queries) // B)
     filters = [searcher.compile_filters(exprs[i * B:(i + 1) * B]) for i in range(nb)]
     topks = _topks(args, B, nb, kmode)
     d_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1), device=dev)
-    o_sc = torch.zeros((2, B, kmax), dtype=torch.float32, device=dev)
-    o_id = torch.zeros((2, B, kmax), dtype=torch.int64, device=dev)
-    o_n = torch.zeros((2, B), dtype=torch.int32, device=dev)
+    o_sc = torch.zeros((D, B, kmax), dtype=torch.float32, device=dev)
+    o_id = torch.zeros((D, B, kmax), dtype=torch.int64, device=dev)
+    o_n = torch.zeros((D, B), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
 
@@ -449,7 +453,7 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
     # times are the stage times and the candidate stage's roofline), or each on its own stream, so
     # that one batch's latency-bound stages (filter, sample threshold, select) overlap the other's
     # candidate pass: the throughput a caller gets from two searchers (the headline value).
-    own_streams = [torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)]
+    own_streams = [torch.cuda.Stream(device=dev) for _ in range(D)]
     mode = {"split": False}
 
     def stream_of(p):
@@ -457,23 +461,23 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
 
     def enqueue(i, d_queries=None):
         j = (rank * 7919 + i) % nb
-        p = i % 2
+        p = i % D
         searchers[p].search_device_async(d_q[j].data_ptr() if d_queries is None else d_queries, B, filters[j],
                                          topks[j], o_sc[p].data_ptr(), o_id[p].data_ptr(), o_n[p].data_ptr(), kmax,
                                          stream_of(p).cuda_stream)
 
     def finish(i):
-        srch = searchers[i % 2]
+        srch = searchers[i % D]
         rc = srch.finish()
         assert rc == 0, srch.last_status(B)
         return srch.last_times()
 
     for i in range(args.warmup):
         enqueue(i)
-        if i > 0:
-            finish(i - 1)
-    if args.warmup:
-        finish(args.warmup - 1)
+        if i >= D - 1:
+            finish(i - (D - 1))
+    for i in range(max(0, args.warmup - (D - 1)), args.warmup):
+        finish(i)
     torch.cuda.synchronize()
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev) if flush_l2 else None
     pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -510,10 +514,11 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
                     pairs[i][1].record(stream)
                     continue
                 enqueue(args.warmup + i)
-                if i > 0:
-                    done(finish(args.warmup + i - 1))
+                if i >= D - 1:
+                    done(finish(args.warmup + i - (D - 1)))
             if not flush_l2:
-                done(finish(args.warmup + args.steps - 1))
+                for i in range(max(0, args.steps - (D - 1)), args.steps):
+                    done(finish(args.warmup + i))
             for t2 in own_streams:
                 stream.wait_stream(t2)
             ev1.record(stream)
@@ -538,11 +543,11 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
     # GPU; the ctypes calls release the interpreter lock.
     from concurrent.futures import ThreadPoolExecutor
     h_q = torch.tensor(np.ascontiguousarray(queries[:nb * B]).reshape(nb, B, -1)).pin_memory()
-    h_sc = torch.zeros((2, B, kmax), dtype=torch.float32).pin_memory()
-    h_id = torch.zeros((2, B, kmax), dtype=torch.int64).pin_memory()
-    h_n = torch.zeros((2, B), dtype=torch.int32).pin_memory()
-    d_stage = torch.zeros((2, B, dim), dtype=torch.float32, device=dev)
-    out_ev = [torch.cuda.Event(), torch.cuda.Event()]
+    h_sc = torch.zeros((D, B, kmax), dtype=torch.float32).pin_memory()
+    h_id = torch.zeros((D, B, kmax), dtype=torch.int64).pin_memory()
+    h_n = torch.zeros((D, B), dtype=torch.int32).pin_memory()
+    d_stage = torch.zeros((D, B, dim), dtype=torch.float32, device=dev)
+    out_ev = [torch.cuda.Event() for _ in range(D)]
 
     def batch_of(i):
         return (rank * 7919 + args.warmup + i) % nb
@@ -551,7 +556,7 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
     # would queue behind the next batch's kernels, and the host, waiting for them before it enqueues
     # the batch after, would leave the GPU idle between batches
     copy_stream = torch.cuda.Stream(device=dev)
-    done_ev = [torch.cuda.Event(), torch.cuda.Event()]
+    done_ev = [torch.cuda.Event() for _ in range(D)]
 
     def e2e_run(steps, pool, ev=None):
         # per step: the next batch's filters compiled on a second host thread, its queries copied in
@@ -561,7 +566,7 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
         pending = []
 
         def retire(i, f):
-            p = i % 2
+            p = i % D
             rc = searchers[p].finish()
             assert rc == 0
             if searchers[p].last_times()["retries"]:
@@ -576,7 +581,7 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
 
         for i in range(steps):
             j = batch_of(i)
-            p = i % 2
+            p = i % D
             f = fut.result()
             if i + 1 < steps:
                 jn = batch_of(i + 1)
@@ -596,17 +601,17 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
                 ev[i][1].record(stream)
                 stream.synchronize()
                 continue
-            if pending:
-                retire(*pending.pop())
             pending.append((i, f))
-        if pending:
-            retire(*pending.pop())
+            if len(pending) == D:
+                retire(*pending.pop(0))
+        while pending:
+            retire(*pending.pop(0))
         for e in out_ev:  # the timed region ends with the last results on the host
             stream.wait_event(e)
         stream.synchronize()
 
-    # each searcher on its own stream, or (each step timed alone) both on the default stream
-    ss = [stream, stream] if flush_l2 else own_streams
+    # each searcher on its own stream, or (each step timed alone) all on the default stream
+    ss = [stream] * D if flush_l2 else own_streams
 
     with ThreadPoolExecutor(1) as pool:
         e2e_run(2, pool)  # warm-up of the compile thread
@@ -662,12 +667,13 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
            "l2": "flushed between steps (256 MB write outside the step's events)" if flush_l2 else
                  "inputs larger than L2",
            "method": method, "learned": learned, "searcher": searcher, "dev": dev,
-           "pipelined": "two searchers of the form alternate batches (enqueue batch i, then finish batch "
-                        "i - 1), each on its own stream so that one batch's filter, sample and select overlap "
-                        "the other's candidate pass (value, e2e); stages_ms and the roofline come from a "
-                        "run of the same batches with both searchers on one stream, where stages do not "
+           "pipelined": f"{D} searchers of the form take batches in turn (enqueue batch i, then finish batch "
+                        f"i - {D - 1}), each on its own stream so that one batch's filter, sample and select "
+                        "overlap another's candidate pass (value, e2e); stages_ms and the roofline come from a "
+                        "run of the same batches with the searchers on one stream, where stages do not "
                         "overlap"}
-    twin.close()
+    for o in others:
+        o.close()
     for f in filters:
         f.close()
     if report:
