@@ -555,7 +555,7 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
     # results go out on a copy stream that waits only for their own batch: on the compute stream they
     # would queue behind the next batch's kernels, and the host, waiting for them before it enqueues
     # the batch after, would leave the GPU idle between batches
-    copy_stream = torch.cuda.Stream(device=dev)
+    copy_stream = stream if flush_l2 else torch.cuda.Stream(device=dev)  # one step at a time: no overlap to gain
     done_ev = [torch.cuda.Event() for _ in range(D)]
 
     def e2e_run(steps, pool, ev=None):
