@@ -569,6 +569,13 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
             p = i % D
             rc = searchers[p].finish()
             assert rc == 0
+            if copy_stream is stream:  # one step at a time: the copies follow the batch on its stream
+                h_sc[p].copy_(o_sc[p], non_blocking=True)
+                h_id[p].copy_(o_id[p], non_blocking=True)
+                h_n[p].copy_(o_n[p], non_blocking=True)
+                out_ev[p].record(stream)
+                f.close()
+                return
             if searchers[p].last_times()["retries"]:
                 done_ev[p].record(ss[p])  # the re-runs ran behind later work on that stream
             copy_stream.wait_event(done_ev[p])
@@ -590,8 +597,11 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
                 flush.fill_(float(i))
                 ev[i][0].record(stream)
             out_ev[p].synchronize()  # this slot's previous results have reached the host
-            with torch.cuda.stream(ss[p]):
+            if ss[p] is stream:
                 d_stage[p].copy_(h_q[j], non_blocking=True)
+            else:
+                with torch.cuda.stream(ss[p]):
+                    d_stage[p].copy_(h_q[j], non_blocking=True)
             searchers[p].search_device_async(d_stage[p].data_ptr(), B, f, topks[j], o_sc[p].data_ptr(),
                                              o_id[p].data_ptr(), o_n[p].data_ptr(), kmax, ss[p].cuda_stream)
             done_ev[p].record(ss[p])  # the batch's work as enqueued (re-runs, if any, come later)
