@@ -94,6 +94,9 @@ def parse_args(argv=None):
                     help="offered Poisson rates (QPS) of the serving sweep")
     ap.add_argument("--serve-wait-us", type=int, default=300)
     ap.add_argument("--serve-slots", type=int, default=3, help="serving-loop slots (concurrent batches)")
+    ap.add_argument("--no-graphs", dest="graphs", action="store_false",
+                    help="end-to-end leg and serving loop: launch every batch directly instead of replaying "
+                         "its captured CUDA graph")
     ap.add_argument("--searchers", type=int, default=4,
                     help="searchers per form taking batches in turn, each on its own stream (at least 2)")
     return ap.parse_args(argv)
@@ -408,7 +411,8 @@ def trained_model(args, ctx, searcher, method):
     return models[method]
 
 
-def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=128, flush_l2=False):
+def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=128, flush_l2=False,
+                 e2e_direct=False):
     """One form of the path (candidate-pass method, with or without the learned threshold) over the
     context's workload: device-resident QPS (CUDA events, max over ranks), end-to-end QPS through the
     C-ABI, stage times and the candidate stage's roofline. With flush_l2 (a corpus that fits in L2),
@@ -623,20 +627,35 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
     # each searcher on its own stream, or (each step timed alone) all on the default stream
     ss = [stream] * D if flush_l2 else own_streams
 
-    with ThreadPoolExecutor(1) as pool:
-        e2e_run(2, pool)  # warm-up of the compile thread
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        barrier()
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for t2 in own_streams:
-            t2.wait_stream(stream)
-        e2e_run(args.steps, pool, pairs)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-    own_e2e = sum(a.elapsed_time(b) for a, b in pairs) if flush_l2 else e0.elapsed_time(e1)
-    e2e = whole_job_qps(world, args.steps, B, max_over_ranks(own_e2e, dev))
+    def timed_e2e(graphs):
+        # graphs: each searcher replays its batch shape's captured CUDA graph (the default stream,
+        # which one step at a time uses, cannot be captured); no stage timing in this leg
+        for srch in searchers:
+            srch.set_timing(False)
+            srch.set_graphs(graphs)
+        with ThreadPoolExecutor(1) as pool:
+            e2e_run(2, pool)  # warm-up of the compile thread (and the graphs' captures)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            barrier()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for t2 in own_streams:
+                t2.wait_stream(stream)
+            e2e_run(args.steps, pool, pairs)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+        st = [srch.graph_stats() for srch in searchers]
+        for srch in searchers:
+            srch.set_graphs(False)
+        assert not any(g["failed"] for g in st), st
+        own = sum(a.elapsed_time(b) for a, b in pairs) if flush_l2 else e0.elapsed_time(e1)
+        return (whole_job_qps(world, args.steps, B, max_over_ranks(own, dev)),
+                {"captures": sum(g["captures"] for g in st), "replays": sum(g["replays"] for g in st)})
+
+    use_graphs = args.graphs and not flush_l2
+    e2e, graph_counts = timed_e2e(use_graphs)
+    e2e_plain = timed_e2e(False)[0] if (e2e_direct and use_graphs) else None
 
     # roofline of the dominant stage, the candidate passes: algorithmic bytes per batch = the corpus
     # rows the passes read (docs x dim x element bytes, +4 B scale for E4M3; a learned form's
@@ -670,7 +689,7 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
                 "peak_note": "measured BF16 GEMM" + ("" if method == "bf16" else " x nominal dense ratio")},
             "bound_frac": (max(alg_bytes / (hbm * 1e9), 0.0 if tpeak is None else flops / (tpeak * 1e12)) / t_s)}
     out = {"value": value, "t_max_ms": t_max, "e2e": e2e, "batch": B, "roofline": roof, "clocks": clocks,
-           "launches": launches,
+           "launches": launches, "e2e_graphs": graph_counts if use_graphs else None,
            "stages_ms": dict(zip(["filter", "sample", "candidates", "select", "total"],
                                  [round(float(x), 4) for x in np.mean(np.array(stage_ms), axis=0)])),
            "form": form_name(method, learned) + _kmode_note(kmode),
@@ -682,6 +701,8 @@ def measure_form(args, ctx, method, learned=False, kmode=None, docs=None, dim=12
                         "overlap another's candidate pass (value, e2e); stages_ms and the roofline come from a "
                         "run of the same batches with the searchers on one stream, where stages do not "
                         "overlap"}
+    if e2e_plain is not None:
+        out["e2e_direct"] = e2e_plain  # the same leg with every batch launched directly
     for o in others:
         o.close()
     for f in filters:
@@ -780,19 +801,26 @@ def data_filters(mix, n, seed, pool_factor=24):
                              pool_factor=pool_factor)
 
 
-def measure_serving(args, ctx, method, rates, model=None, margin=0.0):
+def measure_serving(args, ctx, method, rates, model=None, margin=0.0, graphs=True):
     """p50/p99 latency of single queries through the serving loop (continuous batching) at open-loop
     Poisson arrival rates. Requests mix the workload's filters (selectivity log-uniform in
-    [1e-4, 1]) with per-request K log-uniform in [1, 1000]."""
+    [1e-4, 1]) with per-request K log-uniform in [1, 1000]. graphs: the slots replay each batch
+    shape's captured CUDA graph."""
     import hybridsearchsystem_b200 as hss
     srv = hss.Server(ctx["table"], slots=args.serve_slots, max_batch=args.batch, max_wait_us=args.serve_wait_us,
-                     method=METHODS[method], candidate_cap=args.cand_cap)
+                     method=METHODS[method], candidate_cap=args.cand_cap, graphs=graphs)
     if model is not None:
         srv.set_threshold_model(model, margin)
     srv_slots = srv.stats()["slots"]  # admitted within the device-memory budget
     q, ex = ctx["queries"], ctx["exprs"]
     kk = np.exp(np.random.default_rng(77).uniform(0.0, np.log(1000.0), len(q))).astype(np.uint32) + 1
     kk = np.minimum(kk, 1000)
+    # warm-up at the highest and a low rate (the batch shapes of high and low load captured, with
+    # graphs), not timed
+    for i, (rate, n) in enumerate(((max(rates), 20000), (2000.0, 2000))):
+        idx = (np.arange(n) + 7919 * (i + 1)) % len(q)
+        srv.run_poisson(q[idx], [ex[i] for i in idx], kk[idx], rate, seed=i + 1)
+    warm = srv.stats()
     out = []
     for rate in rates:
         n = int(min(args.serve_requests, max(2000, rate * 0.5)))
@@ -802,15 +830,27 @@ def measure_serving(args, ctx, method, rates, model=None, margin=0.0):
         st = srv.stats()
         out.append({"offered_qps": round(offered), "completed_qps": round(n / wall), "p50_ms": round(st["p50_ms"], 3),
                     "p99_ms": round(st["p99_ms"], 3), "mean_batch": round(st["mean_batch"], 1)})
+    st = srv.stats()
     srv.close()
-    return {"form": form_name(method, model is not None), "slots": srv_slots,
-            "max_wait_us": args.serve_wait_us, "topk": "log-uniform in [1, 1000] per request", "rates": out}
+    graph = None
+    if graphs:
+        graph = {"captures_in_warmup": warm["graph_captures"],
+                 "captures_in_sweep": st["graph_captures"] - warm["graph_captures"],
+                 "replays_in_sweep": st["graph_replays"] - warm["graph_replays"],
+                 "capture_ms_per_shape": round(st["graph_capture_ms"] / max(1, st["graph_captures"]), 3)}
+    return {"form": form_name(method, model is not None), "slots": srv_slots, "graphs": graph,
+            "max_wait_us": args.serve_wait_us, "topk": "log-uniform in [1, 1000] per request",
+            "warmup": "20000 requests at the highest rate, 2000 at 2000 QPS (not timed)", "rates": out}
 
 
 def summary(f, steps):
     d = {"value": f["value"], "e2e_qps": f["e2e"], "ms_per_step": f["t_max_ms"] / steps,
          "stages_ms": f["stages_ms"], "roofline_frac": f["roofline"]["frac"], "form": f["form"],
          "batch": f["batch"], "l2": f["l2"], "clocks": {k: f["clocks"][k] for k in ("sm_mhz", "reasons", "samples")}}
+    if f.get("e2e_graphs"):
+        d["e2e_graphs"] = f["e2e_graphs"]
+    if "e2e_direct" in f:
+        d["e2e_direct_qps"] = f["e2e_direct"]
     if "learned_report" in f:
         d["learned_report"] = f["learned_report"]
     if "parity" in f:
@@ -981,7 +1021,7 @@ def run_ours(args):
         if batch and batch != args.batch:
             a = copy.copy(args)
             a.batch = batch
-        f = measure_form(a, ctx, method, learned=learned, kmode=kmode)
+        f = measure_form(a, ctx, method, learned=learned, kmode=kmode, e2e_direct=key == "chosen")
         if truth is not None and kmode is None:
             f["parity"], last = parity_of_form(f["searcher"], dev, a.batch, pq, pe, truth)
             if key == "chosen":
@@ -1021,12 +1061,15 @@ def run_ours(args):
     if solo and args.serve:
         rates = [float(r) for r in args.serve_rates.split(",")]
         serving = {"chosen": measure_serving(args, ctx, args.method, rates, chosen.get("model"),
-                                             chosen.get("margin", 0.0))}
+                                             chosen.get("margin", 0.0), graphs=args.graphs)}
+        if args.graphs:  # the same sweep with every batch launched directly
+            serving["chosen_direct"] = measure_serving(args, ctx, args.method, rates, chosen.get("model"),
+                                                       chosen.get("margin", 0.0), graphs=False)
         if "chosen_learned" in forms:
             serving["chosen_learned"] = measure_serving(args, ctx, args.method, rates, forms["chosen_learned"]["model"],
-                                                        forms["chosen_learned"]["margin"])
+                                                        forms["chosen_learned"]["margin"], graphs=args.graphs)
         if args.plain:
-            serving["plain_fp32"] = measure_serving(args, ctx, "tf32", rates)
+            serving["plain_fp32"] = measure_serving(args, ctx, "tf32", rates, graphs=args.graphs)
 
     rec = {"metric": METRIC, "value": chosen["value"], "unit": "QPS", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": chosen["t_max_ms"] / args.steps, "higher_is_better": True,
@@ -1037,8 +1080,10 @@ def run_ours(args):
            "e2e": {"value": chosen["e2e"], "unit": "QPS", "h2d_bytes_per_step": B * 128 * 4,
                    "d2h_bytes_per_step": B * K * (4 + 8) + B * 4,
                    "path": "hss_filters_compile (next batch, compile thread) + hss_searcher_search_device_async / "
-                           "hss_searcher_finish per batch (two searchers alternating, each on its own stream), "
-                           "pinned host queries in, results out on a copy stream"},
+                           f"hss_searcher_finish per batch ({max(2, args.searchers)} searchers taking batches in "
+                           "turn, each on its own stream"
+                           + (", each batch's first attempt replayed from its shape's captured CUDA graph"
+                              if args.graphs else "") + "), pinned host queries in, results out on a copy stream"},
            "roofline": chosen["roofline"], "clocks": chosen["clocks"], "gpu_launches": chosen["launches"],
            "stages_ms": chosen["stages_ms"], "forms": {k: summary(v, args.steps) for k, v in forms.items()}}
     if "plain_fp32" in forms:

@@ -66,13 +66,14 @@ class SearcherConfig(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_uint32), ("maxBatch", ctypes.c_uint32), ("maxWaitUs", ctypes.c_uint32),
                 ("method", ctypes.c_int32), ("memoryBudget", ctypes.c_uint64), ("candidateCap", ctypes.c_uint32),
-                ("sampleDocs", ctypes.c_uint32)]
+                ("sampleDocs", ctypes.c_uint32), ("noGraphs", ctypes.c_uint32)]
 
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("slots", ctypes.c_uint32),
                 ("meanBatch", ctypes.c_double), ("p50Ms", ctypes.c_double), ("p99Ms", ctypes.c_double),
-                ("maxMs", ctypes.c_double)]
+                ("maxMs", ctypes.c_double), ("graphCaptures", ctypes.c_uint64), ("graphReplays", ctypes.c_uint64),
+                ("graphCaptureMs", ctypes.c_double)]
 
 
 # (name, restype, argtypes) for every symbol include/hss.h declares.
@@ -127,6 +128,8 @@ SIGNATURES = [
     ("hss_searcher_set_pipeline_test", ctypes.c_int, [vp, ctypes.c_uint32, ctypes.c_uint64]),
     ("hss_searcher_set_timing", ctypes.c_int, [vp, ctypes.c_int32]),
     ("hss_searcher_last_times", ctypes.c_int, [vp, vp, c_u32p, c_u32p]),
+    ("hss_searcher_set_graphs", ctypes.c_int, [vp, ctypes.c_int32]),
+    ("hss_searcher_graph_stats", ctypes.c_int, [vp, vp, vp, vp, c_i32p]),
     ("hss_hash64", ctypes.c_uint64, [ctypes.c_char_p, ctypes.c_uint32]),
     ("hss_posting_serialize", ctypes.c_int64,
      [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, vp, ctypes.c_uint64]),

@@ -312,6 +312,17 @@ class FullRecallSearcher:
     def set_timing(self, on=True):
         check(_lib.load().hss_searcher_set_timing(self._h, int(on)))
 
+    def set_graphs(self, on=True):
+        """CUDA-graph replay per batch shape (hss_searcher_set_graphs): query and output buffers of
+        maxBatch rows."""
+        check(_lib.load().hss_searcher_set_graphs(self._h, int(on)))
+
+    def graph_stats(self):
+        c, r, ms, f = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double(), ctypes.c_int32()
+        check(_lib.load().hss_searcher_graph_stats(self._h, ctypes.byref(c), ctypes.byref(r), ctypes.byref(ms),
+                                                   ctypes.byref(f)))
+        return {"captures": c.value, "replays": r.value, "failed": bool(f.value), "capture_ms": ms.value}
+
     def last_times(self):
         ms = np.zeros(5, np.float32)
         r, l = ctypes.c_uint32(), ctypes.c_uint32()
@@ -324,8 +335,9 @@ class Server:
     """The serving loop (continuous batching over one resident table; include/hss.h, hss_server_*)."""
 
     def __init__(self, table, slots=2, max_batch=256, max_wait_us=200, method=0, memory_budget=0, candidate_cap=0,
-                 sample_docs=0):
-        cfg = _lib.ServerConfig(slots, max_batch, max_wait_us, method, memory_budget, candidate_cap, sample_docs)
+                 sample_docs=0, graphs=True):
+        cfg = _lib.ServerConfig(slots, max_batch, max_wait_us, method, memory_budget, candidate_cap, sample_docs,
+                                0 if graphs else 1)
         h = ctypes.c_void_p()
         check(_lib.load().hss_server_create(table._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -367,7 +379,8 @@ class Server:
         st = _lib.ServerStats()
         check(_lib.load().hss_server_get_stats(self._h, ctypes.byref(st)))
         return {"completed": st.completed, "batches": st.batches, "slots": st.slots, "mean_batch": st.meanBatch,
-                "p50_ms": st.p50Ms, "p99_ms": st.p99Ms, "max_ms": st.maxMs}
+                "p50_ms": st.p50Ms, "p99_ms": st.p99Ms, "max_ms": st.maxMs, "graph_captures": st.graphCaptures,
+                "graph_replays": st.graphReplays, "graph_capture_ms": st.graphCaptureMs}
 
     def reset_stats(self):
         check(_lib.load().hss_server_reset_stats(self._h))

@@ -579,6 +579,22 @@ int hss_searcher_set_timing(hss_searcher* s, int32_t on) {
     return HSS_OK;
 }
 
+int hss_searcher_set_graphs(hss_searcher* s, int32_t on) {
+    if (!s) return SetError(HSS_ERR_INVALID, "null searcher");
+    s->s->SetGraphs(on != 0);
+    return HSS_OK;
+}
+
+int hss_searcher_graph_stats(const hss_searcher* s, uint64_t* captures, uint64_t* replays, double* captureMs,
+                             int32_t* failed) {
+    if (!s) return SetError(HSS_ERR_INVALID, "null searcher");
+    if (captures) *captures = s->s->GraphCaptures();
+    if (replays) *replays = s->s->GraphReplays();
+    if (captureMs) *captureMs = s->s->GraphCaptureMs();
+    if (failed) *failed = s->s->GraphFailure().empty() ? 0 : 1;
+    return HSS_OK;
+}
+
 int hss_searcher_last_times(const hss_searcher* s, float* ms5, uint32_t* retries, uint32_t* launches) {
     if (!s) return SetError(HSS_ERR_INVALID, "null searcher");
     const hss::StageTimes& t = s->s->LastTimes();
@@ -715,6 +731,7 @@ int hss_server_create(hss_table* table, const hss_server_config* cfg, hss_server
         c.searcher.method = static_cast<hss::ScoreMethod>(cfg->method);
         if (cfg->candidateCap) c.searcher.candidateCap = cfg->candidateCap;
         if (cfg->sampleDocs) c.searcher.sampleDocs = cfg->sampleDocs;
+        c.graphs = cfg->noGraphs == 0;
     }
     auto loop = std::make_unique<hss::ServingLoop>(table->t, c);
     if (!loop->Ok()) return SetError(HSS_ERR_CUDA, loop->Error());
@@ -752,6 +769,9 @@ int hss_server_get_stats(const hss_server* s, hss_server_stats* out) {
     out->p50Ms = st.p50Ms;
     out->p99Ms = st.p99Ms;
     out->maxMs = st.maxMs;
+    out->graphCaptures = st.graphCaptures;
+    out->graphReplays = st.graphReplays;
+    out->graphCaptureMs = st.graphCaptureMs;
     return HSS_OK;
 }
 

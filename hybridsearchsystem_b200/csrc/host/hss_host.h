@@ -502,6 +502,31 @@ class FullRecallSearcher {
         m_testHold = holdLoad;
         m_testBudget = waitBudget;
     }
+    // CUDA-graph replay of a batch's first attempt (filter, bounds, doc sample, model, both candidate
+    // passes, select and the status copies). The launches of one batch shape are captured from the
+    // stream once and replayed for every later batch of that shape, the graph copying in each
+    // batch's own filter programs. A shape is: the rows, rounded up to 1, 2, 4, 8, 16 or a multiple
+    // of 16 (at most maxBatch); the largest K, rounded up to a power of two (every K that plans
+    // like K = 1 -- the same doc sample and select variant -- counting as one); the largest operand
+    // count, rounded up to a power of two; the model; the query and output buffers and the output
+    // stride. Rows past nq run as match-nothing queries with K = 1, so with graphs on, dQueries and
+    // the outputs must hold maxBatch rows. Re-runs are launched directly. Off by default; batches
+    // with timing on, Features and the pipeline test launch directly. At most kGraphCacheSize
+    // shapes are kept (least recently used dropped).
+    void SetGraphs(bool on);
+    uint64_t GraphCaptures() const { return m_graphCaptures; }
+    uint64_t GraphReplays() const { return m_graphReplays; }
+    double GraphCaptureMs() const { return m_graphCaptureMs; }  // host time in captures and instantiation
+    // Why a capture failed (graphs then stay off for this searcher); empty when none did.
+    const std::string& GraphFailure() const { return m_graphFailure; }
+    static constexpr size_t kGraphCacheSize = 128;
+    // The rows a batch runs with under graph replay; K and operand counts rounded up to powers of two.
+    static uint32_t GraphRows(uint32_t nq, uint32_t maxBatch);
+    static uint32_t GraphTopK(uint32_t maxK);
+    static uint32_t GraphOperands(uint32_t maxOpnd);
+    // The K a batch's launch plan is made for under graph replay.
+    uint32_t PlanTopK(uint32_t maxK) const;
+
     const StageTimes& LastTimes() const { return m_times; }
     void SetTiming(bool on) { m_timing = on; }
     const SearcherConfig& Config() const { return m_cfg; }
@@ -544,8 +569,46 @@ class FullRecallSearcher {
               uint32_t segCap, uint64_t begin, uint64_t step, uint32_t skip, uint64_t countTiles, const uint32_t* dList,
               uint32_t rows, bool simt);
     uint64_t Sample(const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly = false, float* stats = nullptr);
-    int StageAndFilter(uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks, uint64_t* dBits,
-                       uint64_t bitsStride, uint32_t* maxKOut, cudaStream_t stream);
+    // A batch's small inputs in the pinned staging buffer: per-query program and operand offsets, K,
+    // the programs and operands; rows [nq, rows) as match-nothing queries with K = padK.
+    struct BatchInputs {
+        uint32_t maxK = 0, maxOpnd = 0, np = 0, no = 0;
+    };
+    BatchInputs PrepareInputs(uint32_t nq, uint32_t rows, const FilterExpr* const* exprs, const uint32_t* topks,
+                              uint32_t padK);
+    // Their copy to the device and the filter launch over `rows` queries.
+    int EnqueueFilter(uint32_t rows, const BatchInputs& in, uint64_t* dBits, uint64_t bitsStride, cudaStream_t stream);
+    // The first attempt of the batch in m_b over `rows` queries (directly or under capture). Returns
+    // 1 when the batch ended early (Features), else 0.
+    int EnqueueAttempt(uint32_t rows, const BatchInputs& in, float* dOutScores, int64_t* dOutIds,
+                       uint32_t* dOutCounts, uint32_t outStride);
+    struct GraphKey {
+        uint32_t rows = 0, maxK = 0, maxOpnd = 0, outStride = 0;
+        const void* model = nullptr;
+        float scale = 0, shift = 0;
+        const float* dQueries = nullptr;
+        const void* dOutScores = nullptr;
+        const void* dOutIds = nullptr;
+        const void* dOutCounts = nullptr;
+        bool operator==(const GraphKey& o) const {
+            return rows == o.rows && maxK == o.maxK && maxOpnd == o.maxOpnd && outStride == o.outStride &&
+                   model == o.model && scale == o.scale && shift == o.shift && dQueries == o.dQueries &&
+                   dOutScores == o.dOutScores && dOutIds == o.dOutIds && dOutCounts == o.dOutCounts;
+        }
+    };
+    struct GraphEntry {
+        GraphKey key;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphNode_t progCopy = nullptr, opndCopy = nullptr;  // the batch's programs and operands
+        Batch batch;  // the launch plan the capture made (segments, select parameters, counts)
+        uint64_t used = 0;
+    };
+    // Replays (capturing first when new) the first attempt of a batch shape; 0 or a negative status.
+    int EnqueueGraph(const GraphKey& key, uint32_t rows, const BatchInputs& in, float* dOutScores, int64_t* dOutIds,
+                     uint32_t* dOutCounts, uint32_t outStride);
+    void DropGraphs();
+    uint64_t SampleWant(uint32_t maxK) const;
 
     int32_t m_deviceId;
     std::shared_ptr<DataTable> m_table;
@@ -604,6 +667,11 @@ class FullRecallSearcher {
     std::vector<uint8_t> m_lastMiss;
     uint32_t m_testHold = 0;
     long long m_testBudget = 0;
+    bool m_graphs = false;
+    std::vector<GraphEntry> m_graphCache;
+    uint64_t m_graphCaptures = 0, m_graphReplays = 0, m_graphClock = 0;
+    double m_graphCaptureMs = 0;
+    std::string m_graphFailure;
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -622,12 +690,17 @@ struct ServingConfig {
     uint32_t maxWaitUs = 200;
     uint64_t memoryBudget = 0;  // bytes for the slots' arenas; 0 = half of the free device memory
     SearcherConfig searcher;    // maxBatch is taken from above
+    // Replay each batch shape's captured CUDA graph (FullRecallSearcher::SetGraphs); the output
+    // stride of a batch is then its largest K rounded up to a power of two.
+    bool graphs = true;
 };
 
 struct ServingStats {
     uint64_t completed = 0, batches = 0;
     uint32_t slots = 0;
     double meanBatch = 0, p50Ms = 0, p99Ms = 0, maxMs = 0;
+    uint64_t graphCaptures = 0, graphReplays = 0;  // over all slots
+    double graphCaptureMs = 0;                     // host time the slots spent capturing
 };
 
 class ServingLoop {
@@ -679,6 +752,8 @@ class ServingLoop {
         int64_t *hId = nullptr, *dId = nullptr;
         uint32_t *hCnt = nullptr, *dCnt = nullptr;
         uint64_t modelGen = 0;
+        uint64_t captures = 0, replays = 0;  // the searcher's graph counters after its last batch
+        double captureMs = 0;
         std::thread worker;
     };
     void Worker(Slot* slot);

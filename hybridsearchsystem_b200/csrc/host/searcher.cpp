@@ -11,6 +11,7 @@
 // A query whose candidate list overflowed gets a higher (still safe) threshold from step 5 and is
 // re-run through steps 4-5 alone.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -178,6 +179,7 @@ FullRecallSearcher::~FullRecallSearcher() {
     for (auto& e : m_ev)
         if (e) cudaEventDestroy(e);
     if (m_evStatus) cudaEventDestroy(m_evStatus);
+    DropGraphs();
 }
 
 bool FullRecallSearcher::Allocate(void* dArena, size_t arenaBytes) {
@@ -283,58 +285,77 @@ void FullRecallSearcher::ClearQueries() {
     m_topKs.clear();
 }
 
-int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exprs, const uint32_t* topks,
-                                       uint64_t* dBits, uint64_t bitsStride, uint32_t* maxKOut, cudaStream_t stream) {
+FullRecallSearcher::BatchInputs FullRecallSearcher::PrepareInputs(uint32_t nq, uint32_t rows,
+                                                                  const FilterExpr* const* exprs,
+                                                                  const uint32_t* topks, uint32_t padK) {
     const StageLayout SL = MakeLayout(m_cfg.maxBatch);
     uint8_t* H = m_hStage;
-    uint8_t* D = m_dStage;
     auto* progOff = reinterpret_cast<uint32_t*>(H + SL.progOff);
     auto* opndOff = reinterpret_cast<uint32_t*>(H + SL.opndOff);
     auto* topk = reinterpret_cast<uint32_t*>(H + SL.topk);
     auto* prog = reinterpret_cast<uint32_t*>(H + SL.prog);
     auto* opnd = reinterpret_cast<uint32_t*>(H + SL.opnd);
-    uint32_t np = 0, no = 0, maxOpnd = 0, maxK = 0;
-    for (uint32_t q = 0; q < nq; ++q) {
+    BatchInputs in;
+    uint32_t np = 0, no = 0;
+    // match-nothing: [AND, 1, 0] over the all-zero posting row
+    auto matchNothing = [&] {
+        prog[np++] = AND;
+        prog[np++] = 1;
+        prog[np++] = 0;
+        opnd[no++] = m_table->PostingRows() - 1;
+        in.maxOpnd = std::max(in.maxOpnd, 1u);
+    };
+    for (uint32_t q = 0; q < rows; ++q) {
         progOff[q] = np;
         opndOff[q] = no;
+        if (q >= nq) {
+            topk[q] = padK;
+            in.maxK = std::max(in.maxK, padK);
+            matchNothing();
+            continue;
+        }
         topk[q] = topks ? topks[q] : 0u;
-        maxK = std::max(maxK, topk[q]);
+        in.maxK = std::max(in.maxK, topk[q]);
         const FilterExpr* e = exprs[q];
         if (e == nullptr || e->emptyTree) continue;  // empty program: match all
         const uint32_t pl = static_cast<uint32_t>(e->postExpr.size());
         const uint32_t ol = static_cast<uint32_t>(e->postingRows.size());
         if (pl > static_cast<uint32_t>(kMaxProgram) || ol > static_cast<uint32_t>(kMaxOperands) || pl == 0) {
-            // Over the kernel's limits: reported in the status and run as match-nothing
-            // ([AND, 1, 0] over the all-zero posting row).
+            // Over the kernel's limits: reported in the status and run as match-nothing.
             m_lastStatus[q] |= kStatusBadProgram;
-            prog[np++] = AND;
-            prog[np++] = 1;
-            prog[np++] = 0;
-            opnd[no++] = m_table->PostingRows() - 1;
-            maxOpnd = std::max(maxOpnd, 1u);
+            matchNothing();
             continue;
         }
         std::memcpy(prog + np, e->postExpr.data(), pl * 4ull);
         std::memcpy(opnd + no, e->postingRows.data(), ol * 4ull);
         np += pl;
         no += ol;
-        maxOpnd = std::max(maxOpnd, ol);
+        in.maxOpnd = std::max(in.maxOpnd, ol);
     }
-    progOff[nq] = np;
-    opndOff[nq] = no;
+    progOff[rows] = np;
+    opndOff[rows] = no;
     for (uint32_t q = 0; q < nq; ++q)
         if (topk[q] > static_cast<uint32_t>(kMaxTopK)) m_lastStatus[q] |= kStatusTopKTooLarge;
-    *maxKOut = maxK;
+    in.np = np;
+    in.no = no;
+    return in;
+}
 
+int FullRecallSearcher::EnqueueFilter(uint32_t rows, const BatchInputs& in, uint64_t* dBits, uint64_t bitsStride,
+                                      cudaStream_t stream) {
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    uint8_t* H = m_hStage;
+    uint8_t* D = m_dStage;
     const DataTable& T = *m_table;
     cudaError_t ce = cudaSuccess;
     auto ck = [&](cudaError_t e) {
         if (ce == cudaSuccess && e != cudaSuccess) ce = e;
     };
-    // one H2D for the small per-batch inputs (offsets, topk, programs, operands)
+    // the small per-batch inputs: offsets and K, then the programs and operands (at least one entry
+    // each, so that a replayed graph can resize both copies)
     ck(cudaMemcpyAsync(D, H, SL.counters, cudaMemcpyHostToDevice, stream));
-    ck(cudaMemcpyAsync(D + SL.prog, H + SL.prog, np * 4ull, cudaMemcpyHostToDevice, stream));
-    ck(cudaMemcpyAsync(D + SL.opnd, H + SL.opnd, no * 4ull, cudaMemcpyHostToDevice, stream));
+    ck(cudaMemcpyAsync(D + SL.prog, H + SL.prog, std::max(in.np, 1u) * 4ull, cudaMemcpyHostToDevice, stream));
+    ck(cudaMemcpyAsync(D + SL.opnd, H + SL.opnd, std::max(in.no, 1u) * 4ull, cudaMemcpyHostToDevice, stream));
     ck(cudaMemsetAsync(D + SL.counters, 0, SL.prog - SL.counters, stream));
 
     if (m_cfg.densePostings && T.DeviceDensePostings()) {
@@ -350,10 +371,10 @@ int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exp
         F.out_stride = bitsStride;
         F.pass_count = reinterpret_cast<uint32_t*>(D + SL.passCount);
         F.status = reinterpret_cast<int32_t*>(D + SL.status);
-        F.nq = nq;
+        F.nq = rows;
         F.seg_num = T.GetSegmentNum();
         F.doc_num = T.GetDocNum();
-        F.max_opnd = maxOpnd;
+        F.max_opnd = in.maxOpnd;
         F.sm_count = m_numSms;
         ck(launch_filter_dense(F, stream));
         return ce == cudaSuccess ? 0 : static_cast<int>(ce);
@@ -370,11 +391,11 @@ int FullRecallSearcher::StageAndFilter(uint32_t nq, const FilterExpr* const* exp
     F.out_stride = bitsStride;
     F.pass_count = reinterpret_cast<uint32_t*>(D + SL.passCount);
     F.status = reinterpret_cast<int32_t*>(D + SL.status);
-    F.nq = nq;
+    F.nq = rows;
     F.seg_num = T.GetSegmentNum();
     F.docs_per_seg = T.GetDocNumPerSegment();
     F.doc_num = T.GetDocNum();
-    F.max_opnd = maxOpnd;
+    F.max_opnd = in.maxOpnd;
     ck(launch_filter_batch(F, stream));
     return ce == cudaSuccess ? 0 : static_cast<int>(ce);
 }
@@ -389,8 +410,8 @@ int FullRecallSearcher::FilterDevice(uint32_t nq, const FilterExpr* const* exprs
         return -1;
     }
     if (cudaSetDevice(m_deviceId) != cudaSuccess) return -2;
-    uint32_t maxK = 0;
-    if (StageAndFilter(nq, exprs, nullptr, dOutBits, outStrideWords, &maxK, stream) != 0) return -2;
+    const BatchInputs in = PrepareInputs(nq, nq, exprs, nullptr, 0);
+    if (EnqueueFilter(nq, in, dOutBits, outStrideWords, stream) != 0) return -2;
     const StageLayout SL = MakeLayout(m_cfg.maxBatch);
     auto* hStatus = reinterpret_cast<int32_t*>(m_hStage + SL.status);
     cudaError_t e = cudaSuccess;
@@ -423,6 +444,7 @@ int FullRecallSearcher::SetThresholdModel(std::shared_ptr<ThresholdModel> model,
     }
     m_model = std::move(model);
     m_margin = margin;
+    DropGraphs();  // the captured launches hold the model's parameters and the margin
     return 0;
 }
 
@@ -659,13 +681,192 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
         }
     }
     if (cudaSetDevice(m_deviceId) != cudaSuccess) return -2;
-    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
-    uint8_t* H = m_hStage;
-    uint8_t* D = m_dStage;
     m_b = Batch{};
     m_b.dQueries = dQueries;
     m_b.nq = nq;
     m_b.stream = stream;
+    if (!m_evStatus && cudaEventCreateWithFlags(&m_evStatus, cudaEventDisableTiming) != cudaSuccess) return -2;
+    const bool graph = m_graphs && !m_timing && m_featuresOut == nullptr && m_testHold == 0;
+    const uint32_t rows = graph ? GraphRows(nq, m_cfg.maxBatch) : nq;
+    BatchInputs in = PrepareInputs(nq, rows, exprs, topks, std::min(1u, outStride));
+    int rc;
+    if (graph) {
+        in.maxK = PlanTopK(in.maxK);
+        in.maxOpnd = GraphOperands(in.maxOpnd);
+        GraphKey key;
+        key.rows = rows;
+        key.maxK = in.maxK;
+        key.maxOpnd = in.maxOpnd;
+        key.outStride = outStride;
+        key.model = m_model.get();
+        key.scale = m_model ? m_model->scale : 0.0f;
+        key.shift = m_model ? m_model->shift : 0.0f;
+        key.dQueries = dQueries;
+        key.dOutScores = dOutScores;
+        key.dOutIds = dOutIds;
+        key.dOutCounts = dOutCounts;
+        rc = EnqueueGraph(key, rows, in, dOutScores, dOutIds, dOutCounts, outStride);
+    } else {
+        rc = EnqueueAttempt(rows, in, dOutScores, dOutIds, dOutCounts, outStride);
+        if (rc == 1) {  // Features: done, nothing pending
+            if (m_b.ce == cudaSuccess) return 0;
+            m_err = cudaGetErrorString(m_b.ce);
+            return -2;
+        }
+        rc = 0;
+    }
+    if (rc == 0) Ck(cudaEventRecord(m_evStatus, stream));
+    m_lastSegs.assign(nq, {m_b.se.segs, m_b.se.seg_cap});
+    if (rc != 0 || m_b.ce != cudaSuccess) {
+        if (m_err.empty() || m_b.ce != cudaSuccess) m_err = cudaGetErrorString(m_b.ce);
+        return -2;
+    }
+    m_b.pending = true;
+    return 0;
+}
+
+uint32_t FullRecallSearcher::GraphRows(uint32_t nq, uint32_t maxBatch) {
+    uint32_t r = 1;
+    if (nq <= 16) {
+        while (r < nq) r <<= 1;
+    } else {
+        r = (nq + 15) / 16 * 16;
+    }
+    return std::max(nq, std::min(r, maxBatch));
+}
+
+uint32_t FullRecallSearcher::GraphTopK(uint32_t maxK) {
+    uint32_t k = 1;
+    while (k < maxK && k < static_cast<uint32_t>(kMaxTopK)) k <<= 1;
+    return maxK == 0 ? 0u : std::max(maxK, std::min(k, static_cast<uint32_t>(kMaxTopK)));
+}
+
+uint64_t FullRecallSearcher::SampleWant(uint32_t maxK) const {
+    // the doc sample whose threshold keeps the full pass within the list capacity
+    return std::max<uint64_t>(m_cfg.sampleDocs, (4ull * std::max<uint32_t>(maxK, 1u) * m_table->GetDocNum() +
+                                                 m_cfg.candidateCap - 1) / m_cfg.candidateCap);
+}
+
+uint32_t FullRecallSearcher::PlanTopK(uint32_t maxK) const {
+    // A batch's K enters its launch plan through the doc sample's size (without a model) and the
+    // select variant (K > 256): every K up to `flat` plans as K = 1 does.
+    uint32_t flat = 1;
+    while (flat < 256 && (m_model || SampleWant(flat * 2) == SampleWant(1))) flat <<= 1;
+    return maxK == 0 ? 0u : std::max(GraphTopK(maxK), flat);
+}
+
+uint32_t FullRecallSearcher::GraphOperands(uint32_t maxOpnd) {
+    // powers of two: the filter kernel takes any bound at least the batch's largest operand count,
+    // and up to 8 (its shared-memory form) a power of two stays within 8
+    uint32_t o = 1;
+    while (o < maxOpnd) o <<= 1;
+    return maxOpnd == 0 ? 0u : o;
+}
+
+void FullRecallSearcher::SetGraphs(bool on) {
+    if (!on) DropGraphs();
+    m_graphs = on;
+}
+
+void FullRecallSearcher::DropGraphs() {
+    for (GraphEntry& g : m_graphCache) {
+        // an exec still running is released when it completes
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    m_graphCache.clear();
+}
+
+int FullRecallSearcher::EnqueueGraph(const GraphKey& key, uint32_t rows, const BatchInputs& in, float* dOutScores,
+                                     int64_t* dOutIds, uint32_t* dOutCounts, uint32_t outStride) {
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    cudaStream_t stream = m_b.stream;
+    GraphEntry* g = nullptr;
+    for (GraphEntry& e : m_graphCache)
+        if (e.key == key) g = &e;
+    if (g == nullptr) {
+        // capture this shape's launches (nothing runs while the stream captures)
+        GraphEntry e;
+        e.key = key;
+        const auto t0 = std::chrono::steady_clock::now();
+        cudaError_t ce = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (ce == cudaSuccess) {
+            (void)EnqueueAttempt(rows, in, dOutScores, dOutIds, dOutCounts, outStride);
+            ce = cudaStreamEndCapture(stream, &e.graph);
+        }
+        if (ce == cudaSuccess && m_b.ce == cudaSuccess)
+            ce = cudaGraphInstantiate(&e.exec, e.graph, 0);
+        // the two copies whose sizes follow the batch's programs
+        size_t n = 0;
+        if (ce == cudaSuccess && m_b.ce == cudaSuccess) ce = cudaGraphGetNodes(e.graph, nullptr, &n);
+        std::vector<cudaGraphNode_t> nodes(n);
+        if (ce == cudaSuccess && m_b.ce == cudaSuccess && n) ce = cudaGraphGetNodes(e.graph, nodes.data(), &n);
+        for (size_t i = 0; ce == cudaSuccess && i < n; ++i) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(nodes[i], &t) != cudaSuccess || t != cudaGraphNodeTypeMemcpy) continue;
+            cudaMemcpy3DParms p{};
+            if (cudaGraphMemcpyNodeGetParams(nodes[i], &p) != cudaSuccess) continue;
+            if (p.dstPtr.ptr == m_dStage + SL.prog) e.progCopy = nodes[i];
+            if (p.dstPtr.ptr == m_dStage + SL.opnd) e.opndCopy = nodes[i];
+        }
+        if (ce == cudaSuccess && m_b.ce == cudaSuccess && (!e.progCopy || !e.opndCopy)) ce = cudaErrorUnknown;
+        if (ce != cudaSuccess || m_b.ce != cudaSuccess) {
+            // nothing of the batch ran: graphs off for this searcher, the batch launched directly
+            if (e.exec) cudaGraphExecDestroy(e.exec);
+            if (e.graph) cudaGraphDestroy(e.graph);
+            m_graphFailure = cudaGetErrorString(ce != cudaSuccess ? ce : m_b.ce);
+            cudaGetLastError();
+            m_graphs = false;
+            const uint32_t nq = m_b.nq;
+            const float* dq = m_b.dQueries;
+            m_b = Batch{};
+            m_b.dQueries = dq;
+            m_b.nq = nq;
+            m_b.stream = stream;
+            return EnqueueAttempt(rows, in, dOutScores, dOutIds, dOutCounts, outStride) == 0 && m_b.ce == cudaSuccess
+                       ? 0
+                       : -2;
+        }
+        e.batch = m_b;
+        if (m_graphCache.size() >= kGraphCacheSize) {
+            auto lru = std::min_element(m_graphCache.begin(), m_graphCache.end(),
+                                        [](const GraphEntry& x, const GraphEntry& y) { return x.used < y.used; });
+            cudaGraphExecDestroy(lru->exec);
+            cudaGraphDestroy(lru->graph);
+            m_graphCache.erase(lru);
+        }
+        m_graphCache.push_back(e);
+        g = &m_graphCache.back();
+        ++m_graphCaptures;
+        m_graphCaptureMs += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    } else {
+        // the launch plan is the shape's: restore it around this batch's own rows and stream
+        const uint32_t nq = m_b.nq;
+        m_b = g->batch;
+        m_b.nq = nq;
+        m_b.stream = stream;
+        m_b.ce = cudaSuccess;
+        m_b.pending = false;
+        ++m_graphReplays;
+    }
+    g->used = ++m_graphClock;
+    uint8_t* H = m_hStage;
+    uint8_t* D = m_dStage;
+    Ck(cudaGraphExecMemcpyNodeSetParams1D(g->exec, g->progCopy, D + SL.prog, H + SL.prog,
+                                          std::max(in.np, 1u) * 4ull, cudaMemcpyHostToDevice));
+    Ck(cudaGraphExecMemcpyNodeSetParams1D(g->exec, g->opndCopy, D + SL.opnd, H + SL.opnd,
+                                          std::max(in.no, 1u) * 4ull, cudaMemcpyHostToDevice));
+    Ck(cudaGraphLaunch(g->exec, stream));
+    return m_b.ce == cudaSuccess ? 0 : -2;
+}
+
+int FullRecallSearcher::EnqueueAttempt(uint32_t nq, const BatchInputs& in, float* dOutScores, int64_t* dOutIds,
+                                       uint32_t* dOutCounts, uint32_t outStride) {
+    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
+    uint8_t* H = m_hStage;
+    uint8_t* D = m_dStage;
+    const float* dQueries = m_b.dQueries;
+    cudaStream_t stream = m_b.stream;
     auto* dTopk = reinterpret_cast<uint32_t*>(D + SL.topk);
     auto* dEpsMain = reinterpret_cast<float*>(D + SL.epsMain);
     auto* dTheta = reinterpret_cast<float*>(D + SL.theta);
@@ -675,8 +876,8 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
     const DataTable& T = *m_table;
     const uint64_t words = T.GetBitmapWords();
     if (m_timing) Ck(cudaEventRecord(m_ev[0], stream));
-    uint32_t maxK = 0;
-    if (StageAndFilter(nq, exprs, topks, m_dBits, words, &maxK, stream) != 0) Ck(cudaErrorUnknown);
+    const uint32_t maxK = in.maxK;
+    if (EnqueueFilter(nq, in, m_dBits, words, stream) != 0) Ck(cudaErrorUnknown);
     ++m_b.launches;
     Stage(nullptr, nq);
     ++m_b.launches;
@@ -687,9 +888,7 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
     // capacity; with one, the prediction sets the threshold and the sample only feeds the features
     // (which are made from the same sample size, with or without a model set).
     const bool learned = static_cast<bool>(m_model);
-    m_b.wantRerun = std::max<uint64_t>(
-        m_cfg.sampleDocs,
-        (4ull * std::max<uint32_t>(maxK, 1u) * T.GetDocNum() + m_cfg.candidateCap - 1) / m_cfg.candidateCap);
+    m_b.wantRerun = SampleWant(maxK);
     m_b.want = learned || m_featuresOut != nullptr ? m_cfg.sampleDocs : m_b.wantRerun;
     m_b.learned = learned;
     const bool wantStats = learned || m_featuresOut != nullptr;
@@ -701,11 +900,7 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
         Ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
                           m_featuresOut, stream));
         Ck(cudaStreamSynchronize(stream));
-        if (m_b.ce != cudaSuccess) {
-            m_err = cudaGetErrorString(m_b.ce);
-            return -2;
-        }
-        return 0;
+        return 1;
     }
     auto* dThetaPr = reinterpret_cast<float*>(D + SL.thetaPr);
     if (learned) {
@@ -789,7 +984,6 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
         Cand(dTheta, m_dCandScore, m_dCandLoc, dCandCount, C, 0, SE.seg_cap, 0, 1, 0, tilesM, nullptr, nq, false);
         ++m_b.launches;
     }
-    m_lastSegs.assign(nq, {SE.segs, SE.seg_cap});
     if (m_timing) Ck(cudaEventRecord(m_ev[3], stream));
 
     // 3. exact rescoring and the top K
@@ -797,16 +991,9 @@ int FullRecallSearcher::SearchEnqueue(const float* dQueries, uint32_t nq, const 
     ++m_b.launches;
     if (m_timing) Ck(cudaEventRecord(m_ev[4], stream));
     // the statuses that decide re-runs (and the tensor-core pass's error bits), on the host when
-    // m_evStatus completes
+    // m_evStatus (recorded by the caller) completes
     Ck(cudaMemcpyAsync(H + SL.status, dStatus, nq * 4ull, cudaMemcpyDeviceToHost, stream));
     if (m_tcFormat >= 0) Ck(cudaMemcpyAsync(H + SL.errWord, m_dError, 4, cudaMemcpyDeviceToHost, stream));
-    if (!m_evStatus) Ck(cudaEventCreateWithFlags(&m_evStatus, cudaEventDisableTiming));
-    Ck(cudaEventRecord(m_evStatus, stream));
-    if (m_b.ce != cudaSuccess) {
-        m_err = cudaGetErrorString(m_b.ce);
-        return -2;
-    }
-    m_b.pending = true;
     return 0;
 }
 

@@ -62,6 +62,12 @@ ServingLoop::ServingLoop(std::shared_ptr<DataTable> table, const ServingConfig& 
             m_slots.push_back(std::move(slot));
             return;
         }
+        // rows past a batch's own (graph replay pads a batch to its shape) read finite queries
+        if (!CudaOkS(cudaMemset(slot->dQ, 0, B * m_dim * 4), &m_err, "cudaMemset")) {
+            m_slots.push_back(std::move(slot));
+            return;
+        }
+        slot->searcher->SetGraphs(m_cfg.graphs);
         cudaMemGetInfo(&after, &total);
         if (i == 0) perSlot = before > after ? before - after : 1;
         m_slots.push_back(std::move(slot));
@@ -160,19 +166,22 @@ void ServingLoop::RunBatch(Slot* slot, std::vector<std::shared_ptr<Request>>& ba
         topks[i] = batch[i]->topK;
         stride = std::max(stride, std::min<uint32_t>(batch[i]->topK, kMaxTopK));
     }
+    // graph replay: device rows of kMaxTopK entries whatever the batch's K (one stride for every
+    // batch shape); the host takes the first `stride` entries of each row
+    const uint32_t dStride = m_cfg.graphs ? static_cast<uint32_t>(kMaxTopK) : stride;
     cudaError_t e = cudaMemcpyAsync(slot->dQ, slot->hQ, static_cast<size_t>(n) * m_dim * 4, cudaMemcpyHostToDevice,
                                     slot->stream);
     int rc = e == cudaSuccess ? slot->searcher->SearchDevice(slot->dQ, n, exprs.data(), topks.data(), slot->dSc,
-                                                             slot->dId, slot->dCnt, stride, slot->stream)
+                                                             slot->dId, slot->dCnt, dStride, slot->stream)
                               : -2;
     if (rc >= 0) {
         e = cudaMemcpyAsync(slot->hCnt, slot->dCnt, n * 4ull, cudaMemcpyDeviceToHost, slot->stream);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(slot->hSc, slot->dSc, static_cast<size_t>(n) * stride * 4, cudaMemcpyDeviceToHost,
-                                slot->stream);
+            e = cudaMemcpy2DAsync(slot->hSc, stride * 4ull, slot->dSc, dStride * 4ull, stride * 4ull, n,
+                                  cudaMemcpyDeviceToHost, slot->stream);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(slot->hId, slot->dId, static_cast<size_t>(n) * stride * 8, cudaMemcpyDeviceToHost,
-                                slot->stream);
+            e = cudaMemcpy2DAsync(slot->hId, stride * 8ull, slot->dId, dStride * 8ull, stride * 8ull, n,
+                                  cudaMemcpyDeviceToHost, slot->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(slot->stream);
         if (e != cudaSuccess) rc = -2;
     }
@@ -197,6 +206,9 @@ void ServingLoop::RunBatch(Slot* slot, std::vector<std::shared_ptr<Request>>& ba
         }
         ++m_batches;
         m_batched += n;
+        slot->captures = slot->searcher->GraphCaptures();
+        slot->replays = slot->searcher->GraphReplays();
+        slot->captureMs = slot->searcher->GraphCaptureMs();
     }
     m_cvDone.notify_all();
 }
@@ -237,6 +249,11 @@ ServingStats ServingLoop::Stats() const {
         s.p50Ms = pct(0.50);
         s.p99Ms = pct(0.99);
         s.maxMs = v.back();
+    }
+    for (const auto& slot : m_slots) {
+        s.graphCaptures += slot->captures;
+        s.graphReplays += slot->replays;
+        s.graphCaptureMs += slot->captureMs;
     }
     return s;
 }

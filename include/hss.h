@@ -300,6 +300,22 @@ int hss_searcher_set_timing(hss_searcher* s, int32_t on);
  * HSS_ERR_CUDA ("timed out waiting on its pipeline"), and the searcher stays usable. */
 int hss_searcher_set_pipeline_test(hss_searcher* s, uint32_t holdLoad, uint64_t waitBudgetCycles);
 int hss_searcher_last_times(const hss_searcher* s, float* ms5, uint32_t* retries, uint32_t* launches);
+/* CUDA-graph replay of each batch's first attempt (no counterpart in the reference, whose ACL
+ * launches are issued per call). A batch shape -- rows rounded up to 1, 2, 4, 8, 16 or a multiple of
+ * 16 (at most maxBatch), the largest K rounded up to a power of two (the K that plan alike as one),
+ * the filters' largest operand count rounded up to a power of two, the threshold model, the query
+ * and output pointers and outStride -- is captured
+ * from the stream at its first batch and replayed for every later one, the graph copying in each
+ * batch's filter programs; re-runs are launched directly. The rows past nq run as match-nothing
+ * queries with K = 1: with graphs on, dQueries and the outputs of hss_searcher_search_device must
+ * hold maxBatch rows, and the stream must not be the legacy default stream (it cannot be captured).
+ * Results are the same as without. Off by default. */
+int hss_searcher_set_graphs(hss_searcher* s, int32_t on);
+/* Shapes captured and batches replayed so far, the host milliseconds spent capturing and
+ * instantiating; *failed = 1 when a capture failed (graphs are then off for this searcher and its
+ * batches launch directly). Any pointer may be NULL. */
+int hss_searcher_graph_stats(const hss_searcher* s, uint64_t* captures, uint64_t* replays, double* captureMs,
+                             int32_t* failed);
 
 /* ---- learned threshold predictor ----
  * An MLP (feature row -> hidden -> hidden -> 1, GELU) that predicts a query's K-th filtered score,
@@ -376,11 +392,15 @@ typedef struct hss_server_config {
     uint64_t memoryBudget; /* bytes for the slots' arenas; 0 = half the free device memory */
     uint32_t candidateCap; /* as in hss_searcher_config; 0 = default */
     uint32_t sampleDocs;
+    uint32_t noGraphs;     /* 1: launch every batch directly (default 0: slots replay captured CUDA
+                              graphs per batch shape, hss_searcher_set_graphs) */
 } hss_server_config;
 typedef struct hss_server_stats {
     uint64_t completed, batches;
     uint32_t slots;
     double meanBatch, p50Ms, p99Ms, maxMs; /* latency from submission to results on the host */
+    uint64_t graphCaptures, graphReplays;  /* over all slots */
+    double graphCaptureMs;                 /* host time the slots spent capturing and instantiating */
 } hss_server_stats;
 
 int hss_server_create(hss_table* table, const hss_server_config* cfg, hss_server** out);

@@ -42,12 +42,13 @@ def _same(got, want, i):
     assert (sc.view(np.uint32) == ws[i][:c].view(np.uint32)).all(), i
 
 
+@pytest.mark.parametrize("graphs", [True, False], ids=["graphs", "direct"])
 @pytest.mark.parametrize("method", [0, 2], ids=["simt", "bf16"])
-def test_results_same_alone_and_in_the_mix(torch_cuda, method):
+def test_results_same_alone_and_in_the_mix(torch_cuda, method, graphs):
     mix, vec, bits, table = _world()
     q, exprs, topks = _requests(mix, 96, 130)
     want = oracle.topk(q, exprs, topks, vec, bits, threads=8)
-    srv = hss.Server(table, slots=3, max_batch=32, max_wait_us=2000, method=method)
+    srv = hss.Server(table, slots=3, max_batch=32, max_wait_us=2000, method=method, graphs=graphs)
     for i in range(len(q)):  # alone: one query on the GPU at a time
         _same(srv.wait(srv.submit(exprs[i], q[i], int(topks[i]))), want, i)
     assert srv.stats()["mean_batch"] == 1.0
@@ -68,6 +69,10 @@ def test_results_same_alone_and_in_the_mix(torch_cuda, method):
         _same(srv.wait(ids[i]), want, i)
     st = srv.stats()
     assert st["completed"] == len(q) and st["mean_batch"] > 1.0, st
+    if graphs:  # batch shapes captured once, replayed for later batches of the same shape
+        assert st["graph_captures"] > 0 and st["graph_replays"] > 0, st
+    else:
+        assert st["graph_captures"] == 0 and st["graph_replays"] == 0, st
     srv.close()
 
 
