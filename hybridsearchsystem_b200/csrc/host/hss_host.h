@@ -569,6 +569,7 @@ class FullRecallSearcher {
               uint32_t segCap, uint64_t begin, uint64_t step, uint32_t skip, uint64_t countTiles, const uint32_t* dList,
               uint32_t rows, bool simt);
     uint64_t Sample(const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly = false, float* stats = nullptr);
+    void SampleTiles(uint64_t want, uint32_t rows, bool simt, uint64_t* count, uint64_t* step) const;
     // A batch's small inputs in the pinned staging buffer: per-query program and operand offsets, K,
     // the programs and operands; rows [nq, rows) as match-nothing queries with K = padK.
     struct BatchInputs {

@@ -618,14 +618,20 @@ void FullRecallSearcher::Cand(const float* theta, float* score, uint32_t* loc, u
 
 // The doc sample: evenly spaced tiles, every filtered doc kept; its K-th best bounds the threshold.
 // Returns the sample's tile count.
+// Tiles (and their step) of a doc sample of `want` docs for `rows` queries.
+void FullRecallSearcher::SampleTiles(uint64_t want, uint32_t rows, bool simt, uint64_t* count, uint64_t* step) const {
+    const uint32_t unit = UnitOf(rows, simt);
+    const uint64_t tilesU = TilesOf(unit);
+    const uint64_t sampTiles = std::min<uint64_t>(tilesU, std::max<uint64_t>(1, (want + unit - 1) / unit));
+    *step = std::max<uint64_t>(1, tilesU / sampTiles);
+    *count = std::min<uint64_t>(sampTiles, (tilesU + *step - 1) / *step);
+}
+
 uint64_t FullRecallSearcher::Sample(const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly, float* stats) {
     const StageLayout SL = MakeLayout(m_cfg.maxBatch);
     uint8_t* D = m_dStage;
-    const uint32_t unit = UnitOf(rows, simt);
-    const uint64_t tilesU = TilesOf(unit);
-    const uint64_t sampTiles = std::min<uint64_t>(tilesU, std::max<uint64_t>(1, (m_b.want + unit - 1) / unit));
-    const uint64_t step = std::max<uint64_t>(1, tilesU / sampTiles);
-    const uint64_t count = std::min<uint64_t>(sampTiles, (tilesU + step - 1) / step);
+    uint64_t count = 0, step = 1;
+    SampleTiles(m_b.want, rows, simt, &count, &step);
     const uint32_t segs = SegsOf(rows, count, m_sampCap, simt);
     const uint32_t segCap = SegCapOf(rows, count, m_sampCap, segs, simt);
     auto* dSampCount = reinterpret_cast<uint32_t*>(D + SL.sampCount);
@@ -748,10 +754,11 @@ uint64_t FullRecallSearcher::SampleWant(uint32_t maxK) const {
 }
 
 uint32_t FullRecallSearcher::PlanTopK(uint32_t maxK) const {
-    // A batch's K enters its launch plan through the doc sample's size (without a model) and the
-    // select variant (K > 256): every K up to `flat` plans as K = 1 does.
+    // A batch's K enters its launch plan through the doc sample's size (without a model: the sample;
+    // with one: pass A's share) and the select variant (K > 256): every K up to `flat` plans as
+    // K = 1 does.
     uint32_t flat = 1;
-    while (flat < 256 && (m_model || SampleWant(flat * 2) == SampleWant(1))) flat <<= 1;
+    while (flat < 256 && SampleWant(flat * 2) == SampleWant(1)) flat <<= 1;
     return maxK == 0 ? 0u : std::max(GraphTopK(maxK), flat);
 }
 
@@ -923,7 +930,15 @@ int FullRecallSearcher::EnqueueAttempt(uint32_t nq, const BatchInputs& in, float
     // candidates form one segmented list.
     const uint32_t C = m_cfg.candidateCap;
     const uint64_t tilesM = TilesOf(UnitOf(nq, false));
-    uint32_t split = static_cast<uint32_t>(std::sqrt(static_cast<double>(tilesM) / static_cast<double>(sampCount)));
+    // Pass A's share as the sample that bounds the full pass would set it: with a model the sample
+    // stays small, but pass A's proven K-th best still raises the threshold of pass B as far as
+    // without one (a pass A of 1/8 of the corpus at K = 1000 and 10M docs rather than 1/17)
+    uint64_t splitSample = sampCount;
+    if (learned) {
+        uint64_t step = 1;
+        SampleTiles(m_b.wantRerun, nq, false, &splitSample, &step);
+    }
+    uint32_t split = static_cast<uint32_t>(std::sqrt(static_cast<double>(tilesM) / static_cast<double>(splitSample)));
     split = std::min<uint32_t>(split, 64);
     SelectLaunch& SE = m_b.se;
     SE.vec = T.DeviceVectors();
