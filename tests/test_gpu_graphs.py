@@ -107,3 +107,26 @@ def test_replay_with_a_threshold_model(torch_cuda):
             assert retries > 0  # threshold misses re-run after replays
     st = s.graph_stats()
     assert (st["captures"], st["replays"], st["failed"]) == (6, 6, False), st
+
+
+def test_default_stream_falls_back_to_direct_launches(torch_cuda):
+    # the legacy default stream cannot be captured: the searcher reports the failed capture, turns
+    # graphs off and launches the batch directly, with the same results
+    torch = torch_cuda
+    mix, vec, bits, table, bufs = _world(torch, 81)
+    s = hss.FullRecallSearcher(table, max_batch=B, method=2)
+    s.set_graphs(True)
+    d_q, sc, ids, cnt = bufs
+    nq, k = 20, 50
+    q = mix.queries(nq, seed=82)
+    ex = _filters(mix, nq, 83)
+    d_q[:nq].copy_(torch.from_numpy(q).to("cuda:0"))
+    torch.cuda.synchronize()
+    f = s.compile_filters(ex)
+    assert s.search_device(d_q.data_ptr(), nq, f, [k] * nq, sc.data_ptr(), ids.data_ptr(), cnt.data_ptr(), STRIDE,
+                           0) == 0
+    torch.cuda.synchronize()
+    want = oracle.topk(q, ex, [k] * nq, vec, bits, threads=8)
+    _check(sc.cpu().numpy(), ids.cpu().numpy(), cnt.cpu().numpy(), want, nq)
+    st = s.graph_stats()
+    assert (st["captures"], st["replays"], st["failed"]) == (0, 0, True), st
