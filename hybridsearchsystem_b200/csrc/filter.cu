@@ -484,7 +484,7 @@ constexpr int kWideW = 8;
 constexpr uint32_t kWideTW = kWideT * kWideW;  // words per tile
 constexpr uint32_t kWideGS = 2 * kWideT;       // words between a thread's word pairs
 constexpr uint32_t kWideMaxTilesPerCta = 4;    // word tiles per CTA at most (consecutive, across segments)
-constexpr uint32_t kWideCtasPerSm = 5;         // resident CTAs per SM (__launch_bounds__ below)
+constexpr uint32_t kWideCtasPerSm = 6;         // resident CTAs per SM (__launch_bounds__ below; 80 registers)
 constexpr uint32_t kWideMaxOpnd = 8;          // operand rows held in shared memory
 
 // True exactly when eval_words would accept the program (same rules, no evaluation).
