@@ -470,9 +470,9 @@ cudaError_t launch_filter_dense_wpt(const DenseFilterLaunch& L, cudaStream_t str
 
 // ---------------------------------------------------------------------------------------------
 // The dense filter for programs of at most kWideMaxOpnd operands. A CTA takes tiles_per_cta (1, 2 or
-// 4) consecutive word tiles of one query's bitmap, across segment boundaries; 128 threads each own 8
-// of a tile's 1024 words (2 adjacent words in each of 4 groups of 256), so the per-op decode is
-// shared by 8 words.
+// 4) consecutive word tiles of one query's bitmap, across segment boundaries; 128 threads each own 4
+// of a tile's 512 words (2 adjacent words in each of 2 groups of 256), so the per-op decode is
+// shared by 4 words, and 10 CTAs per SM keep many operand loads in flight.
 // Operands are read straight from the dense posting matrix as 16-byte read-only loads:
 // the batch's queries share rows, so most reads hit L2, and without staging buffers sized for the
 // batch's largest program the SM holds as many CTAs as registers allow. One thread checks the program
@@ -480,11 +480,11 @@ cudaError_t launch_filter_dense_wpt(const DenseFilterLaunch& L, cudaStream_t str
 // evaluation stack stays in registers; only entries under it (a sibling subtree still waiting for its
 // parent) go to a local array.
 constexpr int kWideT = 128;
-constexpr int kWideW = 8;
+constexpr int kWideW = 4;
 constexpr uint32_t kWideTW = kWideT * kWideW;  // words per tile
 constexpr uint32_t kWideGS = 2 * kWideT;       // words between a thread's word pairs
 constexpr uint32_t kWideMaxTilesPerCta = 4;    // word tiles per CTA at most (consecutive, across segments)
-constexpr uint32_t kWideCtasPerSm = 6;         // resident CTAs per SM (__launch_bounds__ below; 80 registers)
+constexpr uint32_t kWideCtasPerSm = 10;        // resident CTAs per SM (__launch_bounds__ below; 48 registers)
 constexpr uint32_t kWideMaxOpnd = 8;          // operand rows held in shared memory
 
 // True exactly when eval_words would accept the program (same rules, no evaluation).
