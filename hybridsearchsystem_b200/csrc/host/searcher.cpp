@@ -64,7 +64,7 @@ double TcAccumulationBound(int format, uint32_t d) {
 // Offsets of the packed per-batch staging buffer.
 struct StageLayout {
     size_t progOff, opndOff, topk, epsMain, epsSamp, negInf, theta, thetaPr, qlist, errWord, counters, passCount,
-        candCount, sampCount, status, prog, opnd, total;
+        candCount, sampCount, status, theta1, prog, opnd, total;
 };
 
 StageLayout MakeLayout(uint32_t B) {
@@ -85,9 +85,10 @@ StageLayout MakeLayout(uint32_t B) {
     L.thetaPr = take(B * 4ull);  // proven thresholds beside predicted ones (learned threshold)
     L.qlist = take(B * 4ull);
     L.errWord = take(4);  // host copy of the tensor-core pass's error bits
-    L.counters = at;  // zeroed per batch: passCount and status
+    L.counters = at;  // zeroed per batch: passCount, status and theta1
     L.passCount = take(B * 4ull);
     L.status = take(B * 4ull);
+    L.theta1 = take(B * 4ull);  // the doc sample's proven thresholds, copied out with the statuses
     L.prog = take(static_cast<size_t>(B) * kMaxProgram * 4ull);
     L.opnd = take(static_cast<size_t>(B) * kMaxOperands * 4ull);
     // per-segment candidate counts: every producing CTA writes its own, no clearing
@@ -627,7 +628,8 @@ void FullRecallSearcher::SampleTiles(uint64_t want, uint32_t rows, bool simt, ui
     *count = std::min<uint64_t>(sampTiles, (tilesU + *step - 1) / *step);
 }
 
-uint64_t FullRecallSearcher::Sample(const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly, float* stats) {
+uint64_t FullRecallSearcher::Sample(const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly, float* stats,
+                                    float* thetaCopy) {
     const StageLayout SL = MakeLayout(m_cfg.maxBatch);
     uint8_t* D = m_dStage;
     uint64_t count = 0, step = 1;
@@ -651,6 +653,7 @@ uint64_t FullRecallSearcher::Sample(const uint32_t* dList, uint32_t rows, bool s
     ST.qlist = dList;
     ST.nq_list = rows;
     ST.stats = stats;
+    ST.theta_also = raiseOnly ? nullptr : thetaCopy;
     Ck(launch_sample_threshold(ST, m_b.stream));
     return count;
 }
@@ -899,10 +902,11 @@ int FullRecallSearcher::EnqueueAttempt(uint32_t nq, const BatchInputs& in, float
     m_b.want = learned || m_featuresOut != nullptr ? m_cfg.sampleDocs : m_b.wantRerun;
     m_b.learned = learned;
     const bool wantStats = learned || m_featuresOut != nullptr;
-    const uint64_t sampCount = Sample(nullptr, nq, false, false, wantStats ? m_dStats : nullptr);
+    // the sample's proven thresholds (theta_1) are also kept in theta1, copied to the host with the
+    // statuses (a copy here would stall the stream between the sample and the passes)
+    const uint64_t sampCount = Sample(nullptr, nq, false, false, wantStats ? m_dStats : nullptr,
+                                      reinterpret_cast<float*>(D + SL.theta1));
     m_b.launches += 2;
-    // the sample's proven thresholds (theta_1), read after the batch's first synchronisation
-    Ck(cudaMemcpyAsync(H + SL.theta, dTheta, nq * 4ull, cudaMemcpyDeviceToHost, stream));
     if (m_featuresOut) {
         Ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
                           m_featuresOut, stream));
@@ -919,7 +923,6 @@ int FullRecallSearcher::EnqueueAttempt(uint32_t nq, const BatchInputs& in, float
         Ck(launch_predict_theta(m_dYp, dEpsMain, reinterpret_cast<const uint32_t*>(D + SL.passCount), dTopk,
                                 m_dStats, nq, m_model->scale, m_model->shift, m_margin, dTheta, dThetaPr, m_dYp,
                                 stream));
-        Ck(cudaMemcpyAsync(m_hThetaA, m_dYp, nq * 4ull, cudaMemcpyDeviceToHost, stream));
         m_b.launches += 5;
     }
     if (m_timing) Ck(cudaEventRecord(m_ev[2], stream));
@@ -1007,8 +1010,11 @@ int FullRecallSearcher::EnqueueAttempt(uint32_t nq, const BatchInputs& in, float
     if (m_timing) Ck(cudaEventRecord(m_ev[4], stream));
     // the statuses that decide re-runs (and the tensor-core pass's error bits), on the host when
     // m_evStatus (recorded by the caller) completes
-    Ck(cudaMemcpyAsync(H + SL.status, dStatus, nq * 4ull, cudaMemcpyDeviceToHost, stream));
+    // one copy for the statuses and theta_1 (theta1 follows status in the staging layout)
+    Ck(cudaMemcpyAsync(H + SL.status, dStatus, (SL.theta1 - SL.status) + nq * 4ull, cudaMemcpyDeviceToHost, stream));
     if (m_tcFormat >= 0) Ck(cudaMemcpyAsync(H + SL.errWord, m_dError, 4, cudaMemcpyDeviceToHost, stream));
+    // the model's thresholds (m_dYp is not written after the prediction)
+    if (learned) Ck(cudaMemcpyAsync(m_hThetaA, m_dYp, nq * 4ull, cudaMemcpyDeviceToHost, stream));
     return 0;
 }
 
@@ -1040,7 +1046,7 @@ int FullRecallSearcher::SearchFinish() {
             Ck(cudaStreamSynchronize(stream));
         }
         if (firstSync && m_b.ce == cudaSuccess) {
-            const float* h1 = reinterpret_cast<const float*>(H + SL.theta);
+            const float* h1 = reinterpret_cast<const float*>(H + SL.theta1);
             m_lastTheta1.assign(h1, h1 + nq);
             if (m_b.learned)
                 m_lastThetaA.assign(m_hThetaA, m_hThetaA + nq);

@@ -124,7 +124,7 @@ struct SampleThresholdLaunch {
     const float* eps_sample;   // [nq] error bound of the sample pass
     const float* eps_main;     // [nq] error bound of the main pass
     float* theta;              // [nq] out
-    float* theta_also;         // [nq] or null: raised with theta (raise_only launches)
+    float* theta_also;         // [nq] or null: raised with theta (raise_only launches), else a copy of it
     const uint32_t* qlist;
     uint32_t nq_list;
     float* stats;              // [nq][kSampleStats] or null (layout at kSampleStats)

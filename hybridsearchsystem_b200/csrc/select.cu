@@ -502,7 +502,10 @@ __global__ void __launch_bounds__(kST) sample_threshold_kernel(SampleThresholdLa
         if (L.theta_also && L.raise_only && threadIdx.x == 0) L.theta_also[qi] = fmaxf(L.theta_also[qi], t);
     }
     __syncthreads();  // every thread has read the old theta
-    if (threadIdx.x == 0) L.theta[qi] = theta;
+    if (threadIdx.x == 0) {
+        L.theta[qi] = theta;
+        if (L.theta_also && !L.raise_only) L.theta_also[qi] = theta;
+    }
 }
 
 // Byte offset of the shared-memory candidate arrays of select_topk_kernel: after SelectSmem and the
