@@ -572,12 +572,15 @@ class FullRecallSearcher {
                     float* thetaCopy = nullptr);
     void SampleTiles(uint64_t want, uint32_t rows, bool simt, uint64_t* count, uint64_t* step) const;
     // A batch's small inputs in the pinned staging buffer: per-query program and operand offsets, K,
-    // the programs and operands; rows [nq, rows) as match-nothing queries with K = padK.
+    // the programs and then their operands (operand offsets count from the program array's start);
+    // rows [nq, rows) as match-nothing queries with K = padK.
     struct BatchInputs {
         uint32_t maxK = 0, maxOpnd = 0, np = 0, no = 0;
     };
     BatchInputs PrepareInputs(uint32_t nq, uint32_t rows, const FilterExpr* const* exprs, const uint32_t* topks,
                               uint32_t padK);
+    // Bytes of the batch's one host-to-device input copy.
+    size_t InputBytes(const BatchInputs& in) const;
     // Their copy to the device and the filter launch over `rows` queries.
     int EnqueueFilter(uint32_t rows, const BatchInputs& in, uint64_t* dBits, uint64_t bitsStride, cudaStream_t stream);
     // The first attempt of the batch in m_b over `rows` queries (directly or under capture). Returns
@@ -602,7 +605,7 @@ class FullRecallSearcher {
         GraphKey key;
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
-        cudaGraphNode_t progCopy = nullptr, opndCopy = nullptr;  // the batch's programs and operands
+        cudaGraphNode_t inputCopy = nullptr;  // the batch's inputs (its size follows the programs)
         Batch batch;  // the launch plan the capture made (segments, select parameters, counts)
         uint64_t used = 0;
     };

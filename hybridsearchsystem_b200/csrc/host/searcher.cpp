@@ -89,8 +89,9 @@ StageLayout MakeLayout(uint32_t B) {
     L.passCount = take(B * 4ull);
     L.status = take(B * 4ull);
     L.theta1 = take(B * 4ull);  // the doc sample's proven thresholds, copied out with the statuses
-    L.prog = take(static_cast<size_t>(B) * kMaxProgram * 4ull);
-    L.opnd = take(static_cast<size_t>(B) * kMaxOperands * 4ull);
+    // the programs, then their operand rows (one host-to-device copy of [0, prog + words))
+    L.prog = take(static_cast<size_t>(B) * (kMaxProgram + kMaxOperands) * 4ull);
+    L.opnd = take(static_cast<size_t>(B) * kMaxOperands * 4ull);  // host only: operands while programs are laid out
     // per-segment candidate counts: every producing CTA writes its own, no clearing
     L.candCount = take(static_cast<size_t>(B) * kMaxCandSegs * 4ull);
     L.sampCount = take(static_cast<size_t>(B) * kMaxCandSegs * 4ull);
@@ -337,9 +338,18 @@ FullRecallSearcher::BatchInputs FullRecallSearcher::PrepareInputs(uint32_t nq, u
     opndOff[rows] = no;
     for (uint32_t q = 0; q < nq; ++q)
         if (topk[q] > static_cast<uint32_t>(kMaxTopK)) m_lastStatus[q] |= kStatusTopKTooLarge;
+    // the operand rows follow the programs (offsets from the program array's start), and the
+    // counters go over zeroed, so that one copy brings every input
+    std::memcpy(prog + np, opnd, no * 4ull);
+    for (uint32_t q = 0; q <= rows; ++q) opndOff[q] += np;
+    std::memset(H + SL.counters, 0, SL.prog - SL.counters);
     in.np = np;
     in.no = no;
     return in;
+}
+
+size_t FullRecallSearcher::InputBytes(const BatchInputs& in) const {
+    return MakeLayout(m_cfg.maxBatch).prog + std::max(in.np + in.no, 1u) * 4ull;
 }
 
 int FullRecallSearcher::EnqueueFilter(uint32_t rows, const BatchInputs& in, uint64_t* dBits, uint64_t bitsStride,
@@ -352,18 +362,15 @@ int FullRecallSearcher::EnqueueFilter(uint32_t rows, const BatchInputs& in, uint
     auto ck = [&](cudaError_t e) {
         if (ce == cudaSuccess && e != cudaSuccess) ce = e;
     };
-    // the small per-batch inputs: offsets and K, then the programs and operands (at least one entry
-    // each, so that a replayed graph can resize both copies)
-    ck(cudaMemcpyAsync(D, H, SL.counters, cudaMemcpyHostToDevice, stream));
-    ck(cudaMemcpyAsync(D + SL.prog, H + SL.prog, std::max(in.np, 1u) * 4ull, cudaMemcpyHostToDevice, stream));
-    ck(cudaMemcpyAsync(D + SL.opnd, H + SL.opnd, std::max(in.no, 1u) * 4ull, cudaMemcpyHostToDevice, stream));
-    ck(cudaMemsetAsync(D + SL.counters, 0, SL.prog - SL.counters, stream));
+    // the per-batch inputs in one copy: offsets and K, the zeroed counters, the programs and their
+    // operands (at least one word, so that a replayed graph can resize the copy)
+    ck(cudaMemcpyAsync(D, H, InputBytes(in), cudaMemcpyHostToDevice, stream));
 
     if (m_cfg.densePostings && T.DeviceDensePostings()) {
         DenseFilterLaunch F{};
         F.prog = reinterpret_cast<const uint32_t*>(D + SL.prog);
         F.prog_off = reinterpret_cast<const uint32_t*>(D + SL.progOff);
-        F.opnd_row = reinterpret_cast<const uint32_t*>(D + SL.opnd);
+        F.opnd_row = reinterpret_cast<const uint32_t*>(D + SL.prog);
         F.opnd_off = reinterpret_cast<const uint32_t*>(D + SL.opndOff);
         F.dense = T.DeviceDensePostings();
         F.rows = T.PostingRows();
@@ -383,7 +390,7 @@ int FullRecallSearcher::EnqueueFilter(uint32_t rows, const BatchInputs& in, uint
     FilterLaunch F{};
     F.prog = reinterpret_cast<const uint32_t*>(D + SL.prog);
     F.prog_off = reinterpret_cast<const uint32_t*>(D + SL.progOff);
-    F.opnd_row = reinterpret_cast<const uint32_t*>(D + SL.opnd);
+    F.opnd_row = reinterpret_cast<const uint32_t*>(D + SL.prog);
     F.opnd_off = reinterpret_cast<const uint32_t*>(D + SL.opndOff);
     F.table = T.DevicePostingTable();
     F.row_stride = T.GetSegmentNum();
@@ -789,7 +796,6 @@ void FullRecallSearcher::DropGraphs() {
 
 int FullRecallSearcher::EnqueueGraph(const GraphKey& key, uint32_t rows, const BatchInputs& in, float* dOutScores,
                                      int64_t* dOutIds, uint32_t* dOutCounts, uint32_t outStride) {
-    const StageLayout SL = MakeLayout(m_cfg.maxBatch);
     cudaStream_t stream = m_b.stream;
     GraphEntry* g = nullptr;
     for (GraphEntry& e : m_graphCache)
@@ -806,7 +812,7 @@ int FullRecallSearcher::EnqueueGraph(const GraphKey& key, uint32_t rows, const B
         }
         if (ce == cudaSuccess && m_b.ce == cudaSuccess)
             ce = cudaGraphInstantiate(&e.exec, e.graph, 0);
-        // the two copies whose sizes follow the batch's programs
+        // the input copy, whose size follows the batch's programs
         size_t n = 0;
         if (ce == cudaSuccess && m_b.ce == cudaSuccess) ce = cudaGraphGetNodes(e.graph, nullptr, &n);
         std::vector<cudaGraphNode_t> nodes(n);
@@ -816,10 +822,9 @@ int FullRecallSearcher::EnqueueGraph(const GraphKey& key, uint32_t rows, const B
             if (cudaGraphNodeGetType(nodes[i], &t) != cudaSuccess || t != cudaGraphNodeTypeMemcpy) continue;
             cudaMemcpy3DParms p{};
             if (cudaGraphMemcpyNodeGetParams(nodes[i], &p) != cudaSuccess) continue;
-            if (p.dstPtr.ptr == m_dStage + SL.prog) e.progCopy = nodes[i];
-            if (p.dstPtr.ptr == m_dStage + SL.opnd) e.opndCopy = nodes[i];
+            if (p.dstPtr.ptr == m_dStage) e.inputCopy = nodes[i];
         }
-        if (ce == cudaSuccess && m_b.ce == cudaSuccess && (!e.progCopy || !e.opndCopy)) ce = cudaErrorUnknown;
+        if (ce == cudaSuccess && m_b.ce == cudaSuccess && !e.inputCopy) ce = cudaErrorUnknown;
         if (ce != cudaSuccess || m_b.ce != cudaSuccess) {
             // nothing of the batch ran: graphs off for this searcher, the batch launched directly
             if (e.exec) cudaGraphExecDestroy(e.exec);
@@ -862,10 +867,7 @@ int FullRecallSearcher::EnqueueGraph(const GraphKey& key, uint32_t rows, const B
     g->used = ++m_graphClock;
     uint8_t* H = m_hStage;
     uint8_t* D = m_dStage;
-    Ck(cudaGraphExecMemcpyNodeSetParams1D(g->exec, g->progCopy, D + SL.prog, H + SL.prog,
-                                          std::max(in.np, 1u) * 4ull, cudaMemcpyHostToDevice));
-    Ck(cudaGraphExecMemcpyNodeSetParams1D(g->exec, g->opndCopy, D + SL.opnd, H + SL.opnd,
-                                          std::max(in.no, 1u) * 4ull, cudaMemcpyHostToDevice));
+    Ck(cudaGraphExecMemcpyNodeSetParams1D(g->exec, g->inputCopy, D, H, InputBytes(in), cudaMemcpyHostToDevice));
     Ck(cudaGraphLaunch(g->exec, stream));
     return m_b.ce == cudaSuccess ? 0 : -2;
 }
@@ -908,7 +910,7 @@ int FullRecallSearcher::EnqueueAttempt(uint32_t nq, const BatchInputs& in, float
                                       reinterpret_cast<float*>(D + SL.theta1));
     m_b.launches += 2;
     if (m_featuresOut) {
-        Ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
+        Ck(LaunchFeatures(T, D, SL.opndOff, SL.prog, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
                           m_featuresOut, stream));
         Ck(cudaStreamSynchronize(stream));
         return 1;
@@ -917,7 +919,7 @@ int FullRecallSearcher::EnqueueAttempt(uint32_t nq, const BatchInputs& in, float
     if (learned) {
         // the model's predicted K-th score minus the margin and the error bound, never below theta_1;
         // theta_1 stays in dThetaPr for the select step's check
-        Ck(LaunchFeatures(T, D, SL.opndOff, SL.opnd, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
+        Ck(LaunchFeatures(T, D, SL.opndOff, SL.prog, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
                           m_dX, stream));
         if (m_model->Forward(m_dX, nq, m_dYp, stream) != 0) Ck(cudaErrorUnknown);
         Ck(launch_predict_theta(m_dYp, dEpsMain, reinterpret_cast<const uint32_t*>(D + SL.passCount), dTopk,
