@@ -1,7 +1,7 @@
 """End-to-end parity of the searcher on the GPU, through the C-ABI: every query's doc ids must equal
 the oracle's ground truth bit for bit and in order (score descending, doc id ascending), and every
-returned score must equal the ground truth's FP32 score bit for bit (tolerance 0; the north star allows
-1e-5 relative). Covers one and many segments, all posting layouts, tie-heavy corpora, K above the hit
+returned score must equal the ground truth's FP32 score bit for bit (tolerance 0; the path's
+specification allows 1e-5 relative). Covers one and many segments, all posting layouts, tie-heavy corpora, K above the hit
 count, the K limits, empty and match-nothing filters, candidate-list overflow re-runs, a doc-id offset,
 the device-resident API and a saved / reloaded index."""
 import numpy as np
