@@ -130,3 +130,31 @@ def test_default_stream_falls_back_to_direct_launches(torch_cuda):
     _check(sc.cpu().numpy(), ids.cpu().numpy(), cnt.cpu().numpy(), want, nq)
     st = s.graph_stats()
     assert (st["captures"], st["replays"], st["failed"]) == (0, 0, True), st
+
+
+@pytest.mark.parametrize("method", [0, 2], ids=["simt", "bf16"])
+def test_replay_of_edge_batches(torch_cuda, method):
+    # match-all and NOT filters, K = 0, K at the output stride over a match-all filter, K above a
+    # filter's hits: captured, then replayed with other queries and the filters' order reversed (other
+    # program offsets, the same shape); every batch equals the ground truth
+    torch = torch_cuda
+    mix, vec, bits, table, bufs = _world(torch, 91)
+    d_q, sc, ids, cnt = bufs
+    s = hss.FullRecallSearcher(table, max_batch=B, candidate_cap=1 << 16, method=method)
+    s.set_graphs(True)
+    stream = torch.cuda.Stream()
+    ex = ["", "NOT 1", "1 OR 2 OR 3 OR NOT 4", "5 AND 6 AND 7", "8", "NOT 9 AND 10", "", "11 OR 12"]
+    kk = [0, 1, 7, STRIDE, 100, 2000, 64, 300]
+    for j in range(3):
+        q = mix.queries(len(ex), seed=92 + j)
+        e, k = (ex, kk) if j % 2 == 0 else (ex[::-1], kk[::-1])
+        f = s.compile_filters(e)
+        with torch.cuda.stream(stream):
+            d_q[:len(e)].copy_(torch.from_numpy(q).to("cuda:0"))
+        assert s.search_device(d_q.data_ptr(), len(e), f, k, sc.data_ptr(), ids.data_ptr(), cnt.data_ptr(), STRIDE,
+                               stream.cuda_stream) == 0
+        stream.synchronize()
+        want = oracle.topk(q, e, k, vec, bits, threads=8)
+        _check(sc.cpu().numpy(), ids.cpu().numpy(), cnt.cpu().numpy(), want, len(e))
+    st = s.graph_stats()
+    assert (st["captures"], st["replays"], st["failed"]) == (1, 2, False), st
