@@ -568,8 +568,10 @@ class FullRecallSearcher {
     void Cand(const float* theta, float* score, uint32_t* loc, uint32_t* count, uint32_t cap, uint32_t segBase,
               uint32_t segCap, uint64_t begin, uint64_t step, uint32_t skip, uint64_t countTiles, const uint32_t* dList,
               uint32_t rows, bool simt);
+    // The doc sample of m_b.want docs and its threshold (raised, with raiseOnly); the pass keeps the
+    // filtered docs at or above emitTheta (null: every filtered doc).
     uint64_t Sample(const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly = false, float* stats = nullptr,
-                    float* thetaCopy = nullptr);
+                    float* thetaCopy = nullptr, const float* emitTheta = nullptr);
     void SampleTiles(uint64_t want, uint32_t rows, bool simt, uint64_t* count, uint64_t* step) const;
     // A batch's small inputs in the pinned staging buffer: per-query program and operand offsets, K,
     // the programs and then their operands (operand offsets count from the program array's start);

@@ -636,7 +636,7 @@ void FullRecallSearcher::SampleTiles(uint64_t want, uint32_t rows, bool simt, ui
 }
 
 uint64_t FullRecallSearcher::Sample(const uint32_t* dList, uint32_t rows, bool simt, bool raiseOnly, float* stats,
-                                    float* thetaCopy) {
+                                    float* thetaCopy, const float* emitTheta) {
     const StageLayout SL = MakeLayout(m_cfg.maxBatch);
     uint8_t* D = m_dStage;
     uint64_t count = 0, step = 1;
@@ -644,8 +644,8 @@ uint64_t FullRecallSearcher::Sample(const uint32_t* dList, uint32_t rows, bool s
     const uint32_t segs = SegsOf(rows, count, m_sampCap, simt);
     const uint32_t segCap = SegCapOf(rows, count, m_sampCap, segs, simt);
     auto* dSampCount = reinterpret_cast<uint32_t*>(D + SL.sampCount);
-    Cand(reinterpret_cast<const float*>(D + SL.negInf), m_dSampScore, m_dSampLoc, dSampCount, m_sampCap, 0, segCap, 0,
-         step, 0, count, dList, rows, simt);
+    Cand(emitTheta ? emitTheta : reinterpret_cast<const float*>(D + SL.negInf), m_dSampScore, m_dSampLoc, dSampCount,
+         m_sampCap, 0, segCap, 0, step, 0, count, dList, rows, simt);
     SampleThresholdLaunch ST{};
     ST.score = m_dSampScore;
     ST.count = dSampCount;
@@ -660,7 +660,7 @@ uint64_t FullRecallSearcher::Sample(const uint32_t* dList, uint32_t rows, bool s
     ST.qlist = dList;
     ST.nq_list = rows;
     ST.stats = stats;
-    ST.theta_also = raiseOnly ? nullptr : thetaCopy;
+    ST.theta_also = thetaCopy;  // a copy of theta, or (raise_only) raised with it
     Ck(launch_sample_threshold(ST, m_b.stream));
     return count;
 }
@@ -906,9 +906,23 @@ int FullRecallSearcher::EnqueueAttempt(uint32_t nq, const BatchInputs& in, float
     const bool wantStats = learned || m_featuresOut != nullptr;
     // the sample's proven thresholds (theta_1) are also kept in theta1, copied to the host with the
     // statuses (a copy here would stall the stream between the sample and the passes)
-    const uint64_t sampCount = Sample(nullptr, nq, false, false, wantStats ? m_dStats : nullptr,
-                                      reinterpret_cast<float*>(D + SL.theta1));
-    m_b.launches += 2;
+    auto* dTheta1 = reinterpret_cast<float*>(D + SL.theta1);
+    uint64_t sampCount;
+    if (m_b.want > m_cfg.sampleDocs) {
+        // A sample grown with K in two steps: the sample_docs sample's proven threshold first, then the
+        // grown sample keeps only the docs above it. Its K-th best is the same whenever it has K docs
+        // above that threshold (and raises theta_1 then); otherwise theta_1 stays. Every doc of the
+        // grown sample is otherwise stored and walked (K = 1000 at 10M: about 76k per query).
+        const uint64_t grown = m_b.want;
+        m_b.want = m_cfg.sampleDocs;
+        (void)Sample(nullptr, nq, false, false, nullptr, dTheta1);
+        m_b.want = grown;
+        sampCount = Sample(nullptr, nq, false, true, nullptr, dTheta1, dTheta);
+        m_b.launches += 4;
+    } else {
+        sampCount = Sample(nullptr, nq, false, false, wantStats ? m_dStats : nullptr, dTheta1);
+        m_b.launches += 2;
+    }
     if (m_featuresOut) {
         Ck(LaunchFeatures(T, D, SL.opndOff, SL.prog, SL.passCount, SL.topk, m_dStats, dQueries, nq, FeatureDim(),
                           m_featuresOut, stream));
