@@ -815,9 +815,10 @@ def measure_serving(args, ctx, method, rates, model=None, margin=0.0, graphs=Tru
     q, ex = ctx["queries"], ctx["exprs"]
     kk = np.exp(np.random.default_rng(77).uniform(0.0, np.log(1000.0), len(q))).astype(np.uint32) + 1
     kk = np.minimum(kk, 1000)
-    # warm-up at the highest and a low rate (the batch shapes of high and low load captured, with
-    # graphs), not timed
-    for i, (rate, n) in enumerate(((max(rates), 20000), (2000.0, 2000))):
+    # warm-up at every rate of the sweep (with graphs, the batch shapes each load level forms are
+    # captured once, as in a server that runs for long), not timed
+    for i, rate in enumerate(rates):
+        n = int(min(20000, max(2000, rate * 0.1)))
         idx = (np.arange(n) + 7919 * (i + 1)) % len(q)
         srv.run_poisson(q[idx], [ex[i] for i in idx], kk[idx], rate, seed=i + 1)
     warm = srv.stats()
@@ -840,7 +841,7 @@ def measure_serving(args, ctx, method, rates, model=None, margin=0.0, graphs=Tru
                  "capture_ms_per_shape": round(st["graph_capture_ms"] / max(1, st["graph_captures"]), 3)}
     return {"form": form_name(method, model is not None), "slots": srv_slots, "graphs": graph,
             "max_wait_us": args.serve_wait_us, "topk": "log-uniform in [1, 1000] per request",
-            "warmup": "20000 requests at the highest rate, 2000 at 2000 QPS (not timed)", "rates": out}
+            "warmup": "at each rate, max(2000, 0.1 s of) requests (not timed)", "rates": out}
 
 
 def summary(f, steps):
