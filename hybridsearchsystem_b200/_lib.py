@@ -66,7 +66,7 @@ class SearcherConfig(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_uint32), ("maxBatch", ctypes.c_uint32), ("maxWaitUs", ctypes.c_uint32),
                 ("method", ctypes.c_int32), ("memoryBudget", ctypes.c_uint64), ("candidateCap", ctypes.c_uint32),
-                ("sampleDocs", ctypes.c_uint32), ("noGraphs", ctypes.c_uint32)]
+                ("sampleDocs", ctypes.c_uint32), ("graphs", ctypes.c_uint32)]
 
 
 class ServerStats(ctypes.Structure):

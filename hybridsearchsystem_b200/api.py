@@ -335,9 +335,9 @@ class Server:
     """The serving loop (continuous batching over one resident table; include/hss.h, hss_server_*)."""
 
     def __init__(self, table, slots=2, max_batch=256, max_wait_us=200, method=0, memory_budget=0, candidate_cap=0,
-                 sample_docs=0, graphs=True):
+                 sample_docs=0, graphs=False):
         cfg = _lib.ServerConfig(slots, max_batch, max_wait_us, method, memory_budget, candidate_cap, sample_docs,
-                                0 if graphs else 1)
+                                1 if graphs else 0)
         h = ctypes.c_void_p()
         check(_lib.load().hss_server_create(table._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

@@ -731,7 +731,7 @@ int hss_server_create(hss_table* table, const hss_server_config* cfg, hss_server
         c.searcher.method = static_cast<hss::ScoreMethod>(cfg->method);
         if (cfg->candidateCap) c.searcher.candidateCap = cfg->candidateCap;
         if (cfg->sampleDocs) c.searcher.sampleDocs = cfg->sampleDocs;
-        c.graphs = cfg->noGraphs == 0;
+        c.graphs = cfg->graphs != 0;
     }
     auto loop = std::make_unique<hss::ServingLoop>(table->t, c);
     if (!loop->Ok()) return SetError(HSS_ERR_CUDA, loop->Error());

@@ -697,9 +697,10 @@ struct ServingConfig {
     uint32_t maxWaitUs = 200;
     uint64_t memoryBudget = 0;  // bytes for the slots' arenas; 0 = half of the free device memory
     SearcherConfig searcher;    // maxBatch is taken from above
-    // Replay each batch shape's captured CUDA graph (FullRecallSearcher::SetGraphs); the output
-    // stride of a batch is then its largest K rounded up to a power of two.
-    bool graphs = true;
+    // Replay each batch shape's captured CUDA graph (FullRecallSearcher::SetGraphs); the device
+    // rows of every batch then hold kMaxTopK entries. Off by default: measured no faster than direct
+    // launches here, and a capture now and then takes tens of ms of host time.
+    bool graphs = false;
 };
 
 struct ServingStats {

@@ -392,8 +392,8 @@ typedef struct hss_server_config {
     uint64_t memoryBudget; /* bytes for the slots' arenas; 0 = half the free device memory */
     uint32_t candidateCap; /* as in hss_searcher_config; 0 = default */
     uint32_t sampleDocs;
-    uint32_t noGraphs;     /* 1: launch every batch directly (default 0: slots replay captured CUDA
-                              graphs per batch shape, hss_searcher_set_graphs) */
+    uint32_t graphs;       /* 1: the slots replay captured CUDA graphs per batch shape
+                              (hss_searcher_set_graphs); default 0: every batch launched directly */
 } hss_server_config;
 typedef struct hss_server_stats {
     uint64_t completed, batches;
