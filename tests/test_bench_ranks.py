@@ -63,3 +63,51 @@ def test_reference_arm_prints_once_under_torchrun():
     rec = json.loads(lines[0])
     assert rec["impl"] == "reference" and rec["n_gpus"] == 2 and rec["value"] > 0
     assert rec["e2e"]["h2d_bytes_per_step"] == 0 and rec["cpu_baseline"]["cores"] >= 1
+
+
+def test_serving_sweep_record_with_and_without_graphs(monkeypatch):
+    # the bench's serving bookkeeping on CPU, with a stand-in for the serving loop: warm-up at every
+    # rate, one record per rate, capture counts split into warm-up and sweep only with graphs
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    import bench
+    import hybridsearchsystem_b200 as hss
+
+    calls = []
+
+    class FakeServer:
+        def __init__(self, table, **kw):
+            self.graphs = kw.get("graphs")
+            self.captures = 0
+
+        def stats(self):
+            return {"slots": 3, "completed": 0, "batches": 0, "mean_batch": 2.0, "p50_ms": 1.0, "p99_ms": 2.0,
+                    "max_ms": 3.0, "graph_captures": self.captures, "graph_replays": 4 * self.captures,
+                    "graph_capture_ms": 0.5 * self.captures}
+
+        def set_threshold_model(self, model, margin):
+            pass
+
+        def reset_stats(self):
+            pass
+
+        def run_poisson(self, q, exprs, topks, rate, seed=0):
+            calls.append((self.graphs, rate, len(q)))
+            if self.graphs:
+                self.captures += 2
+            return np.ones(len(q)), rate, len(q) / rate
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(hss, "Server", FakeServer)
+    args = bench.parse_args([])
+    ctx = {"table": None, "queries": np.zeros((64, 128), np.float32), "exprs": [""] * 64}
+    rates = [1000.0, 50000.0, 200000.0]
+    direct = bench.measure_serving(args, ctx, "bf16", rates, graphs=False)
+    assert direct["graphs"] is None and [r["offered_qps"] for r in direct["rates"]] == [1000, 50000, 200000]
+    graphs = bench.measure_serving(args, ctx, "bf16", rates, graphs=True)
+    assert graphs["graphs"]["captures_in_warmup"] == 6 and graphs["graphs"]["captures_in_sweep"] == 6
+    # a warm-up run at every rate before the timed ones, for each sweep
+    assert [c[1] for c in calls[:3]] == rates and [c[1] for c in calls[3:6]] == rates
